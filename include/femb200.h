@@ -1,0 +1,196 @@
+/*
+ * femb200.h — C ABI of the B200-native TET4 FEM static-solve path.
+ *
+ * The reference (monostylegc/simul, backend/fea/fem) is Python + Taichi and has
+ * no native FFI; each entry point below replaces the Python/Taichi call named in
+ * its comment (paths relative to the reference project root).  A Python host
+ * binds these with ctypes (simul_b200/_lib.py); any C caller can use them.
+ *
+ * Conventions
+ *  - Every function returns an int status (FEM_OK = 0).  The message of the
+ *    last failure on a context is returned by fem_last_error(ctx); failures of
+ *    fem_ctx_create are reported by fem_last_error(NULL) (thread-local).
+ *  - Mesh set-up arrays (FemMeshDesc, material tables) are HOST pointers.
+ *  - All per-call arrays are DEVICE pointers on the context's device, in the
+ *    caller's node / element order, row-major (node-major, xyz inner).
+ *  - The context owns its scratch memory and CUDA graphs; caller-visible
+ *    buffers belong to the caller.  Work is issued on the context's stream;
+ *    calls that return host values synchronise that stream.
+ *  - One context per stream.  Contexts share no mutable state; calls on one
+ *    context must not overlap.
+ *  - Device loops carry iteration caps; exhausting one returns FEM_ERR_BUDGET
+ *    instead of spinning.
+ */
+#ifndef FEMB200_H
+#define FEMB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; map onto backend/fea/fem/validation.py:18-66 */
+enum {
+  FEM_OK = 0,
+  FEM_ERR_INVALID = 1,      /* FEAValidationError (validation.py:18-41) */
+  FEM_ERR_CUDA = 2,         /* CUDA runtime failure */
+  FEM_ERR_NAN = 3,          /* FEAConvergenceError(reason="nan_divergence"), static_solver.py:174-182 */
+  FEM_NOT_CONVERGED = 4,    /* converged=False in the solve dict */
+  FEM_ERR_BUDGET = 5,       /* a capped device loop ran out of iterations */
+  FEM_ERR_STATE = 6,        /* call order violated (e.g. matvec before any residual) */
+  FEM_CANCELLED = 7         /* progress callback returned 0 (static_solver.py:203-216) */
+};
+
+/* constitutive models (backend/fea/fem/material/*.py) */
+enum {
+  FEM_LINEAR_ELASTIC = 0,        /* linear_elastic.py:22-176 */
+  FEM_NEO_HOOKEAN = 1,           /* neo_hookean.py:31-226 */
+  FEM_MOONEY_RIVLIN = 2,         /* mooney_rivlin.py:36-294 (volumetric term as written) */
+  FEM_J2 = 3,                    /* j2_plasticity.py:33-526, 3D small strain */
+  FEM_TRANSVERSE_ISOTROPIC = 4,  /* transverse_isotropic.py:36-399, small strain */
+  FEM_FIBRE_MOONEY_RIVLIN = 5    /* hyperelastic fibre-reinforced MR; no reference counterpart */
+};
+
+enum { FEM_PRECOND_NONE = 0, FEM_PRECOND_JACOBI = 1 };
+
+/* line-search policy of fem_newton_solve */
+enum {
+  FEM_LS_REFERENCE = 0,  /* halve alpha up to 5x while |R| does not drop; keep the last trial
+                            (static_solver.py:235-253) */
+  FEM_LS_GUARDED = 1,    /* full step unless the trial residual is non-finite or grows more than
+                            1e6x; then halve (up to 5x) */
+  FEM_LS_NONE = 2
+};
+
+#define FEM_MAX_MATERIALS 16
+
+/* Mesh description: replaces FEMesh(n_nodes, n_elements, TET4) +
+ * initialize_from_numpy (core/mesh.py:25-121).  HOST pointers. */
+typedef struct {
+  int64_t n_nodes;
+  int64_t n_elements;
+  const double* X;        /* (n_nodes, 3) reference coordinates */
+  const int32_t* conn;    /* (n_elements, 4) TET4 connectivity */
+  int32_t device;         /* CUDA device ordinal */
+  int32_t nodes_per_block;/* 0 = default (256); 128 / 256 / 512 accepted */
+  void* stream;           /* cudaStream_t; NULL = a context-owned stream */
+} FemMeshDesc;
+
+/* One material of the table: replaces the MaterialBase subclasses'
+ * constructors (material/base.py:16-63 and framework/material.py:85-138).
+ * Unused fields are ignored for a model.  All moduli are multiplied by the
+ * per-element scale given to fem_set_materials (sigma_y is not). */
+typedef struct {
+  int32_t model;
+  double E, nu;                 /* LE / NH / J2 */
+  double sigma_y, H;            /* J2: yield stress, linear isotropic hardening */
+  double C10, C01, D1;          /* MR and fibre MR (D1 <= 1e-20: no volumetric term) */
+  double C_voigt[36];           /* TI: global 6x6, Voigt [11,22,33,23,13,12] */
+  double fiber_dir[2][3];       /* fibre MR: unit fibre directions */
+  double fiber_E;               /* fibre MR: fibre stiffness (tension only) */
+  int32_t n_fibers;             /* fibre MR: 0..2 */
+} FemMaterial;
+
+typedef struct {
+  int32_t max_iterations;   /* Newton iterations, default 50 (static_solver.py:37) */
+  double tol;               /* relative residual vs the first residual of the solve (Q8) */
+  int32_t line_search;      /* FEM_LS_* */
+  int32_t precond;          /* FEM_PRECOND_* */
+  int32_t cg_max_iterations;/* per Newton iteration */
+  double cg_rtol_min;       /* lower bound of the inexact-Newton forcing term */
+  double cg_rtol_max;       /* upper bound of the forcing term */
+  int32_t auto_commit;      /* commit J2 history after a converged solve */
+  int32_t verbose;
+  /* optional progress callback: return 0 to cancel (static_solver.py:203-216) */
+  int32_t (*progress)(void* user, int32_t iteration, double residual, double relative_residual);
+  void* progress_user;
+} FemSolveParams;
+
+typedef struct {
+  int32_t converged;
+  int32_t iterations;       /* reference semantics: Newton loop passes (static_solver.py:260-265) */
+  double residual;
+  double relative_residual;
+  int32_t cancelled;
+  int32_t cg_iterations;    /* total over the solve */
+  int32_t residual_evals;
+  double first_residual;
+} FemSolveResult;
+
+/* ---- lifecycle ---- */
+/* FEMesh.__init__ + initialize_from_numpy + _compute_reference_quantities
+ * (core/mesh.py:25-151).  Reorders nodes/elements internally (Morton) and
+ * builds the node-block gather tables; callers keep their own order. */
+int fem_ctx_create(const FemMeshDesc* desc, void** ctx_out);
+int fem_ctx_destroy(void* ctx);
+const char* fem_last_error(void* ctx);
+/* sizes/statistics: out[0]=n_nodes out[1]=n_elements out[2]=n_blocks
+ * out[3]=block element entries (incl. redundant) out[4]=nodes_per_block
+ * out[5]=device bytes held */
+int fem_ctx_info(void* ctx, int64_t* out6);
+/* cudaStream_t of the context (as void*) */
+void* fem_ctx_stream(void* ctx);
+
+/* ---- set-up ---- */
+/* material table + per-element material id (uint8, host, nullable = all 0)
+ * and per-element modulus scale (float, host, nullable = all 1).
+ * Replaces StaticSolver(material=..., materials={id: mat}) with the element
+ * ids of FEMesh.material_id (static_solver.py:32-71, core/mesh.py:78-79),
+ * honouring per-element materials in the residual. */
+int fem_set_materials(void* ctx, const FemMaterial* table, int32_t n_materials,
+                      const uint8_t* elem_material /*host*/, const float* elem_scale /*host*/);
+/* Dirichlet mask / values and external forces, device pointers (n_nodes,3);
+ * NULL keeps the previous array.  Replaces set_fixed_nodes / set_fixed_dofs /
+ * set_nodal_forces (core/mesh.py:329-399). */
+int fem_set_bc(void* ctx, const uint8_t* fixed_mask, const double* fixed_values,
+               const double* f_ext);
+/* u = fixed value on fixed DOFs — apply_boundary_conditions (core/mesh.py:321-327) */
+int fem_apply_bc(void* ctx);
+int fem_set_displacement(void* ctx, const double* u);
+int fem_get_displacement(void* ctx, double* u_out);
+
+/* ---- kernels ---- */
+/* dN/dX (n_elements,4,3) and Gauss volumes (n_elements) —
+ * _compute_reference_quantities (core/mesh.py:123-151).  Either may be NULL. */
+int fem_reference_quantities(void* ctx, double* dNdX_out, double* vol_out);
+/* F (n_elements,3,3) and Cauchy stress (n_elements,3,3) at displacement u
+ * (NULL = context u) — compute_deformation_gradient (core/mesh.py:293-313)
+ * + MaterialBase.compute_stress (e.g. neo_hookean.py:91-129,
+ * j2_plasticity.py:159-249; J2 starts from the committed history). */
+int fem_compute_stress(void* ctx, const double* u, double* F_out, double* sigma_out);
+/* Fused F -> stress -> element forces -> deterministic node gather (FP64).
+ * f_out (nullable) receives the negative internal force (the reference's
+ * mesh.f), residual_out (nullable) R = f_ext + f with fixed DOFs zeroed;
+ * *rnorm (nullable) = ||R||.  Also refreshes the tangent state used by
+ * fem_tangent_matvec / fem_pcg.  Replaces compute_deformation_gradient +
+ * compute_stress + compute_nodal_forces (neo_hookean.py:131-190 etc.) and the
+ * residual of static_solver.py:161-172. */
+int fem_element_forces(void* ctx, const double* u, double* f_out, double* residual_out,
+                       double* rnorm);
+/* y = K_T x with the consistent tangent at the last fem_element_forces state;
+ * fixed DOFs of x are ignored and of y zeroed (FP32).  Matrix-free
+ * replacement of _assemble_tangent_stiffness (static_solver.py:349-397,
+ * assembly.py:20-287). */
+int fem_tangent_matvec(void* ctx, const float* x, float* y);
+/* Preconditioned CG on K_T du = r (free DOFs), FP32 vectors, FP64 dots.
+ * Replaces _solve_linear_system (static_solver.py:399-462). */
+int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol,
+            int32_t max_iterations, int32_t* iterations_out, double* rel_residual_out);
+/* One static solve at the current loads — StaticSolver.solve / _solve_newton
+ * (static_solver.py:73-99, 135-265), Newton in FP64 with inexact PCG inner
+ * solves in FP32 (mixed-precision iterative refinement). */
+int fem_newton_solve(void* ctx, const FemSolveParams* params, FemSolveResult* result);
+void fem_default_solve_params(FemSolveParams* p);
+
+/* ---- J2 history (j2_plasticity.py:103-123, 513-520) ---- */
+int fem_commit_history(void* ctx);
+int fem_reset_history(void* ctx);
+/* plastic strain (n_elements,3,3) and equivalent plastic strain (n_elements),
+ * committed state; either may be NULL. */
+int fem_get_history(void* ctx, double* ep_out, double* epe_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEMB200_H */

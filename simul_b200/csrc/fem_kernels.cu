@@ -1,0 +1,854 @@
+// sm_100a kernels of the TET4 static-solve path.
+//
+// Element kernels run one CTA per node block (nb consecutive internal nodes,
+// nb = blockDim.x).  A CTA walks its element list in chunks of nb elements:
+// every thread evaluates one element (F -> stress -> four slot vectors) into
+// shared memory, then every thread sums, for the node it owns, the slot
+// vectors of that chunk in the fixed order of the node's slot list.  No
+// atomics touch the outputs, so results are bitwise reproducible; elements
+// shared by two blocks are evaluated by both (about 1.4x redundant work at
+// nb = 256 on Morton-ordered meshes) instead of staging per-element forces in
+// HBM.  This replaces the reference's ti.atomic_add scatter
+// (e.g. backend/fea/fem/material/neo_hookean.py:190).
+#include <cuda_runtime.h>
+
+#include "fem_internal.h"
+
+namespace femb200 {
+
+// ───────────────────────── reductions ─────────────────────────
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (w == 0) {
+    r = (l < NT / 32) ? sh[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+// Publishes this block's partial(s) and reports whether it is the last block
+// to arrive; the last block then owns the fixed-order final sum.
+__device__ __forceinline__ bool publish_partial(const Reduce& red, int site, int nval,
+                                                const double* vals, bool* am_last) {
+  if (threadIdx.x == 0) {
+    for (int v = 0; v < nval; ++v)
+      red.partials[(size_t)(site * 2 + v) * red.max_blocks + blockIdx.x] = vals[v];
+    __threadfence();
+    unsigned int t = atomicAdd(&red.counters[site], 1u);
+    *am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  return *am_last;
+}
+
+template <int NT>
+__device__ __forceinline__ double final_sum(const Reduce& red, int site, int v, double* sh) {
+  __threadfence();
+  double acc = 0.0;
+  const double* p = red.partials + (size_t)(site * 2 + v) * red.max_blocks;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) acc += __ldcg(p + i);
+  return block_sum<NT>(acc, sh);
+}
+
+// ───────────────────────── residual (FP64) ─────────────────────────
+
+template <int NB, int MODEL>
+__global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ ResArgs a) {
+  // 12 x NB doubles of slot vectors: dynamic (96 KB at NB = 512)
+  extern __shared__ double sdyn[];
+  double(*sf)[NB] = reinterpret_cast<double(*)[NB]>(sdyn);
+  __shared__ double sred[NB / 32];
+  __shared__ bool am_last;
+  const MeshDev& m = a.m;
+  const int b = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int node = b * NB + tid;
+  const bool has_node = node < m.n_nodes;
+  int cur = 0, end = 0;
+  if (has_node) {
+    cur = m.node_row[node];
+    end = m.node_row[node + 1];
+  }
+  double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+  const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
+  const int home_end = e0 + m.blk_home[b];
+  for (int c0 = e0; c0 < e1; c0 += NB) {
+    const int idx = c0 + tid;
+    if (idx < e1) {
+      const int e = __ldg(m.blk_elems + idx);
+      const int4 cn = __ldg(m.conn + e);
+      const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+      double xv[4][3], uv[4][3];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          xv[k][d] = __ldg(m.X64 + 3 * nid[k] + d);
+          uv[k][d] = __ldg(a.u + 3 * nid[k] + d);
+        }
+      TetGeom<double> g;
+      tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+      double D[3][3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) D[k][d] = uv[k + 1][d] - uv[0][d];
+      double Hg[9];
+      grad_from_diffs(D, g, Hg);
+      const DevMat<double>& mat = a.matD[__ldg(m.mat_id + e)];
+      const double scale = (double)__ldg(m.scale + e);
+      const int model = MODEL >= 0 ? MODEL : mat.model;
+      double S[9];
+      float pay[kPay];
+      if (model == M_NH) {
+        nh_stress(mat, scale, Hg, S, pay);
+      } else if (model == M_MR || model == M_FMR) {
+        mr_stress(mat, scale, Hg, S, pay);
+      } else if (model == M_J2) {
+        double ep[6], epn[6], epe_n;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ep[k] = a.ep_c[(size_t)k * m.n_elems + e];
+        const double epe = a.epe_c[e];
+        j2_stress(mat, scale, Hg, ep, epe, S, epn, epe_n, pay);
+        if (idx < home_end) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) a.ep_t[(size_t)k * m.n_elems + e] = epn[k];
+          a.epe_t[e] = epe_n;
+        }
+      } else if (model == M_TI) {
+        ti_stress(mat, scale, Hg, S);
+      } else {
+        le_stress(mat, scale, Hg, S);
+      }
+      if (idx < home_end && model_has_payload<MODEL>(model)) {
+#pragma unroll
+        for (int k = 0; k < kPay; ++k) a.payload[(size_t)k * m.n_elems + e] = pay[k];
+      }
+      double f[4][3];
+      slot_vectors(S, g, -g.s6, f);
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sf[3 * s + d][tid] = f[s][d];
+    }
+    __syncthreads();
+    const int base = c0 - e0;
+    const int lim = base + NB;
+    while (cur < end) {
+      const uint32_t ent = __ldg(m.node_slots + cur);
+      const int li = (int)(ent >> 2);
+      if (li >= lim) break;
+      const int t = li - base;
+      const int s = (int)(ent & 3u);
+      acc0 += sf[3 * s + 0][t];
+      acc1 += sf[3 * s + 1][t];
+      acc2 += sf[3 * s + 2][t];
+      ++cur;
+    }
+    __syncthreads();
+  }
+  double r2 = 0.0;
+  if (has_node) {
+    const uint8_t fx = m.fixed[node];
+    const double accs[3] = {acc0, acc1, acc2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double fn = accs[d];
+      if (a.fneg) a.fneg[3 * node + d] = fn;
+      const double r = ((fx >> d) & 1) ? 0.0 : a.f_ext[3 * node + d] + fn;
+      a.R[3 * node + d] = r;
+      r2 += r * r;
+    }
+  }
+  double bsum = block_sum<NB>(r2, sred);
+  if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
+    double tot = final_sum<NB>(a.red, a.red_site, 0, sred);
+    if (tid == 0) {
+      *a.rnorm2 = tot;
+      a.red.counters[a.red_site] = 0u;
+    }
+  }
+}
+
+// ───────────────────────── tangent matvec (FP32) ─────────────────────────
+
+template <int NB, int MODEL, bool CG>
+__global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvArgs a) {
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  __shared__ float sf[12][NB];
+  __shared__ double sred[NB / 32];
+  __shared__ bool am_last;
+  const MeshDev& m = a.m;
+  const int b = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int node = b * NB + tid;
+  const bool has_node = node < m.n_nodes;
+  int cur = 0, end = 0;
+  if (has_node) {
+    cur = m.node_row[node];
+    end = m.node_row[node + 1];
+  }
+  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+  const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
+  for (int c0 = e0; c0 < e1; c0 += NB) {
+    const int idx = c0 + tid;
+    if (idx < e1) {
+      const int e = __ldg(m.blk_elems + idx);
+      const int4 cn = __ldg(m.conn + e);
+      const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+      float xv[4][3], pv[4][3];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 X = __ldg(m.X32 + nid[k]);
+        xv[k][0] = X.x;
+        xv[k][1] = X.y;
+        xv[k][2] = X.z;
+        const uint8_t fx = __ldg(m.fixed + nid[k]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float v = __ldg(a.x + 3 * nid[k] + d);
+          pv[k][d] = (a.mask_input && ((fx >> d) & 1)) ? 0.f : v;
+        }
+      }
+      TetGeom<float> g;
+      tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+      float D[3][3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) D[k][d] = pv[k + 1][d] - pv[0][d];
+      float dF[9];
+      grad_from_diffs(D, g, dF);
+      const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
+      const float scale = __ldg(m.scale + e);
+      float pay[kPay];
+      if (model_has_payload<MODEL>(mat.model)) {
+#pragma unroll
+        for (int k = 0; k < kPay; ++k) pay[k] = __ldg(a.payload + (size_t)k * m.n_elems + e);
+      }
+      float dP[9];
+      dP_any<MODEL>(mat, scale, pay, dF, dP);
+      float f[4][3];
+      slot_vectors(dP, g, g.s6, f);
+#pragma unroll
+      for (int s = 0; s < 4; ++s)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sf[3 * s + d][tid] = f[s][d];
+    }
+    __syncthreads();
+    const int base = c0 - e0;
+    const int lim = base + NB;
+    while (cur < end) {
+      const uint32_t ent = __ldg(m.node_slots + cur);
+      const int li = (int)(ent >> 2);
+      if (li >= lim) break;
+      const int t = li - base;
+      const int s = (int)(ent & 3u);
+      acc0 += sf[3 * s + 0][t];
+      acc1 += sf[3 * s + 1][t];
+      acc2 += sf[3 * s + 2][t];
+      ++cur;
+    }
+    __syncthreads();
+  }
+  double pap = 0.0;
+  if (has_node) {
+    const uint8_t fx = m.fixed[node];
+    const float accs[3] = {acc0, acc1, acc2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float yv = ((fx >> d) & 1) ? 0.f : accs[d];
+      a.y[3 * node + d] = yv;
+      if (CG) pap += (double)yv * (double)a.x[3 * node + d];
+    }
+  }
+  if (CG) {
+    double bsum = block_sum<NB>(pap, sred);
+    if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
+      double tot = final_sum<NB>(a.red, a.red_site, 0, sred);
+      if (tid == 0) {
+        CGState* st = a.cg;
+        st->pAp = tot;
+        if (!(tot > 0.0) || !isfinite(tot)) {
+          st->done = 3;
+          st->status = 3;
+          st->alpha = 0.0;
+        } else {
+          st->alpha = st->rz / tot;
+        }
+        a.red.counters[a.red_site] = 0u;
+      }
+    }
+  }
+}
+
+// ───────────────────────── Jacobi diagonal (FP32) ─────────────────────────
+
+template <int NB, int MODEL>
+__global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagArgs a) {
+  __shared__ float sf[12][NB];
+  const MeshDev& m = a.m;
+  const int b = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int node = b * NB + tid;
+  const bool has_node = node < m.n_nodes;
+  int cur = 0, end = 0;
+  if (has_node) {
+    cur = m.node_row[node];
+    end = m.node_row[node + 1];
+  }
+  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+  const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
+  for (int c0 = e0; c0 < e1; c0 += NB) {
+    const int idx = c0 + tid;
+    if (idx < e1) {
+      const int e = __ldg(m.blk_elems + idx);
+      const int4 cn = __ldg(m.conn + e);
+      const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+      float xv[4][3];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 X = __ldg(m.X32 + nid[k]);
+        xv[k][0] = X.x;
+        xv[k][1] = X.y;
+        xv[k][2] = X.z;
+      }
+      TetGeom<float> g;
+      tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+      const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
+      const float scale = __ldg(m.scale + e);
+      float pay[kPay];
+      if (model_has_payload<MODEL>(mat.model)) {
+#pragma unroll
+        for (int k = 0; k < kPay; ++k) pay[k] = __ldg(a.payload + (size_t)k * m.n_elems + e);
+      }
+      float w[4][3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        w[1][j] = g.c[0][j];
+        w[2][j] = g.c[1][j];
+        w[3][j] = g.c[2][j];
+        w[0][j] = -(g.c[0][j] + g.c[1][j] + g.c[2][j]);
+      }
+#pragma unroll
+      for (int s = 0; s < 4; ++s) {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+          float dF[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) dF[k] = 0.f;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) dF[3 * i + j] = w[s][j] * g.inv_det;
+          float dP[9];
+          dP_any<MODEL>(mat, scale, pay, dF, dP);
+          sf[3 * s + i][tid] =
+              g.s6 * (dP[3 * i] * w[s][0] + dP[3 * i + 1] * w[s][1] + dP[3 * i + 2] * w[s][2]);
+        }
+      }
+    }
+    __syncthreads();
+    const int base = c0 - e0;
+    const int lim = base + NB;
+    while (cur < end) {
+      const uint32_t ent = __ldg(m.node_slots + cur);
+      const int li = (int)(ent >> 2);
+      if (li >= lim) break;
+      const int t = li - base;
+      const int s = (int)(ent & 3u);
+      acc0 += sf[3 * s + 0][t];
+      acc1 += sf[3 * s + 1][t];
+      acc2 += sf[3 * s + 2][t];
+      ++cur;
+    }
+    __syncthreads();
+  }
+  if (has_node) {
+    const uint8_t fx = m.fixed[node];
+    const float accs[3] = {acc0, acc1, acc2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float dv = accs[d];
+      a.dinv[3 * node + d] = (((fx >> d) & 1) || !(dv > 0.f)) ? 0.f : 1.f / dv;
+    }
+  }
+}
+
+// ───────────────────────── PCG vector kernels ─────────────────────────
+// Vectors are float [ndof4 * 4] with a zero tail; fixed DOFs carry dinv = 0,
+// so z, p and x stay zero there without masks.
+
+constexpr int kVecThreads = 256;
+
+__global__ void __launch_bounds__(kVecThreads) cg_init_kernel(const double* __restrict__ b,
+                                                              float* r, float* x, float* p,
+                                                              const float* __restrict__ dinv,
+                                                              int ndof4, CGState* cg, double rtol,
+                                                              int maxit, Reduce red, int site) {
+  __shared__ double sred[kVecThreads / 32];
+  __shared__ bool am_last;
+  const int i = blockIdx.x * kVecThreads + threadIdx.x;
+  double rz = 0.0, rr = 0.0;
+  if (i < ndof4) {
+    const double2 b0 = reinterpret_cast<const double2*>(b)[2 * i];
+    const double2 b1 = reinterpret_cast<const double2*>(b)[2 * i + 1];
+    const float4 rv = make_float4((float)b0.x, (float)b0.y, (float)b1.x, (float)b1.y);
+    const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
+    const float4 zv = make_float4(dv.x * rv.x, dv.y * rv.y, dv.z * rv.z, dv.w * rv.w);
+    reinterpret_cast<float4*>(r)[i] = rv;
+    reinterpret_cast<float4*>(p)[i] = zv;
+    reinterpret_cast<float4*>(x)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z + (double)rv.w * zv.w;
+    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+  }
+  double v[2];
+  v[0] = block_sum<kVecThreads>(rz, sred);
+  v[1] = block_sum<kVecThreads>(rr, sred);
+  if (publish_partial(red, site, 2, v, &am_last)) {
+    double trz = final_sum<kVecThreads>(red, site, 0, sred);
+    double trr = final_sum<kVecThreads>(red, site, 1, sred);
+    if (threadIdx.x == 0) {
+      cg->rz = trz;
+      cg->rr = trr;
+      cg->rr0 = trr;
+      cg->tol2 = rtol * rtol * trr;
+      cg->alpha = 0.0;
+      cg->beta = 0.0;
+      cg->pAp = 0.0;
+      cg->iter = 0;
+      cg->max_iter = maxit;
+      cg->status = isfinite(trr) ? 0 : 3;
+      cg->done = (!isfinite(trr)) ? 3 : ((trr == 0.0 || !(trz > 0.0)) ? 1 : 0);
+      red.counters[site] = 0u;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) cg_update_kernel(float* x, float* r,
+                                                                const float* __restrict__ p,
+                                                                const float* __restrict__ y,
+                                                                const float* __restrict__ dinv,
+                                                                int ndof4, CGState* cg, Reduce red,
+                                                                int site) {
+  if (cg->done) return;
+  __shared__ double sred[kVecThreads / 32];
+  __shared__ bool am_last;
+  const float alpha = (float)cg->alpha;
+  const int i = blockIdx.x * kVecThreads + threadIdx.x;
+  double rz = 0.0, rr = 0.0;
+  if (i < ndof4) {
+    float4 xv = reinterpret_cast<float4*>(x)[i];
+    float4 rv = reinterpret_cast<float4*>(r)[i];
+    const float4 pv = reinterpret_cast<const float4*>(p)[i];
+    const float4 yv = reinterpret_cast<const float4*>(y)[i];
+    const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
+    xv.x += alpha * pv.x; xv.y += alpha * pv.y; xv.z += alpha * pv.z; xv.w += alpha * pv.w;
+    rv.x -= alpha * yv.x; rv.y -= alpha * yv.y; rv.z -= alpha * yv.z; rv.w -= alpha * yv.w;
+    reinterpret_cast<float4*>(x)[i] = xv;
+    reinterpret_cast<float4*>(r)[i] = rv;
+    rz = (double)rv.x * (dv.x * rv.x) + (double)rv.y * (dv.y * rv.y) +
+         (double)rv.z * (dv.z * rv.z) + (double)rv.w * (dv.w * rv.w);
+    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+  }
+  double v[2];
+  v[0] = block_sum<kVecThreads>(rz, sred);
+  v[1] = block_sum<kVecThreads>(rr, sred);
+  if (publish_partial(red, site, 2, v, &am_last)) {
+    double trz = final_sum<kVecThreads>(red, site, 0, sred);
+    double trr = final_sum<kVecThreads>(red, site, 1, sred);
+    if (threadIdx.x == 0) {
+      cg->beta = trz / cg->rz;
+      cg->rz = trz;
+      cg->rr = trr;
+      cg->iter += 1;
+      if (!isfinite(trr) || !isfinite(trz)) {
+        cg->done = 3;
+        cg->status = 3;
+      } else if (trr <= cg->tol2) {
+        cg->done = 1;
+      } else if (cg->iter >= cg->max_iter) {
+        cg->done = 2;
+      }
+      red.counters[site] = 0u;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) cg_pupdate_kernel(float* p,
+                                                                 const float* __restrict__ r,
+                                                                 const float* __restrict__ dinv,
+                                                                 int ndof4, const CGState* cg) {
+  if (cg->done) return;
+  const float beta = (float)cg->beta;
+  const int i = blockIdx.x * kVecThreads + threadIdx.x;
+  if (i < ndof4) {
+    float4 pv = reinterpret_cast<float4*>(p)[i];
+    const float4 rv = reinterpret_cast<const float4*>(r)[i];
+    const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
+    pv.x = dv.x * rv.x + beta * pv.x;
+    pv.y = dv.y * rv.y + beta * pv.y;
+    pv.z = dv.z * rv.z + beta * pv.z;
+    pv.w = dv.w * rv.w + beta * pv.w;
+    reinterpret_cast<float4*>(p)[i] = pv;
+  }
+}
+
+// ───────────────────────── element-parallel helpers (FP64) ─────────────────────────
+
+template <int MODEL>
+__global__ void stress_kernel(const MeshDev m, const DevMat<double>* matD, const double* u,
+                              const double* ep_c, const double* epe_c, const int* perm_elem,
+                              double* F_out, double* sig_out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.n_elems) return;
+  const int4 cn = m.conn[e];
+  const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+  double xv[4][3], uv[4][3];
+  for (int k = 0; k < 4; ++k)
+    for (int d = 0; d < 3; ++d) {
+      xv[k][d] = m.X64[3 * nid[k] + d];
+      uv[k][d] = u[3 * nid[k] + d];
+    }
+  TetGeom<double> g;
+  tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+  double D[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int d = 0; d < 3; ++d) D[k][d] = uv[k + 1][d] - uv[0][d];
+  double Hg[9], F[9];
+  grad_from_diffs(D, g, Hg);
+  for (int k = 0; k < 9; ++k) F[k] = Hg[k] + ((k % 4 == 0) ? 1.0 : 0.0);
+  const DevMat<double>& mat = matD[m.mat_id[e]];
+  const double scale = (double)m.scale[e];
+  const int model = MODEL >= 0 ? MODEL : mat.model;
+  double sig[9];
+  float pay[kPay];
+  if (model == M_NH || model == M_MR || model == M_FMR) {
+    // Cauchy stress sigma = P F^T / J_s (the stress kernels of neo_hookean.py:99-129 and
+    // mooney_rivlin.py:150-190 evaluate the same tensor directly)
+    double P[9];
+    if (model == M_NH)
+      nh_stress(mat, scale, Hg, P, pay);
+    else
+      mr_stress(mat, scale, Hg, P, pay);
+    const double J = det3(F);
+    const double Js = J > kJFloor ? J : kJFloor;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        sig[3 * i + j] =
+            (P[3 * i] * F[3 * j] + P[3 * i + 1] * F[3 * j + 1] + P[3 * i + 2] * F[3 * j + 2]) / Js;
+  } else if (model == M_J2) {
+    double ep[6], epn[6], epe_n;
+    for (int k = 0; k < 6; ++k) ep[k] = ep_c[(size_t)k * m.n_elems + e];
+    j2_stress(mat, scale, Hg, ep, epe_c[e], sig, epn, epe_n, pay);
+  } else if (model == M_TI) {
+    ti_stress(mat, scale, Hg, sig);
+  } else {
+    le_stress(mat, scale, Hg, sig);
+  }
+  const int eu = perm_elem[e];
+  for (int k = 0; k < 9; ++k) {
+    if (F_out) F_out[(size_t)9 * eu + k] = F[k];
+    if (sig_out) sig_out[(size_t)9 * eu + k] = sig[k];
+  }
+}
+
+__global__ void refq_kernel(const MeshDev m, const int* perm_elem, double* dNdX, double* vol) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= m.n_elems) return;
+  const int4 cn = m.conn[e];
+  const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+  double xv[4][3];
+  for (int k = 0; k < 4; ++k)
+    for (int d = 0; d < 3; ++d) xv[k][d] = m.X64[3 * nid[k] + d];
+  TetGeom<double> g;
+  tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+  const int eu = perm_elem[e];
+  if (dNdX) {
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) {
+        const double v = g.c[k][j] * g.inv_det;
+        dNdX[(size_t)12 * eu + 3 * (k + 1) + j] = v;
+        s += v;
+      }
+      dNdX[(size_t)12 * eu + j] = -s;
+    }
+  }
+  if (vol) vol[eu] = g.vol;
+}
+
+// ───────────────────────── small helpers ─────────────────────────
+
+template <typename TI, typename TO>
+__global__ void gather3_kernel(const TI* in_user, TO* out_int, const int* perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int src = perm[i];
+  for (int d = 0; d < 3; ++d) out_int[3 * i + d] = (TO)in_user[3 * src + d];
+}
+
+template <typename TI, typename TO>
+__global__ void scatter3_kernel(const TI* in_int, TO* out_user, const int* perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int dst = perm[i];
+  for (int d = 0; d < 3; ++d) out_user[3 * dst + d] = (TO)in_int[3 * i + d];
+}
+
+__global__ void gather_mask_kernel(const uint8_t* in_user, uint8_t* out_int, const int* perm,
+                                   int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int src = perm[i];
+  uint8_t bits = 0;
+  for (int d = 0; d < 3; ++d) bits |= (in_user[3 * src + d] ? 1 : 0) << d;
+  out_int[i] = bits;
+}
+
+__global__ void apply_bc_kernel(double* u, const double* fixed_vals, const uint8_t* fixed, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t fx = fixed[i];
+  for (int d = 0; d < 3; ++d)
+    if ((fx >> d) & 1) u[3 * i + d] = fixed_vals[3 * i + d];
+}
+
+__global__ void u_update_kernel(double* u, const double* u_base, const float* du, double alpha,
+                                int ndof) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ndof) return;
+  u[i] = u_base[i] + alpha * (double)du[i];
+}
+
+__global__ void d2f_masked_kernel(const double* in, float* out, const uint8_t* fixed, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t fx = fixed[i];
+  for (int d = 0; d < 3; ++d) out[3 * i + d] = ((fx >> d) & 1) ? 0.f : (float)in[3 * i + d];
+}
+
+__global__ void gather3_masked_kernel(const double* in_user, double* out_int, const int* perm,
+                                      const uint8_t* fixed, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int src = perm[i];
+  const uint8_t fx = fixed[i];
+  for (int d = 0; d < 3; ++d) out_int[3 * i + d] = ((fx >> d) & 1) ? 0.0 : in_user[3 * src + d];
+}
+
+__global__ void dinv_identity_kernel(float* dinv, const uint8_t* fixed, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t fx = fixed[i];
+  for (int d = 0; d < 3; ++d) dinv[3 * i + d] = ((fx >> d) & 1) ? 0.f : 1.f;
+}
+
+__global__ void __launch_bounds__(256) bc_delta_kernel(const double* u, const double* fixed_vals,
+                                                       const uint8_t* fixed, float* dc, int n,
+                                                       Reduce red, int site, double* dc2) {
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  double acc = 0.0;
+  if (i < n) {
+    const uint8_t fx = fixed[i];
+    for (int d = 0; d < 3; ++d) {
+      const double v = ((fx >> d) & 1) ? fixed_vals[3 * i + d] - u[3 * i + d] : 0.0;
+      dc[3 * i + d] = (float)v;
+      acc += v * v;
+    }
+  }
+  double bsum = block_sum<256>(acc, sred);
+  if (publish_partial(red, site, 1, &bsum, &am_last)) {
+    double tot = final_sum<256>(red, site, 0, sred);
+    if (threadIdx.x == 0) {
+      *dc2 = tot;
+      red.counters[site] = 0u;
+    }
+  }
+}
+
+__global__ void rhs_minus_kernel(const double* R, const float* y, const uint8_t* fixed, double* out,
+                                 int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t fx = fixed[i];
+  for (int d = 0; d < 3; ++d)
+    out[3 * i + d] = ((fx >> d) & 1) ? 0.0 : R[3 * i + d] - (double)y[3 * i + d];
+}
+
+// ───────────────────────── launchers ─────────────────────────
+
+static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+
+template <int NB, int MODEL>
+static void residual_go(const ResArgs& a, cudaStream_t s) {
+  const size_t smem = sizeof(double) * 12 * NB;
+  cudaFuncSetAttribute(residual_kernel<NB, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  residual_kernel<NB, MODEL><<<a.m.n_blocks, NB, smem, s>>>(a);
+}
+
+template <int NB>
+static void residual_nb(const ResArgs& a, int model, cudaStream_t s) {
+  switch (model) {
+    case M_LE: residual_go<NB, M_LE>(a, s); break;
+    case M_NH: residual_go<NB, M_NH>(a, s); break;
+    case M_MR: residual_go<NB, M_MR>(a, s); break;
+    case M_J2: residual_go<NB, M_J2>(a, s); break;
+    case M_TI: residual_go<NB, M_TI>(a, s); break;
+    case M_FMR: residual_go<NB, M_FMR>(a, s); break;
+    default: residual_go<NB, -1>(a, s); break;
+  }
+}
+
+void launch_residual(const ResArgs& a, int model, cudaStream_t s) {
+  switch (a.m.nb) {
+    case 128: residual_nb<128>(a, model, s); break;
+    case 512: residual_nb<512>(a, model, s); break;
+    default: residual_nb<256>(a, model, s); break;
+  }
+}
+
+template <int NB, bool CG>
+static void matvec_nb(const MvArgs& a, int model, cudaStream_t s) {
+  dim3 grid(a.m.n_blocks);
+  switch (model) {
+    case M_LE: matvec_kernel<NB, M_LE, CG><<<grid, NB, 0, s>>>(a); break;
+    case M_NH: matvec_kernel<NB, M_NH, CG><<<grid, NB, 0, s>>>(a); break;
+    case M_MR: matvec_kernel<NB, M_MR, CG><<<grid, NB, 0, s>>>(a); break;
+    case M_J2: matvec_kernel<NB, M_J2, CG><<<grid, NB, 0, s>>>(a); break;
+    case M_TI: matvec_kernel<NB, M_TI, CG><<<grid, NB, 0, s>>>(a); break;
+    case M_FMR: matvec_kernel<NB, M_FMR, CG><<<grid, NB, 0, s>>>(a); break;
+    default: matvec_kernel<NB, -1, CG><<<grid, NB, 0, s>>>(a); break;
+  }
+}
+
+void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
+  const bool cg = a.cg != nullptr;
+  switch (a.m.nb) {
+    case 128: cg ? matvec_nb<128, true>(a, model, s) : matvec_nb<128, false>(a, model, s); break;
+    case 512: cg ? matvec_nb<512, true>(a, model, s) : matvec_nb<512, false>(a, model, s); break;
+    default: cg ? matvec_nb<256, true>(a, model, s) : matvec_nb<256, false>(a, model, s); break;
+  }
+}
+
+template <int NB>
+static void diag_nb(const DiagArgs& a, int model, cudaStream_t s) {
+  dim3 grid(a.m.n_blocks);
+  switch (model) {
+    case M_LE: diag_kernel<NB, M_LE><<<grid, NB, 0, s>>>(a); break;
+    case M_NH: diag_kernel<NB, M_NH><<<grid, NB, 0, s>>>(a); break;
+    case M_MR: diag_kernel<NB, M_MR><<<grid, NB, 0, s>>>(a); break;
+    case M_J2: diag_kernel<NB, M_J2><<<grid, NB, 0, s>>>(a); break;
+    case M_TI: diag_kernel<NB, M_TI><<<grid, NB, 0, s>>>(a); break;
+    case M_FMR: diag_kernel<NB, M_FMR><<<grid, NB, 0, s>>>(a); break;
+    default: diag_kernel<NB, -1><<<grid, NB, 0, s>>>(a); break;
+  }
+}
+
+void launch_diag(const DiagArgs& a, int model, cudaStream_t s) {
+  switch (a.m.nb) {
+    case 128: diag_nb<128>(a, model, s); break;
+    case 512: diag_nb<512>(a, model, s); break;
+    default: diag_nb<256>(a, model, s); break;
+  }
+}
+
+void launch_cg_init(const double* b, float* r, float* x, float* p, const float* dinv, int ndof4,
+                    CGState* cg, double rtol, int maxit, Reduce red, int site, cudaStream_t s) {
+  cg_init_kernel<<<nblk(ndof4, kVecThreads), kVecThreads, 0, s>>>(b, r, x, p, dinv, ndof4, cg,
+                                                                  rtol, maxit, red, site);
+}
+
+void launch_cg_update(float* x, float* r, const float* p, const float* y, const float* dinv,
+                      int ndof4, CGState* cg, Reduce red, int site, cudaStream_t s) {
+  cg_update_kernel<<<nblk(ndof4, kVecThreads), kVecThreads, 0, s>>>(x, r, p, y, dinv, ndof4, cg,
+                                                                    red, site);
+}
+
+void launch_cg_pupdate(float* p, const float* r, const float* dinv, int ndof4, CGState* cg,
+                       cudaStream_t s) {
+  cg_pupdate_kernel<<<nblk(ndof4, kVecThreads), kVecThreads, 0, s>>>(p, r, dinv, ndof4, cg);
+}
+
+void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
+                   const double* ep_c, const double* epe_c, const int* perm_elem, double* F_out,
+                   double* sig_out, cudaStream_t s) {
+  const int t = 128;
+  switch (model) {
+    case M_LE: stress_kernel<M_LE><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
+    case M_NH: stress_kernel<M_NH><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
+    case M_J2: stress_kernel<M_J2><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
+    default: stress_kernel<-1><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
+  }
+}
+
+void launch_refq(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol,
+                 cudaStream_t s) {
+  refq_kernel<<<nblk(m.n_elems, 128), 128, 0, s>>>(m, perm_elem, dNdX, vol);
+}
+
+void launch_gather_d(const double* in_user, double* out_int, const int* perm, int n,
+                     cudaStream_t s) {
+  gather3_kernel<double, double><<<nblk(n, 256), 256, 0, s>>>(in_user, out_int, perm, n);
+}
+void launch_scatter_d(const double* in_int, double* out_user, const int* perm, int n,
+                      cudaStream_t s) {
+  scatter3_kernel<double, double><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
+}
+void launch_gather_f(const float* in_user, float* out_int, const int* perm, int n,
+                     cudaStream_t s) {
+  gather3_kernel<float, float><<<nblk(n, 256), 256, 0, s>>>(in_user, out_int, perm, n);
+}
+void launch_scatter_f(const float* in_int, float* out_user, const int* perm, int n,
+                      cudaStream_t s) {
+  scatter3_kernel<float, float><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
+}
+void launch_scatter_f2d(const float* in_int, double* out_user, const int* perm, int n,
+                        cudaStream_t s) {
+  scatter3_kernel<float, double><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
+}
+void launch_gather_mask(const uint8_t* in_user, uint8_t* out_int, const int* perm, int n,
+                        cudaStream_t s) {
+  gather_mask_kernel<<<nblk(n, 256), 256, 0, s>>>(in_user, out_int, perm, n);
+}
+void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, int n,
+                     cudaStream_t s) {
+  apply_bc_kernel<<<nblk(n, 256), 256, 0, s>>>(u, fixed_vals, fixed, n);
+}
+void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int ndof,
+                     cudaStream_t s) {
+  u_update_kernel<<<nblk(ndof, 256), 256, 0, s>>>(u, u_base, du, alpha, ndof);
+}
+void launch_gather_d_masked(const double* in_user, double* out_int, const int* perm,
+                            const uint8_t* fixed, int n, cudaStream_t s) {
+  gather3_masked_kernel<<<nblk(n, 256), 256, 0, s>>>(in_user, out_int, perm, fixed, n);
+}
+void launch_dinv_identity(float* dinv, const uint8_t* fixed, int n, cudaStream_t s) {
+  dinv_identity_kernel<<<nblk(n, 256), 256, 0, s>>>(dinv, fixed, n);
+}
+void launch_bc_delta(const double* u, const double* fixed_vals, const uint8_t* fixed, float* dc,
+                     int n, Reduce red, int site, double* dc2, cudaStream_t s) {
+  bc_delta_kernel<<<nblk(n, 256), 256, 0, s>>>(u, fixed_vals, fixed, dc, n, red, site, dc2);
+}
+void launch_rhs_minus(const double* R, const float* y, const uint8_t* fixed, double* out, int n,
+                      cudaStream_t s) {
+  rhs_minus_kernel<<<nblk(n, 256), 256, 0, s>>>(R, y, fixed, out, n);
+}
+void launch_d2f_masked(const double* in, float* out, const uint8_t* fixed, int n,
+                       cudaStream_t s) {
+  d2f_masked_kernel<<<nblk(n, 256), 256, 0, s>>>(in, out, fixed, n);
+}
+
+}  // namespace femb200

@@ -1,0 +1,214 @@
+"""Deterministic TET4 input generators for the static-solve workloads.
+
+* ``cantilever_bar``  — structured hex grid, every hex split into 6 Kuhn tets
+  along its (0,0,0)->(1,1,1) diagonal; tip traction turned into consistent
+  nodal forces (area/3 of every loaded boundary triangle to each vertex).
+* ``vertebral_body``  — voxelised elliptic cylinder (semi-axes 15 x 12 mm,
+  height 25 mm) on an n^3 grid of spacing 32/n mm, every voxel split into
+  5 tets with parity-alternating orientation so neighbouring voxels share
+  face diagonals; 2-voxel cortical shell (E = 12 GPa) around a smoothed
+  lognormal cancellous core (median 300 MPa).
+
+The reference builds HEX8 grids (``framework/_adapters/fem_adapter.py:41-70``)
+and voxel HEX8 meshes (``preprocessing/voxel_to_hex.py:11-68``); these
+generators produce the tetrahedral equivalents the TET4 hot path consumes.
+All arrays are NumPy; units are mm, N, MPa.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+# Kuhn (6-tet) split: every permutation of the axes walks 000 -> 111.
+_KUHN_PERMS = ((0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0))
+
+# 5-tet split: corner bits (x, y, z) of the hex.  Even voxels keep the
+# "central" tet on the even corners, odd voxels on the odd ones.
+_FIVE_EVEN = ((0b000, 0b110, 0b101, 0b011),
+              (0b100, 0b000, 0b110, 0b101),
+              (0b010, 0b000, 0b011, 0b110),
+              (0b001, 0b000, 0b101, 0b011),
+              (0b111, 0b110, 0b011, 0b101))
+_FIVE_ODD = ((0b100, 0b010, 0b001, 0b111),
+             (0b000, 0b100, 0b001, 0b010),
+             (0b110, 0b100, 0b010, 0b111),
+             (0b101, 0b100, 0b111, 0b001),
+             (0b011, 0b010, 0b001, 0b111))
+
+
+@dataclass
+class TetMesh:
+    """A TET4 mesh with boundary data, in the caller's (generator) order."""
+    X: np.ndarray                    # (Nn,3) float64
+    conn: np.ndarray                 # (Ne,4) int32, positively oriented
+    E: Optional[np.ndarray] = None   # (Ne,) per-element Young's modulus
+    fixed_mask: Optional[np.ndarray] = None   # (Nn,3) bool
+    fixed_vals: Optional[np.ndarray] = None   # (Nn,3) float64 (full-load value)
+    f_ext: Optional[np.ndarray] = None        # (Nn,3) float64 (full-load value)
+    info: dict = field(default_factory=dict)
+
+    @property
+    def n_nodes(self):
+        return self.X.shape[0]
+
+    @property
+    def n_elements(self):
+        return self.conn.shape[0]
+
+
+def _orient(X, conn):
+    """Swap nodes 2,3 of negatively oriented tets so det J > 0."""
+    e = X[conn]
+    d = np.einsum("ei,ei->e", np.cross(e[:, 1] - e[:, 0], e[:, 2] - e[:, 0]), e[:, 3] - e[:, 0])
+    neg = d < 0
+    conn = conn.copy()
+    conn[neg, 2], conn[neg, 3] = conn[neg, 3].copy(), conn[neg, 2].copy()
+    return conn
+
+
+def boundary_triangles(conn: np.ndarray) -> np.ndarray:
+    """Faces (k,3) used by exactly one tet."""
+    faces = np.concatenate([conn[:, [0, 1, 2]], conn[:, [0, 1, 3]],
+                            conn[:, [0, 2, 3]], conn[:, [1, 2, 3]]])
+    key = np.sort(faces, axis=1)
+    _, idx, cnt = np.unique(key, axis=0, return_index=True, return_counts=True)
+    return faces[idx[cnt == 1]]
+
+
+def traction_nodal_forces(X, conn, face_select, traction) -> np.ndarray:
+    """Consistent nodal forces of a uniform traction on boundary triangles.
+
+    ``face_select(centroids) -> bool mask``; each selected triangle gives
+    area/3 * traction to each of its vertices.
+    """
+    tri = boundary_triangles(conn)
+    c = X[tri].mean(axis=1)
+    tri = tri[face_select(c)]
+    p = X[tri]
+    area = 0.5 * np.linalg.norm(np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]), axis=1)
+    f = np.zeros_like(X)
+    contrib = (area / 3.0)[:, None] * np.asarray(traction, dtype=np.float64)[None, :]
+    for k in range(3):
+        np.add.at(f, tri[:, k], contrib)
+    return f
+
+
+def structured_tets(nx, ny, nz, L=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0)):
+    """Structured (nx,ny,nz) hex grid split into 6 Kuhn tets per hex."""
+    xs = origin[0] + np.linspace(0.0, L[0], nx + 1)
+    ys = origin[1] + np.linspace(0.0, L[1], ny + 1)
+    zs = origin[2] + np.linspace(0.0, L[2], nz + 1)
+    Z, Y, Xg = np.meshgrid(zs, ys, xs, indexing="ij")
+    X = np.stack([Xg.ravel(), Y.ravel(), Z.ravel()], axis=1)
+
+    def nid(i, j, k):
+        return i + (nx + 1) * (j + (ny + 1) * k)
+
+    ii, jj, kk = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    order = np.lexsort((ii, jj, kk))
+    ii, jj, kk = ii[order], jj[order], kk[order]
+    tets = []
+    for perm in _KUHN_PERMS:
+        cur = np.zeros((ii.size, 3), dtype=np.int64)
+        verts = [nid(ii, jj, kk)]
+        for ax in perm:
+            cur[:, ax] += 1
+            verts.append(nid(ii + cur[:, 0], jj + cur[:, 1], kk + cur[:, 2]))
+        tets.append(np.stack(verts, axis=1))
+    conn = np.stack(tets, axis=1).reshape(-1, 4)
+    return X, _orient(X, conn).astype(np.int32)
+
+
+def cantilever_bar(nx=20, ny=4, nz=4, length=10.0, width=1.0, height=1.0,
+                   E=17e3, nu=0.3, traction=50.0) -> TetMesh:
+    """Neo-Hookean cantilever bar (1,920 tets, 525 nodes at the default grid).
+
+    x = 0 face fully fixed; uniform traction ``traction`` (MPa) in -z on the
+    x = length face as consistent nodal forces (total -traction*width*height N).
+    """
+    X, conn = structured_tets(nx, ny, nz, (length, width, height))
+    fixed = np.zeros((X.shape[0], 3), dtype=bool)
+    fixed[np.isclose(X[:, 0], 0.0)] = True
+    tol = 1e-9 * length
+    f = traction_nodal_forces(X, conn, lambda c: np.abs(c[:, 0] - length) < tol,
+                              (0.0, 0.0, -traction))
+    return TetMesh(X=X, conn=conn, E=np.full(conn.shape[0], float(E)), fixed_mask=fixed,
+                   fixed_vals=np.zeros_like(X), f_ext=f,
+                   info={"kind": "cantilever_bar", "grid": (nx, ny, nz), "nu": nu})
+
+
+def voxel_tets(mask: np.ndarray, h: float, origin=(0.0, 0.0, 0.0)):
+    """Split every True voxel of ``mask`` (indexed [i,j,k] = x,y,z) into 5 tets.
+
+    Returns node coordinates, connectivity and the voxel index of each tet.
+    """
+    nx, ny, nz = mask.shape
+    vi, vj, vk = np.nonzero(mask)
+    nvox = vi.size
+    # global corner id on the (n+1)^3 lattice, compacted afterwards
+    def lat(i, j, k):
+        return (i * (ny + 1) + j) * (nz + 1) + k
+    corners = np.empty((nvox, 8), dtype=np.int64)
+    for b in range(8):
+        corners[:, b] = lat(vi + (b >> 2 & 1), vj + (b >> 1 & 1), vk + (b & 1))
+    # bit layout used by the split tables is (x<<2 | y<<1 | z) — matches b above
+    parity = (vi + vj + vk) & 1
+    conn = np.empty((nvox, 5, 4), dtype=np.int64)
+    for t in range(5):
+        for a in range(4):
+            conn[:, t, a] = np.where(parity == 0,
+                                     corners[np.arange(nvox), _FIVE_EVEN[t][a]],
+                                     corners[np.arange(nvox), _FIVE_ODD[t][a]])
+    conn = conn.reshape(-1, 4)
+    used, inv = np.unique(conn, return_inverse=True)
+    conn = inv.reshape(-1, 4)
+    i = used // ((ny + 1) * (nz + 1))
+    j = (used // (nz + 1)) % (ny + 1)
+    k = used % (nz + 1)
+    X = np.stack([origin[0] + i * h, origin[1] + j * h, origin[2] + k * h], axis=1).astype(np.float64)
+    voxel_of_tet = np.repeat(np.arange(nvox), 5)
+    return X, _orient(X, conn).astype(np.int32), voxel_of_tet, (vi, vj, vk)
+
+
+def vertebral_body(n=64, seed=0, a=15.0, b=12.0, height=25.0, extent=32.0,
+                   E_cortical=12e3, E_core_median=300.0, core_sigma=0.3,
+                   smooth_voxels=3.0, shell_voxels=2, nu=0.3,
+                   axial_strain=0.02) -> TetMesh:
+    """Synthetic vertebral body of the plain-method workload.
+
+    Voxel (i,j,k) of spacing h = extent/n is inside when its centre satisfies
+    (x/a)^2 + (y/b)^2 <= 1 and 0 <= z < height.  Bottom face fixed; the top
+    face gets u_z = -axial_strain*height (full load; callers step it).
+    """
+    from scipy import ndimage
+
+    h = extent / n
+    c = (np.arange(n) + 0.5) * h
+    xc = c - extent / 2.0
+    zc = c
+    Xv, Yv, Zv = np.meshgrid(xc, xc, zc, indexing="ij")
+    mask = ((Xv / a) ** 2 + (Yv / b) ** 2 <= 1.0) & (Zv >= 0.0) & (Zv < height)
+    core = ndimage.binary_erosion(mask, iterations=shell_voxels)
+    rng = np.random.default_rng(seed)
+    z = ndimage.gaussian_filter(rng.standard_normal(mask.shape), sigma=smooth_voxels)
+    zc_ = z[core]
+    z = (z - zc_.mean()) / zc_.std()
+    Evox = np.where(core, E_core_median * np.exp(core_sigma * z), E_cortical)
+    X, conn, vox, (vi, vj, vk) = voxel_tets(mask, h, origin=(-extent / 2.0, -extent / 2.0, 0.0))
+    E = Evox[vi, vj, vk][vox]
+    top_z = X[:, 2].max()
+    fixed = np.zeros((X.shape[0], 3), dtype=bool)
+    fixed_vals = np.zeros_like(X)
+    bottom = np.isclose(X[:, 2], 0.0)
+    top = np.isclose(X[:, 2], top_z)
+    fixed[bottom] = True
+    fixed[top, 2] = True
+    fixed_vals[top, 2] = -axial_strain * top_z
+    return TetMesh(X=X, conn=conn, E=E.astype(np.float64), fixed_mask=fixed,
+                   fixed_vals=fixed_vals, f_ext=np.zeros_like(X),
+                   info={"kind": "vertebral_body", "n": n, "h": h, "seed": seed, "nu": nu,
+                         "n_voxels": int(mask.sum()), "height": float(top_z),
+                         "shell_elements": int(np.sum(E == E_cortical))})

@@ -1,0 +1,318 @@
+"""GPU parity of libfemb200 against the FP64 oracle's golden fixtures.
+
+All calls go through the C ABI (directly or via the simul_b200 host mirror).
+Tolerances: FP64 residual / stress kernels 1e-9 (relative to the field's max),
+FP32 tangent matvec 2e-5 relative L2, converged displacements 1e-6 relative L2.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import fem_oracle as O
+from simul_b200 import _lib, meshgen
+from simul_b200 import fem as B
+from tests.golden import gen_golden as G
+
+pytestmark = pytest.mark.gpu
+
+FIBRES = G.FIBRES
+
+
+def _rel_max(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def make_material(key, E=None):
+    if key == "nh":
+        return B.NeoHookean(17e3, 0.3)
+    if key == "mr":
+        return B.MooneyRivlin(0.18, 0.045, 0.5)
+    if key == "fmr":
+        return B.FibreReinforcedMooneyRivlin(0.18, 0.045, 0.5, FIBRES, 500.0)
+    if key == "le":
+        return B.LinearElastic(1e3, 0.3)
+    if key == "ti":
+        return B.TransverseIsotropic(17e3, 11.5e3, 0.3, 0.35, 3.3e3, fiber_direction=(1.0, 1.0, 0.0))
+    if key == "j2":
+        return B.J2Plasticity(E, 0.3, 100.0, hardening_modulus=0.02 * E)
+    raise KeyError(key)
+
+
+def make_mesh(X, conn, cuda, nb=0):
+    mesh = B.FEMesh(X.shape[0], conn.shape[0], device=cuda, nodes_per_block=nb)
+    mesh.initialize_from_numpy(X, conn)
+    return mesh
+
+
+def dev(a, cuda, dtype=torch.float64):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=cuda)
+
+
+def ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+@pytest.fixture(scope="module")
+def bar():
+    return meshgen.cantilever_bar()
+
+
+@pytest.fixture(scope="module")
+def vox():
+    return G.vox_mesh()
+
+
+def test_fixture_meshes_unchanged(bar, vox):
+    np.testing.assert_allclose(G.mesh_checksum(bar.X, bar.conn), np.load(G.path_of("bar_nh_forces"))["mesh_sum"])
+    np.testing.assert_allclose(G.mesh_checksum(vox.X, vox.conn), np.load(G.path_of("vox12_j2_forces"))["mesh_sum"])
+
+
+def test_reference_quantities(cuda, bar):
+    ref = np.load(G.path_of("bar_nh_forces"))
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    assert _rel_max(mesh.dNdX.cpu().numpy(), ref["dNdX"]) < 1e-12
+    assert _rel_max(mesh.elem_vol.cpu().numpy(), ref["vol"]) < 1e-12
+    assert mesh.elem_vol.sum().item() == pytest.approx(10.0, rel=1e-12)
+
+
+@pytest.mark.parametrize("key", ["nh", "mr", "fmr", "le", "ti"])
+@pytest.mark.parametrize("nb", [128, 256, 512])
+def test_element_forces_and_stress(cuda, bar, key, nb):
+    ref = np.load(G.path_of(f"bar_{key}_forces"))
+    mesh = make_mesh(bar.X, bar.conn, cuda, nb)
+    mat = make_material(key)
+    mesh.u.copy_(dev(ref["u"], cuda))
+    mat.compute_nodal_forces(mesh)
+    assert _rel_max(mesh.get_nodal_forces(), ref["f"]) < 1e-9
+    mat.compute_stress(mesh)
+    assert _rel_max(mesh.get_stress(), ref["sigma"]) < 1e-9
+    if key == "nh":
+        assert _rel_max(mesh.F.cpu().numpy(), ref["F"]) < 1e-12
+
+
+@pytest.mark.parametrize("key", ["nh", "mr", "fmr", "le", "ti"])
+def test_tangent_matvec(cuda, bar, key):
+    ref = np.load(G.path_of(f"bar_{key}_forces"))
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    mat = make_material(key)
+    mesh.u.copy_(dev(ref["u"], cuda))
+    mat.compute_nodal_forces(mesh)          # refreshes the tangent state
+    x = dev(ref["p"], cuda, torch.float32)
+    y = torch.empty_like(x)
+    lib = _lib.load()
+    assert lib.fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0, _lib.last_error(mesh.ctx)
+    # the matvec ignores fixed DOFs; the fixture has none set on this mesh (no BC pushed)
+    assert _rel_l2(y.cpu().numpy().astype(np.float64), ref["y"]) < 2e-5
+
+
+def test_j2_forces_history_and_tangent(cuda, vox):
+    ref = np.load(G.path_of("vox12_j2_forces"))
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = make_material("j2", E=vox.E)
+    mesh.u.copy_(dev(ref["u"], cuda))
+    mat.compute_nodal_forces(mesh)
+    assert _rel_max(mesh.get_nodal_forces(), ref["f"]) < 1e-9
+    x = dev(ref["p"], cuda, torch.float32)
+    y = torch.empty_like(x)
+    assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0
+    assert _rel_l2(y.cpu().numpy().astype(np.float64), ref["y"]) < 2e-5
+    # trial history of the residual pass, committed explicitly
+    assert _lib.load().fem_commit_history(mesh.ctx) == 0
+    assert _rel_max(mat.get_plastic_strain(), ref["epe"]) < 1e-9
+    assert _rel_max(mat.get_plastic_strain_tensor(), ref["ep"]) < 1e-9
+    assert mat.get_yield_status().sum() > 0
+    # stress from the committed state at the same u equals sigma after the return map
+    mat.compute_stress(mesh)
+    s_gpu = mesh.get_stress()
+    sig_chk, _ = O.cauchy_stress(O.Material("j2", E=vox.E, nu=0.3, sigma_y=100.0, H=0.02 * vox.E),
+                                 O.deformation_gradient(ref["u"], vox.conn.astype(np.int64),
+                                                        O.reference_quantities(vox.X, vox.conn)[0]),
+                                 O.J2State(ref["ep"], ref["epe"]))
+    assert _rel_max(s_gpu, sig_chk) < 1e-9
+    mat.reset_state()
+    assert np.all(mat.get_plastic_strain() == 0)
+
+
+def test_forces_bitwise_deterministic(cuda, vox):
+    ref = np.load(G.path_of("vox12_j2_forces"))
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = make_material("j2", E=vox.E)
+    mesh.u.copy_(dev(ref["u"], cuda))
+    outs, ys = [], []
+    x = dev(ref["p"], cuda, torch.float32)
+    for _ in range(3):
+        mat.compute_nodal_forces(mesh)
+        outs.append(mesh.f.clone())
+        y = torch.empty_like(x)
+        assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0
+        ys.append(y)
+    for o in outs[1:]:
+        assert torch.equal(o, outs[0])
+    for o in ys[1:]:
+        assert torch.equal(o, ys[0])
+
+
+def test_pcg_solves_tangent_system(cuda, bar):
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    mat = B.LinearElastic(17e3, 0.3)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    mat.compute_nodal_forces(mesh)
+    lib = _lib.load()
+    r = dev(bar.f_ext, cuda)
+    du = torch.zeros_like(r)
+    it = C.c_int32()
+    rel = C.c_double()
+    rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_JACOBI, ptr(r), ptr(du), 1e-6, 5000, C.byref(it), C.byref(rel))
+    assert rc == 0, _lib.last_error(mesh.ctx)
+    assert 0 < it.value < 5000 and rel.value <= 1e-6
+    # FP64 oracle: linear elasticity solved directly
+    m = O.Mesh(bar.X, bar.conn)
+    u_ref, _ = O.consistent_newton(m, O.Material("linear_elastic", E=17e3, nu=0.3), bar.f_ext,
+                                   bar.fixed_mask, bar.fixed_vals, tol=1e-12, line_search=False)
+    assert _rel_l2(du.cpu().numpy(), u_ref) < 1e-4
+    # unpreconditioned CG converges too (more iterations)
+    it2 = C.c_int32()
+    rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_NONE, ptr(r), ptr(du), 1e-6, 20000, C.byref(it2), C.byref(rel))
+    assert rc == 0 and it2.value > 0
+
+
+def test_newton_bar_matches_oracle(cuda, bar):
+    ref = np.load(G.path_of("bar_nh_steps"))
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    solver = B.StaticSolver(mesh, B.NeoHookean(17e3, 0.3), tol=1e-10)
+    for k in range(ref["u_steps"].shape[0]):
+        mesh.set_nodal_forces(np.arange(bar.n_nodes), bar.f_ext * (k + 1) / 10.0)
+        res = solver.solve(verbose=False)
+        assert res["converged"], res
+        assert res["relative_residual"] < 1e-10
+        assert _rel_l2(mesh.get_displacements(), ref["u_steps"][k]) < 1e-6
+
+
+def test_newton_j2_steps_match_oracle(cuda, vox):
+    ref = np.load(G.path_of("vox12_j2_steps"))
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = make_material("j2", E=vox.E)
+    lf = float(ref["load_factor"])
+    total = int(ref["n_total"])
+    solver = B.StaticSolver(mesh, mat, tol=1e-10)
+    for k in range(ref["u_steps"].shape[0]):
+        vals = vox.fixed_vals * (k + 1) / total * lf
+        idx = np.where(vox.fixed_mask.reshape(-1))[0]
+        mesh.set_fixed_dofs(idx, vals.reshape(-1)[idx])
+        res = solver.solve(verbose=False)
+        assert res["converged"], res
+        assert _rel_l2(mesh.get_displacements(), ref["u_steps"][k]) < 1e-6
+        epe_ref = ref["epe_steps"][k]
+        assert np.max(np.abs(mat.get_plastic_strain() - epe_ref)) <= 1e-6 * max(epe_ref.max(), 1e-12) + 1e-12
+    assert ref["epe_steps"][-1].max() > 0
+
+
+def test_reference_line_search_policy_converges(cuda, bar):
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    mesh.set_nodal_forces(np.arange(bar.n_nodes), bar.f_ext / 10.0)
+    solver = B.StaticSolver(mesh, B.NeoHookean(17e3, 0.3), tol=1e-10, line_search="reference")
+    res = solver.solve(verbose=False)
+    ref = np.load(G.path_of("bar_nh_steps"))
+    assert res["converged"]
+    assert _rel_l2(mesh.get_displacements(), ref["u_steps"][0]) < 1e-6
+
+
+def test_single_element_and_unit_volume(cuda):
+    X = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+    conn = np.array([[0, 1, 2, 3]], dtype=np.int32)
+    mesh = make_mesh(X, conn, cuda)
+    assert mesh.elem_vol.item() == pytest.approx(1.0 / 6.0, rel=1e-14)
+    u = np.array([[0.0, 0, 0], [0.01, 0, 0], [0, -0.003, 0], [0.001, 0, 0.002]])
+    mesh.u.copy_(dev(u, cuda))
+    mat = B.NeoHookean(1e3, 0.3)
+    mat.compute_nodal_forces(mesh)
+    m = O.Mesh(X, conn)
+    f_ref = O.internal_state(m, O.Material("neo_hookean", E=1e3, nu=0.3), u)[3]
+    assert _rel_max(mesh.get_nodal_forces(), f_ref) < 1e-12
+    # sum of internal forces vanishes (equilibrium of a free element)
+    assert np.abs(mesh.get_nodal_forces().sum(axis=0)).max() < 1e-12
+
+
+def test_inverted_element_orientation_is_handled(cuda):
+    # negatively oriented connectivity: volumes via |det J|, forces identical
+    X = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+    u = np.array([[0.0, 0, 0], [0.01, 0, 0], [0, -0.003, 0], [0.001, 0, 0.002]])
+    out = []
+    for conn in (np.array([[0, 1, 2, 3]], np.int32), np.array([[0, 2, 1, 3]], np.int32)):
+        mesh = make_mesh(X, conn, cuda)
+        mesh.u.copy_(dev(u, cuda))
+        B.NeoHookean(1e3, 0.3).compute_nodal_forces(mesh)
+        out.append(mesh.get_nodal_forces())
+    assert _rel_max(out[1], out[0]) < 1e-12
+
+
+def test_invalid_inputs_raise(cuda):
+    X = np.array([[0.0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+    with pytest.raises(B.FEAValidationError):
+        make_mesh(X, np.array([[0, 1, 2, 4]], np.int32), cuda)
+    with pytest.raises(B.FEAValidationError):
+        make_mesh(X, np.array([[0, 1, 1, 3]], np.int32), cuda)
+    with pytest.raises(B.FEAValidationError):
+        B.NeoHookean(1e3, 0.5)
+    with pytest.raises(B.FEAValidationError):
+        B.J2Plasticity(1e3, 0.3, -1.0)
+    mesh = make_mesh(X, np.array([[0, 1, 2, 3]], np.int32), cuda)
+    with pytest.raises(B.FEAValidationError):
+        mesh.set_fixed_nodes(np.array([7]))
+    lib = _lib.load()
+    x = torch.zeros(4, 3, dtype=torch.float32, device=cuda)
+    # matvec before any residual evaluation: state error, not a fault
+    assert lib.fem_tangent_matvec(mesh.ctx, ptr(x), ptr(x)) == _lib.FEM_ERR_STATE
+
+
+def test_nan_load_raises_convergence_error(cuda, bar):
+    # fault injected on the host: a NaN in the external force
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    f = bar.f_ext.copy()
+    f[-1, 2] = np.nan
+    mesh.set_nodal_forces(np.arange(bar.n_nodes), f)
+    solver = B.StaticSolver(mesh, B.NeoHookean(17e3, 0.3))
+    with pytest.raises(B.FEAConvergenceError) as ei:
+        solver.solve(verbose=False)
+    assert ei.value.reason == "nan_divergence"
+
+
+def test_progress_callback_cancels(cuda, bar):
+    mesh = make_mesh(bar.X, bar.conn, cuda)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    mesh.set_nodal_forces(np.arange(bar.n_nodes), bar.f_ext / 10.0)
+    seen = []
+
+    def cb(info):
+        seen.append(info)
+        return info["iteration"] < 1
+
+    res = B.StaticSolver(mesh, B.NeoHookean(17e3, 0.3), tol=1e-10).solve(verbose=False, progress_callback=cb)
+    assert res.get("cancelled") and res["iterations"] == 1 and not res["converged"]
+    assert [s["iteration"] for s in seen] == [0, 1]
+
+
+def test_multi_material_table(cuda, bar):
+    # two materials by element id: the residual honours both (no first-material quirk)
+    ids = (bar.X[bar.conn].mean(axis=1)[:, 0] > 5.0).astype(np.int32)
+    mesh = B.FEMesh(bar.n_nodes, bar.n_elements, device=cuda)
+    mesh.initialize_from_numpy(bar.X, bar.conn, material_ids=ids)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    mesh.set_nodal_forces(np.arange(bar.n_nodes), bar.f_ext / 100.0)
+    solver = B.StaticSolver(mesh, materials={0: B.NeoHookean(17e3, 0.3), 1: B.NeoHookean(4e3, 0.3)}, tol=1e-10)
+    res = solver.solve(verbose=False)
+    assert res["converged"]
+    m = O.Mesh(bar.X, bar.conn)
+    E = np.where(ids == 1, 4e3, 17e3)
+    u_ref, _ = O.consistent_newton(m, O.Material("neo_hookean", E=E, nu=0.3), bar.f_ext / 100.0,
+                                   bar.fixed_mask, bar.fixed_vals, tol=1e-11, line_search=False)
+    assert _rel_l2(mesh.get_displacements(), u_ref) < 1e-6

@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""Time-to-1e-8 residual of the synthetic vertebral-body J2 static solve on B200.
+
+Workload (one "step"): the 64^3-voxel, 0.5 mm vertebral body (566,000 TET4,
+121,023 nodes), J2 plasticity with per-element E (cortical 12 GPa shell,
+lognormal core around 300 MPa), bottom fixed, top face compressed 2 % in 20
+load steps, every load step solved by Newton (FP64 residual) + Jacobi-PCG
+(FP32 matvecs, FP64 dots) to 1e-8 relative residual.  Each step starts from
+u = 0 and zero plastic history.  Inputs are seeded synthetic data.
+
+``value`` is the device time of one full solve (CUDA events on the solver's
+stream, L2 flushed before every timed step, inputs resident in HBM);
+``e2e`` is the same solve through the public API with the per-solve inputs
+copied from pinned host memory and the displacement copied back.
+``--impl reference`` times the CPU restatement of the same method (the
+reference itself, Python 3.13 + Taichi, cannot run in this image).
+
+One process per GPU (torchrun for N > 1): every rank solves its own replica
+(the single-mesh solve does not shard); ``value`` is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from datetime import timedelta
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-8 residual: learned-FPCG vs Jacobi-PCG (1 B200); elem GB/s"
+UNIT = "s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=64, help="voxels per axis of the vertebral grid")
+    ap.add_argument("--load-steps", type=int, default=20)
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    return ap.parse_args()
+
+
+def world():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def workload_config(args, v):
+    return {"workload": f"vertebral_body_n{args.n}_j2_{args.load_steps}steps",
+            "voxels": int(v.info["n_voxels"]), "tets": int(v.n_elements), "nodes": int(v.n_nodes),
+            "h_mm": v.info["h"], "load_steps": args.load_steps, "tol": args.tol,
+            "material": "J2 sigma_y=100 MPa H=0.02E, E shell 12 GPa / core lognormal(300 MPa, 0.3)",
+            "method": "Newton (FP64 residual) + Jacobi-PCG (FP32 matvec, FP64 dots)",
+            "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas"}
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) over the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def matvec_bytes(n_elements, n_nodes):
+    """Algorithmic bytes of one J2 tangent matvec launch.
+
+    Per element: connectivity 16, tangent payload 32 (n, theta, gamma2),
+    material id 1 + modulus scale 4, node-block slot entries 16.  Per node:
+    coordinates 16 (float4), x 12, y 12, slot row pointer 4, fixed mask 1.
+    """
+    return n_elements * (16 + 32 + 5 + 16) + n_nodes * (16 + 12 + 12 + 4 + 1)
+
+
+def residual_bytes(n_elements, n_nodes):
+    """Algorithmic bytes of one FP64 J2 residual launch: per element conn 16,
+    id+scale 5, slots 16, history read 56 + trial write 56, payload write 32;
+    per node X 24, u 24, f_ext 24, R 24, row 4, mask 1."""
+    return n_elements * (16 + 5 + 16 + 56 + 56 + 32) + n_nodes * (24 + 24 + 24 + 24 + 4 + 1)
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        try:
+            return json.load(open(path))
+        except ValueError:
+            return {}
+    return {}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "of measured"
+    return 6650.0, "of fallback"
+
+
+def build_inputs(args):
+    from simul_b200 import meshgen
+    return meshgen.vertebral_body(n=args.n, seed=0)
+
+
+def cpu_leg(args, v, gpu_cg_total, threads):
+    """C++/OpenMP restatement on the host cores, first load step, scaled."""
+    from oracle.cpu_solver import CpuSolver
+    s = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
+    t = time.perf_counter()
+    info = s.solve(v.fixed_mask, v.fixed_vals / args.load_steps, v.f_ext, tol=args.tol)
+    dt = time.perf_counter() - t
+    return s.n_threads, dt, info
+
+
+def reference_arm(args, rank, ws):
+    if rank != 0:
+        return
+    v = build_inputs(args)
+    from oracle.cpu_solver import CpuSolver
+    threads = args.cpu_threads or os.cpu_count() or 1
+    times = []
+    info = None
+    nthreads = threads
+    for i in range(args.warmup + args.steps):
+        s = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
+        t = time.perf_counter()
+        info = s.solve(v.fixed_mask, v.fixed_vals / args.load_steps, v.f_ext, tol=args.tol)
+        dt = time.perf_counter() - t
+        nthreads = s.n_threads
+        if i >= args.warmup:
+            times.append(dt * args.load_steps)
+    value = float(np.mean(times))
+    sample = (f"load step 1 of {args.load_steps} (elastic, {info['iterations']} Newton / "
+              f"{info['cg_iterations']} CG iterations) timed and multiplied by {args.load_steps}; the "
+              f"plastic steps cost more CG work, so this understates the full CPU solve")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_note": "the reference's Taichi ti.cpu path cannot run here (no taichi, Python 3.12 "
+                              "vs >=3.13); this arm times oracle/cpu_fem.cpp, a C++/OpenMP restatement "
+                              "of the same method"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, ws, local = world()
+    if args.impl == "reference":
+        if ws > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        reference_arm(args, rank, ws)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+
+    import ctypes as C
+
+    from simul_b200 import _lib
+    from simul_b200 import fem as B
+
+    v = build_inputs(args)
+    mesh = B.FEMesh(v.n_nodes, v.n_elements, device=local)
+    mesh.initialize_from_numpy(v.X, v.conn)
+    mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
+    solver = B.StaticSolver(mesh, mat, tol=args.tol)
+    fixed_full = torch.from_numpy(v.fixed_vals).to(dev)
+    fixed_mask = torch.from_numpy(v.fixed_mask.astype(np.int32)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def solve_all():
+        """One full solve from rest: all load steps, each to tol."""
+        mesh.u.zero_()
+        mat.reset_state()
+        mesh.fixed.copy_(fixed_mask)
+        stats = {"newton": 0, "cg": 0, "converged": True, "max_rel": 0.0}
+        for k in range(1, args.load_steps + 1):
+            mesh.fixed_value.copy_(fixed_full * (k / args.load_steps))
+            mesh._bc_dirty = True
+            r = solver.solve(verbose=False)
+            stats["newton"] += r["iterations"]
+            stats["cg"] += r["cg_iterations"]
+            stats["converged"] &= r["converged"]
+            stats["max_rel"] = max(stats["max_rel"], r["relative_residual"])
+        return stats
+
+    for _ in range(args.warmup):
+        solve_all()
+    torch.cuda.synchronize()
+
+    props = torch.cuda.get_device_properties(dev)
+    gid = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local)
+    clocks = ClockSampler(gid)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = mesh.stats()["launches"]
+    step_ms = []
+    last = None
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        last = solve_all()
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    barrier()
+    launches = mesh.stats()["launches"] - launches0
+    clk = clocks.stop()
+    ms = float(np.mean(step_ms))
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # end to end through the public API: per-solve inputs from pinned host memory
+    h_fixed = torch.from_numpy(v.fixed_vals).pin_memory()
+    h_mask = torch.from_numpy(v.fixed_mask.astype(np.int32)).pin_memory()
+    h_fext = torch.from_numpy(v.f_ext).pin_memory()
+    h_u = torch.empty(v.n_nodes, 3, dtype=torch.float64).pin_memory()
+    d_fixed = torch.empty_like(fixed_full)
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d_fixed.copy_(h_fixed, non_blocking=True)
+        mesh.fixed.copy_(h_mask, non_blocking=True)
+        mesh.f_ext.copy_(h_fext, non_blocking=True)
+        mesh.u.zero_()
+        mat.reset_state()
+        for k in range(1, args.load_steps + 1):
+            mesh.fixed_value.copy_(d_fixed * (k / args.load_steps))
+            mesh._bc_dirty = True
+            solver.solve(verbose=False)
+        h_u.copy_(mesh.u, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    h2d = h_fixed.numel() * 8 + h_mask.numel() * 4 + h_fext.numel() * 8
+    d2h = h_u.numel() * 8
+    e2e_s = float(np.mean(e2e_ms)) / 1e3
+    if ws > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    # roofline of the dominant kernel (tangent matvec), CUDA events on the solver stream
+    kms = (C.c_double * 4)()
+    rc = _lib.load().fem_profile_kernels(mesh.ctx, 200, kms)
+    mv_ms = kms[0] if rc == 0 else None
+    info = mesh.info()
+    peak, peak_src = measured_peaks()
+    b_mv = matvec_bytes(info["n_elements"], info["n_nodes"])
+    achieved = b_mv / (mv_ms * 1e-3) / 1e9 if mv_ms else None
+    traffic = load_traffic().get(f"matvec_j2_n{args.n}")
+    line = {"metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 matvec / f64 residual+dots",
+            "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),
+            "method": "jacobi_pcg", "learned_fpcg_s": None,
+            "solve": {"newton_iterations": last["newton"], "cg_iterations": last["cg"],
+                      "all_converged": bool(last["converged"]), "max_relative_residual": last["max_rel"],
+                      "cg_ms_per_iteration": (ms / last["cg"]) if last["cg"] else None},
+            "clocks": clk,
+            "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches // max(args.steps, 1)),
+            "kernel_ms": {"matvec": kms[0], "residual": kms[1], "cg_update": kms[2], "cg_direction": kms[3]},
+            "roofline": {"bound": "hbm", "kernel": "matvec_kernel<J2>", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "frac_nominal_8tbs": (achieved / 8000.0) if achieved else None,
+                         "peak_source": peak_src, "algorithmic_bytes": b_mv,
+                         "traffic": traffic,
+                         "residual_achieved": residual_bytes(info["n_elements"], info["n_nodes"]) / (kms[1] * 1e-3) / 1e9
+                         if rc == 0 else None}}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = args.cpu_threads or os.cpu_count() or 1
+        nthr, dt, cinfo = cpu_leg(args, v, last["cg"], threads)
+        scale = (last["cg"] / max(cinfo["cg_iterations"], 1))
+        line["cpu_baseline"] = {"value": dt * scale, "unit": UNIT, "cores": nthr, "kind": "port",
+                                "sample": f"load step 1 of {args.load_steps} ({cinfo['cg_iterations']} CG "
+                                          f"iterations, {dt:.2f} s) scaled by the GPU solve's CG-iteration "
+                                          f"count ({last['cg']}); C++/OpenMP FP64 restatement"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del solver, mesh
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -129,6 +129,10 @@ const char* fem_last_error(void* ctx);
  * out[3]=block element entries (incl. redundant) out[4]=nodes_per_block
  * out[5]=device bytes held */
 int fem_ctx_info(void* ctx, int64_t* out6);
+/* counters since creation: out[0] kernel launches that did work (library
+ * kernels only), out[1] CG iterations, out[2] residual evaluations,
+ * out[3] CG graph launches */
+int fem_ctx_stats(void* ctx, int64_t* out4);
 /* cudaStream_t of the context (as void*) */
 void* fem_ctx_stream(void* ctx);
 
@@ -182,6 +186,14 @@ int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol
  * solves in FP32 (mixed-precision iterative refinement). */
 int fem_newton_solve(void* ctx, const FemSolveParams* params, FemSolveResult* result);
 void fem_default_solve_params(FemSolveParams* p);
+
+/* Kernel timing (no reference counterpart; the reference has only wall clocks,
+ * framework/_adapters/fem_adapter.py:162-172).  Launches each hot kernel
+ * `reps` times back to back on the context stream at the current tangent
+ * state and writes the mean CUDA-event milliseconds per launch:
+ * ms_out[0] tangent matvec (CG-fused), [1] FP64 residual, [2] CG update,
+ * [3] CG direction update.  Clobbers the context's CG scratch vectors. */
+int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out);
 
 /* ---- J2 history (j2_plasticity.py:103-123, 513-520) ---- */
 int fem_commit_history(void* ctx);

@@ -338,11 +338,12 @@ int cpu_fem_solve(int Nn, int Ne, const double* X, const int* conn, int model, c
   if (has_dc) {
     for (int i = 0; i < n; ++i) ub[i] = u[i] + dc[i];
     ref = std::sqrt(residual(P, ub.data(), fext, ep, epe, st, fe, R.data()));
-    double r_old = std::sqrt(residual(P, u, fext, ep, epe, st, fe, R.data()));
+    residual(P, u, fext, ep, epe, st, fe, R.data());
     evals += 2;
     matvec(P, st, dc.data(), fe, y.data());
     for (int i = 0; i < n; ++i) R[i] -= y[i];
-    double eta = std::min(std::max(0.1 * tol * ref / std::max(r_old, 1e-300), cg_rtol_min), 0.1);
+    // the predictor fixes the elastic state of the step: solve it to 1e-3
+    double eta = std::max(1e-3, cg_rtol_min);
     cg_total += pcg(P, st, R.data(), eta, max_cg, fe, du);
     for (int i = 0; i < n; ++i) u[i] += du[i] + dc[i];
     it = 1;
@@ -359,9 +360,10 @@ int cpu_fem_solve(int Nn, int Ne, const double* X, const int* conn, int model, c
   for (; it < max_newton; ++it) {
     if (res / ref < tol) { conv = true; break; }
     if (max_cg_total > 0 && cg_total >= max_cg_total) break;
-    double eta = 0.1 * tol * ref / res;
-    if (it > 0) eta = std::max(eta, 0.9 * (res / prev) * (res / prev));
-    eta = std::min(std::max(eta, cg_rtol_min), 0.1);
+    // forcing term: aim at the target, follow the residual's contraction, and
+    // solve tightly (1e-3) when the residual did not drop
+    double e2 = (it > 0 && res < prev) ? 0.9 * (res / prev) * (res / prev) : 1e-3;
+    double eta = std::min(std::max(std::max(0.1 * tol * ref / res, e2), cg_rtol_min), 0.1);
     int cap = max_cg;
     if (max_cg_total > 0) cap = std::min(cap, max_cg_total - cg_total);
     cg_total += pcg(P, st, R.data(), eta, cap, fe, du);

@@ -77,6 +77,7 @@ SIGNATURES = {
     "fem_ctx_destroy": (C.c_int, [_VP]),
     "fem_last_error": (C.c_char_p, [_VP]),
     "fem_ctx_info": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
+    "fem_ctx_stats": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "fem_ctx_stream": (C.c_void_p, [_VP]),
     "fem_set_materials": (C.c_int, [_VP, C.POINTER(FemMaterial), C.c_int32, _VP, _VP]),
     "fem_set_bc": (C.c_int, [_VP, _VP, _VP, _VP]),
@@ -91,6 +92,7 @@ SIGNATURES = {
                           C.POINTER(C.c_int32), _DP]),
     "fem_newton_solve": (C.c_int, [_VP, C.POINTER(FemSolveParams), C.POINTER(FemSolveResult)]),
     "fem_default_solve_params": (None, [C.POINTER(FemSolveParams)]),
+    "fem_profile_kernels": (C.c_int, [_VP, C.c_int32, _DP]),
     "fem_commit_history": (C.c_int, [_VP]),
     "fem_reset_history": (C.c_int, [_VP]),
     "fem_get_history": (C.c_int, [_VP, _VP, _VP]),

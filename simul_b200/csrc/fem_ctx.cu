@@ -75,6 +75,10 @@ struct FemCtx {
   CGState* h_cg = nullptr;
   double* h_scalars = nullptr;
 
+  // statistics since creation: kernel launches issued by this library, CG
+  // iterations, residual evaluations, CG graph launches
+  int64_t n_launches = 0, n_cg_iters = 0, n_res_evals = 0, n_graphs = 0;
+
   int model_kind = M_LE;       // single model, or -1 for mixed tables
   bool has_j2 = false;
   bool materials_set = false;
@@ -368,7 +372,8 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->tmpf, nd))) return st;
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
-  c->max_blocks = std::max(c->n_blocks, (c->ndof_pad / 4 + 255) / 256) + 1;
+  // every reducing kernel's grid must fit: node blocks, float4 vector blocks, node-parallel blocks
+  c->max_blocks = std::max({c->n_blocks, (c->ndof_pad / 4 + 255) / 256, (c->Nn + 255) / 256}) + 1;
   if ((st = dalloc(c, &c->partials, (size_t)N_SITES * 2 * c->max_blocks))) return st;
   if ((st = dalloc(c, &c->counters, (size_t)N_SITES))) return st;
   if ((st = dalloc(c, &c->scalars, (size_t)8))) return st;
@@ -422,7 +427,7 @@ int eval_residual(FemCtx* c, double* fneg_out_int, double* rnorm2) {
   a.rnorm2 = c->scalars;
   a.red = c->red();
   a.red_site = SITE_RES;
-  launch_residual(a, c->model_kind, c->stream);
+  ++c->n_launches; launch_residual(a, c->model_kind, c->stream);
   CKL();
   CK(cudaMemcpyAsync(c->h_scalars, c->scalars, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -438,11 +443,11 @@ int compute_dinv(FemCtx* c, int precond) {
     a.matF = c->matF;
     a.payload = c->payload;
     a.dinv = c->dinv;
-    launch_diag(a, c->model_kind, c->stream);
+    ++c->n_launches; launch_diag(a, c->model_kind, c->stream);
     CKL();
   } else {
     // identity on free DOFs: dinv = 1 where not fixed
-    launch_dinv_identity(c->dinv, c->fixed, c->Nn, c->stream);
+    ++c->n_launches; launch_dinv_identity(c->dinv, c->fixed, c->Nn, c->stream);
     CKL();
   }
   return FEM_OK;
@@ -491,7 +496,7 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if ((st = compute_dinv(c, precond))) return st;
   if ((st = ensure_cg_graph(c))) return st;
   const int ndof4 = c->ndof_pad / 4;
-  launch_cg_init(b_int, c->r, c->x, c->p, c->dinv, ndof4, c->cg, rtol, maxit, c->red(), SITE_CGI,
+  ++c->n_launches; launch_cg_init(b_int, c->r, c->x, c->p, c->dinv, ndof4, c->cg, rtol, maxit, c->red(), SITE_CGI,
                  c->stream);
   CKL();
   const int max_batches = maxit / kCGBatch + 2;
@@ -500,11 +505,15 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   int batches = 0;
   while (!c->h_cg->done && batches < max_batches) {
     CK(cudaGraphLaunch(c->cg_graph, c->stream));
+    c->n_graphs++;
     CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     ++batches;
   }
   const CGState& h = *c->h_cg;
+  c->n_cg_iters += h.iter;
+  // kernels that did work: 3 per CG iteration (the rest of a batch exits at entry)
+  c->n_launches += 3LL * h.iter;
   if (iters) *iters = h.iter;
   if (rel) *rel = h.rr0 > 0 ? std::sqrt(h.rr / h.rr0) : 0.0;
   if (h.done == 3) return set_err(c, FEM_ERR_NAN, "PCG breakdown (non-positive curvature or NaN) at iteration %d", h.iter);
@@ -606,6 +615,16 @@ int fem_ctx_info(void* ctx, int64_t* out) {
   return FEM_OK;
 }
 
+int fem_ctx_stats(void* ctx, int64_t* out) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  if (!c || !out) return FEM_ERR_INVALID;
+  out[0] = c->n_launches;
+  out[1] = c->n_cg_iters;
+  out[2] = c->n_res_evals;
+  out[3] = c->n_graphs;
+  return FEM_OK;
+}
+
 void* fem_ctx_stream(void* ctx) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   return c ? (void*)c->stream : nullptr;
@@ -688,15 +707,15 @@ int fem_set_bc(void* ctx, const uint8_t* fixed_mask, const double* fixed_values,
   int st;
   if ((st = check_ctx(c))) return st;
   if (fixed_mask) {
-    launch_gather_mask(fixed_mask, c->fixed, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_gather_mask(fixed_mask, c->fixed, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
   if (fixed_values) {
-    launch_gather_d(fixed_values, c->fixed_vals, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_gather_d(fixed_values, c->fixed_vals, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
   if (f_ext) {
-    launch_gather_d(f_ext, c->fext, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_gather_d(f_ext, c->fext, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -708,7 +727,7 @@ int fem_apply_bc(void* ctx) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   int st;
   if ((st = check_ctx(c))) return st;
-  launch_apply_bc(c->u, c->fixed_vals, c->fixed, c->Nn, c->stream);
+  ++c->n_launches; launch_apply_bc(c->u, c->fixed_vals, c->fixed, c->Nn, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;
@@ -719,7 +738,7 @@ int fem_set_displacement(void* ctx, const double* u) {
   int st;
   if ((st = check_ctx(c))) return st;
   if (!u) return set_err(c, FEM_ERR_INVALID, "null displacement");
-  launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
+  ++c->n_launches; launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   c->tangent_valid = false;
@@ -731,7 +750,7 @@ int fem_get_displacement(void* ctx, double* u_out) {
   int st;
   if ((st = check_ctx(c))) return st;
   if (!u_out) return set_err(c, FEM_ERR_INVALID, "null output");
-  launch_scatter_d(c->u, u_out, c->d_perm_node, c->Nn, c->stream);
+  ++c->n_launches; launch_scatter_d(c->u, u_out, c->d_perm_node, c->Nn, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;
@@ -741,7 +760,7 @@ int fem_reference_quantities(void* ctx, double* dNdX_out, double* vol_out) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   int st;
   if ((st = check_ctx(c))) return st;
-  launch_refq(c->mesh(), c->d_perm_elem, dNdX_out, vol_out, c->stream);
+  ++c->n_launches; launch_refq(c->mesh(), c->d_perm_elem, dNdX_out, vol_out, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;
@@ -753,10 +772,10 @@ int fem_compute_stress(void* ctx, const double* u, double* F_out, double* sigma_
   if ((st = check_ctx(c))) return st;
   if (!c->materials_set) return set_err(c, FEM_ERR_STATE, "materials not set");
   if (u) {
-    launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
-  launch_stress(c->mesh(), c->matD, c->model_kind, c->u, c->ep_c, c->epe_c, c->d_perm_elem, F_out,
+  ++c->n_launches; launch_stress(c->mesh(), c->matD, c->model_kind, c->u, c->ep_c, c->epe_c, c->d_perm_elem, F_out,
                 sigma_out, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
@@ -769,17 +788,17 @@ int fem_element_forces(void* ctx, const double* u, double* f_out, double* residu
   if ((st = check_ctx(c))) return st;
   if (!c->materials_set) return set_err(c, FEM_ERR_STATE, "materials not set");
   if (u) {
-    launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
   double r2 = 0;
   if ((st = eval_residual(c, f_out ? c->tmpd : nullptr, &r2))) return st;
   if (f_out) {
-    launch_scatter_d(c->tmpd, f_out, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_scatter_d(c->tmpd, f_out, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
   if (residual_out) {
-    launch_scatter_d(c->R, residual_out, c->d_perm_node, c->Nn, c->stream);
+    ++c->n_launches; launch_scatter_d(c->R, residual_out, c->d_perm_node, c->Nn, c->stream);
     CKL();
   }
   CK(cudaStreamSynchronize(c->stream));
@@ -793,7 +812,7 @@ int fem_tangent_matvec(void* ctx, const float* xin, float* yout) {
   if ((st = check_ctx(c))) return st;
   if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
   if (!xin || !yout) return set_err(c, FEM_ERR_INVALID, "null vector");
-  launch_gather_f(xin, c->tmpf, c->d_perm_node, c->Nn, c->stream);
+  ++c->n_launches; launch_gather_f(xin, c->tmpf, c->d_perm_node, c->Nn, c->stream);
   CKL();
   MvArgs mv;
   mv.m = c->mesh();
@@ -805,9 +824,9 @@ int fem_tangent_matvec(void* ctx, const float* xin, float* yout) {
   mv.red = c->red();
   mv.red_site = SITE_MV;
   mv.mask_input = 1;
-  launch_matvec(mv, c->model_kind, c->stream);
+  ++c->n_launches; launch_matvec(mv, c->model_kind, c->stream);
   CKL();
-  launch_scatter_f(c->y, yout, c->d_perm_node, c->Nn, c->stream);
+  ++c->n_launches; launch_scatter_f(c->y, yout, c->d_perm_node, c->Nn, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;
@@ -821,7 +840,7 @@ int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol
   if (!r || !du) return set_err(c, FEM_ERR_INVALID, "null vector");
   if (maxit <= 0 || !(rtol > 0)) return set_err(c, FEM_ERR_INVALID, "need max_iterations > 0 and rtol > 0");
   // caller order -> internal order, fixed DOFs of the right-hand side zeroed
-  launch_gather_d_masked(r, c->tmpd, c->d_perm_node, c->fixed, c->Nn, c->stream);
+  ++c->n_launches; launch_gather_d_masked(r, c->tmpd, c->d_perm_node, c->fixed, c->Nn, c->stream);
   CKL();
   int it = 0;
   double rl = 0;
@@ -829,7 +848,7 @@ int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol
   if (iters) *iters = it;
   if (rel) *rel = rl;
   if (st && st != FEM_NOT_CONVERGED) return st;
-  launch_scatter_f2d(c->x, du, c->d_perm_node, c->Nn, c->stream);
+  ++c->n_launches; launch_scatter_f2d(c->x, du, c->d_perm_node, c->Nn, c->stream);
   CKL();
   CK(cudaStreamSynchronize(c->stream));
   return st;
@@ -869,7 +888,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
   // Newton.  Relative convergence is measured, as in the reference
   // (static_solver.py:159-218), against the residual of the state it evaluates
   // first: the previous u with the new prescribed values applied.
-  launch_bc_delta(c->u, c->fixed_vals, c->fixed, c->tmpf, c->Nn, c->red(), SITE_AUX,
+  ++c->n_launches; launch_bc_delta(c->u, c->fixed_vals, c->fixed, c->tmpf, c->Nn, c->red(), SITE_AUX,
                   c->scalars + 1, c->stream);
   CKL();
   CK(cudaMemcpyAsync(c->h_scalars + 1, c->scalars + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -880,7 +899,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
   int it0 = 0;
   if (has_dc) {
     CK(cudaMemcpyAsync(c->u_base, c->u, c->ndof_pad * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    launch_apply_bc(c->u, c->fixed_vals, c->fixed, c->Nn, c->stream);
+    ++c->n_launches; launch_apply_bc(c->u, c->fixed_vals, c->fixed, c->Nn, c->stream);
     CKL();
     if ((st = eval_residual(c, nullptr, &r2))) return st;
     ref_norm = std::sqrt(r2);
@@ -901,24 +920,23 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     mv.red = c->red();
     mv.red_site = SITE_MV;
     mv.mask_input = 0;
-    launch_matvec(mv, c->model_kind, c->stream);
+    ++c->n_launches; launch_matvec(mv, c->model_kind, c->stream);
     CKL();
-    launch_rhs_minus(c->R, c->y, c->fixed, c->tmpd, c->Nn, c->stream);
+    ++c->n_launches; launch_rhs_minus(c->R, c->y, c->fixed, c->tmpd, c->Nn, c->stream);
     CKL();
-    const double r_old = std::sqrt(r2);
-    double eta = 0.1 * prm.tol * ref_norm / std::max(r_old, 1e-300);
-    eta = std::min(std::max(eta, prm.cg_rtol_min), prm.cg_rtol_max);
+    // the predictor fixes the elastic state of the step: solve it to 1e-3
+    const double eta = std::max(1e-3, prm.cg_rtol_min);
     int cgit = 0;
     double cgrel = 0;
     st = run_pcg(c, c->tmpd, prm.precond, eta, prm.cg_max_iterations, &cgit, &cgrel);
     out.cg_iterations += cgit;
     if (st && st != FEM_NOT_CONVERGED) return st;
-    launch_u_update(c->u, c->u_base, c->x, 1.0, c->ndof, c->stream);
+    ++c->n_launches; launch_u_update(c->u, c->u_base, c->x, 1.0, c->ndof, c->stream);
     CKL();
     it0 = 1;
   }
   // apply_boundary_conditions (core/mesh.py:321-327): prescribed DOFs held exactly
-  launch_apply_bc(c->u, c->fixed_vals, c->fixed, c->Nn, c->stream);
+  ++c->n_launches; launch_apply_bc(c->u, c->fixed_vals, c->fixed, c->Nn, c->stream);
   CKL();
   if ((st = eval_residual(c, nullptr, &r2))) return st;
   out.residual_evals += 1;
@@ -951,9 +969,12 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
       converged = true;
       break;
     }
-    // inexact-Newton forcing term: aim straight at the target, within [min, max]
-    double eta = 0.1 * prm.tol * ref / res_norm;
-    if (it > 0 && prev_norm > 0) eta = std::max(eta, 0.9 * (res_norm / prev_norm) * (res_norm / prev_norm));
+    // inexact-Newton forcing term: aim at the target, follow the residual's
+    // contraction (Eisenstat-Walker), and solve tightly (1e-3) when the
+    // residual did not drop — loose solves there let J2 iterations wander
+    const bool dropped = it > it0 && res_norm < prev_norm;
+    const double ew = dropped ? 0.9 * (res_norm / prev_norm) * (res_norm / prev_norm) : 1e-3;
+    double eta = std::max(0.1 * prm.tol * ref / res_norm, ew);
     eta = std::min(std::max(eta, prm.cg_rtol_min), prm.cg_rtol_max);
     int cgit = 0;
     double cgrel = 0;
@@ -970,7 +991,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     double trial = res_norm;
     const int n_trials = prm.line_search == FEM_LS_NONE ? 1 : 5;
     for (int ls = 0; ls < n_trials; ++ls) {
-      launch_u_update(c->u, c->u_base, c->x, alpha, c->ndof, c->stream);
+      ++c->n_launches; launch_u_update(c->u, c->u_base, c->x, alpha, c->ndof, c->stream);
       CKL();
       if ((st = eval_residual(c, nullptr, &r2))) return st;
       out.residual_evals++;
@@ -1003,6 +1024,81 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
   out.relative_residual = res_norm / ref;
   if (res) *res = out;
   return converged ? FEM_OK : FEM_NOT_CONVERGED;
+}
+
+int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
+  if (reps <= 0 || !ms_out) return set_err(c, FEM_ERR_INVALID, "need reps > 0 and an output array");
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int ndof4 = c->ndof_pad / 4;
+  // a CG state that never finishes, so the fused kernels do their full work
+  CGState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.rz = 1.0;
+  hs.rr = 1.0;
+  hs.rr0 = 1.0;
+  hs.tol2 = 0.0;
+  hs.alpha = 1e-30;
+  hs.beta = 0.0;
+  hs.max_iter = 1 << 30;
+  auto reset_cg = [&]() { return cudaMemcpyAsync(c->cg, &hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream); };
+  MvArgs mv;
+  mv.m = c->mesh();
+  mv.matF = c->matF;
+  mv.payload = c->payload;
+  mv.x = c->p;
+  mv.y = c->y;
+  mv.cg = c->cg;
+  mv.red = c->red();
+  mv.red_site = SITE_MV;
+  mv.mask_input = 1;
+  ResArgs ra;
+  ra.m = c->mesh();
+  ra.matD = c->matD;
+  ra.u = c->u;
+  ra.f_ext = c->fext;
+  ra.R = c->tmpd;
+  ra.fneg = nullptr;
+  ra.payload = c->payload;
+  ra.ep_c = c->ep_c;
+  ra.epe_c = c->epe_c;
+  ra.ep_t = c->ep_t;
+  ra.epe_t = c->epe_t;
+  ra.rnorm2 = c->scalars + 2;
+  ra.red = c->red();
+  ra.red_site = SITE_RES;
+  for (int k = 0; k < 4; ++k) {
+    CK(reset_cg());
+    for (int w = 0; w < 2; ++w) {
+      if (k == 0) launch_matvec(mv, c->model_kind, c->stream);
+      if (k == 1) launch_residual(ra, c->model_kind, c->stream);
+      if (k == 2) launch_cg_update(c->tmpf, c->r, c->p, c->y, c->dinv, ndof4, c->cg, c->red(), SITE_CGU, c->stream);
+      if (k == 3) launch_cg_pupdate(c->tmpf, c->r, c->dinv, ndof4, c->cg, c->stream);
+    }
+    CK(reset_cg());
+    CK(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < reps; ++r) {
+      if (k == 0) launch_matvec(mv, c->model_kind, c->stream);
+      if (k == 1) launch_residual(ra, c->model_kind, c->stream);
+      if (k == 2) launch_cg_update(c->tmpf, c->r, c->p, c->y, c->dinv, ndof4, c->cg, c->red(), SITE_CGU, c->stream);
+      if (k == 3) launch_cg_pupdate(c->tmpf, c->r, c->dinv, ndof4, c->cg, c->stream);
+    }
+    CK(cudaEventRecord(e1, c->stream));
+    CKL();
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    ms_out[k] = ms / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->tangent_valid = true;
+  return FEM_OK;
 }
 
 int fem_commit_history(void* ctx) {

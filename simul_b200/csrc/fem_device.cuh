@@ -478,4 +478,9 @@ __device__ __forceinline__ bool model_has_payload(int model) {
   return md == M_NH || md == M_MR || md == M_FMR || md == M_J2;
 }
 
+// payload words a model uses: NH F^-1 + ln J (10), MR F (9), J2 n + theta + gamma2 (8)
+__host__ __device__ __forceinline__ int model_pay_words(int model) {
+  return model == M_NH ? 10 : (model == M_J2 ? 8 : ((model == M_MR || model == M_FMR) ? 9 : 0));
+}
+
 }  // namespace femb200

@@ -129,9 +129,11 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
       } else {
         le_stress(mat, scale, Hg, S);
       }
-      if (idx < home_end && model_has_payload<MODEL>(model)) {
+      if (idx < home_end) {
+        const int npay = model_pay_words(model);
 #pragma unroll
-        for (int k = 0; k < kPay; ++k) a.payload[(size_t)k * m.n_elems + e] = pay[k];
+        for (int k = 0; k < kPay; ++k)
+          if (k < npay) a.payload[(size_t)k * m.n_elems + e] = pay[k];
       }
       double f[4][3];
       slot_vectors(S, g, -g.s6, f);
@@ -233,9 +235,11 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
       const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
       const float scale = __ldg(m.scale + e);
       float pay[kPay];
-      if (model_has_payload<MODEL>(mat.model)) {
+      {
+        const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
 #pragma unroll
-        for (int k = 0; k < kPay; ++k) pay[k] = __ldg(a.payload + (size_t)k * m.n_elems + e);
+        for (int k = 0; k < kPay; ++k)
+          pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
       }
       float dP[9];
       dP_any<MODEL>(mat, scale, pay, dF, dP);
@@ -329,9 +333,11 @@ __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagAr
       const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
       const float scale = __ldg(m.scale + e);
       float pay[kPay];
-      if (model_has_payload<MODEL>(mat.model)) {
+      {
+        const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
 #pragma unroll
-        for (int k = 0; k < kPay; ++k) pay[k] = __ldg(a.payload + (size_t)k * m.n_elems + e);
+        for (int k = 0; k < kPay; ++k)
+          pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
       }
       float w[4][3];
 #pragma unroll

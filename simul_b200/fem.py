@@ -126,7 +126,7 @@ class FEMesh:
 
     def __del__(self):
         ctx = getattr(self, "_ctx", None)
-        if ctx is not None and _lib._lib is not None:
+        if ctx is not None and _lib is not None and getattr(_lib, "_lib", None) is not None:
             try:
                 _lib._lib.fem_ctx_destroy(ctx)
             except Exception:
@@ -144,6 +144,11 @@ class FEMesh:
         _check(_lib.load().fem_ctx_info(self.ctx, out), self.ctx, "fem_ctx_info")
         return {"n_nodes": out[0], "n_elements": out[1], "n_blocks": out[2],
                 "block_element_entries": out[3], "nodes_per_block": out[4], "device_bytes": out[5]}
+
+    def stats(self) -> dict:
+        out = (C.c_int64 * 4)()
+        _check(_lib.load().fem_ctx_stats(self.ctx, out), self.ctx, "fem_ctx_stats")
+        return {"launches": out[0], "cg_iterations": out[1], "residual_evals": out[2], "cg_graphs": out[3]}
 
     # ---- boundary conditions (core/mesh.py:321-399) ----
     def set_fixed_nodes(self, node_ids, values=None, dofs=None):

@@ -134,7 +134,7 @@ def test_j2_forces_history_and_tangent(cuda, vox):
                                  O.deformation_gradient(ref["u"], vox.conn.astype(np.int64),
                                                         O.reference_quantities(vox.X, vox.conn)[0]),
                                  O.J2State(ref["ep"], ref["epe"]))
-    assert _rel_max(s_gpu, sig_chk) < 1e-9
+    assert _rel_max(s_gpu, sig_chk) < 1e-8
     mat.reset_state()
     assert np.all(mat.get_plastic_strain() == 0)
 

@@ -195,6 +195,18 @@ void fem_default_solve_params(FemSolveParams* p);
  * [3] CG direction update.  Clobbers the context's CG scratch vectors. */
 int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out);
 
+/* Allocation-free FP64 dot product, *result = sum_i a[i] b[i] (device pointers,
+ * issued on `stream`, a cudaStream_t or NULL).  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc (an application whose
+ * allocator owns all device memory, a loop that forbids allocation after
+ * start-up): it is the deterministic fixed-order reduction the solver uses for
+ * its dots and norms, with its partial sums in a static 16 KB device array
+ * instead of context scratch.  n <= 8,388,608 (larger n: FEM_ERR_INVALID).
+ * The first call on a device looks up that array's address there; make it
+ * before any stream capture.  Calls share the array: calls that overlap on the
+ * GPU race and must be serialised.  Errors: fem_last_error(NULL). */
+int fem_dot_f64_noalloc(const double* a, const double* b, int64_t n, double* result, void* stream);
+
 /* ---- J2 history (j2_plasticity.py:103-123, 513-520) ---- */
 int fem_commit_history(void* ctx);
 int fem_reset_history(void* ctx);

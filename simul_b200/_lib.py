@@ -93,6 +93,7 @@ SIGNATURES = {
     "fem_newton_solve": (C.c_int, [_VP, C.POINTER(FemSolveParams), C.POINTER(FemSolveResult)]),
     "fem_default_solve_params": (None, [C.POINTER(FemSolveParams)]),
     "fem_profile_kernels": (C.c_int, [_VP, C.c_int32, _DP]),
+    "fem_dot_f64_noalloc": (C.c_int, [_VP, _VP, C.c_int64, _VP, _VP]),
     "fem_commit_history": (C.c_int, [_VP]),
     "fem_reset_history": (C.c_int, [_VP]),
     "fem_get_history": (C.c_int, [_VP, _VP, _VP]),

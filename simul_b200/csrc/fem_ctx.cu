@@ -531,6 +531,16 @@ int check_ctx(FemCtx* c) {
 
 }  // namespace
 
+int femb200::set_global_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_create_error = buf;
+  return code;
+}
+
 // ───────────────────────── C ABI ─────────────────────────
 
 extern "C" {

@@ -81,6 +81,10 @@ struct DiagArgs {
   float* dinv;              // [3 Nn] 1/diag(K) on free DOFs, 0 elsewhere
 };
 
+// Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
+// returns `code`.
+int set_global_error(int code, const char* fmt, ...);
+
 // launchers (fem_kernels.cu)
 void launch_residual(const ResArgs& a, int model, cudaStream_t s);
 void launch_matvec(const MvArgs& a, int model, cudaStream_t s);

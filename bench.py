@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--precond", default="two_level", choices=["jacobi", "two_level"],
+                    help="preconditioner of the timed solve; Jacobi-PCG is timed beside it")
+    ap.add_argument("--no-jacobi-baseline", action="store_true")
     return ap.parse_args()
 
 
@@ -62,7 +65,7 @@ def workload_config(args, v):
             "voxels": int(v.info["n_voxels"]), "tets": int(v.n_elements), "nodes": int(v.n_nodes),
             "h_mm": v.info["h"], "load_steps": args.load_steps, "tol": args.tol,
             "material": "J2 sigma_y=100 MPa H=0.02E, E shell 12 GPa / core lognormal(300 MPa, 0.3)",
-            "method": "Newton (FP64 residual) + Jacobi-PCG (FP32 matvec, FP64 dots)",
+            "method": f"Newton (FP64 residual) + {args.precond} PCG (FP32 matvec, FP64 dots)",
             "l2": "flushed (256 MB write) before every timed step", "parallelism": "replicas"}
 
 
@@ -228,13 +231,13 @@ def main():
     mesh = B.FEMesh(v.n_nodes, v.n_elements, device=local)
     mesh.initialize_from_numpy(v.X, v.conn)
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
-    solver = B.StaticSolver(mesh, mat, tol=args.tol)
+    solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond)
     fixed_full = torch.from_numpy(v.fixed_vals).to(dev)
     fixed_mask = torch.from_numpy(v.fixed_mask.astype(np.int32)).to(dev)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
-    def solve_all():
+    def solve_all(solver=solver):
         """One full solve from rest: all load steps, each to tol."""
         mesh.u.zero_()
         mat.reset_state()
@@ -316,6 +319,29 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # the plain method timed beside the chosen one (same mesh, same clocks regime)
+    jac = None
+    if args.precond != "jacobi" and not args.no_jacobi_baseline:
+        jsolver = B.StaticSolver(mesh, mat, tol=args.tol, precond="jacobi")
+        solve_all(jsolver)
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        jl = solve_all(jsolver)
+        e1.record(stream)
+        e1.synchronize()
+        jms = e0.elapsed_time(e1)
+        if ws > 1:
+            t = torch.tensor([jms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            jms = float(t.item())
+        jac = {"s": jms / 1e3, "newton_iterations": jl["newton"], "cg_iterations": jl["cg"],
+               "all_converged": bool(jl["converged"]), "max_relative_residual": jl["max_rel"],
+               "speedup_of_timed_method": jms / ms, "timed_once_after_one_warmup": True}
+        del jsolver
+
     # roofline of the dominant kernel (tangent matvec), CUDA events on the solver stream
     kms = (C.c_double * 4)()
     rc = _lib.load().fem_profile_kernels(mesh.ctx, 200, kms)
@@ -324,12 +350,15 @@ def main():
     peak, peak_src = measured_peaks()
     b_mv = matvec_bytes(info["n_elements"], info["n_nodes"])
     achieved = b_mv / (mv_ms * 1e-3) / 1e9 if mv_ms else None
-    traffic = load_traffic().get(f"matvec_j2_n{args.n}")
+    st = mesh.stats()
+    variant = st["matvec_variant"]
+    traffic = load_traffic().get(f"matvec_{variant}_j2_n{args.n}")
     line = {"metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 matvec / f64 residual+dots",
             "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),
-            "method": "jacobi_pcg", "learned_fpcg_s": None,
+            "method": f"{args.precond}_pcg", "learned_fpcg_s": None, "jacobi_pcg": jac,
+            "coarse": mesh.coarse_info() if args.precond == "two_level" else None,
             "solve": {"newton_iterations": last["newton"], "cg_iterations": last["cg"],
                       "all_converged": bool(last["converged"]), "max_relative_residual": last["max_rel"],
                       "cg_ms_per_iteration": (ms / last["cg"]) if last["cg"] else None},
@@ -337,7 +366,10 @@ def main():
             "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches // max(args.steps, 1)),
             "kernel_ms": {"matvec": kms[0], "residual": kms[1], "cg_update": kms[2], "cg_direction": kms[3]},
-            "roofline": {"bound": "hbm", "kernel": "matvec_kernel<J2>", "achieved": achieved, "peak": peak,
+            "matvec_variant": {"chosen": variant, "ns_per_launch": st["matvec_ns"]},
+            "roofline": {"bound": "hbm", "kernel": ("matvec_kernel<J2> (fused node-block)" if variant == "fused"
+                                                    else "elem_mv_kernel<J2> + node_gather_kernel (two-phase)"),
+                         "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "frac_nominal_8tbs": (achieved / 8000.0) if achieved else None,
                          "peak_source": peak_src, "algorithmic_bytes": b_mv,

@@ -52,7 +52,11 @@ enum {
   FEM_FIBRE_MOONEY_RIVLIN = 5    /* hyperelastic fibre-reinforced MR; no reference counterpart */
 };
 
-enum { FEM_PRECOND_NONE = 0, FEM_PRECOND_JACOBI = 1 };
+/* preconditioners of fem_pcg / fem_newton_solve.  The reference factorises the
+ * assembled tangent instead (static_solver.py:399-462).  TWO_LEVEL adds to
+ * Jacobi a Galerkin coarse correction on a lattice of trilinear cells:
+ * z = D^-1 r + P (P^T K P)^-1 P^T r. */
+enum { FEM_PRECOND_NONE = 0, FEM_PRECOND_JACOBI = 1, FEM_PRECOND_TWO_LEVEL = 2, FEM_PRECOND_LEARNED = 3 };
 
 /* line-search policy of fem_newton_solve */
 enum {
@@ -131,8 +135,56 @@ const char* fem_last_error(void* ctx);
 int fem_ctx_info(void* ctx, int64_t* out6);
 /* counters since creation: out[0] kernel launches that did work (library
  * kernels only), out[1] CG iterations, out[2] residual evaluations,
- * out[3] CG graph launches */
-int fem_ctx_stats(void* ctx, int64_t* out4);
+ * out[3] CG graph launches; matvec variant selection: out[4] variant in use
+ * (0 fused node-block, 1 two-phase), out[5] / out[6] timed ns per launch of
+ * the fused / two-phase variant (0 if not timed), out[7] 1 if the choice was
+ * made by timing */
+int fem_ctx_stats(void* ctx, int64_t* out8);
+
+/* Option keys of fem_set_option (no reference counterpart: the reference has
+ * one matvec formulation, backend/fea/fem/material/nonlinear/base.py:110-145). */
+enum {
+  /* -1 (default): time both tangent-matvec variants on the first PCG solve
+   * and keep the faster; 0: fused node-block kernel; 1: element pass writing
+   * slot vectors in node order plus a node gather */
+  FEM_OPT_MATVEC_VARIANT = 1,
+  /* two-level preconditioner: lattice cell edge in mesh lengths (default 8;
+   * the cube root of 5x the mean element volume, i.e. the voxel edge of
+   * 5-tet voxel meshes); grown automatically past 4096 coarse nodes */
+  FEM_OPT_COARSE_CELL = 2,
+  /* two-level preconditioner: PCG solves one coarse assembly serves
+   * (default 1: reassembled at every tangent) */
+  FEM_OPT_COARSE_REUSE = 3,
+  /* learned preconditioner: 1 (default) adds the two-level coarse correction
+   * to the network's output, 0 uses the network alone */
+  FEM_OPT_LEARNED_COARSE = 4
+};
+int fem_set_option(void* ctx, int32_t key, int64_t value);
+/* Learned preconditioner (no reference counterpart).  A message-passing
+ * network over mesh nodes (4 layers, width 64, BF16 weights on tcgen05 tensor
+ * cores, FP32 accumulation) maps a residual r to a correction
+ *   z = D^-1 r + s D^-1/2 net(D^-1/2 r / s, fixed bits, log-modulus) (+ coarse)
+ * used by flexible PCG (FEM_PRECOND_LEARNED); Jacobi-based PCG reruns the
+ * solve when the flexible one breaks down or exhausts its iterations.
+ * Parameters: FP32, flat order W_e[64][16], b_e[64], 4 x (W_l[64][128],
+ * b_l[64]), W_d[3][64], b_d[3] (34,307 values), host arrays. */
+int fem_mpnn_set_weights(void* ctx, const float* w, int64_t n);
+int fem_mpnn_get_weights(void* ctx, float* w, int64_t n);
+/* z = M(r) at the current tangent (caller order, N x 3 FP32 device arrays) */
+int fem_mpnn_forward(void* ctx, const float* r, float* z);
+/* out[0] flexible solves that fell back to Jacobi-based PCG, out[1] 1 if
+ * weights are set */
+int fem_learned_stats(void* ctx, int64_t* out2);
+
+/* Known-answer check of the tensor-core path the learned preconditioner uses
+ * (no reference counterpart): D (128 x N, FP32) = A (128 x K) B^T (B: N x K),
+ * BF16 row-major device arrays, one tcgen05 tile; N, K multiples of 16 in
+ * [16, 256].  Errors go to fem_last_error(NULL). */
+int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t K, void* stream);
+/* two-level preconditioner state: out[0] lattice cells, [1] coarse nodes,
+ * [2] coarse DOFs, [3] cell edge, [4] assemblies so far, [5] ms of the last
+ * assembly + factorisation (CUDA events) */
+int fem_coarse_info(void* ctx, double* out6);
 /* cudaStream_t of the context (as void*) */
 void* fem_ctx_stream(void* ctx);
 

@@ -459,6 +459,17 @@ def assemble(Ke, conn, n_nodes):
     return sp.coo_matrix((Ke.reshape(-1), (rows, cols)), shape=(3 * n_nodes, 3 * n_nodes)).tocsr()
 
 
+def solve_tangent(mat, F, tang, mesh, rhs, fixed_mask):
+    """Direct FP64 solve of K_ff x_f = rhs_f (x = 0 on fixed DOFs): the exact
+    answer the GPU PCG paths approximate."""
+    K = assemble(element_stiffness(tangent_A(mat, F, tang), mesh.dNdX, mesh.vol),
+                 np.asarray(mesh.conn, dtype=np.int64), mesh.X.shape[0])
+    free = ~np.asarray(fixed_mask, dtype=bool).reshape(-1)
+    x = np.zeros(K.shape[0])
+    x[free] = spsolve(K[free][:, free].tocsc(), np.asarray(rhs, dtype=np.float64).reshape(-1)[free])
+    return x.reshape(-1, 3)
+
+
 def tangent_matvec(mat, F, tang, dNdX, vol, conn, p):
     """Matrix-free y = K_T p, p (Nn,3): the operator the GPU matvec applies."""
     dF = np.einsum("eai,eaj->eij", p[conn], dNdX)

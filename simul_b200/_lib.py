@@ -27,12 +27,21 @@ FEM_FIBRE_MOONEY_RIVLIN = 5
 
 FEM_PRECOND_NONE = 0
 FEM_PRECOND_JACOBI = 1
+FEM_PRECOND_TWO_LEVEL = 2
+FEM_PRECOND_LEARNED = 3
 
 FEM_LS_REFERENCE = 0
 FEM_LS_GUARDED = 1
 FEM_LS_NONE = 2
 
 FEM_MAX_MATERIALS = 16
+
+FEM_OPT_MATVEC_VARIANT = 1
+FEM_OPT_COARSE_CELL = 2
+FEM_OPT_COARSE_REUSE = 3
+FEM_OPT_LEARNED_COARSE = 4
+MPNN_PARAMS = 34307
+MATVEC_VARIANTS = {0: "fused", 1: "two_phase"}
 
 
 class FemMeshDesc(C.Structure):
@@ -79,6 +88,13 @@ SIGNATURES = {
     "fem_ctx_info": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "fem_ctx_stats": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "fem_ctx_stream": (C.c_void_p, [_VP]),
+    "fem_set_option": (C.c_int, [_VP, C.c_int32, C.c_int64]),
+    "fem_coarse_info": (C.c_int, [_VP, _DP]),
+    "fem_selftest_umma": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32, _VP]),
+    "fem_mpnn_set_weights": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int64]),
+    "fem_mpnn_get_weights": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int64]),
+    "fem_mpnn_forward": (C.c_int, [_VP, _VP, _VP]),
+    "fem_learned_stats": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "fem_set_materials": (C.c_int, [_VP, C.POINTER(FemMaterial), C.c_int32, _VP, _VP]),
     "fem_set_bc": (C.c_int, [_VP, _VP, _VP, _VP]),
     "fem_apply_bc": (C.c_int, [_VP]),

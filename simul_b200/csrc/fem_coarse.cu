@@ -1,0 +1,499 @@
+// Two-level preconditioner of the PCG solve: Jacobi on the mesh plus a
+// Galerkin coarse correction on a regular lattice of trilinear cells,
+//
+//   z = D^-1 r + P Ac^-1 P^T r,   Ac = P^T K_T P   (free DOFs only).
+//
+// P interpolates coarse-node displacements trilinearly to the mesh nodes.
+// Each mesh node lives in one lattice cell (the cell of one of its elements);
+// each element is assembled in the cell of its centroid with its nodes'
+// trilinear weights clamped to that cell.  On voxel meshes whose cells are
+// whole multiples of the voxel, both views of P coincide and Ac is exactly
+// P^T K P; elsewhere Ac is a sum of per-element Galerkin blocks, still SPD.
+//
+// No reference counterpart: the reference solves the assembled system with
+// spsolve / ILU-CG (backend/fea/fem/solver/static_solver.py:399-462).
+#include <cuda_runtime.h>
+
+#include "fem_internal.h"
+#include "fem_reduce.cuh"
+
+namespace femb200 {
+
+namespace {
+
+__device__ __forceinline__ float tri_weight(float tx, float ty, float tz, int corner) {
+  const float wx = (corner & 4) ? tx : 1.f - tx;
+  const float wy = (corner & 2) ? ty : 1.f - ty;
+  const float wz = (corner & 1) ? tz : 1.f - tz;
+  return wx * wy * wz;
+}
+
+// local coordinates of a point in lattice cell ijk, clamped to [0, 1]
+__device__ __forceinline__ void cell_local(const CoarseDev& c, int3 ijk, float x, float y, float z,
+                                           float t[3]) {
+  t[0] = fminf(fmaxf((x - c.lo.x) * c.inv_H - (float)ijk.x, 0.f), 1.f);
+  t[1] = fminf(fmaxf((y - c.lo.y) * c.inv_H - (float)ijk.y, 0.f), 1.f);
+  t[2] = fminf(fmaxf((z - c.lo.z) * c.inv_H - (float)ijk.z, 0.f), 1.f);
+}
+
+template <int NT>
+__device__ __forceinline__ float block_sum_f(float v, float* sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  float r = 0.f;
+  if (w == 0) {
+    r = (l < NT / 32) ? sh[l] : 0.f;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+}  // namespace
+
+// ───────────────────────── coarse operator assembly ─────────────────────────
+// One CTA per lattice cell.  Chunks of kCellThreads elements: each thread
+// writes its element's 12x12 tangent (fixed rows and columns zeroed) and the
+// 4x8 trilinear weights to shared memory; then each thread owns up to five of
+// the cell's 24x24 block entries and adds w_a,c1 K_ab w_b,c2 over the chunk,
+// in element order (FP32 products, FP64 accumulation).
+constexpr int kCellThreads = 128;
+constexpr int kCellEntries = 576;  // (8 corners x 3)^2
+constexpr int kCellOwned = (kCellEntries + kCellThreads - 1) / kCellThreads;
+
+template <int MODEL>
+__global__ void __launch_bounds__(kCellThreads) coarse_cell_kernel(const __grid_constant__ CoarseArgs a) {
+  extern __shared__ __align__(16) float s_cell[];
+  float* sK = s_cell;                                // [kCellThreads][144]
+  float* sW = s_cell + kCellThreads * 144;           // [kCellThreads][32]
+  const MeshDev& m = a.m;
+  const CoarseDev& c = a.c;
+  const int cell = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int3 ijk = c.cell_ijk[cell];
+  const int e0 = c.cell_elem_ptr[cell], e1 = c.cell_elem_ptr[cell + 1];
+  double acc[kCellOwned];
+#pragma unroll
+  for (int k = 0; k < kCellOwned; ++k) acc[k] = 0.0;
+  for (int c0 = e0; c0 < e1; c0 += kCellThreads) {
+    const int idx = c0 + tid;
+    float* K = sK + tid * 144;
+    float* W = sW + tid * 32;
+    if (idx < e1) {
+      const int e = __ldg(c.cell_elems + idx);
+      const int4 cn = __ldg(m.conn + e);
+      const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+      float xv[4][3];
+      int fx[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 X = __ldg(m.X32 + nid[k]);
+        xv[k][0] = X.x;
+        xv[k][1] = X.y;
+        xv[k][2] = X.z;
+        fx[k] = (int)m.fixed[nid[k]];
+        float t[3];
+        cell_local(c, ijk, X.x, X.y, X.z, t);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) W[k * 8 + q] = tri_weight(t[0], t[1], t[2], q);
+      }
+      TetGeom<float> g;
+      tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+      const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
+      const float scale = __ldg(m.scale + e);
+      float pay[kPay];
+      {
+        const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
+#pragma unroll
+        for (int k = 0; k < kPay; ++k)
+          pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
+      }
+      float w[4][3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        w[1][j] = g.c[0][j];
+        w[2][j] = g.c[1][j];
+        w[3][j] = g.c[2][j];
+        w[0][j] = -(g.c[0][j] + g.c[1][j] + g.c[2][j]);
+      }
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+#pragma unroll
+        for (int d2 = 0; d2 < 3; ++d2) {
+          const bool col_fixed = (fx[b] >> d2) & 1;
+          float dF[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) dF[k] = 0.f;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) dF[3 * d2 + j] = w[b][j] * g.inv_det;
+          float dP[9];
+          dP_any<MODEL>(mat, scale, pay, dF, dP);
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa)
+#pragma unroll
+            for (int d1 = 0; d1 < 3; ++d1) {
+              const float v = g.s6 * (dP[3 * d1] * w[aa][0] + dP[3 * d1 + 1] * w[aa][1] +
+                                      dP[3 * d1 + 2] * w[aa][2]);
+              const bool row_fixed = (fx[aa] >> d1) & 1;
+              K[(3 * aa + d1) * 12 + 3 * b + d2] = (col_fixed || row_fixed) ? 0.f : v;
+            }
+        }
+      }
+    }
+    __syncthreads();
+    const int nvalid = min(kCellThreads, e1 - c0);
+#pragma unroll
+    for (int k = 0; k < kCellOwned; ++k) {
+      const int q = tid + k * kCellThreads;
+      if (q < kCellEntries) {
+        const int r = q / 24, col = q - 24 * r;
+        const int c1 = r / 3, d1 = r - 3 * c1;
+        const int c2 = col / 3, d2 = col - 3 * c2;
+        for (int el = 0; el < nvalid; ++el) {
+          const float* K = sK + el * 144;
+          const float* W = sW + el * 32;
+          float s = 0.f;
+#pragma unroll
+          for (int aa = 0; aa < 4; ++aa) {
+            float t = 0.f;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) t += K[(3 * aa + d1) * 12 + 3 * b + d2] * W[b * 8 + c2];
+            s += W[aa * 8 + c1] * t;
+          }
+          acc[k] += (double)s;
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < kCellOwned; ++k) {
+    const int q = tid + k * kCellThreads;
+    if (q < kCellEntries) c.blocks[(size_t)cell * kCellEntries + q] = acc[k];
+  }
+}
+
+// Dense Ac (column-major, symmetric) from the cell blocks: entry (I, J) adds
+// the blocks of the cells that hold both coarse nodes, in ascending cell
+// order.  A DOF no free mesh DOF reaches gets a unit diagonal.
+__global__ void coarse_dense_kernel(const __grid_constant__ CoarseDev c) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = c.n_dof;
+  if (q >= (int64_t)n * n) return;
+  const int I = (int)(q % n), J = (int)(q / n);
+  const int nI = I / 3, dI = I - 3 * nI;
+  const int nJ = J / 3, dJ = J - 3 * nJ;
+  double acc = 0.0;
+  for (int k = 0; k < 8; ++k) {
+    const int ent = c.cn_cells[nI * 8 + k];
+    if (ent < 0) break;
+    const int cell = ent >> 3, cI = ent & 7;
+    int cJ = -1;
+#pragma unroll
+    for (int t = 0; t < 8; ++t)
+      if (c.cell_corner[cell * 8 + t] == nJ) cJ = t;
+    if (cJ >= 0) acc += c.blocks[(size_t)cell * kCellEntries + (3 * cI + dI) * 24 + 3 * cJ + dJ];
+  }
+  if (I == J && !(acc > 0.0)) acc = 1.0;
+  c.Ac[q] = acc;
+}
+
+// FP32 symmetric copy of the inverse whose lower triangle potri wrote.
+__global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = c.n_dof;
+  if (q >= (int64_t)n * n) return;
+  const int row = (int)(q / n), col = (int)(q % n);
+  const int lo = max(row, col), hi = min(row, col);
+  // column-major lower triangle: element (lo, hi) at hi * n + lo
+  c.Ainv[q] = (float)c.Ac[(size_t)hi * n + lo];
+}
+
+// ───────────────────────── per-iteration application ─────────────────────────
+
+// cell_r[cell][3 corner + d] = sum over the cell's nodes of w_corner r_d
+__global__ void __launch_bounds__(kCellThreads) coarse_restrict_kernel(
+    const __grid_constant__ CoarseArgs a, const float* __restrict__ r, const CGState* cg) {
+  if (cg && cg->done) return;
+  __shared__ float sh[kCellThreads / 32];
+  const CoarseDev& c = a.c;
+  const int cell = blockIdx.x;
+  const int3 ijk = c.cell_ijk[cell];
+  const int n0 = c.cell_node_ptr[cell], n1 = c.cell_node_ptr[cell + 1];
+  float acc[24];
+#pragma unroll
+  for (int k = 0; k < 24; ++k) acc[k] = 0.f;
+  for (int i = n0 + threadIdx.x; i < n1; i += kCellThreads) {
+    const int node = __ldg(c.cell_nodes + i);
+    const float4 X = __ldg(a.m.X32 + node);
+    const float4 rv = reinterpret_cast<const float4*>(r)[node];
+    float t[3];
+    cell_local(c, ijk, X.x, X.y, X.z, t);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float wq = tri_weight(t[0], t[1], t[2], q);
+      acc[3 * q] += wq * rv.x;
+      acc[3 * q + 1] += wq * rv.y;
+      acc[3 * q + 2] += wq * rv.z;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 24; ++k) {
+    const float v = block_sum_f<kCellThreads>(acc[k], sh);
+    if (threadIdx.x == 0) c.cell_r[cell * 24 + k] = v;
+  }
+}
+
+// y_c = Ainv r_c; every CTA first gathers r_c from the cell partials (fixed
+// order), then one warp per row.
+constexpr int kCoarseMvThreads = 256;
+
+__global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
+    const __grid_constant__ CoarseDev c, const CGState* cg) {
+  if (cg && cg->done) return;
+  extern __shared__ __align__(16) float s_rc[];
+  const int n = c.n_dof;
+  for (int I = threadIdx.x; I < n; I += kCoarseMvThreads) {
+    const int nI = I / 3, dI = I - 3 * nI;
+    float v = 0.f;
+    for (int k = 0; k < 8; ++k) {
+      const int ent = c.cn_cells[nI * 8 + k];
+      if (ent < 0) break;
+      v += c.cell_r[(ent >> 3) * 24 + 3 * (ent & 7) + dI];
+    }
+    s_rc[I] = v;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row = blockIdx.x * (kCoarseMvThreads / 32) + warp;
+  if (row >= n) return;
+  const float* Arow = c.Ainv + (size_t)row * n;
+  float s = 0.f;
+  for (int j = lane; j < n; j += 32) s += __ldg(Arow + j) * s_rc[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) c.yc[row] = s;
+}
+
+// z = D^-1 r + P y_c (zero on fixed DOFs) and r.z.  INIT: p = z, rz set;
+// otherwise beta = rz_new / rz_old (Fletcher-Reeves, exact for a fixed SPD
+// preconditioner) and rz replaced.
+template <bool INIT>
+__global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ CoarseArgs a,
+                                                    const float* __restrict__ r,
+                                                    const float* __restrict__ dinv, float* z,
+                                                    float* p, CGState* cg, Reduce red, int site) {
+  if (cg->done) return;
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const CoarseDev& c = a.c;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  double rz = 0.0;
+  if (i < a.m.n_nodes) {
+    const float4 rv = reinterpret_cast<const float4*>(r)[i];
+    const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
+    const float4 X = __ldg(a.m.X32 + i);
+    const int cell = __ldg(c.node_cell + i);
+    const int3 ijk = c.cell_ijk[cell];
+    float t[3];
+    cell_local(c, ijk, X.x, X.y, X.z, t);
+    float cz[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int cnode = __ldg(c.cell_corner + cell * 8 + q);
+      const float wq = tri_weight(t[0], t[1], t[2], q);
+      cz[0] += wq * c.yc[3 * cnode];
+      cz[1] += wq * c.yc[3 * cnode + 1];
+      cz[2] += wq * c.yc[3 * cnode + 2];
+    }
+    const int fx = (int)a.m.fixed[i];
+    float4 zv;
+    zv.x = (fx & 1) ? 0.f : dv.x * rv.x + cz[0];
+    zv.y = (fx & 2) ? 0.f : dv.y * rv.y + cz[1];
+    zv.z = (fx & 4) ? 0.f : dv.z * rv.z + cz[2];
+    zv.w = 0.f;
+    reinterpret_cast<float4*>(INIT ? p : z)[i] = zv;
+    rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
+  }
+  double v = block_sum<256>(rz, sred);
+  if (publish_partial(red, site, 1, &v, &am_last)) {
+    const double trz = final_sum<256>(red, site, 0, sred);
+    if (threadIdx.x == 0) {
+      if (INIT) {
+        cg->beta = 0.0;
+      } else {
+        cg->beta = trz / cg->rz;
+      }
+      cg->rz = trz;
+      if (!isfinite(trz) || !(trz > 0.0)) {
+        cg->done = 3;
+        cg->status = 3;
+      }
+      red.counters[site] = 0u;
+    }
+  }
+}
+
+// p = z + beta p
+__global__ void __launch_bounds__(256) tl_pupdate_kernel(float* p, const float* __restrict__ z,
+                                                         int n_nodes, const CGState* cg) {
+  if (cg->done) return;
+  const float beta = (float)cg->beta;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= n_nodes) return;
+  float4 pv = reinterpret_cast<float4*>(p)[i];
+  const float4 zv = reinterpret_cast<const float4*>(z)[i];
+  pv.x = zv.x + beta * pv.x;
+  pv.y = zv.y + beta * pv.y;
+  pv.z = zv.z + beta * pv.z;
+  reinterpret_cast<float4*>(p)[i] = pv;
+}
+
+// Flexible PCG step around a nonlinear preconditioner output z (already in
+// `z`): optionally z += P yc (coarse correction), then rz = r.z and z.q.
+// INIT: p = z.  Otherwise Polak-Ribiere beta = (r.z - alpha z.q) / rz_old,
+// using r_new - r_old = -alpha q.
+template <bool INIT, bool COARSE>
+__global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ CoarseArgs a,
+                                                        const float* __restrict__ r,
+                                                        const float* __restrict__ q, float* z, float* p,
+                                                        CGState* cg, Reduce red, int site) {
+  if (cg->done) return;
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  double rz = 0.0, zq = 0.0;
+  if (i < a.m.n_nodes) {
+    const float4 rv = reinterpret_cast<const float4*>(r)[i];
+    float4 zv = reinterpret_cast<const float4*>(z)[i];
+    if (COARSE) {
+      const CoarseDev& c = a.c;
+      const float4 X = __ldg(a.m.X32 + i);
+      const int cell = __ldg(c.node_cell + i);
+      const int3 ijk = c.cell_ijk[cell];
+      float t[3];
+      cell_local(c, ijk, X.x, X.y, X.z, t);
+      float cz[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const int cnode = __ldg(c.cell_corner + cell * 8 + k);
+        const float wk = tri_weight(t[0], t[1], t[2], k);
+        cz[0] += wk * c.yc[3 * cnode];
+        cz[1] += wk * c.yc[3 * cnode + 1];
+        cz[2] += wk * c.yc[3 * cnode + 2];
+      }
+      const int fx = (int)a.m.fixed[i];
+      zv.x = (fx & 1) ? 0.f : zv.x + cz[0];
+      zv.y = (fx & 2) ? 0.f : zv.y + cz[1];
+      zv.z = (fx & 4) ? 0.f : zv.z + cz[2];
+      zv.w = 0.f;
+      reinterpret_cast<float4*>(z)[i] = zv;
+    }
+    if (INIT) reinterpret_cast<float4*>(p)[i] = zv;
+    rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
+    if (!INIT) {
+      const float4 qv = reinterpret_cast<const float4*>(q)[i];
+      zq = (double)zv.x * qv.x + (double)zv.y * qv.y + (double)zv.z * qv.z;
+    }
+  }
+  double v[2];
+  v[0] = block_sum<256>(rz, sred);
+  v[1] = block_sum<256>(zq, sred);
+  if (publish_partial(red, site, 2, v, &am_last)) {
+    const double trz = final_sum<256>(red, site, 0, sred);
+    const double tzq = final_sum<256>(red, site, 1, sred);
+    if (threadIdx.x == 0) {
+      cg->beta = INIT ? 0.0 : (trz - cg->alpha * tzq) / cg->rz;
+      cg->rz = trz;
+      if (!isfinite(trz) || !(trz > 0.0) || !isfinite(cg->beta)) {
+        cg->done = 3;
+        cg->status = 3;
+      }
+      red.counters[site] = 0u;
+    }
+  }
+}
+
+// ───────────────────────── launchers ─────────────────────────
+
+static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+size_t coarse_cell_smem() { return sizeof(float) * kCellThreads * (144 + 32); }
+
+void prepare_coarse_kernels(int model, int n_dof) {
+  const int smem = (int)coarse_cell_smem();
+  switch (model) {
+    case M_LE: cudaFuncSetAttribute(coarse_cell_kernel<M_LE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    case M_NH: cudaFuncSetAttribute(coarse_cell_kernel<M_NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    case M_MR: cudaFuncSetAttribute(coarse_cell_kernel<M_MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    case M_J2: cudaFuncSetAttribute(coarse_cell_kernel<M_J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    case M_TI: cudaFuncSetAttribute(coarse_cell_kernel<M_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    case M_FMR: cudaFuncSetAttribute(coarse_cell_kernel<M_FMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    default: cudaFuncSetAttribute(coarse_cell_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+  }
+  cudaFuncSetAttribute(coarse_mv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(float) * (size_t)n_dof));
+}
+
+void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s) {
+  const size_t smem = coarse_cell_smem();
+  const int g = a.c.n_cells;
+  switch (model) {
+    case M_LE: coarse_cell_kernel<M_LE><<<g, kCellThreads, smem, s>>>(a); break;
+    case M_NH: coarse_cell_kernel<M_NH><<<g, kCellThreads, smem, s>>>(a); break;
+    case M_MR: coarse_cell_kernel<M_MR><<<g, kCellThreads, smem, s>>>(a); break;
+    case M_J2: coarse_cell_kernel<M_J2><<<g, kCellThreads, smem, s>>>(a); break;
+    case M_TI: coarse_cell_kernel<M_TI><<<g, kCellThreads, smem, s>>>(a); break;
+    case M_FMR: coarse_cell_kernel<M_FMR><<<g, kCellThreads, smem, s>>>(a); break;
+    default: coarse_cell_kernel<-1><<<g, kCellThreads, smem, s>>>(a); break;
+  }
+  const int64_t nn = (int64_t)a.c.n_dof * a.c.n_dof;
+  coarse_dense_kernel<<<nblk(nn, 256), 256, 0, s>>>(a.c);
+}
+
+void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s) {
+  const int64_t nn = (int64_t)c.n_dof * c.n_dof;
+  coarse_sym_kernel<<<nblk(nn, 256), 256, 0, s>>>(c);
+}
+
+void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
+  coarse_restrict_kernel<<<a.c.n_cells, kCellThreads, 0, s>>>(a, r, cg);
+  const int rows_per_cta = kCoarseMvThreads / 32;
+  coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(
+      a.c, cg);
+}
+
+void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* dinv, float* z, float* p,
+                  CGState* cg, Reduce red, int site, cudaStream_t s) {
+  const int g = nblk(a.m.n_nodes, 256);
+  if (init)
+    tl_rz_kernel<true><<<g, 256, 0, s>>>(a, r, dinv, z, p, cg, red, site);
+  else
+    tl_rz_kernel<false><<<g, 256, 0, s>>>(a, r, dinv, z, p, cg, red, site);
+}
+
+void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q, float* z,
+                      float* p, CGState* cg, Reduce red, int site, cudaStream_t s) {
+  const int g = nblk(a.m.n_nodes, 256);
+  if (init) {
+    if (coarse)
+      fpcg_dots_kernel<true, true><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+    else
+      fpcg_dots_kernel<true, false><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+  } else {
+    if (coarse)
+      fpcg_dots_kernel<false, true><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+    else
+      fpcg_dots_kernel<false, false><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+  }
+}
+
+void launch_tl_pupdate(float* p, const float* z, int n_nodes, const CGState* cg, cudaStream_t s) {
+  tl_pupdate_kernel<<<nblk(n_nodes, 256), 256, 0, s>>>(p, z, n_nodes, cg);
+}
+
+}  // namespace femb200

@@ -5,6 +5,7 @@
 // element kernels use.  Callers keep their own numbering: every per-call array
 // is permuted on entry and exit.
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -24,7 +25,10 @@ namespace {
 
 thread_local std::string g_create_error;
 
-enum { SITE_RES = 0, SITE_MV = 1, SITE_CGI = 2, SITE_CGU = 3, SITE_AUX = 4, N_SITES = 5 };
+enum { SITE_RES = 0, SITE_MV = 1, SITE_CGI = 2, SITE_CGU = 3, SITE_AUX = 4, SITE_RZ = 5, N_SITES = 6 };
+// captured CG iteration graphs: Jacobi / identity preconditioner, two-level,
+// learned (flexible PCG)
+enum { GRAPH_JACOBI = 0, GRAPH_TWO_LEVEL = 1, GRAPH_LEARNED = 2, N_GRAPHS = 3 };
 constexpr int kCGBatch = 32;  // CG iterations per captured graph launch
 
 struct FemCtx {
@@ -49,6 +53,8 @@ struct FemCtx {
   int* blk_elems = nullptr;
   int* node_row = nullptr;
   uint32_t* node_slots = nullptr;
+  int4* spos = nullptr;
+  int max_slots = 0;
   uint8_t* fixed = nullptr;
   double* fixed_vals = nullptr;
   double* fext = nullptr;
@@ -61,7 +67,9 @@ struct FemCtx {
   double* epe_c = nullptr;
   double* ep_t = nullptr;
   double* epe_t = nullptr;
+  // FP32 node vectors, one float4 per node
   float *r = nullptr, *x = nullptr, *p = nullptr, *y = nullptr, *dinv = nullptr, *tmpf = nullptr;
+  float4* stage = nullptr;  // [4 Ne] two-phase matvec slot vectors
   int* d_perm_node = nullptr;
   int* d_perm_elem = nullptr;
   DevMat<double>* matD = nullptr;
@@ -83,9 +91,48 @@ struct FemCtx {
   bool has_j2 = false;
   bool materials_set = false;
   bool tangent_valid = false;
-  cudaGraphExec_t cg_graph = nullptr;
-  int cg_graph_model = -2;
-  int cg_graph_precond = -1;
+  cudaGraphExec_t cg_graph[N_GRAPHS] = {nullptr, nullptr, nullptr};
+  int cg_graph_model[N_GRAPHS] = {-2, -2, -2};
+  int cg_graph_variant[N_GRAPHS] = {-1, -1, -1};
+  int cg_graph_flags[N_GRAPHS] = {-1, -1, -1};
+
+  // learned preconditioner: node graph, features, weights, activations
+  MpnnDev mdev{};
+  bool mpnn_built = false;
+  bool mpnn_feat_valid = false;
+  bool mpnn_has_weights = false;
+  bool learned_coarse = true;   // add the two-level coarse correction to M(r)
+  std::vector<void*> mpnn_bufs;
+  float* mpnn_w = nullptr;
+  __nv_bfloat16 *We_p = nullptr, *Wl_p = nullptr, *WlT_p = nullptr;
+  float* cfeat = nullptr;
+  std::vector<double> elem_modulus;  // internal element order
+  int64_t n_fallbacks = 0;
+  int* h_err = nullptr;
+
+  // two-level preconditioner: coarse lattice tables (built on first use),
+  // dense coarse operator and its inverse, cuSOLVER handle and workspace
+  CoarseDev cdev{};
+  bool coarse_built = false;
+  bool coarse_valid = false;   // Ainv matches the current tangent policy
+  int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
+  int coarse_reuse = 1;        // PCG solves one assembly serves
+  int coarse_uses = 0;
+  double coarse_H = 0.0;
+  int64_t n_coarse_assemblies = 0;
+  double coarse_ms_last = 0.0;
+  std::vector<void*> coarse_bufs;
+  cusolverDnHandle_t solver = nullptr;
+  double* sol_work = nullptr;
+  int sol_lwork = 0;
+  int* sol_info = nullptr;
+  int* h_info = nullptr;
+  // matvec variant: forced by fem_set_option (>= 0) or chosen by timing both
+  int mv_forced = -1;
+  int mv_variant = MV_FUSED;
+  bool mv_tuned = false;
+  int mv_tuned_model = -2;
+  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0};
 
   MeshDev mesh() const {
     MeshDev m;
@@ -104,6 +151,8 @@ struct FemCtx {
     m.node_row = node_row;
     m.node_slots = node_slots;
     m.fixed = fixed;
+    m.max_slots = max_slots;
+    m.spos = spos;
     return m;
   }
   Reduce red() const {
@@ -182,7 +231,19 @@ void free_ctx(FemCtx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->cg_graph) cudaGraphExecDestroy(c->cg_graph);
+  for (int k = 0; k < N_GRAPHS; ++k)
+    if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+  for (void* p : c->coarse_bufs)
+    if (p) cudaFree(p);
+  for (void* p : c->mpnn_bufs)
+    if (p) cudaFree(p);
+  if (c->h_err) cudaFreeHost(c->h_err);
+  if (c->sol_work) cudaFree(c->sol_work);
+  if (c->sol_info) cudaFree(c->sol_info);
+  if (c->h_info) cudaFreeHost(c->h_info);
+  if (c->solver) cusolverDnDestroy(c->solver);
+  if (c->stage) cudaFree(c->stage);
+  if (c->spos) cudaFree(c->spos);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
                   c->u, c->u_base, c->R, c->tmpd, c->payload, c->ep_c, c->epe_c, c->ep_t,
@@ -277,7 +338,9 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   std::vector<uint32_t> node_slots(arow[Nn]);
   blk_elems.reserve((size_t)Ne * 3 / 2);
   std::vector<int> foreign;
-  std::vector<uint32_t> ents;
+  std::vector<std::pair<uint32_t, int>> ents;  // (li << 2 | slot, element)
+  std::vector<int4> spos(Ne);
+  int max_slots = 0;
   for (int b = 0; b < nblkn; ++b) {
     const int n0 = b * nb, n1 = std::min(Nn, n0 + nb);
     const int h0 = hs[b], h1 = hs[b + 1];
@@ -303,13 +366,25 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
         } else {
           li = (h1 - h0) + (int)(std::lower_bound(foreign.begin(), foreign.end(), e) - foreign.begin());
         }
-        ents.push_back(((uint32_t)li << 2) | (uint32_t)s);
+        ents.push_back({((uint32_t)li << 2) | (uint32_t)s, e});
       }
       std::sort(ents.begin(), ents.end());
       node_row[n + 1] = node_row[n] + (int)ents.size();
-      std::copy(ents.begin(), ents.end(), node_slots.begin() + node_row[n]);
+      for (size_t k = 0; k < ents.size(); ++k) {
+        const int pos = node_row[n] + (int)k;
+        node_slots[pos] = ents[k].first;
+        (&spos[ents[k].second].x)[ents[k].first & 3] = pos;
+      }
     }
+    max_slots = std::max(max_slots, node_row[n1] - node_row[n0]);
   }
+  c->max_slots = max_slots;
+  // the fused residual kernel stages 12 NB doubles plus the block's slot list
+  const size_t smem_need = sizeof(double) * 12 * (size_t)nb + sizeof(uint32_t) * (size_t)max_slots;
+  if (smem_need > 200u * 1024u)
+    return set_err(nullptr, FEM_ERR_INVALID,
+                   "node block of %d nodes needs %zu bytes of shared memory (max 204800): use a smaller block",
+                   nb, smem_need);
   blk_ptr[nblkn] = (int)blk_elems.size();
   c->blk_entries = (int64_t)blk_elems.size();
 
@@ -330,6 +405,7 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   if ((st = dalloc(c, &c->blk_elems, blk_elems.size()))) return st;
   if ((st = dalloc(c, &c->node_row, node_row.size()))) return st;
   if ((st = dalloc(c, &c->node_slots, node_slots.size()))) return st;
+  if ((st = dalloc(c, &c->spos, (size_t)Ne))) return st;
   if ((st = dalloc(c, &c->d_perm_node, (size_t)Nn))) return st;
   if ((st = dalloc(c, &c->d_perm_elem, (size_t)Ne))) return st;
   CK(cudaMemcpyAsync(c->X64, X64.data(), X64.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -340,6 +416,7 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   CK(cudaMemcpyAsync(c->blk_elems, blk_elems.data(), blk_elems.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->node_row, node_row.data(), node_row.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->node_slots, node_slots.data(), node_slots.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->spos, spos.data(), spos.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_perm_node, c->perm_node.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_perm_elem, c->perm_elem.data(), Ne * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   // the host vectors go out of scope: finish the copies first
@@ -348,7 +425,7 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
 }
 
 int alloc_state(FemCtx* c) {
-  const size_t nd = (size_t)c->ndof_pad, Ne = (size_t)c->Ne;
+  const size_t nd = (size_t)c->ndof_pad, Ne = (size_t)c->Ne, nf = 4 * (size_t)c->Nn;
   int st;
   if ((st = dalloc(c, &c->mat_id, Ne))) return st;
   if ((st = dalloc(c, &c->scale, Ne))) return st;
@@ -364,16 +441,17 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->epe_c, Ne))) return st;
   if ((st = dalloc(c, &c->ep_t, Ne * 6))) return st;
   if ((st = dalloc(c, &c->epe_t, Ne))) return st;
-  if ((st = dalloc(c, &c->r, nd))) return st;
-  if ((st = dalloc(c, &c->x, nd))) return st;
-  if ((st = dalloc(c, &c->p, nd))) return st;
-  if ((st = dalloc(c, &c->y, nd))) return st;
-  if ((st = dalloc(c, &c->dinv, nd))) return st;
-  if ((st = dalloc(c, &c->tmpf, nd))) return st;
+  if ((st = dalloc(c, &c->r, nf))) return st;
+  if ((st = dalloc(c, &c->x, nf))) return st;
+  if ((st = dalloc(c, &c->p, nf))) return st;
+  if ((st = dalloc(c, &c->y, nf))) return st;
+  if ((st = dalloc(c, &c->dinv, nf))) return st;
+  if ((st = dalloc(c, &c->tmpf, nf))) return st;
+  if ((st = dalloc(c, &c->stage, 4 * Ne))) return st;
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
-  // every reducing kernel's grid must fit: node blocks, float4 vector blocks, node-parallel blocks
-  c->max_blocks = std::max({c->n_blocks, (c->ndof_pad / 4 + 255) / 256, (c->Nn + 255) / 256}) + 1;
+  // every reducing kernel's grid must fit: node blocks and node-parallel blocks
+  c->max_blocks = std::max(c->n_blocks, (c->Nn + 255) / 256) + 1;
   if ((st = dalloc(c, &c->partials, (size_t)N_SITES * 2 * c->max_blocks))) return st;
   if ((st = dalloc(c, &c->counters, (size_t)N_SITES))) return st;
   if ((st = dalloc(c, &c->scalars, (size_t)8))) return st;
@@ -410,6 +488,16 @@ DevMat<T> to_dev(const FemMaterial& s) {
 }
 
 // ───────────────────────── kernels wrappers ─────────────────────────
+
+// Matvec arguments with the mesh tables and the context's variant filled in.
+MvArgs make_mv(const FemCtx* c) {
+  MvArgs mv;
+  std::memset(&mv, 0, sizeof(mv));
+  mv.m = c->mesh();
+  mv.variant = c->mv_variant;
+  mv.stage = c->stage;
+  return mv;
+}
 
 int eval_residual(FemCtx* c, double* fneg_out_int, double* rnorm2) {
   ResArgs a;
@@ -453,9 +541,17 @@ int compute_dinv(FemCtx* c, int precond) {
   return FEM_OK;
 }
 
-void enqueue_cg_iter(FemCtx* c) {
-  MvArgs mv;
-  mv.m = c->mesh();
+CoarseArgs coarse_args(const FemCtx* c) {
+  CoarseArgs a;
+  a.m = c->mesh();
+  a.c = c->cdev;
+  a.matF = c->matF;
+  a.payload = c->payload;
+  return a;
+}
+
+void enqueue_cg_iter(FemCtx* c, int kind) {
+  MvArgs mv = make_mv(c);
   mv.matF = c->matF;
   mv.payload = c->payload;
   mv.x = c->p;
@@ -464,27 +560,456 @@ void enqueue_cg_iter(FemCtx* c) {
   mv.red = c->red();
   mv.red_site = SITE_MV;
   mv.mask_input = 1;
-  const int ndof4 = c->ndof_pad / 4;
   launch_matvec(mv, c->model_kind, c->stream);
-  launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, ndof4, c->cg, c->red(), SITE_CGU, c->stream);
-  launch_cg_pupdate(c->p, c->r, c->dinv, ndof4, c->cg, c->stream);
+  if (kind == GRAPH_LEARNED) {
+    const CoarseArgs ca = coarse_args(c);
+    launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream, 0);
+    launch_mpnn_forward(c->mdev, c->r, c->dinv, c->tmpf, c->cg, c->red(), SITE_RZ, c->stream);
+    if (c->learned_coarse) launch_coarse_apply(ca, c->r, c->cg, c->stream);
+    launch_fpcg_dots(ca, false, c->learned_coarse, c->r, c->y, c->tmpf, c->p, c->cg, c->red(), SITE_RZ,
+                     c->stream);
+    launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
+    return;
+  }
+  if (kind == GRAPH_TWO_LEVEL) {
+    const CoarseArgs ca = coarse_args(c);
+    launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream, 0);
+    launch_coarse_apply(ca, c->r, c->cg, c->stream);
+    launch_tl_rz(ca, false, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
+    launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
+    return;
+  }
+  launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream);
+  launch_cg_pupdate(c->p, c->r, c->dinv, c->Nn, c->cg, c->stream);
 }
 
-int ensure_cg_graph(FemCtx* c) {
-  if (c->cg_graph && c->cg_graph_model == c->model_kind) return FEM_OK;
-  if (c->cg_graph) {
-    cudaGraphExecDestroy(c->cg_graph);
-    c->cg_graph = nullptr;
+// A CG state that never finishes, so the fused CG kernels do their full work
+// when timed outside a solve.
+CGState endless_cg() {
+  CGState hs;
+  std::memset(&hs, 0, sizeof(hs));
+  hs.rz = 1.0;
+  hs.rr = 1.0;
+  hs.rr0 = 1.0;
+  hs.tol2 = 0.0;
+  hs.alpha = 1e-30;
+  hs.beta = 0.0;
+  hs.max_iter = 1 << 30;
+  return hs;
+}
+
+// Picks the matvec variant for the current material tables: the forced one
+// when fem_set_option set it, else the faster of the two on this mesh, timed
+// with CUDA events as they run inside CG (3 warm-up + 10 timed launches each,
+// p = 1 on free DOFs).  The CG state is reset by cg_init afterwards.
+int choose_matvec_variant(FemCtx* c) {
+  if (c->mv_forced >= 0) {
+    c->mv_variant = c->mv_forced;
+    return FEM_OK;
   }
+  if (c->mv_tuned && c->mv_tuned_model == c->model_kind) return FEM_OK;
+  const CGState hs = endless_cg();
+  CK(cudaMemcpyAsync(c->cg, &hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
+  launch_dinv_identity(c->p, c->fixed, c->Nn, c->stream);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  for (int v = 0; v < MV_N_VARIANTS; ++v) {
+    MvArgs mv = make_mv(c);
+    mv.variant = v;
+    mv.matF = c->matF;
+    mv.payload = c->payload;
+    mv.x = c->p;
+    mv.y = c->y;
+    mv.cg = c->cg;
+    mv.red = c->red();
+    mv.red_site = SITE_MV;
+    mv.mask_input = 1;
+    for (int w = 0; w < 3; ++w) launch_matvec(mv, c->model_kind, c->stream);
+    CK(cudaEventRecord(e0, c->stream));
+    constexpr int kReps = 10;
+    for (int r = 0; r < kReps; ++r) launch_matvec(mv, c->model_kind, c->stream);
+    CK(cudaEventRecord(e1, c->stream));
+    CKL();
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    c->mv_ns[v] = 1e6 * ms / kReps;
+    c->n_launches += (v == MV_TWO_PHASE ? 2 : 1) * 13;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->mv_variant = c->mv_ns[MV_TWO_PHASE] < c->mv_ns[MV_FUSED] ? MV_TWO_PHASE : MV_FUSED;
+  c->mv_tuned = true;
+  c->mv_tuned_model = c->model_kind;
+  return FEM_OK;
+}
+
+int ensure_cg_graph(FemCtx* c, int kind) {
+  int st;
+  if ((st = choose_matvec_variant(c))) return st;
+  const int flags = kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0;
+  if (c->cg_graph[kind] && c->cg_graph_model[kind] == c->model_kind &&
+      c->cg_graph_variant[kind] == c->mv_variant && c->cg_graph_flags[kind] == flags)
+    return FEM_OK;
+  if (c->cg_graph[kind]) {
+    cudaGraphExecDestroy(c->cg_graph[kind]);
+    c->cg_graph[kind] = nullptr;
+  }
+  prepare_kernels(c->mesh(), c->model_kind);
+  if (kind == GRAPH_TWO_LEVEL || (kind == GRAPH_LEARNED && c->learned_coarse))
+    prepare_coarse_kernels(c->model_kind, c->cdev.n_dof);
+  if (kind == GRAPH_LEARNED) prepare_mpnn_kernels();
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < kCGBatch; ++i) enqueue_cg_iter(c);
+  for (int i = 0; i < kCGBatch; ++i) enqueue_cg_iter(c, kind);
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&c->cg_graph, g, 0);
+  e = cudaGraphInstantiate(&c->cg_graph[kind], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-  c->cg_graph_model = c->model_kind;
+  c->cg_graph_model[kind] = c->model_kind;
+  c->cg_graph_variant[kind] = c->mv_variant;
+  c->cg_graph_flags[kind] = flags;
+  return FEM_OK;
+}
+
+template <typename T>
+int coarse_upload(FemCtx* c, const T** dst, const std::vector<T>& v) {
+  T* d = nullptr;
+  int st;
+  if ((st = dalloc(c, &d, v.size()))) return st;
+  c->coarse_bufs.push_back(d);
+  if (!v.empty()) CK(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  *dst = d;
+  return FEM_OK;
+}
+
+template <typename T>
+int coarse_alloc(FemCtx* c, T** dst, size_t n) {
+  int st;
+  if ((st = dalloc(c, dst, n))) return st;
+  c->coarse_bufs.push_back(*dst);
+  return FEM_OK;
+}
+
+// Builds the coarse lattice: cell edge H = coarse_cell_voxels x the mesh
+// length (cube root of 5 x the mean element volume: the voxel edge on
+// 5-tet voxel meshes), grown by 25 % steps until at most kMaxCoarseNodes
+// coarse nodes remain.  Elements go to the cell of their centroid; a node to
+// the cell of its lowest-numbered element.
+constexpr int kMaxCoarseNodes = 4096;
+
+int build_coarse(FemCtx* c) {
+  const int Nn = c->Nn, Ne = c->Ne;
+  std::vector<double> X(3 * (size_t)Nn);
+  std::vector<int4> conn(Ne);
+  CK(cudaMemcpyAsync(X.data(), c->X64, X.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(conn.data(), c->conn, conn.size() * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = hi[d] = X[d];
+    for (int i = 0; i < Nn; ++i) {
+      lo[d] = std::min(lo[d], X[3 * i + d]);
+      hi[d] = std::max(hi[d], X[3 * i + d]);
+    }
+  }
+  double vsum = 0.0;
+  std::vector<double> cen(3 * (size_t)Ne);
+  for (int e = 0; e < Ne; ++e) {
+    const int* cn = &conn[e].x;
+    double a[3], b[3], cc[3];
+    for (int d = 0; d < 3; ++d) {
+      a[d] = X[3 * cn[1] + d] - X[3 * cn[0] + d];
+      b[d] = X[3 * cn[2] + d] - X[3 * cn[0] + d];
+      cc[d] = X[3 * cn[3] + d] - X[3 * cn[0] + d];
+      cen[3 * e + d] = 0.25 * (X[3 * cn[0] + d] + X[3 * cn[1] + d] + X[3 * cn[2] + d] + X[3 * cn[3] + d]);
+    }
+    const double det = a[0] * (b[1] * cc[2] - b[2] * cc[1]) - a[1] * (b[0] * cc[2] - b[2] * cc[0]) +
+                       a[2] * (b[0] * cc[1] - b[1] * cc[0]);
+    vsum += std::fabs(det) / 6.0;
+  }
+  const double hmesh = std::cbrt(5.0 * vsum / std::max(Ne, 1));
+  double H = c->coarse_cell_voxels * hmesh;
+  std::vector<int> ecell(Ne), cell_of_lin, act_lin, cn_of_lat;
+  int g[3];
+  int n_cells = 0, n_cn = 0;
+  for (int attempt = 0; attempt < 64; ++attempt) {
+    for (int d = 0; d < 3; ++d) g[d] = std::max(1, (int)std::ceil((hi[d] - lo[d]) / H - 1e-9));
+    const int64_t ncell_lat = (int64_t)g[0] * g[1] * g[2];
+    if (ncell_lat > (1 << 26)) {
+      H *= 1.25;
+      continue;
+    }
+    cell_of_lin.assign(ncell_lat, -1);
+    for (int e = 0; e < Ne; ++e) {
+      int ijk[3];
+      for (int d = 0; d < 3; ++d)
+        ijk[d] = std::min(g[d] - 1, std::max(0, (int)std::floor((cen[3 * e + d] - lo[d]) / H)));
+      const int lin = (ijk[0] * g[1] + ijk[1]) * g[2] + ijk[2];
+      ecell[e] = lin;
+      cell_of_lin[lin] = 0;
+    }
+    act_lin.clear();
+    for (int64_t l = 0; l < ncell_lat; ++l)
+      if (cell_of_lin[l] == 0) {
+        cell_of_lin[l] = (int)act_lin.size();
+        act_lin.push_back((int)l);
+      }
+    n_cells = (int)act_lin.size();
+    // coarse nodes: corners of active cells on the (g+1)^3 lattice
+    const int64_t nlat = (int64_t)(g[0] + 1) * (g[1] + 1) * (g[2] + 1);
+    cn_of_lat.assign(nlat, -1);
+    for (int cl = 0; cl < n_cells; ++cl) {
+      const int l = act_lin[cl];
+      const int i = l / (g[1] * g[2]), j = (l / g[2]) % g[1], k = l % g[2];
+      for (int q = 0; q < 8; ++q) {
+        const int64_t ln = ((int64_t)(i + (q >> 2 & 1)) * (g[1] + 1) + (j + (q >> 1 & 1))) * (g[2] + 1) +
+                           (k + (q & 1));
+        cn_of_lat[ln] = 0;
+      }
+    }
+    n_cn = 0;
+    for (int64_t l = 0; l < nlat; ++l)
+      if (cn_of_lat[l] == 0) cn_of_lat[l] = n_cn++;
+    if (n_cn <= kMaxCoarseNodes) break;
+    H *= 1.25;
+  }
+  if (n_cn > kMaxCoarseNodes)
+    return set_err(c, FEM_ERR_INVALID, "coarse lattice: could not reach %d coarse nodes", kMaxCoarseNodes);
+  // tables
+  std::vector<int3> cell_ijk(n_cells);
+  std::vector<int> cell_corner(8 * (size_t)n_cells);
+  for (int cl = 0; cl < n_cells; ++cl) {
+    const int l = act_lin[cl];
+    const int i = l / (g[1] * g[2]), j = (l / g[2]) % g[1], k = l % g[2];
+    cell_ijk[cl] = make_int3(i, j, k);
+    for (int q = 0; q < 8; ++q) {
+      const int64_t ln = ((int64_t)(i + (q >> 2 & 1)) * (g[1] + 1) + (j + (q >> 1 & 1))) * (g[2] + 1) +
+                         (k + (q & 1));
+      cell_corner[8 * cl + q] = cn_of_lat[ln];
+    }
+  }
+  std::vector<int> cn_cells(8 * (size_t)n_cn, -1), cn_fill(n_cn, 0);
+  for (int cl = 0; cl < n_cells; ++cl)
+    for (int q = 0; q < 8; ++q) {
+      const int cnode = cell_corner[8 * cl + q];
+      cn_cells[8 * cnode + cn_fill[cnode]++] = cl * 8 + q;
+    }
+  std::vector<int> node_cell(Nn, -1);
+  std::vector<int> cell_elem_ptr(n_cells + 1, 0), cell_elems(Ne);
+  for (int e = 0; e < Ne; ++e) cell_elem_ptr[cell_of_lin[ecell[e]] + 1]++;
+  for (int cl = 0; cl < n_cells; ++cl) cell_elem_ptr[cl + 1] += cell_elem_ptr[cl];
+  {
+    std::vector<int> fill(cell_elem_ptr.begin(), cell_elem_ptr.end() - 1);
+    for (int e = 0; e < Ne; ++e) {
+      const int cl = cell_of_lin[ecell[e]];
+      cell_elems[fill[cl]++] = e;
+      const int* cn = &conn[e].x;
+      for (int k = 0; k < 4; ++k)
+        if (node_cell[cn[k]] < 0) node_cell[cn[k]] = cl;
+    }
+  }
+  for (int i = 0; i < Nn; ++i)
+    if (node_cell[i] < 0) node_cell[i] = 0;  // node of no element: its DOFs carry no stiffness
+  std::vector<int> cell_node_ptr(n_cells + 1, 0), cell_nodes(Nn);
+  for (int i = 0; i < Nn; ++i) cell_node_ptr[node_cell[i] + 1]++;
+  for (int cl = 0; cl < n_cells; ++cl) cell_node_ptr[cl + 1] += cell_node_ptr[cl];
+  {
+    std::vector<int> fill(cell_node_ptr.begin(), cell_node_ptr.end() - 1);
+    for (int i = 0; i < Nn; ++i) cell_nodes[fill[node_cell[i]]++] = i;
+  }
+  CoarseDev& cd = c->cdev;
+  cd.n_cells = n_cells;
+  cd.n_cn = n_cn;
+  cd.n_dof = 3 * n_cn;
+  cd.inv_H = (float)(1.0 / H);
+  cd.lo = make_float3((float)lo[0], (float)lo[1], (float)lo[2]);
+  int st;
+  if ((st = coarse_upload(c, &cd.cell_ijk, cell_ijk))) return st;
+  if ((st = coarse_upload(c, &cd.cell_corner, cell_corner))) return st;
+  if ((st = coarse_upload(c, &cd.cell_node_ptr, cell_node_ptr))) return st;
+  if ((st = coarse_upload(c, &cd.cell_nodes, cell_nodes))) return st;
+  if ((st = coarse_upload(c, &cd.cell_elem_ptr, cell_elem_ptr))) return st;
+  if ((st = coarse_upload(c, &cd.cell_elems, cell_elems))) return st;
+  if ((st = coarse_upload(c, &cd.node_cell, node_cell))) return st;
+  if ((st = coarse_upload(c, &cd.cn_cells, cn_cells))) return st;
+  const size_t nd = (size_t)cd.n_dof;
+  if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * 576))) return st;
+  if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
+  if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
+  if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * 24))) return st;
+  if ((st = coarse_alloc(c, &cd.yc, nd))) return st;
+  if (!c->solver) {
+    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cusolverDnCreate failed");
+  }
+  cusolverDnSetStream(c->solver, c->stream);
+  int lw1 = 0, lw2 = 0;
+  if (cusolverDnDpotrf_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, cd.n_dof, cd.Ac, cd.n_dof, &lw1) !=
+          CUSOLVER_STATUS_SUCCESS ||
+      cusolverDnDpotri_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, cd.n_dof, cd.Ac, cd.n_dof, &lw2) !=
+          CUSOLVER_STATUS_SUCCESS)
+    return set_err(c, FEM_ERR_CUDA, "cuSOLVER workspace query failed");
+  if (c->sol_work) cudaFree(c->sol_work);
+  c->sol_work = nullptr;
+  c->sol_lwork = std::max(lw1, lw2);
+  CK(cudaMalloc(reinterpret_cast<void**>(&c->sol_work), sizeof(double) * (size_t)std::max(c->sol_lwork, 1)));
+  if (!c->sol_info) CK(cudaMalloc(reinterpret_cast<void**>(&c->sol_info), sizeof(int)));
+  if (!c->h_info) CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_info), sizeof(int)));
+  CK(cudaStreamSynchronize(c->stream));
+  c->coarse_H = H;
+  c->coarse_built = true;
+  c->coarse_valid = false;
+  return FEM_OK;
+}
+
+// Assembles Ac = P^T K_T P at the current tangent and inverts it (FP64
+// Cholesky + inverse, then an FP32 copy), unless the reuse policy keeps the
+// previous one.
+int ensure_coarse(FemCtx* c) {
+  int st;
+  if (!c->coarse_built && (st = build_coarse(c))) return st;
+  if (c->coarse_valid && c->coarse_uses < c->coarse_reuse) {
+    ++c->coarse_uses;
+    return FEM_OK;
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, c->stream));
+  prepare_coarse_kernels(c->model_kind, c->cdev.n_dof);
+  const CoarseArgs ca = coarse_args(c);
+  launch_coarse_assemble(ca, c->model_kind, c->stream);
+  c->n_launches += 2;
+  CKL();
+  const int n = c->cdev.n_dof;
+  if (cusolverDnDpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
+                       c->sol_info) != CUSOLVER_STATUS_SUCCESS)
+    return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotrf failed to launch");
+  CK(cudaMemcpyAsync(c->h_info, c->sol_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (*c->h_info != 0)
+    return set_err(c, FEM_ERR_NAN, "coarse operator is not positive definite (potrf info %d)", *c->h_info);
+  if (cusolverDnDpotri(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
+                       c->sol_info) != CUSOLVER_STATUS_SUCCESS)
+    return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotri failed to launch");
+  launch_coarse_symmetrize(c->cdev, c->stream);
+  ++c->n_launches;
+  CKL();
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->coarse_ms_last = ms;
+  ++c->n_coarse_assemblies;
+  c->coarse_valid = true;
+  c->coarse_uses = 1;
+  return FEM_OK;
+}
+
+template <typename T>
+int mpnn_alloc(FemCtx* c, T** dst, size_t n) {
+  int st;
+  if ((st = dalloc(c, dst, n))) return st;
+  c->mpnn_bufs.push_back(*dst);
+  return FEM_OK;
+}
+
+// Node graph of the learned preconditioner (nodes sharing an element, ids
+// ascending), activations and weight buffers; the log-modulus node feature is
+// refreshed whenever the material tables change.
+int ensure_mpnn(FemCtx* c) {
+  const int Nn = c->Nn, Ne = c->Ne;
+  int st;
+  if (!c->mpnn_built) {
+    std::vector<int4> conn(Ne);
+    CK(cudaMemcpyAsync(conn.data(), c->conn, conn.size() * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<uint64_t> pairs;
+    pairs.reserve((size_t)Ne * 12);
+    for (int e = 0; e < Ne; ++e) {
+      const int* cn = &conn[e].x;
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b)
+          if (a != b) pairs.push_back(((uint64_t)(uint32_t)cn[a] << 32) | (uint32_t)cn[b]);
+    }
+    std::sort(pairs.begin(), pairs.end());
+    pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+    std::vector<int> ptr(Nn + 1, 0), idx(pairs.size());
+    for (size_t k = 0; k < pairs.size(); ++k) {
+      ptr[(pairs[k] >> 32) + 1]++;
+      idx[k] = (int)(pairs[k] & 0xffffffffu);
+    }
+    for (int i = 0; i < Nn; ++i) ptr[i + 1] += ptr[i];
+    std::vector<float> dinv(Nn);
+    for (int i = 0; i < Nn; ++i) dinv[i] = ptr[i + 1] > ptr[i] ? 1.0f / (float)(ptr[i + 1] - ptr[i]) : 0.f;
+    MpnnDev& m = c->mdev;
+    int *d_ptr, *d_idx;
+    float* d_deg;
+    if ((st = mpnn_alloc(c, &d_ptr, ptr.size()))) return st;
+    if ((st = mpnn_alloc(c, &d_idx, idx.size()))) return st;
+    if ((st = mpnn_alloc(c, &d_deg, dinv.size()))) return st;
+    if ((st = mpnn_alloc(c, &c->cfeat, (size_t)Nn))) return st;
+    CK(cudaMemcpyAsync(d_ptr, ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(d_deg, dinv.data(), dinv.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    m.n_nodes = Nn;
+    m.adj_ptr = d_ptr;
+    m.adj_idx = d_idx;
+    m.deg_inv = d_deg;
+    m.cfeat = c->cfeat;
+    m.fixed = c->fixed;
+    for (int l = 0; l <= kMpnnLayers; ++l) {
+      __nv_bfloat16* h;
+      if ((st = mpnn_alloc(c, &h, (size_t)Nn * kMpnnHidden))) return st;
+      m.H[l] = h;
+    }
+    for (int l = 0; l < kMpnnLayers; ++l) {
+      uint64_t* mk;
+      if ((st = mpnn_alloc(c, &mk, (size_t)Nn))) return st;
+      m.mask[l] = mk;
+    }
+    double* scal;
+    int* err;
+    if ((st = mpnn_alloc(c, &scal, (size_t)4))) return st;
+    if ((st = mpnn_alloc(c, &err, (size_t)1))) return st;
+    m.scal = scal;
+    m.err = err;
+    if (!c->h_err) CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_err), sizeof(int)));
+    CK(cudaStreamSynchronize(c->stream));
+    c->mpnn_built = true;
+  }
+  if (!c->mpnn_feat_valid) {
+    if (c->elem_modulus.size() != (size_t)Ne)
+      return set_err(c, FEM_ERR_STATE, "learned preconditioner: materials not set");
+    std::vector<int4> conn(Ne);
+    CK(cudaMemcpyAsync(conn.data(), c->conn, conn.size() * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<double> acc(Nn, 0.0), cnt(Nn, 0.0);
+    for (int e = 0; e < Ne; ++e) {
+      const int* cn = &conn[e].x;
+      for (int a = 0; a < 4; ++a) {
+        acc[cn[a]] += c->elem_modulus[e];
+        cnt[cn[a]] += 1.0;
+      }
+    }
+    double mean = 0.0;
+    std::vector<double> lm(Nn);
+    for (int i = 0; i < Nn; ++i) {
+      lm[i] = cnt[i] > 0 ? std::log(acc[i] / cnt[i]) : 0.0;
+      mean += lm[i];
+    }
+    mean /= std::max(Nn, 1);
+    std::vector<float> cf(Nn);
+    for (int i = 0; i < Nn; ++i) cf[i] = (float)(lm[i] - mean);
+    CK(cudaMemcpyAsync(c->cfeat, cf.data(), cf.size() * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->mpnn_feat_valid = true;
+  }
   return FEM_OK;
 }
 
@@ -493,18 +1018,40 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
             double* rel) {
   if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
   int st;
-  if ((st = compute_dinv(c, precond))) return st;
-  if ((st = ensure_cg_graph(c))) return st;
-  const int ndof4 = c->ndof_pad / 4;
-  ++c->n_launches; launch_cg_init(b_int, c->r, c->x, c->p, c->dinv, ndof4, c->cg, rtol, maxit, c->red(), SITE_CGI,
-                 c->stream);
+  const bool tl = precond == FEM_PRECOND_TWO_LEVEL;
+  const bool learned = precond == FEM_PRECOND_LEARNED;
+  const int kind = learned ? GRAPH_LEARNED : (tl ? GRAPH_TWO_LEVEL : GRAPH_JACOBI);
+  if (learned && !c->mpnn_has_weights)
+    return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights (fem_mpnn_set_weights)");
+  if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : precond))) return st;
+  if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
+  if (learned && (st = ensure_mpnn(c))) return st;
+  if ((st = ensure_cg_graph(c, kind))) return st;
+  ++c->n_launches; launch_cg_init(b_int, c->r, c->x, c->p, c->dinv, c->Nn, c->cg, rtol, maxit, c->red(), SITE_CGI,
+                 c->stream, (tl || learned) ? 0 : 1);
   CKL();
+  if (learned) {
+    const CoarseArgs ca = coarse_args(c);
+    launch_mpnn_forward(c->mdev, c->r, c->dinv, c->tmpf, c->cg, c->red(), SITE_RZ, c->stream);
+    if (c->learned_coarse) launch_coarse_apply(ca, c->r, c->cg, c->stream);
+    launch_fpcg_dots(ca, true, c->learned_coarse, c->r, c->y, c->tmpf, c->p, c->cg, c->red(), SITE_RZ,
+                     c->stream);
+    c->n_launches += 6 + 1 + (c->learned_coarse ? 2 : 0);
+    CKL();
+  }
+  if (tl) {
+    const CoarseArgs ca = coarse_args(c);
+    launch_coarse_apply(ca, c->r, c->cg, c->stream);
+    launch_tl_rz(ca, true, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
+    c->n_launches += 3;
+    CKL();
+  }
   const int max_batches = maxit / kCGBatch + 2;
   CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   int batches = 0;
   while (!c->h_cg->done && batches < max_batches) {
-    CK(cudaGraphLaunch(c->cg_graph, c->stream));
+    CK(cudaGraphLaunch(c->cg_graph[kind], c->stream));
     c->n_graphs++;
     CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -512,8 +1059,27 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   }
   const CGState& h = *c->h_cg;
   c->n_cg_iters += h.iter;
-  // kernels that did work: 3 per CG iteration (the rest of a batch exits at entry)
-  c->n_launches += 3LL * h.iter;
+  // kernels that did work: 3 (Jacobi), 6 (two-level) or 11 + 2 (learned,
+  // + coarse) per CG iteration; the rest of a batch exits at entry
+  c->n_launches += (tl ? 6LL : (learned ? (11LL + (c->learned_coarse ? 2 : 0)) : 3LL)) * h.iter;
+  if (learned) {
+    CK(cudaMemcpyAsync(c->h_err, c->mdev.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (*c->h_err) return set_err(c, FEM_ERR_BUDGET, "learned preconditioner: tensor-core wait gave up");
+    if (h.done == 2 || h.done == 3) {
+      // Jacobi-based PCG is the fallback: the flexible solve broke down or ran
+      // out of iterations; the same convergence test judges the rerun
+      ++c->n_fallbacks;
+      int it2 = 0;
+      double rel2 = 0;
+      const int fb = c->learned_coarse ? FEM_PRECOND_TWO_LEVEL : FEM_PRECOND_JACOBI;
+      const int iters_done = h.iter;
+      st = run_pcg(c, b_int, fb, rtol, maxit, &it2, &rel2);
+      if (iters) *iters = iters_done + it2;
+      if (rel) *rel = rel2;
+      return st;
+    }
+  }
   if (iters) *iters = h.iter;
   if (rel) *rel = h.rr0 > 0 ? std::sqrt(h.rr / h.rr0) : 0.0;
   if (h.done == 3) return set_err(c, FEM_ERR_NAN, "PCG breakdown (non-positive curvature or NaN) at iteration %d", h.iter);
@@ -632,6 +1198,136 @@ int fem_ctx_stats(void* ctx, int64_t* out) {
   out[1] = c->n_cg_iters;
   out[2] = c->n_res_evals;
   out[3] = c->n_graphs;
+  out[4] = c->mv_variant;
+  out[5] = (int64_t)std::llround(c->mv_ns[MV_FUSED]);
+  out[6] = (int64_t)std::llround(c->mv_ns[MV_TWO_PHASE]);
+  out[7] = c->mv_tuned ? 1 : 0;
+  return FEM_OK;
+}
+
+int fem_learned_stats(void* ctx, int64_t* out2) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  if (!c || !out2) return FEM_ERR_INVALID;
+  out2[0] = c->n_fallbacks;
+  out2[1] = c->mpnn_has_weights ? 1 : 0;
+  return FEM_OK;
+}
+
+int fem_set_option(void* ctx, int32_t key, int64_t value) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  switch (key) {
+    case FEM_OPT_MATVEC_VARIANT:
+      if (value < -1 || value >= MV_N_VARIANTS)
+        return set_err(c, FEM_ERR_INVALID, "matvec variant %lld not in {-1 (auto), 0 (fused), 1 (two-phase)}",
+                       (long long)value);
+      c->mv_forced = (int)value;
+      c->mv_variant = value >= 0 ? (int)value : MV_FUSED;
+      c->mv_tuned = false;
+      return FEM_OK;
+    case FEM_OPT_COARSE_CELL:
+      if (value < 1 || value > 64)
+        return set_err(c, FEM_ERR_INVALID, "coarse cell edge %lld not in [1, 64] mesh lengths", (long long)value);
+      if (value != c->coarse_cell_voxels) {
+        CK(cudaStreamSynchronize(c->stream));
+        for (void* p : c->coarse_bufs)
+          if (p) cudaFree(p);
+        c->coarse_bufs.clear();
+        c->coarse_cell_voxels = (int)value;
+        c->coarse_built = false;
+        c->coarse_valid = false;
+        // the captured two-level graph holds the old coarse buffers
+        if (c->cg_graph[GRAPH_TWO_LEVEL]) cudaGraphExecDestroy(c->cg_graph[GRAPH_TWO_LEVEL]);
+        c->cg_graph[GRAPH_TWO_LEVEL] = nullptr;
+      }
+      return FEM_OK;
+    case FEM_OPT_LEARNED_COARSE:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "learned coarse flag must be 0 or 1");
+      c->learned_coarse = value != 0;
+      return FEM_OK;
+    case FEM_OPT_COARSE_REUSE:
+      if (value < 1 || value > (1 << 20))
+        return set_err(c, FEM_ERR_INVALID, "coarse reuse count %lld not in [1, 2^20]", (long long)value);
+      c->coarse_reuse = (int)value;
+      return FEM_OK;
+    default:
+      return set_err(c, FEM_ERR_INVALID, "unknown option key %d", key);
+  }
+}
+
+int fem_mpnn_set_weights(void* ctx, const float* w, int64_t n) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!w || n != kMpnnParams)
+    return set_err(c, FEM_ERR_INVALID, "learned preconditioner takes %d parameters (got %lld)", kMpnnParams,
+                   (long long)n);
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(w[i])) return set_err(c, FEM_ERR_INVALID, "parameter %lld is not finite", (long long)i);
+  if (!c->mpnn_w) {
+    if ((st = mpnn_alloc(c, &c->mpnn_w, (size_t)kMpnnParams))) return st;
+    if ((st = mpnn_alloc(c, &c->We_p, (size_t)kMpnnHidden * kMpnnIn))) return st;
+    if ((st = mpnn_alloc(c, &c->Wl_p, (size_t)kMpnnLayers * kMpnnHidden * 2 * kMpnnHidden))) return st;
+    if ((st = mpnn_alloc(c, &c->WlT_p, (size_t)kMpnnLayers * kMpnnHidden * 2 * kMpnnHidden))) return st;
+  }
+  CK(cudaMemcpyAsync(c->mpnn_w, w, sizeof(float) * kMpnnParams, cudaMemcpyHostToDevice, c->stream));
+  ++c->n_launches; launch_mpnn_pack(c->mpnn_w, c->We_p, c->Wl_p, c->WlT_p, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  c->mdev.w = c->mpnn_w;
+  c->mdev.We_p = c->We_p;
+  c->mdev.Wl_p = c->Wl_p;
+  c->mdev.WlT_p = c->WlT_p;
+  c->mpnn_has_weights = true;
+  return FEM_OK;
+}
+
+int fem_mpnn_get_weights(void* ctx, float* w, int64_t n) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!w || n != kMpnnParams)
+    return set_err(c, FEM_ERR_INVALID, "learned preconditioner has %d parameters (got %lld)", kMpnnParams,
+                   (long long)n);
+  if (!c->mpnn_has_weights) return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights");
+  CK(cudaMemcpyAsync(w, c->mpnn_w, sizeof(float) * kMpnnParams, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return FEM_OK;
+}
+
+int fem_mpnn_forward(void* ctx, const float* r, float* z) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!r || !z) return set_err(c, FEM_ERR_INVALID, "null vector");
+  if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
+  if (!c->mpnn_has_weights) return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights");
+  if ((st = compute_dinv(c, FEM_PRECOND_JACOBI))) return st;
+  if ((st = ensure_mpnn(c))) return st;
+  prepare_mpnn_kernels();
+  CK(cudaMemsetAsync(c->mdev.err, 0, sizeof(int), c->stream));
+  ++c->n_launches; launch_gather_f(r, c->r, c->d_perm_node, c->Nn, c->stream);
+  launch_mpnn_forward(c->mdev, c->r, c->dinv, c->y, nullptr, c->red(), SITE_RZ, c->stream);
+  c->n_launches += 6;
+  CKL();
+  ++c->n_launches; launch_scatter_f(c->y, z, c->d_perm_node, c->Nn, c->stream);
+  CKL();
+  CK(cudaMemcpyAsync(c->h_err, c->mdev.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (*c->h_err) return set_err(c, FEM_ERR_BUDGET, "learned preconditioner: tensor-core wait gave up");
+  return FEM_OK;
+}
+
+int fem_coarse_info(void* ctx, double* out6) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  if (!c || !out6) return FEM_ERR_INVALID;
+  out6[0] = c->cdev.n_cells;
+  out6[1] = c->cdev.n_cn;
+  out6[2] = c->cdev.n_dof;
+  out6[3] = c->coarse_H;
+  out6[4] = (double)c->n_coarse_assemblies;
+  out6[5] = c->coarse_ms_last;
   return FEM_OK;
 }
 
@@ -700,6 +1396,20 @@ int fem_set_materials(void* ctx, const FemMaterial* table, int32_t n, const uint
   } else if (kind == -1 && !elem_mat) {
     kind = table[0].model;
   }
+  // stiffness scale per element for the learned preconditioner's node feature
+  c->elem_modulus.assign(c->Ne, 0.0);
+  for (int e = 0; e < c->Ne; ++e) {
+    const FemMaterial& s = table[ids[e]];
+    double mod;
+    if (s.model == FEM_TRANSVERSE_ISOTROPIC)
+      mod = (s.C_voigt[0] + s.C_voigt[7] + s.C_voigt[14]) / 3.0;
+    else if (s.model == FEM_MOONEY_RIVLIN || s.model == FEM_FIBRE_MOONEY_RIVLIN)
+      mod = (s.D1 > 0 ? 2.0 / s.D1 : 0.0) + 8.0 * (s.C10 + s.C01) / 3.0;
+    else
+      mod = s.E * (1.0 - s.nu) / ((1.0 + s.nu) * (1.0 - 2.0 * s.nu));
+    c->elem_modulus[e] = std::max(mod, 1e-30) * sc[e];
+  }
+  c->mpnn_feat_valid = false;
   CK(cudaMemcpyAsync(c->matD, md.data(), md.size() * sizeof(DevMat<double>), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->matF, mf.data(), mf.size() * sizeof(DevMat<float>), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->mat_id, ids.data(), ids.size(), cudaMemcpyHostToDevice, c->stream));
@@ -709,6 +1419,7 @@ int fem_set_materials(void* ctx, const FemMaterial* table, int32_t n, const uint
   c->has_j2 = has_j2;
   c->materials_set = true;
   c->tangent_valid = false;
+  c->coarse_valid = false;
   return FEM_OK;
 }
 
@@ -719,6 +1430,10 @@ int fem_set_bc(void* ctx, const uint8_t* fixed_mask, const double* fixed_values,
   if (fixed_mask) {
     ++c->n_launches; launch_gather_mask(fixed_mask, c->fixed, c->d_perm_node, c->Nn, c->stream);
     CKL();
+    // the matvec kernels read the fixed bits from the w lane of the FP32 coordinates
+    ++c->n_launches; launch_x32_mask(c->X32, c->fixed, c->Nn, c->stream);
+    CKL();
+    c->coarse_valid = false;
   }
   if (fixed_values) {
     ++c->n_launches; launch_gather_d(fixed_values, c->fixed_vals, c->d_perm_node, c->Nn, c->stream);
@@ -824,8 +1539,7 @@ int fem_tangent_matvec(void* ctx, const float* xin, float* yout) {
   if (!xin || !yout) return set_err(c, FEM_ERR_INVALID, "null vector");
   ++c->n_launches; launch_gather_f(xin, c->tmpf, c->d_perm_node, c->Nn, c->stream);
   CKL();
-  MvArgs mv;
-  mv.m = c->mesh();
+  MvArgs mv = make_mv(c);
   mv.matF = c->matF;
   mv.payload = c->payload;
   mv.x = c->tmpf;
@@ -849,6 +1563,8 @@ int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol
   if ((st = check_ctx(c))) return st;
   if (!r || !du) return set_err(c, FEM_ERR_INVALID, "null vector");
   if (maxit <= 0 || !(rtol > 0)) return set_err(c, FEM_ERR_INVALID, "need max_iterations > 0 and rtol > 0");
+  if (precond < FEM_PRECOND_NONE || precond > FEM_PRECOND_TWO_LEVEL)
+    return set_err(c, FEM_ERR_INVALID, "unknown preconditioner %d", precond);
   // caller order -> internal order, fixed DOFs of the right-hand side zeroed
   ++c->n_launches; launch_gather_d_masked(r, c->tmpd, c->d_perm_node, c->fixed, c->Nn, c->stream);
   CKL();
@@ -890,6 +1606,8 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     fem_default_solve_params(&prm);
   if (prm.max_iterations <= 0 || !(prm.tol > 0))
     return set_err(c, FEM_ERR_INVALID, "need max_iterations > 0 and tol > 0");
+  if (prm.precond < FEM_PRECOND_NONE || prm.precond > FEM_PRECOND_TWO_LEVEL)
+    return set_err(c, FEM_ERR_INVALID, "unknown preconditioner %d", prm.precond);
   FemSolveResult out;
   std::memset(&out, 0, sizeof(out));
   // Change of the prescribed values in this solve.  It is carried by the first
@@ -920,8 +1638,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
       if (res) *res = out;
       return set_err(c, FEM_ERR_NAN, "NaN/Inf residual at iteration 0");
     }
-    MvArgs mv;
-    mv.m = c->mesh();
+    MvArgs mv = make_mv(c);
     mv.matF = c->matF;
     mv.payload = c->payload;
     mv.x = c->tmpf;
@@ -941,7 +1658,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     st = run_pcg(c, c->tmpd, prm.precond, eta, prm.cg_max_iterations, &cgit, &cgrel);
     out.cg_iterations += cgit;
     if (st && st != FEM_NOT_CONVERGED) return st;
-    ++c->n_launches; launch_u_update(c->u, c->u_base, c->x, 1.0, c->ndof, c->stream);
+    ++c->n_launches; launch_u_update(c->u, c->u_base, c->x, 1.0, c->Nn, c->stream);
     CKL();
     it0 = 1;
   }
@@ -1001,7 +1718,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     double trial = res_norm;
     const int n_trials = prm.line_search == FEM_LS_NONE ? 1 : 5;
     for (int ls = 0; ls < n_trials; ++ls) {
-      ++c->n_launches; launch_u_update(c->u, c->u_base, c->x, alpha, c->ndof, c->stream);
+      ++c->n_launches; launch_u_update(c->u, c->u_base, c->x, alpha, c->Nn, c->stream);
       CKL();
       if ((st = eval_residual(c, nullptr, &r2))) return st;
       out.residual_evals++;
@@ -1045,20 +1762,12 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int ndof4 = c->ndof_pad / 4;
-  // a CG state that never finishes, so the fused kernels do their full work
-  CGState hs;
-  std::memset(&hs, 0, sizeof(hs));
-  hs.rz = 1.0;
-  hs.rr = 1.0;
-  hs.rr0 = 1.0;
-  hs.tol2 = 0.0;
-  hs.alpha = 1e-30;
-  hs.beta = 0.0;
-  hs.max_iter = 1 << 30;
+  const int nn = c->Nn;
+  const CGState hs = endless_cg();
+  // a nonzero direction: p = 1 on free DOFs
+  launch_dinv_identity(c->p, c->fixed, c->Nn, c->stream);
   auto reset_cg = [&]() { return cudaMemcpyAsync(c->cg, &hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream); };
-  MvArgs mv;
-  mv.m = c->mesh();
+  MvArgs mv = make_mv(c);
   mv.matF = c->matF;
   mv.payload = c->payload;
   mv.x = c->p;
@@ -1087,16 +1796,16 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
     for (int w = 0; w < 2; ++w) {
       if (k == 0) launch_matvec(mv, c->model_kind, c->stream);
       if (k == 1) launch_residual(ra, c->model_kind, c->stream);
-      if (k == 2) launch_cg_update(c->tmpf, c->r, c->p, c->y, c->dinv, ndof4, c->cg, c->red(), SITE_CGU, c->stream);
-      if (k == 3) launch_cg_pupdate(c->tmpf, c->r, c->dinv, ndof4, c->cg, c->stream);
+      if (k == 2) launch_cg_update(c->tmpf, c->r, c->p, c->y, c->dinv, nn, c->cg, c->red(), SITE_CGU, c->stream);
+      if (k == 3) launch_cg_pupdate(c->tmpf, c->r, c->dinv, nn, c->cg, c->stream);
     }
     CK(reset_cg());
     CK(cudaEventRecord(e0, c->stream));
     for (int r = 0; r < reps; ++r) {
       if (k == 0) launch_matvec(mv, c->model_kind, c->stream);
       if (k == 1) launch_residual(ra, c->model_kind, c->stream);
-      if (k == 2) launch_cg_update(c->tmpf, c->r, c->p, c->y, c->dinv, ndof4, c->cg, c->red(), SITE_CGU, c->stream);
-      if (k == 3) launch_cg_pupdate(c->tmpf, c->r, c->dinv, ndof4, c->cg, c->stream);
+      if (k == 2) launch_cg_update(c->tmpf, c->r, c->p, c->y, c->dinv, nn, c->cg, c->red(), SITE_CGU, c->stream);
+      if (k == 3) launch_cg_pupdate(c->tmpf, c->r, c->dinv, nn, c->cg, c->stream);
     }
     CK(cudaEventRecord(e1, c->stream));
     CKL();

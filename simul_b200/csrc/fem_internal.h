@@ -2,6 +2,7 @@
 // (fem_kernels.cu).  Not part of the public ABI.
 #pragma once
 #include <cstdint>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "fem_device.cuh"
@@ -29,6 +30,8 @@ struct MeshDev {
   const int* node_row;      // [Nn + 1]
   const uint32_t* node_slots;
   const uint8_t* fixed;     // [Nn] bit d set = DOF d fixed
+  int max_slots;            // largest slot-list range of one block (shared memory sizing)
+  const int4* spos;         // [Ne] position of each (element, slot) in node_slots order
 };
 
 // Last-block reduction bookkeeping: one slot per reduction site.
@@ -37,6 +40,9 @@ struct Reduce {
   unsigned int* counters;   // [n_sites]
   int max_blocks;
 };
+
+// FP32 node vectors (CG r, x, p, y, diag^-1, scratch) hold one float4 per
+// node (xyz, 0); FP64 node vectors (u, R, f_ext, prescribed values) 3 doubles.
 
 // Device-resident PCG state (read by every CG kernel, advanced by the last
 // block of each reduction so no host round trip is needed per iteration).
@@ -66,19 +72,88 @@ struct MvArgs {
   MeshDev m;
   const DevMat<float>* matF;
   const float* payload;
-  const float* x;           // [3 Nn (padded)]
+  const float* x;           // [Nn] float4 (xyz, 0)
   float* y;
   CGState* cg;              // non-null: CG-fused (early exit, p.Ap, alpha)
   Reduce red;
   int red_site;
   int mask_input;           // 1: fixed DOFs of x read as zero (K_ff x); 0: K_f,all x
+  int variant;              // MV_FUSED (node-block) or MV_TWO_PHASE (element pass + node gather)
+  float4* stage;            // [4 Ne] slot vectors in node_slots order (two-phase scratch)
 };
+
+enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_N_VARIANTS = 2 };
 
 struct DiagArgs {
   MeshDev m;
   const DevMat<float>* matF;
   const float* payload;
-  float* dinv;              // [3 Nn] 1/diag(K) on free DOFs, 0 elsewhere
+  float* dinv;              // [Nn] float4: 1/diag(K) on free DOFs, 0 elsewhere
+};
+
+// Coarse lattice of the two-level preconditioner (fem_coarse.cu).  Cells
+// are the non-empty lattice cells (ascending lattice index); coarse nodes are
+// their corners (ascending lattice index); corner q of a cell is the lattice
+// offset (q >> 2 & 1, q >> 1 & 1, q & 1).
+struct CoarseDev {
+  int n_cells;
+  int n_cn;                 // coarse nodes
+  int n_dof;                // 3 n_cn
+  float inv_H;              // 1 / cell edge
+  float3 lo;                // lattice origin
+  const int3* cell_ijk;     // [n_cells] lattice coordinates
+  const int* cell_corner;   // [n_cells * 8] coarse node of each corner
+  const int* cell_node_ptr; // [n_cells + 1] into cell_nodes (each node in one cell)
+  const int* cell_nodes;
+  const int* cell_elem_ptr; // [n_cells + 1] into cell_elems (cell of the centroid)
+  const int* cell_elems;
+  const int* node_cell;     // [Nn]
+  const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
+  double* blocks;           // [n_cells][24 * 24] Galerkin block of each cell
+  double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
+  float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric)
+  float* cell_r;            // [n_cells][24] restricted residual per cell
+  float* yc;                // [n_dof] coarse correction
+};
+
+struct CoarseArgs {
+  MeshDev m;
+  CoarseDev c;
+  const DevMat<float>* matF;
+  const float* payload;
+};
+
+// Learned preconditioner (fem_mpnn.cu).  Flat FP32 parameter order:
+// W_e [64][16], b_e [64], then per layer W_l [64][128], b_l [64], then
+// W_d [3][64], b_d [3].
+constexpr int kMpnnHidden = 64;
+constexpr int kMpnnIn = 16;
+constexpr int kMpnnLayers = 4;
+constexpr int kMpnnOffWe = 0;
+constexpr int kMpnnOffBe = kMpnnHidden * kMpnnIn;
+__host__ __device__ constexpr int kMpnnOffW(int l) {
+  return kMpnnOffBe + kMpnnHidden + l * (kMpnnHidden * 2 * kMpnnHidden + kMpnnHidden);
+}
+__host__ __device__ constexpr int kMpnnOffB(int l) { return kMpnnOffW(l) + kMpnnHidden * 2 * kMpnnHidden; }
+constexpr int kMpnnOffWd = kMpnnOffW(kMpnnLayers);
+constexpr int kMpnnOffBd = kMpnnOffWd + 3 * kMpnnHidden;
+constexpr int kMpnnParams = kMpnnOffBd + 3;
+
+struct MpnnDev {
+  int n_nodes;
+  const int* adj_ptr;           // [Nn + 1] node graph (nodes sharing an element), ids ascending
+  const int* adj_idx;
+  const float* deg_inv;         // [Nn] 1 / |N(i)| (0 for isolated nodes)
+  const float* cfeat;           // [Nn] log-modulus feature
+  const uint8_t* fixed;         // [Nn]
+  const float* w;               // [kMpnnParams] FP32 master parameters
+  const __nv_bfloat16* We_p;    // packed W_e  [64 x 16]  (K-major canonical)
+  const __nv_bfloat16* Wl_p;    // packed W_l  [layers][64 x 128]
+  const __nv_bfloat16* WlT_p;   // packed W_l^T [layers][128 x 64]
+  __nv_bfloat16* H[kMpnnLayers + 1];  // [Nn][64] hidden states per layer
+  uint64_t* mask[kMpnnLayers];  // [Nn] relu masks of the message-passing layers
+  double* scal;                 // [0] s = RMS |D^-1/2 r|
+  int* err;                     // set when an MMA completion wait gives up
 };
 
 // Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
@@ -88,12 +163,44 @@ int set_global_error(int code, const char* fmt, ...);
 // launchers (fem_kernels.cu)
 void launch_residual(const ResArgs& a, int model, cudaStream_t s);
 void launch_matvec(const MvArgs& a, int model, cudaStream_t s);
+// sets the shared-memory limits the captured CG graph's kernels need
+void prepare_kernels(const MeshDev& m, int model);
 void launch_diag(const DiagArgs& a, int model, cudaStream_t s);
-void launch_cg_init(const double* b, float* r, float* x, float* p, const float* dinv, int ndof4,
-                    CGState* cg, double rtol, int maxit, Reduce red, int site, cudaStream_t s);
+// coarse lattice (fem_coarse.cu)
+size_t coarse_cell_smem();
+void prepare_coarse_kernels(int model, int n_dof);
+// cell Galerkin blocks + dense Ac (FP64, column-major)
+void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
+// Ainv = FP32 symmetric copy of the lower triangle left in Ac
+void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);
+// yc = Ainv P^T r (skipped once cg->done is set, when cg is non-null)
+void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s);
+// z = D^-1 r + P yc, rz and beta (init: into p, beta = 0)
+void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* dinv, float* z, float* p,
+                  CGState* cg, Reduce red, int site, cudaStream_t s);
+void launch_tl_pupdate(float* p, const float* z, int n_nodes, const CGState* cg, cudaStream_t s);
+// flexible PCG: [z += P yc], rz = r.z, z.q; init: p = z; else Polak-Ribiere beta
+void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q, float* z,
+                      float* p, CGState* cg, Reduce red, int site, cudaStream_t s);
+
+// learned preconditioner (fem_mpnn.cu)
+void prepare_mpnn_kernels();
+void launch_mpnn_pack(const float* w, __nv_bfloat16* We_p, __nv_bfloat16* Wl_p, __nv_bfloat16* WlT_p,
+                      cudaStream_t s);
+// z = M(r) (skipped once cg->done is set, when cg is non-null)
+void launch_mpnn_forward(const MpnnDev& m, const float* r, const float* dinv, float* z, const CGState* cg,
+                         Reduce red, int site, cudaStream_t s);
+
+// PCG vector kernels.  precond_in_update = 1: Jacobi z = D^-1 r is applied
+// inside cg_init / cg_update (rz, beta there); 0: an external preconditioner
+// kernel computes rz and beta.
+void launch_cg_init(const double* b, float* r, float* x, float* p, const float* dinv, int n_nodes,
+                    CGState* cg, double rtol, int maxit, Reduce red, int site, cudaStream_t s,
+                    int precond_in_update = 1);
 void launch_cg_update(float* x, float* r, const float* p, const float* y, const float* dinv,
-                      int ndof4, CGState* cg, Reduce red, int site, cudaStream_t s);
-void launch_cg_pupdate(float* p, const float* r, const float* dinv, int ndof4, CGState* cg,
+                      int n_nodes, CGState* cg, Reduce red, int site, cudaStream_t s,
+                      int precond_in_update = 1);
+void launch_cg_pupdate(float* p, const float* r, const float* dinv, int n_nodes, CGState* cg,
                        cudaStream_t s);
 void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
                    const double* ep_c, const double* epe_c, const int* perm_elem, double* F_out,
@@ -112,8 +219,11 @@ void launch_gather_mask(const uint8_t* in_user, uint8_t* out_int, const int* per
                         cudaStream_t s);
 void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, int n,
                      cudaStream_t s);
-void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int ndof,
+// u[3n+d] = u_base[3n+d] + alpha du[4n+d] for n < n_nodes
+void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int n_nodes,
                      cudaStream_t s);
+// X32[n].w = fixed bits of node n
+void launch_x32_mask(float4* X32, const uint8_t* fixed, int n, cudaStream_t s);
 void launch_gather_d_masked(const double* in_user, double* out_int, const int* perm,
                             const uint8_t* fixed, int n, cudaStream_t s);
 void launch_dinv_identity(float* dinv, const uint8_t* fixed, int n, cudaStream_t s);
@@ -123,6 +233,5 @@ void launch_bc_delta(const double* u, const double* fixed_vals, const uint8_t* f
 // out = R - y on free DOFs, 0 on fixed DOFs
 void launch_rhs_minus(const double* R, const float* y, const uint8_t* fixed, double* out, int n,
                       cudaStream_t s);
-void launch_d2f_masked(const double* in, float* out, const uint8_t* fixed, int n, cudaStream_t s);
 
 }  // namespace femb200

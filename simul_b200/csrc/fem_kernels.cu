@@ -13,59 +13,57 @@
 #include <cuda_runtime.h>
 
 #include "fem_internal.h"
+#include "fem_reduce.cuh"
 
 namespace femb200 {
 
-// ───────────────────────── reductions ─────────────────────────
-
-template <int NT>
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  double r = 0.0;
-  if (w == 0) {
-    r = (l < NT / 32) ? sh[l] : 0.0;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+// Loads this block's node slot lists (one contiguous range of node_slots)
+// into shared memory and returns the calling thread's node range within it.
+// The caller's first __syncthreads makes the copy visible.
+template <int NB>
+__device__ __forceinline__ void load_block_slots(const MeshDev& m, int b, uint32_t* s_slots,
+                                                 int& cur, int& end) {
+  const int n0 = b * NB;
+  const int n1 = min(n0 + NB, m.n_nodes);
+  const int s0 = __ldg(m.node_row + n0);
+  const int s1 = __ldg(m.node_row + n1);
+  for (int i = threadIdx.x; i < s1 - s0; i += NB) s_slots[i] = __ldg(m.node_slots + s0 + i);
+  const int node = n0 + (int)threadIdx.x;
+  cur = end = 0;
+  if (node < m.n_nodes) {
+    cur = __ldg(m.node_row + node) - s0;
+    end = __ldg(m.node_row + node + 1) - s0;
   }
-  return r;  // valid in thread 0
 }
 
-// Publishes this block's partial(s) and reports whether it is the last block
-// to arrive; the last block then owns the fixed-order final sum.
-__device__ __forceinline__ bool publish_partial(const Reduce& red, int site, int nval,
-                                                const double* vals, bool* am_last) {
-  if (threadIdx.x == 0) {
-    for (int v = 0; v < nval; ++v)
-      red.partials[(size_t)(site * 2 + v) * red.max_blocks + blockIdx.x] = vals[v];
-    __threadfence();
-    unsigned int t = atomicAdd(&red.counters[site], 1u);
-    *am_last = (t == gridDim.x - 1);
+// Adds, in slot-list order, the slot vectors of the current chunk that belong
+// to this thread's node.  Entries are sorted by local element index, so every
+// chunk consumes a prefix of what is left.
+template <int NB, typename T, typename TA>
+__device__ __forceinline__ void gather_chunk(const uint32_t* s_slots, const T (*sf)[NB], int base,
+                                             int& cur, int end, TA& a0, TA& a1, TA& a2) {
+  const int lim = base + NB;
+  while (cur < end) {
+    const uint32_t ent = s_slots[cur];
+    const int li = (int)(ent >> 2);
+    if (li >= lim) break;
+    const int t = li - base;
+    const int s = (int)(ent & 3u);
+    a0 += sf[3 * s + 0][t];
+    a1 += sf[3 * s + 1][t];
+    a2 += sf[3 * s + 2][t];
+    ++cur;
   }
-  __syncthreads();
-  return *am_last;
-}
-
-template <int NT>
-__device__ __forceinline__ double final_sum(const Reduce& red, int site, int v, double* sh) {
-  __threadfence();
-  double acc = 0.0;
-  const double* p = red.partials + (size_t)(site * 2 + v) * red.max_blocks;
-  for (int i = threadIdx.x; i < (int)gridDim.x; i += NT) acc += __ldcg(p + i);
-  return block_sum<NT>(acc, sh);
 }
 
 // ───────────────────────── residual (FP64) ─────────────────────────
 
 template <int NB, int MODEL>
 __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ ResArgs a) {
-  // 12 x NB doubles of slot vectors: dynamic (96 KB at NB = 512)
-  extern __shared__ double sdyn[];
-  double(*sf)[NB] = reinterpret_cast<double(*)[NB]>(sdyn);
+  // dynamic: 12 x NB doubles of slot vectors, then the block's slot lists
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  double(*sf)[NB] = reinterpret_cast<double(*)[NB]>(s_dyn);
+  uint32_t* s_slots = reinterpret_cast<uint32_t*>(s_dyn + sizeof(double) * 12 * NB);
   __shared__ double sred[NB / 32];
   __shared__ bool am_last;
   const MeshDev& m = a.m;
@@ -73,11 +71,8 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
   const int tid = threadIdx.x;
   const int node = b * NB + tid;
   const bool has_node = node < m.n_nodes;
-  int cur = 0, end = 0;
-  if (has_node) {
-    cur = m.node_row[node];
-    end = m.node_row[node + 1];
-  }
+  int cur, end;
+  load_block_slots<NB>(m, b, s_slots, cur, end);
   double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
   const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
   const int home_end = e0 + m.blk_home[b];
@@ -143,19 +138,7 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
         for (int d = 0; d < 3; ++d) sf[3 * s + d][tid] = f[s][d];
     }
     __syncthreads();
-    const int base = c0 - e0;
-    const int lim = base + NB;
-    while (cur < end) {
-      const uint32_t ent = __ldg(m.node_slots + cur);
-      const int li = (int)(ent >> 2);
-      if (li >= lim) break;
-      const int t = li - base;
-      const int s = (int)(ent & 3u);
-      acc0 += sf[3 * s + 0][t];
-      acc1 += sf[3 * s + 1][t];
-      acc2 += sf[3 * s + 2][t];
-      ++cur;
-    }
+    gather_chunk<NB>(s_slots, sf, c0 - e0, cur, end, acc0, acc1, acc2);
     __syncthreads();
   }
   double r2 = 0.0;
@@ -182,12 +165,16 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
 }
 
 // ───────────────────────── tangent matvec (FP32) ─────────────────────────
+// x and y hold one float4 per node (xyz, 0); X32.w carries the node's
+// fixed-DOF bits, so one 16-byte load per vertex brings geometry and mask.
 
 template <int NB, int MODEL, bool CG>
 __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvArgs a) {
   if (CG) {
     if (a.cg->done) return;
   }
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  uint32_t* s_slots = reinterpret_cast<uint32_t*>(s_dyn);
   __shared__ float sf[12][NB];
   __shared__ double sred[NB / 32];
   __shared__ bool am_last;
@@ -196,13 +183,11 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
   const int tid = threadIdx.x;
   const int node = b * NB + tid;
   const bool has_node = node < m.n_nodes;
-  int cur = 0, end = 0;
-  if (has_node) {
-    cur = m.node_row[node];
-    end = m.node_row[node + 1];
-  }
+  int cur, end;
+  load_block_slots<NB>(m, b, s_slots, cur, end);
   float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
   const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
+  const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
   for (int c0 = e0; c0 < e1; c0 += NB) {
     const int idx = c0 + tid;
     if (idx < e1) {
@@ -213,15 +198,14 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const float4 X = __ldg(m.X32 + nid[k]);
+        const float4 P = __ldg(xin + nid[k]);
         xv[k][0] = X.x;
         xv[k][1] = X.y;
         xv[k][2] = X.z;
-        const uint8_t fx = __ldg(m.fixed + nid[k]);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float v = __ldg(a.x + 3 * nid[k] + d);
-          pv[k][d] = (a.mask_input && ((fx >> d) & 1)) ? 0.f : v;
-        }
+        const int fx = a.mask_input ? (int)X.w : 0;
+        pv[k][0] = (fx & 1) ? 0.f : P.x;
+        pv[k][1] = (fx & 2) ? 0.f : P.y;
+        pv[k][2] = (fx & 4) ? 0.f : P.z;
       }
       TetGeom<float> g;
       tet_geom(xv[0], xv[1], xv[2], xv[3], g);
@@ -251,30 +235,18 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
         for (int d = 0; d < 3; ++d) sf[3 * s + d][tid] = f[s][d];
     }
     __syncthreads();
-    const int base = c0 - e0;
-    const int lim = base + NB;
-    while (cur < end) {
-      const uint32_t ent = __ldg(m.node_slots + cur);
-      const int li = (int)(ent >> 2);
-      if (li >= lim) break;
-      const int t = li - base;
-      const int s = (int)(ent & 3u);
-      acc0 += sf[3 * s + 0][t];
-      acc1 += sf[3 * s + 1][t];
-      acc2 += sf[3 * s + 2][t];
-      ++cur;
-    }
+    gather_chunk<NB>(s_slots, sf, c0 - e0, cur, end, acc0, acc1, acc2);
     __syncthreads();
   }
   double pap = 0.0;
   if (has_node) {
     const uint8_t fx = m.fixed[node];
-    const float accs[3] = {acc0, acc1, acc2};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float yv = ((fx >> d) & 1) ? 0.f : accs[d];
-      a.y[3 * node + d] = yv;
-      if (CG) pap += (double)yv * (double)a.x[3 * node + d];
+    const float4 yv = make_float4((fx & 1) ? 0.f : acc0, (fx & 2) ? 0.f : acc1,
+                                  (fx & 4) ? 0.f : acc2, 0.f);
+    reinterpret_cast<float4*>(a.y)[node] = yv;
+    if (CG) {
+      const float4 pv = xin[node];
+      pap = (double)yv.x * pv.x + (double)yv.y * pv.y + (double)yv.z * pv.z;
     }
   }
   if (CG) {
@@ -297,21 +269,146 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
   }
 }
 
+// ───────────────────────── two-phase tangent matvec (FP32) ─────────────────────────
+// Phase 1: one thread per element, no barriers and no redundant evaluation;
+// each slot vector is stored at its position in the node-major slot list.
+// Phase 2: one thread per node sums its contiguous slot range in list order,
+// so the result is the same fixed-order (bitwise reproducible) sum.
+
+template <int MODEL, bool MASK>
+__device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
+  const MeshDev& m = a.m;
+  const int4 cn = __ldg(m.conn + e);
+  const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+  const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
+  float xv[4][3], pv[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float4 X = __ldg(m.X32 + nid[k]);
+    const float4 P = __ldg(xin + nid[k]);
+    xv[k][0] = X.x;
+    xv[k][1] = X.y;
+    xv[k][2] = X.z;
+    // CG directions are zero on fixed DOFs already; only a standalone
+    // matvec masks its input
+    const int fx = MASK ? (int)X.w : 0;
+    pv[k][0] = (fx & 1) ? 0.f : P.x;
+    pv[k][1] = (fx & 2) ? 0.f : P.y;
+    pv[k][2] = (fx & 4) ? 0.f : P.z;
+  }
+  const int mid = (int)__ldg(m.mat_id + e);
+  const float scl = __ldg(m.scale + e);
+  const DevMat<float>& mat = a.matF[mid];
+  float pay[kPay];
+  {
+    const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
+#pragma unroll
+    for (int k = 0; k < kPay; ++k)
+      pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
+  }
+  const int4 sp = __ldg(m.spos + e);
+  TetGeom<float> g;
+  tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+  float D[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) D[k][d] = pv[k + 1][d] - pv[0][d];
+  float dF[9];
+  grad_from_diffs(D, g, dF);
+  float dP[9];
+  dP_any<MODEL>(mat, scl, pay, dF, dP);
+  float f[4][3];
+  slot_vectors(dP, g, g.s6, f);
+  __stcg(a.stage + sp.x, make_float4(f[0][0], f[0][1], f[0][2], 0.f));
+  __stcg(a.stage + sp.y, make_float4(f[1][0], f[1][1], f[1][2], 0.f));
+  __stcg(a.stage + sp.z, make_float4(f[2][0], f[2][1], f[2][2], 0.f));
+  __stcg(a.stage + sp.w, make_float4(f[3][0], f[3][1], f[3][2], 0.f));
+}
+
+template <int MODEL, bool CG>
+__global__ void __launch_bounds__(256) elem_mv_kernel(const __grid_constant__ MvArgs a) {
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  if (e >= a.m.n_elems) return;
+  if (!CG && a.mask_input)
+    elem_mv_one<MODEL, true>(a, e);
+  else
+    elem_mv_one<MODEL, false>(a, e);
+}
+
+// One thread per node; batches of 8 independent loads in flight, summed in
+// slot-list order.
+template <bool CG>
+__global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant__ MvArgs a) {
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const MeshDev& m = a.m;
+  const int n = blockIdx.x * 256 + threadIdx.x;
+  double pap = 0.0;
+  if (n < m.n_nodes) {
+    const int j0 = __ldg(m.node_row + n), j1 = __ldg(m.node_row + n + 1);
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    constexpr int kBatch = 8;
+    for (int j = j0; j < j1; j += kBatch) {
+      float4 v[kBatch];
+#pragma unroll
+      for (int k = 0; k < kBatch; ++k)
+        v[k] = (j + k < j1) ? __ldcg(a.stage + j + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int k = 0; k < kBatch; ++k) {
+        a0 += v[k].x;
+        a1 += v[k].y;
+        a2 += v[k].z;
+      }
+    }
+    const uint8_t fx = m.fixed[n];
+    const float4 yv = make_float4((fx & 1) ? 0.f : a0, (fx & 2) ? 0.f : a1, (fx & 4) ? 0.f : a2, 0.f);
+    reinterpret_cast<float4*>(a.y)[n] = yv;
+    if (CG) {
+      const float4 pv = reinterpret_cast<const float4*>(a.x)[n];
+      pap = (double)yv.x * pv.x + (double)yv.y * pv.y + (double)yv.z * pv.z;
+    }
+  }
+  if (CG) {
+    double bsum = block_sum<256>(pap, sred);
+    if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
+      double tot = final_sum<256>(a.red, a.red_site, 0, sred);
+      if (threadIdx.x == 0) {
+        CGState* st = a.cg;
+        st->pAp = tot;
+        if (!(tot > 0.0) || !isfinite(tot)) {
+          st->done = 3;
+          st->status = 3;
+          st->alpha = 0.0;
+        } else {
+          st->alpha = st->rz / tot;
+        }
+        a.red.counters[a.red_site] = 0u;
+      }
+    }
+  }
+}
+
 // ───────────────────────── Jacobi diagonal (FP32) ─────────────────────────
 
 template <int NB, int MODEL>
 __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagArgs a) {
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  uint32_t* s_slots = reinterpret_cast<uint32_t*>(s_dyn);
   __shared__ float sf[12][NB];
   const MeshDev& m = a.m;
   const int b = blockIdx.x;
   const int tid = threadIdx.x;
   const int node = b * NB + tid;
   const bool has_node = node < m.n_nodes;
-  int cur = 0, end = 0;
-  if (has_node) {
-    cur = m.node_row[node];
-    end = m.node_row[node + 1];
-  }
+  int cur, end;
+  load_block_slots<NB>(m, b, s_slots, cur, end);
   float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
   const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
   for (int c0 = e0; c0 < e1; c0 += NB) {
@@ -364,58 +461,46 @@ __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagAr
       }
     }
     __syncthreads();
-    const int base = c0 - e0;
-    const int lim = base + NB;
-    while (cur < end) {
-      const uint32_t ent = __ldg(m.node_slots + cur);
-      const int li = (int)(ent >> 2);
-      if (li >= lim) break;
-      const int t = li - base;
-      const int s = (int)(ent & 3u);
-      acc0 += sf[3 * s + 0][t];
-      acc1 += sf[3 * s + 1][t];
-      acc2 += sf[3 * s + 2][t];
-      ++cur;
-    }
+    gather_chunk<NB>(s_slots, sf, c0 - e0, cur, end, acc0, acc1, acc2);
     __syncthreads();
   }
   if (has_node) {
     const uint8_t fx = m.fixed[node];
     const float accs[3] = {acc0, acc1, acc2};
+    float dv[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float dv = accs[d];
-      a.dinv[3 * node + d] = (((fx >> d) & 1) || !(dv > 0.f)) ? 0.f : 1.f / dv;
-    }
+    for (int d = 0; d < 3; ++d)
+      dv[d] = (((fx >> d) & 1) || !(accs[d] > 0.f)) ? 0.f : 1.f / accs[d];
+    reinterpret_cast<float4*>(a.dinv)[node] = make_float4(dv[0], dv[1], dv[2], 0.f);
   }
 }
 
 // ───────────────────────── PCG vector kernels ─────────────────────────
-// Vectors are float [ndof4 * 4] with a zero tail; fixed DOFs carry dinv = 0,
-// so z, p and x stay zero there without masks.
+// FP32 node vectors hold one float4 per node (xyz, 0); fixed DOFs carry
+// dinv = 0, so z, p and x stay zero there without masks.  One node per thread.
 
 constexpr int kVecThreads = 256;
 
 __global__ void __launch_bounds__(kVecThreads) cg_init_kernel(const double* __restrict__ b,
                                                               float* r, float* x, float* p,
                                                               const float* __restrict__ dinv,
-                                                              int ndof4, CGState* cg, double rtol,
-                                                              int maxit, Reduce red, int site) {
+                                                              int n_nodes, CGState* cg, double rtol,
+                                                              int maxit, Reduce red, int site,
+                                                              int jac) {
+  // b holds 3 doubles per node
   __shared__ double sred[kVecThreads / 32];
   __shared__ bool am_last;
   const int i = blockIdx.x * kVecThreads + threadIdx.x;
   double rz = 0.0, rr = 0.0;
-  if (i < ndof4) {
-    const double2 b0 = reinterpret_cast<const double2*>(b)[2 * i];
-    const double2 b1 = reinterpret_cast<const double2*>(b)[2 * i + 1];
-    const float4 rv = make_float4((float)b0.x, (float)b0.y, (float)b1.x, (float)b1.y);
+  if (i < n_nodes) {
+    const float4 rv = make_float4((float)b[3 * i], (float)b[3 * i + 1], (float)b[3 * i + 2], 0.f);
     const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
-    const float4 zv = make_float4(dv.x * rv.x, dv.y * rv.y, dv.z * rv.z, dv.w * rv.w);
+    const float4 zv = make_float4(dv.x * rv.x, dv.y * rv.y, dv.z * rv.z, 0.f);
     reinterpret_cast<float4*>(r)[i] = rv;
-    reinterpret_cast<float4*>(p)[i] = zv;
+    if (jac) reinterpret_cast<float4*>(p)[i] = zv;
     reinterpret_cast<float4*>(x)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z + (double)rv.w * zv.w;
-    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    rz = jac ? (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z : 0.0;
+    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
   }
   double v[2];
   v[0] = block_sum<kVecThreads>(rz, sred);
@@ -434,7 +519,7 @@ __global__ void __launch_bounds__(kVecThreads) cg_init_kernel(const double* __re
       cg->iter = 0;
       cg->max_iter = maxit;
       cg->status = isfinite(trr) ? 0 : 3;
-      cg->done = (!isfinite(trr)) ? 3 : ((trr == 0.0 || !(trz > 0.0)) ? 1 : 0);
+      cg->done = (!isfinite(trr)) ? 3 : ((trr == 0.0 || (jac && !(trz > 0.0))) ? 1 : 0);
       red.counters[site] = 0u;
     }
   }
@@ -444,27 +529,26 @@ __global__ void __launch_bounds__(kVecThreads) cg_update_kernel(float* x, float*
                                                                 const float* __restrict__ p,
                                                                 const float* __restrict__ y,
                                                                 const float* __restrict__ dinv,
-                                                                int ndof4, CGState* cg, Reduce red,
-                                                                int site) {
+                                                                int n_nodes, CGState* cg, Reduce red,
+                                                                int site, int jac) {
   if (cg->done) return;
   __shared__ double sred[kVecThreads / 32];
   __shared__ bool am_last;
   const float alpha = (float)cg->alpha;
   const int i = blockIdx.x * kVecThreads + threadIdx.x;
   double rz = 0.0, rr = 0.0;
-  if (i < ndof4) {
+  if (i < n_nodes) {
     float4 xv = reinterpret_cast<float4*>(x)[i];
     float4 rv = reinterpret_cast<float4*>(r)[i];
     const float4 pv = reinterpret_cast<const float4*>(p)[i];
     const float4 yv = reinterpret_cast<const float4*>(y)[i];
     const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
-    xv.x += alpha * pv.x; xv.y += alpha * pv.y; xv.z += alpha * pv.z; xv.w += alpha * pv.w;
-    rv.x -= alpha * yv.x; rv.y -= alpha * yv.y; rv.z -= alpha * yv.z; rv.w -= alpha * yv.w;
+    xv.x += alpha * pv.x; xv.y += alpha * pv.y; xv.z += alpha * pv.z;
+    rv.x -= alpha * yv.x; rv.y -= alpha * yv.y; rv.z -= alpha * yv.z;
     reinterpret_cast<float4*>(x)[i] = xv;
     reinterpret_cast<float4*>(r)[i] = rv;
-    rz = (double)rv.x * (dv.x * rv.x) + (double)rv.y * (dv.y * rv.y) +
-         (double)rv.z * (dv.z * rv.z) + (double)rv.w * (dv.w * rv.w);
-    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z + (double)rv.w * rv.w;
+    if (jac) rz = (double)rv.x * (dv.x * rv.x) + (double)rv.y * (dv.y * rv.y) + (double)rv.z * (dv.z * rv.z);
+    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
   }
   double v[2];
   v[0] = block_sum<kVecThreads>(rz, sred);
@@ -473,11 +557,13 @@ __global__ void __launch_bounds__(kVecThreads) cg_update_kernel(float* x, float*
     double trz = final_sum<kVecThreads>(red, site, 0, sred);
     double trr = final_sum<kVecThreads>(red, site, 1, sred);
     if (threadIdx.x == 0) {
-      cg->beta = trz / cg->rz;
-      cg->rz = trz;
+      if (jac) {
+        cg->beta = trz / cg->rz;
+        cg->rz = trz;
+      }
       cg->rr = trr;
       cg->iter += 1;
-      if (!isfinite(trr) || !isfinite(trz)) {
+      if (!isfinite(trr) || (jac && !isfinite(trz))) {
         cg->done = 3;
         cg->status = 3;
       } else if (trr <= cg->tol2) {
@@ -493,18 +579,17 @@ __global__ void __launch_bounds__(kVecThreads) cg_update_kernel(float* x, float*
 __global__ void __launch_bounds__(kVecThreads) cg_pupdate_kernel(float* p,
                                                                  const float* __restrict__ r,
                                                                  const float* __restrict__ dinv,
-                                                                 int ndof4, const CGState* cg) {
+                                                                 int n_nodes, const CGState* cg) {
   if (cg->done) return;
   const float beta = (float)cg->beta;
   const int i = blockIdx.x * kVecThreads + threadIdx.x;
-  if (i < ndof4) {
+  if (i < n_nodes) {
     float4 pv = reinterpret_cast<float4*>(p)[i];
     const float4 rv = reinterpret_cast<const float4*>(r)[i];
     const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
     pv.x = dv.x * rv.x + beta * pv.x;
     pv.y = dv.y * rv.y + beta * pv.y;
     pv.z = dv.z * rv.z + beta * pv.z;
-    pv.w = dv.w * rv.w + beta * pv.w;
     reinterpret_cast<float4*>(p)[i] = pv;
   }
 }
@@ -630,17 +715,39 @@ __global__ void apply_bc_kernel(double* u, const double* fixed_vals, const uint8
 }
 
 __global__ void u_update_kernel(double* u, const double* u_base, const float* du, double alpha,
-                                int ndof) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ndof) return;
-  u[i] = u_base[i] + alpha * (double)du[i];
-}
-
-__global__ void d2f_masked_kernel(const double* in, float* out, const uint8_t* fixed, int n) {
+                                int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint8_t fx = fixed[i];
-  for (int d = 0; d < 3; ++d) out[3 * i + d] = ((fx >> d) & 1) ? 0.f : (float)in[3 * i + d];
+  const float4 d = reinterpret_cast<const float4*>(du)[i];
+  u[3 * i] = u_base[3 * i] + alpha * (double)d.x;
+  u[3 * i + 1] = u_base[3 * i + 1] + alpha * (double)d.y;
+  u[3 * i + 2] = u_base[3 * i + 2] + alpha * (double)d.z;
+}
+
+// float4-per-node <-> 3-per-node caller layout
+__global__ void gather_f4_kernel(const float* in_user, float* out_int, const int* perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int src = perm[i];
+  reinterpret_cast<float4*>(out_int)[i] =
+      make_float4(in_user[3 * src], in_user[3 * src + 1], in_user[3 * src + 2], 0.f);
+}
+
+template <typename TO>
+__global__ void scatter_f4_kernel(const float* in_int, TO* out_user, const int* perm, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int dst = perm[i];
+  const float4 v = reinterpret_cast<const float4*>(in_int)[i];
+  out_user[3 * dst] = (TO)v.x;
+  out_user[3 * dst + 1] = (TO)v.y;
+  out_user[3 * dst + 2] = (TO)v.z;
+}
+
+__global__ void x32_mask_kernel(float4* X32, const uint8_t* fixed, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  X32[i].w = (float)fixed[i];
 }
 
 __global__ void gather3_masked_kernel(const double* in_user, double* out_int, const int* perm,
@@ -656,7 +763,8 @@ __global__ void dinv_identity_kernel(float* dinv, const uint8_t* fixed, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint8_t fx = fixed[i];
-  for (int d = 0; d < 3; ++d) dinv[3 * i + d] = ((fx >> d) & 1) ? 0.f : 1.f;
+  reinterpret_cast<float4*>(dinv)[i] =
+      make_float4((fx & 1) ? 0.f : 1.f, (fx & 2) ? 0.f : 1.f, (fx & 4) ? 0.f : 1.f, 0.f);
 }
 
 __global__ void __launch_bounds__(256) bc_delta_kernel(const double* u, const double* fixed_vals,
@@ -668,11 +776,13 @@ __global__ void __launch_bounds__(256) bc_delta_kernel(const double* u, const do
   double acc = 0.0;
   if (i < n) {
     const uint8_t fx = fixed[i];
+    float dv[3];
     for (int d = 0; d < 3; ++d) {
       const double v = ((fx >> d) & 1) ? fixed_vals[3 * i + d] - u[3 * i + d] : 0.0;
-      dc[3 * i + d] = (float)v;
+      dv[d] = (float)v;
       acc += v * v;
     }
+    reinterpret_cast<float4*>(dc)[i] = make_float4(dv[0], dv[1], dv[2], 0.f);
   }
   double bsum = block_sum<256>(acc, sred);
   if (publish_partial(red, site, 1, &bsum, &am_last)) {
@@ -689,19 +799,32 @@ __global__ void rhs_minus_kernel(const double* R, const float* y, const uint8_t*
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint8_t fx = fixed[i];
-  for (int d = 0; d < 3; ++d)
-    out[3 * i + d] = ((fx >> d) & 1) ? 0.0 : R[3 * i + d] - (double)y[3 * i + d];
+  const float4 yv = reinterpret_cast<const float4*>(y)[i];
+  const float ys[3] = {yv.x, yv.y, yv.z};
+  for (int d = 0; d < 3; ++d) out[3 * i + d] = ((fx >> d) & 1) ? 0.0 : R[3 * i + d] - (double)ys[d];
 }
 
 // ───────────────────────── launchers ─────────────────────────
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
 
+// Raises a kernel's dynamic shared-memory limit to what the launch needs (the
+// default limit counts static + dynamic shared memory).  Skipped while the
+// stream is being captured: prepare_kernels sets the limit beforehand.
+template <typename K>
+static void allow_smem(K kernel, size_t smem, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cs);
+  if (cs != cudaStreamCaptureStatusNone) return;
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+static size_t slots_smem(const MeshDev& m) { return sizeof(uint32_t) * (size_t)m.max_slots; }
+
 template <int NB, int MODEL>
 static void residual_go(const ResArgs& a, cudaStream_t s) {
-  const size_t smem = sizeof(double) * 12 * NB;
-  cudaFuncSetAttribute(residual_kernel<NB, MODEL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
+  const size_t smem = sizeof(double) * 12 * NB + slots_smem(a.m);
+  allow_smem(residual_kernel<NB, MODEL>, smem, s);
   residual_kernel<NB, MODEL><<<a.m.n_blocks, NB, smem, s>>>(a);
 }
 
@@ -726,22 +849,47 @@ void launch_residual(const ResArgs& a, int model, cudaStream_t s) {
   }
 }
 
+template <int NB, int MODEL, bool CG>
+static void matvec_go(const MvArgs& a, cudaStream_t s) {
+  const size_t smem = slots_smem(a.m);
+  allow_smem(matvec_kernel<NB, MODEL, CG>, smem, s);
+  matvec_kernel<NB, MODEL, CG><<<a.m.n_blocks, NB, smem, s>>>(a);
+}
+
 template <int NB, bool CG>
 static void matvec_nb(const MvArgs& a, int model, cudaStream_t s) {
-  dim3 grid(a.m.n_blocks);
   switch (model) {
-    case M_LE: matvec_kernel<NB, M_LE, CG><<<grid, NB, 0, s>>>(a); break;
-    case M_NH: matvec_kernel<NB, M_NH, CG><<<grid, NB, 0, s>>>(a); break;
-    case M_MR: matvec_kernel<NB, M_MR, CG><<<grid, NB, 0, s>>>(a); break;
-    case M_J2: matvec_kernel<NB, M_J2, CG><<<grid, NB, 0, s>>>(a); break;
-    case M_TI: matvec_kernel<NB, M_TI, CG><<<grid, NB, 0, s>>>(a); break;
-    case M_FMR: matvec_kernel<NB, M_FMR, CG><<<grid, NB, 0, s>>>(a); break;
-    default: matvec_kernel<NB, -1, CG><<<grid, NB, 0, s>>>(a); break;
+    case M_LE: matvec_go<NB, M_LE, CG>(a, s); break;
+    case M_NH: matvec_go<NB, M_NH, CG>(a, s); break;
+    case M_MR: matvec_go<NB, M_MR, CG>(a, s); break;
+    case M_J2: matvec_go<NB, M_J2, CG>(a, s); break;
+    case M_TI: matvec_go<NB, M_TI, CG>(a, s); break;
+    case M_FMR: matvec_go<NB, M_FMR, CG>(a, s); break;
+    default: matvec_go<NB, -1, CG>(a, s); break;
   }
+}
+
+template <bool CG>
+static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
+  const int ge = nblk(a.m.n_elems, 256);
+  switch (model) {
+    case M_LE: elem_mv_kernel<M_LE, CG><<<ge, 256, 0, s>>>(a); break;
+    case M_NH: elem_mv_kernel<M_NH, CG><<<ge, 256, 0, s>>>(a); break;
+    case M_MR: elem_mv_kernel<M_MR, CG><<<ge, 256, 0, s>>>(a); break;
+    case M_J2: elem_mv_kernel<M_J2, CG><<<ge, 256, 0, s>>>(a); break;
+    case M_TI: elem_mv_kernel<M_TI, CG><<<ge, 256, 0, s>>>(a); break;
+    case M_FMR: elem_mv_kernel<M_FMR, CG><<<ge, 256, 0, s>>>(a); break;
+    default: elem_mv_kernel<-1, CG><<<ge, 256, 0, s>>>(a); break;
+  }
+  node_gather_kernel<CG><<<nblk(a.m.n_nodes, 256), 256, 0, s>>>(a);
 }
 
 void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
   const bool cg = a.cg != nullptr;
+  if (a.variant == MV_TWO_PHASE) {
+    cg ? two_phase<true>(a, model, s) : two_phase<false>(a, model, s);
+    return;
+  }
   switch (a.m.nb) {
     case 128: cg ? matvec_nb<128, true>(a, model, s) : matvec_nb<128, false>(a, model, s); break;
     case 512: cg ? matvec_nb<512, true>(a, model, s) : matvec_nb<512, false>(a, model, s); break;
@@ -750,16 +898,44 @@ void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
 }
 
 template <int NB>
-static void diag_nb(const DiagArgs& a, int model, cudaStream_t s) {
-  dim3 grid(a.m.n_blocks);
+static void prepare_nb(int model, size_t smem) {
+  auto set = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); };
   switch (model) {
-    case M_LE: diag_kernel<NB, M_LE><<<grid, NB, 0, s>>>(a); break;
-    case M_NH: diag_kernel<NB, M_NH><<<grid, NB, 0, s>>>(a); break;
-    case M_MR: diag_kernel<NB, M_MR><<<grid, NB, 0, s>>>(a); break;
-    case M_J2: diag_kernel<NB, M_J2><<<grid, NB, 0, s>>>(a); break;
-    case M_TI: diag_kernel<NB, M_TI><<<grid, NB, 0, s>>>(a); break;
-    case M_FMR: diag_kernel<NB, M_FMR><<<grid, NB, 0, s>>>(a); break;
-    default: diag_kernel<NB, -1><<<grid, NB, 0, s>>>(a); break;
+    case M_LE: set(matvec_kernel<NB, M_LE, true>); break;
+    case M_NH: set(matvec_kernel<NB, M_NH, true>); break;
+    case M_MR: set(matvec_kernel<NB, M_MR, true>); break;
+    case M_J2: set(matvec_kernel<NB, M_J2, true>); break;
+    case M_TI: set(matvec_kernel<NB, M_TI, true>); break;
+    case M_FMR: set(matvec_kernel<NB, M_FMR, true>); break;
+    default: set(matvec_kernel<NB, -1, true>); break;
+  }
+}
+
+void prepare_kernels(const MeshDev& m, int model) {
+  switch (m.nb) {
+    case 128: prepare_nb<128>(model, slots_smem(m)); break;
+    case 512: prepare_nb<512>(model, slots_smem(m)); break;
+    default: prepare_nb<256>(model, slots_smem(m)); break;
+  }
+}
+
+template <int NB, int MODEL>
+static void diag_go(const DiagArgs& a, cudaStream_t s) {
+  const size_t smem = slots_smem(a.m);
+  allow_smem(diag_kernel<NB, MODEL>, smem, s);
+  diag_kernel<NB, MODEL><<<a.m.n_blocks, NB, smem, s>>>(a);
+}
+
+template <int NB>
+static void diag_nb(const DiagArgs& a, int model, cudaStream_t s) {
+  switch (model) {
+    case M_LE: diag_go<NB, M_LE>(a, s); break;
+    case M_NH: diag_go<NB, M_NH>(a, s); break;
+    case M_MR: diag_go<NB, M_MR>(a, s); break;
+    case M_J2: diag_go<NB, M_J2>(a, s); break;
+    case M_TI: diag_go<NB, M_TI>(a, s); break;
+    case M_FMR: diag_go<NB, M_FMR>(a, s); break;
+    default: diag_go<NB, -1>(a, s); break;
   }
 }
 
@@ -771,21 +947,24 @@ void launch_diag(const DiagArgs& a, int model, cudaStream_t s) {
   }
 }
 
-void launch_cg_init(const double* b, float* r, float* x, float* p, const float* dinv, int ndof4,
-                    CGState* cg, double rtol, int maxit, Reduce red, int site, cudaStream_t s) {
-  cg_init_kernel<<<nblk(ndof4, kVecThreads), kVecThreads, 0, s>>>(b, r, x, p, dinv, ndof4, cg,
-                                                                  rtol, maxit, red, site);
+void launch_cg_init(const double* b, float* r, float* x, float* p, const float* dinv, int n_nodes,
+                    CGState* cg, double rtol, int maxit, Reduce red, int site, cudaStream_t s,
+                    int precond_in_update) {
+  cg_init_kernel<<<nblk(n_nodes, kVecThreads), kVecThreads, 0, s>>>(b, r, x, p, dinv, n_nodes, cg,
+                                                                    rtol, maxit, red, site,
+                                                                    precond_in_update);
 }
 
 void launch_cg_update(float* x, float* r, const float* p, const float* y, const float* dinv,
-                      int ndof4, CGState* cg, Reduce red, int site, cudaStream_t s) {
-  cg_update_kernel<<<nblk(ndof4, kVecThreads), kVecThreads, 0, s>>>(x, r, p, y, dinv, ndof4, cg,
-                                                                    red, site);
+                      int n_nodes, CGState* cg, Reduce red, int site, cudaStream_t s,
+                      int precond_in_update) {
+  cg_update_kernel<<<nblk(n_nodes, kVecThreads), kVecThreads, 0, s>>>(x, r, p, y, dinv, n_nodes, cg,
+                                                                    red, site, precond_in_update);
 }
 
-void launch_cg_pupdate(float* p, const float* r, const float* dinv, int ndof4, CGState* cg,
+void launch_cg_pupdate(float* p, const float* r, const float* dinv, int n_nodes, CGState* cg,
                        cudaStream_t s) {
-  cg_pupdate_kernel<<<nblk(ndof4, kVecThreads), kVecThreads, 0, s>>>(p, r, dinv, ndof4, cg);
+  cg_pupdate_kernel<<<nblk(n_nodes, kVecThreads), kVecThreads, 0, s>>>(p, r, dinv, n_nodes, cg);
 }
 
 void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
@@ -815,15 +994,18 @@ void launch_scatter_d(const double* in_int, double* out_user, const int* perm, i
 }
 void launch_gather_f(const float* in_user, float* out_int, const int* perm, int n,
                      cudaStream_t s) {
-  gather3_kernel<float, float><<<nblk(n, 256), 256, 0, s>>>(in_user, out_int, perm, n);
+  gather_f4_kernel<<<nblk(n, 256), 256, 0, s>>>(in_user, out_int, perm, n);
 }
 void launch_scatter_f(const float* in_int, float* out_user, const int* perm, int n,
                       cudaStream_t s) {
-  scatter3_kernel<float, float><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
+  scatter_f4_kernel<float><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
 }
 void launch_scatter_f2d(const float* in_int, double* out_user, const int* perm, int n,
                         cudaStream_t s) {
-  scatter3_kernel<float, double><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
+  scatter_f4_kernel<double><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
+}
+void launch_x32_mask(float4* X32, const uint8_t* fixed, int n, cudaStream_t s) {
+  x32_mask_kernel<<<nblk(n, 256), 256, 0, s>>>(X32, fixed, n);
 }
 void launch_gather_mask(const uint8_t* in_user, uint8_t* out_int, const int* perm, int n,
                         cudaStream_t s) {
@@ -833,9 +1015,9 @@ void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, 
                      cudaStream_t s) {
   apply_bc_kernel<<<nblk(n, 256), 256, 0, s>>>(u, fixed_vals, fixed, n);
 }
-void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int ndof,
+void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int n,
                      cudaStream_t s) {
-  u_update_kernel<<<nblk(ndof, 256), 256, 0, s>>>(u, u_base, du, alpha, ndof);
+  u_update_kernel<<<nblk(n, 256), 256, 0, s>>>(u, u_base, du, alpha, n);
 }
 void launch_gather_d_masked(const double* in_user, double* out_int, const int* perm,
                             const uint8_t* fixed, int n, cudaStream_t s) {
@@ -851,10 +1033,6 @@ void launch_bc_delta(const double* u, const double* fixed_vals, const uint8_t* f
 void launch_rhs_minus(const double* R, const float* y, const uint8_t* fixed, double* out, int n,
                       cudaStream_t s) {
   rhs_minus_kernel<<<nblk(n, 256), 256, 0, s>>>(R, y, fixed, out, n);
-}
-void launch_d2f_masked(const double* in, float* out, const uint8_t* fixed, int n,
-                       cudaStream_t s) {
-  d2f_masked_kernel<<<nblk(n, 256), 256, 0, s>>>(in, out, fixed, n);
 }
 
 }  // namespace femb200

@@ -146,9 +146,33 @@ class FEMesh:
                 "block_element_entries": out[3], "nodes_per_block": out[4], "device_bytes": out[5]}
 
     def stats(self) -> dict:
-        out = (C.c_int64 * 4)()
+        out = (C.c_int64 * 8)()
         _check(_lib.load().fem_ctx_stats(self.ctx, out), self.ctx, "fem_ctx_stats")
-        return {"launches": out[0], "cg_iterations": out[1], "residual_evals": out[2], "cg_graphs": out[3]}
+        return {"launches": out[0], "cg_iterations": out[1], "residual_evals": out[2], "cg_graphs": out[3],
+                "matvec_variant": _lib.MATVEC_VARIANTS.get(out[4], str(out[4])),
+                "matvec_ns": {"fused": out[5], "two_phase": out[6]}, "matvec_tuned": bool(out[7])}
+
+    def coarse_info(self) -> dict:
+        out = (C.c_double * 6)()
+        _check(_lib.load().fem_coarse_info(self.ctx, out), self.ctx, "fem_coarse_info")
+        return {"cells": int(out[0]), "coarse_nodes": int(out[1]), "coarse_dofs": int(out[2]),
+                "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5]}
+
+    def set_coarse_options(self, cell=None, reuse=None):
+        """Two-level preconditioner: lattice cell edge in mesh lengths and the
+        number of PCG solves one coarse assembly serves."""
+        lib = _lib.load()
+        if cell is not None:
+            _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_CELL, int(cell)), self.ctx, "fem_set_option")
+        if reuse is not None:
+            _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_REUSE, int(reuse)), self.ctx, "fem_set_option")
+
+    def set_matvec_variant(self, variant):
+        """Forces the tangent-matvec variant ("fused", "two_phase") or restores
+        the timed choice (None)."""
+        code = {None: -1, "fused": 0, "two_phase": 1}[variant]
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_MATVEC_VARIANT, code), self.ctx,
+               "fem_set_option")
 
     # ---- boundary conditions (core/mesh.py:321-399) ----
     def set_fixed_nodes(self, node_ids, values=None, dofs=None):
@@ -576,7 +600,8 @@ class TransverseIsotropic(MaterialBase):
 # ───────────────────────── solver ─────────────────────────
 
 _LS = {"reference": _lib.FEM_LS_REFERENCE, "guarded": _lib.FEM_LS_GUARDED, "none": _lib.FEM_LS_NONE}
-_PC = {"jacobi": _lib.FEM_PRECOND_JACOBI, "none": _lib.FEM_PRECOND_NONE}
+_PC = {"jacobi": _lib.FEM_PRECOND_JACOBI, "none": _lib.FEM_PRECOND_NONE,
+       "two_level": _lib.FEM_PRECOND_TWO_LEVEL}
 
 
 class StaticSolver:

@@ -1,0 +1,63 @@
+"""Small, self-terminating workload for kernel profiling (ncu) and timing.
+
+Builds the synthetic vertebral body at ``--n`` voxels per axis, binds J2
+plasticity, evaluates the FP64 residual at a plastic state (top face pushed
+``--strain`` of the height, which yields the cortical shell), and launches each
+hot kernel ``--reps`` times through ``fem_profile_kernels``: the tangent matvec
+(the variant given by ``--variant``), the FP64 residual, the CG update and the
+CG direction update.  The per-launch CUDA-event times are printed as one JSON
+line.  With ``--reps 3`` and ``-k``/``-c`` filters an ncu capture of one kernel
+ends in seconds.
+
+    python -m simul_b200.profile_case --n 64 --variant fused --reps 3
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+
+import numpy as np
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--variant", default="fused", choices=["fused", "two_phase"])
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--strain", type=float, default=0.004)
+    ap.add_argument("--nodes-per-block", type=int, default=0)
+    args = ap.parse_args(argv)
+
+    import torch
+
+    from simul_b200 import _lib, meshgen
+    from simul_b200 import fem as B
+
+    v = meshgen.vertebral_body(n=args.n, seed=0)
+    mesh = B.FEMesh(v.n_nodes, v.n_elements, device=0, nodes_per_block=args.nodes_per_block)
+    mesh.initialize_from_numpy(v.X, v.conn)
+    mesh.set_matvec_variant(args.variant)
+    mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
+    idx = np.where(v.fixed_mask.reshape(-1))[0]
+    vals = (v.fixed_vals * (args.strain / 0.02)).reshape(-1)
+    mesh.set_fixed_dofs(idx, vals[idx])
+    # a smooth compression field with the prescribed values on the boundary
+    top = v.X[:, 2].max()
+    u = np.zeros_like(v.X)
+    u[:, 2] = -args.strain * v.X[:, 2] * (top / max(top, 1e-30))
+    mesh.u.copy_(torch.from_numpy(u))
+    mat.compute_nodal_forces(mesh)
+    ms = (C.c_double * 4)()
+    rc = _lib.load().fem_profile_kernels(mesh.ctx, args.reps, ms)
+    if rc != 0:
+        raise RuntimeError(_lib.last_error(mesh.ctx))
+    torch.cuda.synchronize()
+    info = mesh.info()
+    print(json.dumps({"n": args.n, "tets": info["n_elements"], "nodes": info["n_nodes"],
+                      "variant": args.variant, "reps": args.reps,
+                      "ms": {"matvec": ms[0], "residual": ms[1], "cg_update": ms[2], "cg_direction": ms[3]}}))
+
+
+if __name__ == "__main__":
+    main()

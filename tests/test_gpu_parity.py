@@ -96,10 +96,15 @@ def test_element_forces_and_stress(cuda, bar, key, nb):
         assert _rel_max(mesh.F.cpu().numpy(), ref["F"]) < 1e-12
 
 
+VARIANTS = ["fused", "two_phase"]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("key", ["nh", "mr", "fmr", "le", "ti"])
-def test_tangent_matvec(cuda, bar, key):
+def test_tangent_matvec(cuda, bar, key, variant):
     ref = np.load(G.path_of(f"bar_{key}_forces"))
     mesh = make_mesh(bar.X, bar.conn, cuda)
+    mesh.set_matvec_variant(variant)
     mat = make_material(key)
     mesh.u.copy_(dev(ref["u"], cuda))
     mat.compute_nodal_forces(mesh)          # refreshes the tangent state
@@ -139,9 +144,11 @@ def test_j2_forces_history_and_tangent(cuda, vox):
     assert np.all(mat.get_plastic_strain() == 0)
 
 
-def test_forces_bitwise_deterministic(cuda, vox):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_forces_bitwise_deterministic(cuda, vox, variant):
     ref = np.load(G.path_of("vox12_j2_forces"))
     mesh = make_mesh(vox.X, vox.conn, cuda)
+    mesh.set_matvec_variant(variant)
     mat = make_material("j2", E=vox.E)
     mesh.u.copy_(dev(ref["u"], cuda))
     outs, ys = [], []
@@ -182,6 +189,60 @@ def test_pcg_solves_tangent_system(cuda, bar):
     assert rc == 0 and it2.value > 0
 
 
+def test_two_level_pcg_matches_oracle_with_fewer_iterations(cuda, vox):
+    """Jacobi + trilinear Galerkin coarse correction: same solution as the
+    FP64 oracle, fewer CG iterations than Jacobi alone."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    mesh.set_coarse_options(cell=4)         # 3x3x3 cells on this 12^3-voxel body
+    lib = _lib.load()
+    rng = np.random.default_rng(5)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    r = dev(rhs, cuda)
+    its = {}
+    sols = {}
+    for name, pc in (("jacobi", _lib.FEM_PRECOND_JACOBI), ("two_level", _lib.FEM_PRECOND_TWO_LEVEL)):
+        du = torch.zeros_like(r)
+        it = C.c_int32()
+        rel = C.c_double()
+        rc = lib.fem_pcg(mesh.ctx, pc, ptr(r), ptr(du), 1e-7, 20000, C.byref(it), C.byref(rel))
+        assert rc == 0, _lib.last_error(mesh.ctx)
+        assert rel.value <= 1e-7
+        its[name] = it.value
+        sols[name] = du.cpu().numpy()
+    info = mesh.coarse_info()
+    assert info["assemblies"] == 1 and info["coarse_dofs"] > 0
+    assert its["two_level"] < its["jacobi"] / 2, its
+    # FP64 oracle: K_ff du = rhs_f by a direct solve of the assembled tangent
+    m = O.Mesh(vox.X, vox.conn)
+    mo = O.Material("linear_elastic", E=1e3, nu=0.3)
+    F = O.deformation_gradient(np.zeros_like(vox.X), vox.conn.astype(np.int64), m.dNdX)
+    u_ref = O.solve_tangent(mo, F, None, m, rhs, vox.fixed_mask)
+    for name in sols:
+        assert _rel_l2(sols[name], u_ref) < 1e-5, name
+
+
+def test_newton_j2_two_level_matches_oracle(cuda, vox):
+    ref = np.load(G.path_of("vox12_j2_steps"))
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = make_material("j2", E=vox.E)
+    lf = float(ref["load_factor"])
+    total = int(ref["n_total"])
+    solver = B.StaticSolver(mesh, mat, tol=1e-10, precond="two_level")
+    for k in range(ref["u_steps"].shape[0]):
+        vals = vox.fixed_vals * (k + 1) / total * lf
+        idx = np.where(vox.fixed_mask.reshape(-1))[0]
+        mesh.set_fixed_dofs(idx, vals.reshape(-1)[idx])
+        res = solver.solve(verbose=False)
+        assert res["converged"], res
+        assert _rel_l2(mesh.get_displacements(), ref["u_steps"][k]) < 1e-6
+    assert mesh.coarse_info()["assemblies"] >= ref["u_steps"].shape[0]
+
+
 def test_newton_bar_matches_oracle(cuda, bar):
     ref = np.load(G.path_of("bar_nh_steps"))
     mesh = make_mesh(bar.X, bar.conn, cuda)
@@ -195,9 +256,11 @@ def test_newton_bar_matches_oracle(cuda, bar):
         assert _rel_l2(mesh.get_displacements(), ref["u_steps"][k]) < 1e-6
 
 
-def test_newton_j2_steps_match_oracle(cuda, vox):
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_newton_j2_steps_match_oracle(cuda, vox, variant):
     ref = np.load(G.path_of("vox12_j2_steps"))
     mesh = make_mesh(vox.X, vox.conn, cuda)
+    mesh.set_matvec_variant(variant)
     mat = make_material("j2", E=vox.E)
     lf = float(ref["load_factor"])
     total = int(ref["n_total"])
@@ -212,6 +275,38 @@ def test_newton_j2_steps_match_oracle(cuda, vox):
         epe_ref = ref["epe_steps"][k]
         assert np.max(np.abs(mat.get_plastic_strain() - epe_ref)) <= 1e-6 * max(epe_ref.max(), 1e-12) + 1e-12
     assert ref["epe_steps"][-1].max() > 0
+
+
+def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
+    ref = np.load(G.path_of("vox12_j2_forces"))
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = make_material("j2", E=vox.E)
+    mesh.u.copy_(dev(ref["u"], cuda))
+    mat.compute_nodal_forces(mesh)
+    x = dev(ref["p"], cuda, torch.float32)
+    ys = {}
+    for v in VARIANTS:
+        mesh.set_matvec_variant(v)
+        y = torch.empty_like(x)
+        assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0
+        ys[v] = y.cpu().numpy().astype(np.float64)
+    # both sum each node's slot vectors in the same order; only FMA contraction may differ
+    assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-6
+    # automatic choice: the first PCG solve times both variants and keeps the faster
+    mesh.set_matvec_variant(None)
+    mesh.u.zero_()
+    mat.reset_state()
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, (vox.fixed_vals * 0.01).reshape(-1)[idx])
+    res = B.StaticSolver(mesh, mat, tol=1e-8).solve(verbose=False)
+    assert res["converged"], res
+    st = mesh.stats()
+    assert st["matvec_tuned"]
+    assert st["matvec_ns"]["fused"] > 0 and st["matvec_ns"]["two_phase"] > 0
+    faster = min(st["matvec_ns"], key=st["matvec_ns"].get)
+    assert st["matvec_variant"] == faster
+    assert _lib.load().fem_set_option(mesh.ctx, _lib.FEM_OPT_MATVEC_VARIANT, 7) == _lib.FEM_ERR_INVALID
+    assert "matvec variant" in _lib.last_error(mesh.ctx)
 
 
 def test_reference_line_search_policy_converges(cuda, bar):

@@ -50,9 +50,15 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-threads", type=int, default=0)
-    ap.add_argument("--precond", default="two_level", choices=["jacobi", "two_level"],
+    ap.add_argument("--precond", default="two_level", choices=["jacobi", "two_level", "learned"],
                     help="preconditioner of the timed solve; Jacobi-PCG is timed beside it")
+    ap.add_argument("--weights", default=os.path.join(ROOT, "simul_b200", "weights", "mpnn_vertebra.npz"),
+                    help="learned-preconditioner weights (simul_b200.train_precond)")
+    ap.add_argument("--learned-coarse", type=int, default=1, help="learned: add the coarse correction")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
+    ap.add_argument("--coarse-reuse", type=int, default=1,
+                    help="PCG solves one coarse-operator assembly serves (two-level / learned)")
+    ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
     return ap.parse_args()
 
 
@@ -150,6 +156,16 @@ def measured_peaks():
     return 6650.0, "of fallback"
 
 
+def learned_info(mesh, args):
+    import ctypes as C
+    from simul_b200 import _lib
+    st = (C.c_int64 * 2)()
+    _lib.load().fem_learned_stats(mesh.ctx, st)
+    return {"weights": os.path.relpath(args.weights, ROOT), "coarse_correction": bool(args.learned_coarse),
+            "fallbacks_to_jacobi_pcg": int(st[0]),
+            "network": "4-layer message passing, width 64, BF16 tcgen05 dense layers, FP32 accumulation"}
+
+
 def build_inputs(args):
     from simul_b200 import meshgen
     return meshgen.vertebral_body(n=args.n, seed=0)
@@ -232,6 +248,11 @@ def main():
     mesh.initialize_from_numpy(v.X, v.conn)
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond)
+    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse)
+    if args.precond == "learned":
+        from simul_b200 import learned
+        learned.set_weights(mesh, learned.load(args.weights))
+        learned.set_coarse(mesh, bool(args.learned_coarse))
     fixed_full = torch.from_numpy(v.fixed_vals).to(dev)
     fixed_mask = torch.from_numpy(v.fixed_mask.astype(np.int32)).to(dev)
     stream = torch.cuda.current_stream(dev)
@@ -357,8 +378,12 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 matvec / f64 residual+dots",
             "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),
-            "method": f"{args.precond}_pcg", "learned_fpcg_s": None, "jacobi_pcg": jac,
-            "coarse": mesh.coarse_info() if args.precond == "two_level" else None,
+            "method": ("learned_fpcg" if args.precond == "learned" else f"{args.precond}_pcg"),
+            "learned_fpcg_s": (ms / 1e3) if args.precond == "learned" else None,
+            "learned": (learned_info(mesh, args) if args.precond == "learned" else None),
+            "jacobi_pcg": jac,
+            "coarse": ({**mesh.coarse_info(), "reuse": args.coarse_reuse}
+                       if args.precond in ("two_level", "learned") else None),
             "solve": {"newton_iterations": last["newton"], "cg_iterations": last["cg"],
                       "all_converged": bool(last["converged"]), "max_relative_residual": last["max_rel"],
                       "cg_ms_per_iteration": (ms / last["cg"]) if last["cg"] else None},

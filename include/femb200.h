@@ -175,6 +175,39 @@ int fem_mpnn_forward(void* ctx, const float* r, float* z);
 /* out[0] flexible solves that fell back to Jacobi-based PCG, out[1] 1 if
  * weights are set */
 int fem_learned_stats(void* ctx, int64_t* out2);
+/* grad (host, 34,307 FP32) = d<gz, M(r)>/dw at the current tangent; r, gz:
+ * caller order, N x 3 FP32 device arrays (network only, no coarse part) */
+int fem_mpnn_backward(void* ctx, const float* r, const float* gz, float* grad);
+
+/* Training on (residual, correction) pairs the plain solver produced at this
+ * context's current tangent: R, E device arrays [n_pairs][N][3] FP32 in
+ * caller order, K_ff E_k ~ R_k.  Loss per pair (the preconditioner's A-norm
+ * error, 1 for z = 0): (z.Kz - 2 z.r + e.r) / e.r with z = M(r) (+ coarse
+ * when FEM_OPT_LEARNED_COARSE is set).  Adam (beta 0.9 / 0.999), gradients
+ * averaged over `batch` pairs, forward and backward on the GPU. */
+typedef struct {
+  int32_t steps;
+  int32_t batch;
+  double lr;
+  int32_t seed;              /* sample order */
+  int32_t reset_optimizer;   /* 1: zero the Adam moments first */
+  int32_t (*progress)(void* user, int32_t step, double loss, double unused);
+  void* progress_user;
+} FemTrainParams;
+
+typedef struct {
+  int32_t steps_done;
+  double loss_first;         /* mean loss of the first steps (up to 16) */
+  double loss_last;          /* mean loss of the last steps */
+} FemTrainResult;
+
+int fem_mpnn_train(void* ctx, const float* R, const float* E, int32_t n_pairs, const FemTrainParams* prm,
+                   FemTrainResult* res);
+/* mean loss over the pairs for the network (loss_net) and for the same
+ * preconditioner with the network's output zeroed, i.e. Jacobi (+ coarse)
+ * (loss_base) */
+int fem_mpnn_eval(void* ctx, const float* R, const float* E, int32_t n_pairs, double* loss_net,
+                  double* loss_base);
 
 /* Known-answer check of the tensor-core path the learned preconditioner uses
  * (no reference counterpart): D (128 x N, FP32) = A (128 x K) B^T (B: N x K),
@@ -183,8 +216,9 @@ int fem_learned_stats(void* ctx, int64_t* out2);
 int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t K, void* stream);
 /* two-level preconditioner state: out[0] lattice cells, [1] coarse nodes,
  * [2] coarse DOFs, [3] cell edge, [4] assemblies so far, [5] ms of the last
- * assembly + factorisation (CUDA events) */
-int fem_coarse_info(void* ctx, double* out6);
+ * assembly + factorisation (CUDA events), [6] ms of its assembly part,
+ * [7] PCG solves one assembly serves */
+int fem_coarse_info(void* ctx, double* out8);
 /* cudaStream_t of the context (as void*) */
 void* fem_ctx_stream(void* ctx);
 

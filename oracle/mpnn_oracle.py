@@ -228,8 +228,8 @@ def fpcg(apply_A, precond, b, rtol, maxit):
             return x, it
         z = precond(r)
         rz_new = float(np.sum(r * z))
-        # r_new - r_old = -alpha q  =>  z.(r_new - r_old) = -alpha z.q
-        beta = (rz_new - alpha * float(np.sum(z * q))) / rz
+        # Polak-Ribiere: beta = z.(r_new - r_old) / rz_old, and r_new - r_old = -alpha q
+        beta = -alpha * float(np.sum(z * q)) / rz
         p = z + beta * p
         rz = rz_new
     return x, maxit

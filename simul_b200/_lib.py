@@ -71,6 +71,15 @@ class FemSolveParams(C.Structure):
                 ("progress_user", C.c_void_p)]
 
 
+class FemTrainParams(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("lr", C.c_double), ("seed", C.c_int32),
+                ("reset_optimizer", C.c_int32), ("progress", PROGRESS_FN), ("progress_user", C.c_void_p)]
+
+
+class FemTrainResult(C.Structure):
+    _fields_ = [("steps_done", C.c_int32), ("loss_first", C.c_double), ("loss_last", C.c_double)]
+
+
 class FemSolveResult(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32),
                 ("residual", C.c_double), ("relative_residual", C.c_double),
@@ -95,6 +104,10 @@ SIGNATURES = {
     "fem_mpnn_get_weights": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int64]),
     "fem_mpnn_forward": (C.c_int, [_VP, _VP, _VP]),
     "fem_learned_stats": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
+    "fem_mpnn_backward": (C.c_int, [_VP, _VP, _VP, C.POINTER(C.c_float)]),
+    "fem_mpnn_train": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.POINTER(FemTrainParams),
+                                 C.POINTER(FemTrainResult)]),
+    "fem_mpnn_eval": (C.c_int, [_VP, _VP, _VP, C.c_int32, _DP, _DP]),
     "fem_set_materials": (C.c_int, [_VP, C.POINTER(FemMaterial), C.c_int32, _VP, _VP]),
     "fem_set_bc": (C.c_int, [_VP, _VP, _VP, _VP]),
     "fem_apply_bc": (C.c_int, [_VP]),

@@ -64,6 +64,9 @@ __device__ __forceinline__ float block_sum_f(float v, float* sh) {
 constexpr int kCellThreads = 128;
 constexpr int kCellEntries = 576;  // (8 corners x 3)^2
 constexpr int kCellOwned = (kCellEntries + kCellThreads - 1) / kCellThreads;
+// CTAs per cell: slice s takes chunks s, s + kCellSlices, ... of the cell's
+// elements; the dense kernel adds the slices in order
+constexpr int kCellSlices = 8;
 
 template <int MODEL>
 __global__ void __launch_bounds__(kCellThreads) coarse_cell_kernel(const __grid_constant__ CoarseArgs a) {
@@ -72,14 +75,14 @@ __global__ void __launch_bounds__(kCellThreads) coarse_cell_kernel(const __grid_
   float* sW = s_cell + kCellThreads * 144;           // [kCellThreads][32]
   const MeshDev& m = a.m;
   const CoarseDev& c = a.c;
-  const int cell = blockIdx.x;
+  const int cell = blockIdx.x / kCellSlices, slice = blockIdx.x - cell * kCellSlices;
   const int tid = threadIdx.x;
   const int3 ijk = c.cell_ijk[cell];
   const int e0 = c.cell_elem_ptr[cell], e1 = c.cell_elem_ptr[cell + 1];
   double acc[kCellOwned];
 #pragma unroll
   for (int k = 0; k < kCellOwned; ++k) acc[k] = 0.0;
-  for (int c0 = e0; c0 < e1; c0 += kCellThreads) {
+  for (int c0 = e0 + slice * kCellThreads; c0 < e1; c0 += kCellSlices * kCellThreads) {
     const int idx = c0 + tid;
     float* K = sK + tid * 144;
     float* W = sW + tid * 32;
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kCellThreads) coarse_cell_kernel(const __grid_
 #pragma unroll
   for (int k = 0; k < kCellOwned; ++k) {
     const int q = tid + k * kCellThreads;
-    if (q < kCellEntries) c.blocks[(size_t)cell * kCellEntries + q] = acc[k];
+    if (q < kCellEntries) c.blocks[(size_t)blockIdx.x * kCellEntries + q] = acc[k];
   }
 }
 
@@ -196,7 +199,11 @@ __global__ void coarse_dense_kernel(const __grid_constant__ CoarseDev c) {
 #pragma unroll
     for (int t = 0; t < 8; ++t)
       if (c.cell_corner[cell * 8 + t] == nJ) cJ = t;
-    if (cJ >= 0) acc += c.blocks[(size_t)cell * kCellEntries + (3 * cI + dI) * 24 + 3 * cJ + dJ];
+    if (cJ >= 0) {
+      const size_t off = (size_t)(3 * cI + dI) * 24 + 3 * cJ + dJ;
+      for (int sl = 0; sl < kCellSlices; ++sl)
+        acc += c.blocks[((size_t)cell * kCellSlices + sl) * kCellEntries + off];
+    }
   }
   if (I == J && !(acc > 0.0)) acc = 1.0;
   c.Ac[q] = acc;
@@ -355,8 +362,8 @@ __global__ void __launch_bounds__(256) tl_pupdate_kernel(float* p, const float* 
 
 // Flexible PCG step around a nonlinear preconditioner output z (already in
 // `z`): optionally z += P yc (coarse correction), then rz = r.z and z.q.
-// INIT: p = z.  Otherwise Polak-Ribiere beta = (r.z - alpha z.q) / rz_old,
-// using r_new - r_old = -alpha q.
+// INIT: p = z.  Otherwise Polak-Ribiere beta = z.(r_new - r_old) / rz_old
+// = -alpha z.q / rz_old, using r_new - r_old = -alpha q.
 template <bool INIT, bool COARSE>
 __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ CoarseArgs a,
                                                         const float* __restrict__ r,
@@ -407,7 +414,7 @@ __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ 
     const double trz = final_sum<256>(red, site, 0, sred);
     const double tzq = final_sum<256>(red, site, 1, sred);
     if (threadIdx.x == 0) {
-      cg->beta = INIT ? 0.0 : (trz - cg->alpha * tzq) / cg->rz;
+      cg->beta = INIT ? 0.0 : -cg->alpha * tzq / cg->rz;
       cg->rz = trz;
       if (!isfinite(trz) || !(trz > 0.0) || !isfinite(cg->beta)) {
         cg->done = 3;
@@ -418,11 +425,100 @@ __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ 
   }
 }
 
+// z += P yc on free DOFs (the coarse part of a composite preconditioner)
+__global__ void __launch_bounds__(256) coarse_add_kernel(const __grid_constant__ CoarseArgs a, float* z) {
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= a.m.n_nodes) return;
+  const CoarseDev& c = a.c;
+  const float4 X = __ldg(a.m.X32 + i);
+  const int cell = __ldg(c.node_cell + i);
+  const int3 ijk = c.cell_ijk[cell];
+  float t[3];
+  cell_local(c, ijk, X.x, X.y, X.z, t);
+  float cz[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int cnode = __ldg(c.cell_corner + cell * 8 + k);
+    const float wk = tri_weight(t[0], t[1], t[2], k);
+    cz[0] += wk * c.yc[3 * cnode];
+    cz[1] += wk * c.yc[3 * cnode + 1];
+    cz[2] += wk * c.yc[3 * cnode + 2];
+  }
+  const int fx = (int)a.m.fixed[i];
+  float4 zv = reinterpret_cast<float4*>(z)[i];
+  zv.x = (fx & 1) ? 0.f : zv.x + cz[0];
+  zv.y = (fx & 2) ? 0.f : zv.y + cz[1];
+  zv.z = (fx & 4) ? 0.f : zv.z + cz[2];
+  reinterpret_cast<float4*>(z)[i] = zv;
+}
+
+// Energy loss of one training pair (r, e) with A e = r:
+//   L = (z.Az - 2 z.r + e.r) / e.r = ||z - e||_A^2 / ||e||_A^2
+// out[0] += L; out[1] = 2 / e.r (scale of dL/dz = 2 (Az - r) / e.r)
+__global__ void __launch_bounds__(256) train_loss_kernel(const float* __restrict__ z, const float* __restrict__ q,
+                                                         const float* __restrict__ r, const float* __restrict__ e,
+                                                         int n, double* out, Reduce red, int site) {
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  double zq = 0.0, zr = 0.0, er = 0.0;
+  if (i < n) {
+    const float4 zv = reinterpret_cast<const float4*>(z)[i];
+    const float4 qv = reinterpret_cast<const float4*>(q)[i];
+    const float4 rv = reinterpret_cast<const float4*>(r)[i];
+    const float4 ev = reinterpret_cast<const float4*>(e)[i];
+    zq = (double)zv.x * qv.x + (double)zv.y * qv.y + (double)zv.z * qv.z;
+    zr = (double)zv.x * rv.x + (double)zv.y * rv.y + (double)zv.z * rv.z;
+    er = (double)ev.x * rv.x + (double)ev.y * rv.y + (double)ev.z * rv.z;
+  }
+  double v[2];
+  v[0] = block_sum<256>(zq - 2.0 * zr, sred);
+  v[1] = block_sum<256>(er, sred);
+  if (publish_partial(red, site, 2, v, &am_last)) {
+    const double a = final_sum<256>(red, site, 0, sred);
+    const double b = final_sum<256>(red, site, 1, sred);
+    if (threadIdx.x == 0) {
+      const bool good = b > 0.0 && isfinite(a) && isfinite(b);
+      out[0] += good ? (a + b) / b : 0.0;
+      out[1] = good ? 2.0 / b : 0.0;
+      red.counters[site] = 0u;
+    }
+  }
+}
+
+// gz = scale (q - r) on free DOFs
+__global__ void __launch_bounds__(256) train_grad_z_kernel(const float* __restrict__ q, const float* __restrict__ r,
+                                                           const uint8_t* __restrict__ fixed, const double* scale,
+                                                           float* gz, int n) {
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= n) return;
+  const float sc = (float)scale[1];
+  const float4 qv = reinterpret_cast<const float4*>(q)[i];
+  const float4 rv = reinterpret_cast<const float4*>(r)[i];
+  const int fx = (int)fixed[i];
+  float4 g;
+  g.x = (fx & 1) ? 0.f : sc * (qv.x - rv.x);
+  g.y = (fx & 2) ? 0.f : sc * (qv.y - rv.y);
+  g.z = (fx & 4) ? 0.f : sc * (qv.z - rv.z);
+  g.w = 0.f;
+  reinterpret_cast<float4*>(gz)[i] = g;
+}
+
+// z = D^-1 r (the network's output with a zero decoder)
+__global__ void jacobi_apply_kernel(const float* __restrict__ r, const float* __restrict__ dinv, float* z, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 rv = reinterpret_cast<const float4*>(r)[i];
+  const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
+  reinterpret_cast<float4*>(z)[i] = make_float4(dv.x * rv.x, dv.y * rv.y, dv.z * rv.z, 0.f);
+}
+
 // ───────────────────────── launchers ─────────────────────────
 
 static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 size_t coarse_cell_smem() { return sizeof(float) * kCellThreads * (144 + 32); }
+int coarse_cell_slices() { return kCellSlices; }
 
 void prepare_coarse_kernels(int model, int n_dof) {
   const int smem = (int)coarse_cell_smem();
@@ -441,7 +537,7 @@ void prepare_coarse_kernels(int model, int n_dof) {
 
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s) {
   const size_t smem = coarse_cell_smem();
-  const int g = a.c.n_cells;
+  const int g = a.c.n_cells * kCellSlices;
   switch (model) {
     case M_LE: coarse_cell_kernel<M_LE><<<g, kCellThreads, smem, s>>>(a); break;
     case M_NH: coarse_cell_kernel<M_NH><<<g, kCellThreads, smem, s>>>(a); break;
@@ -494,6 +590,24 @@ void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* 
 
 void launch_tl_pupdate(float* p, const float* z, int n_nodes, const CGState* cg, cudaStream_t s) {
   tl_pupdate_kernel<<<nblk(n_nodes, 256), 256, 0, s>>>(p, z, n_nodes, cg);
+}
+
+void launch_coarse_add(const CoarseArgs& a, float* z, cudaStream_t s) {
+  coarse_add_kernel<<<nblk(a.m.n_nodes, 256), 256, 0, s>>>(a, z);
+}
+
+void launch_train_loss(const float* z, const float* q, const float* r, const float* e, int n, double* out,
+                       Reduce red, int site, cudaStream_t s) {
+  train_loss_kernel<<<nblk(n, 256), 256, 0, s>>>(z, q, r, e, n, out, red, site);
+}
+
+void launch_train_grad_z(const float* q, const float* r, const uint8_t* fixed, const double* scale, float* gz,
+                         int n, cudaStream_t s) {
+  train_grad_z_kernel<<<nblk(n, 256), 256, 0, s>>>(q, r, fixed, scale, gz, n);
+}
+
+void launch_jacobi_apply(const float* r, const float* dinv, float* z, int n, cudaStream_t s) {
+  jacobi_apply_kernel<<<nblk(n, 256), 256, 0, s>>>(r, dinv, z, n);
 }
 
 }  // namespace femb200

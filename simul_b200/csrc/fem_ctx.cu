@@ -109,6 +109,13 @@ struct FemCtx {
   std::vector<double> elem_modulus;  // internal element order
   int64_t n_fallbacks = 0;
   int* h_err = nullptr;
+  // training state: backward buffers, gradient, Adam moments, per-sample vectors
+  MpnnTrain mtrain{};
+  bool mpnn_train_ready = false;
+  float *grad = nullptr, *adam_m = nullptr, *adam_v = nullptr;
+  int adam_t = 0;
+  float *tr_r = nullptr, *tr_e = nullptr, *tr_z = nullptr, *tr_q = nullptr, *tr_g = nullptr;
+  double* tr_scal = nullptr;  // [0] loss sum, [1] dL/dz scale
 
   // two-level preconditioner: coarse lattice tables (built on first use),
   // dense coarse operator and its inverse, cuSOLVER handle and workspace
@@ -120,7 +127,9 @@ struct FemCtx {
   int coarse_uses = 0;
   double coarse_H = 0.0;
   int64_t n_coarse_assemblies = 0;
+  std::vector<uint8_t> fixed_host;  // last constraint pattern (internal order)
   double coarse_ms_last = 0.0;
+  double coarse_ms_assembly = 0.0;   // of which cell blocks + dense assembly
   std::vector<void*> coarse_bufs;
   cusolverDnHandle_t solver = nullptr;
   double* sol_work = nullptr;
@@ -836,7 +845,7 @@ int build_coarse(FemCtx* c) {
   if ((st = coarse_upload(c, &cd.node_cell, node_cell))) return st;
   if ((st = coarse_upload(c, &cd.cn_cells, cn_cells))) return st;
   const size_t nd = (size_t)cd.n_dof;
-  if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * 576))) return st;
+  if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * coarse_cell_slices() * 576))) return st;
   if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
   if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
   if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * 24))) return st;
@@ -884,6 +893,9 @@ int ensure_coarse(FemCtx* c) {
   launch_coarse_assemble(ca, c->model_kind, c->stream);
   c->n_launches += 2;
   CKL();
+  cudaEvent_t em;
+  CK(cudaEventCreate(&em));
+  CK(cudaEventRecord(em, c->stream));
   const int n = c->cdev.n_dof;
   if (cusolverDnDpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
                        c->sol_info) != CUSOLVER_STATUS_SUCCESS)
@@ -900,11 +912,14 @@ int ensure_coarse(FemCtx* c) {
   CKL();
   CK(cudaEventRecord(e1, c->stream));
   CK(cudaEventSynchronize(e1));
-  float ms = 0.f;
+  float ms = 0.f, ms_asm = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventElapsedTime(&ms_asm, e0, em);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  cudaEventDestroy(em);
   c->coarse_ms_last = ms;
+  c->coarse_ms_assembly = ms_asm;
   ++c->n_coarse_assemblies;
   c->coarse_valid = true;
   c->coarse_uses = 1;
@@ -1013,6 +1028,89 @@ int ensure_mpnn(FemCtx* c) {
   return FEM_OK;
 }
 
+int ensure_mpnn_train(FemCtx* c) {
+  if (c->mpnn_train_ready) return FEM_OK;
+  const size_t Nn = (size_t)c->Nn;
+  const int tiles = (c->Nn + 127) / 128;
+  int st;
+  MpnnTrain& t = c->mtrain;
+  if ((st = mpnn_alloc(c, &t.GH, Nn * kMpnnHidden))) return st;
+  if ((st = mpnn_alloc(c, &t.GHn, Nn * kMpnnHidden))) return st;
+  if ((st = mpnn_alloc(c, &t.Q, Nn * kMpnnHidden))) return st;
+  if ((st = mpnn_alloc(c, &t.gpart, (size_t)tiles * kMpnnParams))) return st;
+  if ((st = mpnn_alloc(c, &c->grad, (size_t)kMpnnParams))) return st;
+  if ((st = mpnn_alloc(c, &c->adam_m, (size_t)kMpnnParams))) return st;
+  if ((st = mpnn_alloc(c, &c->adam_v, (size_t)kMpnnParams))) return st;
+  for (float** v : {&c->tr_r, &c->tr_e, &c->tr_z, &c->tr_q, &c->tr_g})
+    if ((st = mpnn_alloc(c, v, 4 * Nn))) return st;
+  if ((st = mpnn_alloc(c, &c->tr_scal, (size_t)4))) return st;
+  c->mpnn_train_ready = true;
+  return FEM_OK;
+}
+
+// Everything a learned-preconditioner call needs at the current tangent.
+int mpnn_prepare(FemCtx* c, bool train, bool coarse) {
+  int st;
+  if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
+  if (!c->mpnn_has_weights) return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights");
+  if ((st = compute_dinv(c, FEM_PRECOND_JACOBI))) return st;
+  if ((st = ensure_mpnn(c))) return st;
+  if (train && (st = ensure_mpnn_train(c))) return st;
+  if (coarse && (st = ensure_coarse(c))) return st;
+  prepare_mpnn_kernels();
+  CK(cudaMemsetAsync(c->mdev.err, 0, sizeof(int), c->stream));
+  c->mtrain.m = c->mdev;
+  return FEM_OK;
+}
+
+// z = M(r) (+ coarse) on internal float4 vectors; base: D^-1 r (+ coarse) instead
+void mpnn_apply(FemCtx* c, const float* r, float* z, bool coarse, bool base) {
+  if (base) {
+    launch_jacobi_apply(r, c->dinv, z, c->Nn, c->stream);
+    ++c->n_launches;
+  } else {
+    launch_mpnn_forward(c->mdev, r, c->dinv, z, nullptr, c->red(), SITE_RZ, c->stream);
+    c->n_launches += 6;
+  }
+  if (coarse) {
+    const CoarseArgs ca = coarse_args(c);
+    launch_coarse_apply(ca, r, nullptr, c->stream);
+    launch_coarse_add(ca, z, c->stream);
+    c->n_launches += 3;
+  }
+}
+
+MvArgs train_mv(FemCtx* c, const float* x, float* y) {
+  MvArgs mv = make_mv(c);
+  mv.matF = c->matF;
+  mv.payload = c->payload;
+  mv.x = x;
+  mv.y = y;
+  mv.cg = nullptr;
+  mv.red = c->red();
+  mv.red_site = SITE_MV;
+  mv.mask_input = 1;
+  return mv;
+}
+
+// One training / evaluation sample k: loss into tr_scal[0] (+=), and with
+// grad: dL/dw added (accumulate) or written into c->grad.
+void mpnn_sample(FemCtx* c, const float* R, const float* E, int k, bool coarse, bool base, bool grad,
+                 bool accumulate) {
+  const size_t stride = 3 * (size_t)c->Nn;
+  launch_gather_f(R + stride * k, c->tr_r, c->d_perm_node, c->Nn, c->stream);
+  launch_gather_f(E + stride * k, c->tr_e, c->d_perm_node, c->Nn, c->stream);
+  mpnn_apply(c, c->tr_r, c->tr_z, coarse, base);
+  launch_matvec(train_mv(c, c->tr_z, c->tr_q), c->model_kind, c->stream);
+  launch_train_loss(c->tr_z, c->tr_q, c->tr_r, c->tr_e, c->Nn, c->tr_scal, c->red(), SITE_AUX, c->stream);
+  c->n_launches += 4 + (c->mv_variant == MV_TWO_PHASE ? 1 : 0);
+  if (grad) {
+    launch_train_grad_z(c->tr_q, c->tr_r, c->fixed, c->tr_scal, c->tr_g, c->Nn, c->stream);
+    launch_mpnn_backward(c->mtrain, c->tr_r, c->dinv, c->tr_g, c->grad, accumulate ? 1 : 0, c->stream);
+    c->n_launches += 1 + 2 + 2 * kMpnnLayers + 1;
+  }
+}
+
 // Solves K_T x = b (b: FP64 internal order, fixed DOFs zero) into c->x.
 int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit, int* iters,
             double* rel) {
@@ -1027,6 +1125,7 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
   if (learned && (st = ensure_mpnn(c))) return st;
   if ((st = ensure_cg_graph(c, kind))) return st;
+  if (learned) CK(cudaMemsetAsync(c->mdev.err, 0, sizeof(int), c->stream));
   ++c->n_launches; launch_cg_init(b_int, c->r, c->x, c->p, c->dinv, c->Nn, c->cg, rtol, maxit, c->red(), SITE_CGI,
                  c->stream, (tl || learned) ? 0 : 1);
   CKL();
@@ -1319,9 +1418,118 @@ int fem_mpnn_forward(void* ctx, const float* r, float* z) {
   return FEM_OK;
 }
 
-int fem_coarse_info(void* ctx, double* out6) {
+int fem_mpnn_backward(void* ctx, const float* r, const float* gz, float* grad_out) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
-  if (!c || !out6) return FEM_ERR_INVALID;
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!r || !gz || !grad_out) return set_err(c, FEM_ERR_INVALID, "null argument");
+  if ((st = mpnn_prepare(c, true, false))) return st;
+  launch_gather_f(r, c->tr_r, c->d_perm_node, c->Nn, c->stream);
+  launch_gather_f(gz, c->tr_g, c->d_perm_node, c->Nn, c->stream);
+  mpnn_apply(c, c->tr_r, c->tr_z, false, false);
+  launch_mpnn_backward(c->mtrain, c->tr_r, c->dinv, c->tr_g, c->grad, 0, c->stream);
+  c->n_launches += 2 + 2 + 2 * kMpnnLayers + 1;
+  CKL();
+  CK(cudaMemcpyAsync(grad_out, c->grad, sizeof(float) * kMpnnParams, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->h_err, c->mdev.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (*c->h_err) return set_err(c, FEM_ERR_BUDGET, "learned preconditioner: tensor-core wait gave up");
+  return FEM_OK;
+}
+
+int fem_mpnn_eval(void* ctx, const float* R, const float* E, int32_t n_pairs, double* loss_net,
+                  double* loss_base) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!R || !E || n_pairs <= 0) return set_err(c, FEM_ERR_INVALID, "need pair arrays and n_pairs > 0");
+  const bool coarse = c->learned_coarse;
+  if ((st = mpnn_prepare(c, true, coarse))) return st;
+  double h[2];
+  for (int pass = 0; pass < 2; ++pass) {
+    CK(cudaMemsetAsync(c->tr_scal, 0, 2 * sizeof(double), c->stream));
+    for (int k = 0; k < n_pairs; ++k) mpnn_sample(c, R, E, k, coarse, pass == 1, false, false);
+    CKL();
+    CK(cudaMemcpyAsync(&h[pass], c->tr_scal, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  if (loss_net) *loss_net = h[0] / n_pairs;
+  if (loss_base) *loss_base = h[1] / n_pairs;
+  return FEM_OK;
+}
+
+int fem_mpnn_train(void* ctx, const float* R, const float* E, int32_t n_pairs, const FemTrainParams* prm,
+                   FemTrainResult* res) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!R || !E || n_pairs <= 0 || !prm) return set_err(c, FEM_ERR_INVALID, "need pairs, n_pairs > 0, params");
+  if (prm->steps <= 0 || prm->batch <= 0 || !(prm->lr > 0))
+    return set_err(c, FEM_ERR_INVALID, "need steps > 0, batch > 0, lr > 0");
+  const bool coarse = c->learned_coarse;
+  if ((st = mpnn_prepare(c, true, coarse))) return st;
+  if (prm->reset_optimizer || c->adam_t == 0) {
+    CK(cudaMemsetAsync(c->adam_m, 0, sizeof(float) * kMpnnParams, c->stream));
+    CK(cudaMemsetAsync(c->adam_v, 0, sizeof(float) * kMpnnParams, c->stream));
+    c->adam_t = 0;
+  }
+  std::vector<double> losses(prm->steps);
+  // sample order: a fixed permutation per epoch (seeded LCG), batches in order
+  std::vector<int> order(n_pairs);
+  uint64_t state = 0x9E3779B97F4A7C15ull ^ (uint64_t)(uint32_t)prm->seed;
+  auto next = [&]() {
+    state = state * 6364136223846793005ull + 1442695040888963407ull;
+    return (uint32_t)(state >> 33);
+  };
+  int pos = n_pairs;
+  for (int step = 0; step < prm->steps; ++step) {
+    CK(cudaMemsetAsync(c->tr_scal, 0, 2 * sizeof(double), c->stream));
+    for (int b = 0; b < prm->batch; ++b) {
+      if (pos >= n_pairs) {
+        std::iota(order.begin(), order.end(), 0);
+        for (int i = n_pairs - 1; i > 0; --i) std::swap(order[i], order[next() % (uint32_t)(i + 1)]);
+        pos = 0;
+      }
+      mpnn_sample(c, R, E, order[pos++], coarse, false, true, b > 0);
+    }
+    ++c->adam_t;
+    launch_mpnn_adam(c->mpnn_w, c->adam_m, c->adam_v, c->grad, 1.0f / prm->batch, (float)prm->lr, c->adam_t,
+                     c->stream);
+    launch_mpnn_pack(c->mpnn_w, c->We_p, c->Wl_p, c->WlT_p, c->stream);
+    c->n_launches += 2;
+    CKL();
+    CK(cudaMemcpyAsync(&losses[step], c->tr_scal, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (prm->progress && (step % 16 == 15 || step + 1 == prm->steps)) {
+      CK(cudaStreamSynchronize(c->stream));
+      if (!prm->progress(prm->progress_user, step + 1, losses[step] / prm->batch, 0.0)) {
+        if (res) res->steps_done = step + 1;
+        return FEM_CANCELLED;
+      }
+    }
+  }
+  CK(cudaMemcpyAsync(c->h_err, c->mdev.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (*c->h_err) return set_err(c, FEM_ERR_BUDGET, "learned preconditioner: tensor-core wait gave up");
+  if (res) {
+    res->steps_done = prm->steps;
+    const int w = std::max(1, std::min(prm->steps / 10, 16));
+    double a = 0, b = 0;
+    for (int i = 0; i < w; ++i) {
+      a += losses[i];
+      b += losses[prm->steps - 1 - i];
+    }
+    res->loss_first = a / (w * prm->batch);
+    res->loss_last = b / (w * prm->batch);
+  }
+  return FEM_OK;
+}
+
+int fem_coarse_info(void* ctx, double* out8) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  if (!c || !out8) return FEM_ERR_INVALID;
+  double* out6 = out8;
+  out8[6] = c->coarse_ms_assembly;
+  out8[7] = (double)c->coarse_reuse;
   out6[0] = c->cdev.n_cells;
   out6[1] = c->cdev.n_cn;
   out6[2] = c->cdev.n_dof;
@@ -1433,7 +1641,14 @@ int fem_set_bc(void* ctx, const uint8_t* fixed_mask, const double* fixed_values,
     // the matvec kernels read the fixed bits from the w lane of the FP32 coordinates
     ++c->n_launches; launch_x32_mask(c->X32, c->fixed, c->Nn, c->stream);
     CKL();
-    c->coarse_valid = false;
+    // a changed constraint pattern changes the coarse operator (K_ff)
+    std::vector<uint8_t> now(c->Nn);
+    CK(cudaMemcpyAsync(now.data(), c->fixed, c->Nn, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (now != c->fixed_host) {
+      c->fixed_host.swap(now);
+      c->coarse_valid = false;
+    }
   }
   if (fixed_values) {
     ++c->n_launches; launch_gather_d(fixed_values, c->fixed_vals, c->d_perm_node, c->Nn, c->stream);
@@ -1563,7 +1778,7 @@ int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol
   if ((st = check_ctx(c))) return st;
   if (!r || !du) return set_err(c, FEM_ERR_INVALID, "null vector");
   if (maxit <= 0 || !(rtol > 0)) return set_err(c, FEM_ERR_INVALID, "need max_iterations > 0 and rtol > 0");
-  if (precond < FEM_PRECOND_NONE || precond > FEM_PRECOND_TWO_LEVEL)
+  if (precond < FEM_PRECOND_NONE || precond > FEM_PRECOND_LEARNED)
     return set_err(c, FEM_ERR_INVALID, "unknown preconditioner %d", precond);
   // caller order -> internal order, fixed DOFs of the right-hand side zeroed
   ++c->n_launches; launch_gather_d_masked(r, c->tmpd, c->d_perm_node, c->fixed, c->Nn, c->stream);
@@ -1606,7 +1821,7 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     fem_default_solve_params(&prm);
   if (prm.max_iterations <= 0 || !(prm.tol > 0))
     return set_err(c, FEM_ERR_INVALID, "need max_iterations > 0 and tol > 0");
-  if (prm.precond < FEM_PRECOND_NONE || prm.precond > FEM_PRECOND_TWO_LEVEL)
+  if (prm.precond < FEM_PRECOND_NONE || prm.precond > FEM_PRECOND_LEARNED)
     return set_err(c, FEM_ERR_INVALID, "unknown preconditioner %d", prm.precond);
   FemSolveResult out;
   std::memset(&out, 0, sizeof(out));

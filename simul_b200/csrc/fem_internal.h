@@ -109,7 +109,7 @@ struct CoarseDev {
   const int* cell_elems;
   const int* node_cell;     // [Nn]
   const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
-  double* blocks;           // [n_cells][24 * 24] Galerkin block of each cell
+  double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
   float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric)
   float* cell_r;            // [n_cells][24] restricted residual per cell
@@ -156,6 +156,15 @@ struct MpnnDev {
   int* err;                     // set when an MMA completion wait gives up
 };
 
+// Training buffers of the learned preconditioner's backward pass.
+struct MpnnTrain {
+  MpnnDev m;
+  float* GH;                    // [Nn][64] gradient w.r.t. the current layer output
+  float* GHn;                   // [Nn][64] self-path part of the gradient w.r.t. its input
+  float* Q;                     // [Nn][64] aggregation-path gradient / deg
+  float* gpart;                 // [tiles][kMpnnParams] per-tile gradient shares
+};
+
 // Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
 // returns `code`.
 int set_global_error(int code, const char* fmt, ...);
@@ -168,6 +177,7 @@ void prepare_kernels(const MeshDev& m, int model);
 void launch_diag(const DiagArgs& a, int model, cudaStream_t s);
 // coarse lattice (fem_coarse.cu)
 size_t coarse_cell_smem();
+int coarse_cell_slices();   // CTAs (and Galerkin block slots) per lattice cell
 void prepare_coarse_kernels(int model, int n_dof);
 // cell Galerkin blocks + dense Ac (FP64, column-major)
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
@@ -190,6 +200,21 @@ void launch_mpnn_pack(const float* w, __nv_bfloat16* We_p, __nv_bfloat16* Wl_p, 
 // z = M(r) (skipped once cg->done is set, when cg is non-null)
 void launch_mpnn_forward(const MpnnDev& m, const float* r, const float* dinv, float* z, const CGState* cg,
                          Reduce red, int site, cudaStream_t s);
+
+// grad (+)= d<gz, M(r)>/dw after a forward pass on the same r (activations kept)
+void launch_mpnn_backward(const MpnnTrain& t, const float* r, const float* dinv, const float* gz, float* grad,
+                          int accumulate, cudaStream_t s);
+void launch_mpnn_adam(float* w, float* mom, float* var, const float* grad, float gscale, float lr, int step,
+                      cudaStream_t s);
+
+// training helpers (fem_coarse.cu)
+void launch_coarse_add(const CoarseArgs& a, float* z, cudaStream_t s);
+// out[0] += energy loss of (z, r, e) with q = A z; out[1] = 2 / e.r
+void launch_train_loss(const float* z, const float* q, const float* r, const float* e, int n, double* out,
+                       Reduce red, int site, cudaStream_t s);
+void launch_train_grad_z(const float* q, const float* r, const uint8_t* fixed, const double* scale, float* gz,
+                         int n, cudaStream_t s);
+void launch_jacobi_apply(const float* r, const float* dinv, float* z, int n, cudaStream_t s);
 
 // PCG vector kernels.  precond_in_update = 1: Jacobi z = D^-1 r is applied
 // inside cg_init / cg_update (rz, beta there); 0: an external preconditioner

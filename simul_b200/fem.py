@@ -153,10 +153,11 @@ class FEMesh:
                 "matvec_ns": {"fused": out[5], "two_phase": out[6]}, "matvec_tuned": bool(out[7])}
 
     def coarse_info(self) -> dict:
-        out = (C.c_double * 6)()
+        out = (C.c_double * 8)()
         _check(_lib.load().fem_coarse_info(self.ctx, out), self.ctx, "fem_coarse_info")
         return {"cells": int(out[0]), "coarse_nodes": int(out[1]), "coarse_dofs": int(out[2]),
-                "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5]}
+                "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5],
+                "last_assembly_kernels_ms": out[6], "reuse": int(out[7])}
 
     def set_coarse_options(self, cell=None, reuse=None):
         """Two-level preconditioner: lattice cell edge in mesh lengths and the

@@ -216,7 +216,7 @@ def test_two_level_pcg_matches_oracle_with_fewer_iterations(cuda, vox):
         sols[name] = du.cpu().numpy()
     info = mesh.coarse_info()
     assert info["assemblies"] == 1 and info["coarse_dofs"] > 0
-    assert its["two_level"] < its["jacobi"] / 2, its
+    assert its["two_level"] < 0.6 * its["jacobi"], its
     # FP64 oracle: K_ff du = rhs_f by a direct solve of the assembled tangent
     m = O.Mesh(vox.X, vox.conn)
     mo = O.Material("linear_elastic", E=1e3, nu=0.3)

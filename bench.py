@@ -55,9 +55,11 @@ def parse():
     ap.add_argument("--weights", default=os.path.join(ROOT, "simul_b200", "weights", "mpnn_vertebra.npz"),
                     help="learned-preconditioner weights (simul_b200.train_precond)")
     ap.add_argument("--learned-coarse", type=int, default=1, help="learned: add the coarse correction")
+    ap.add_argument("--matvec-variant", default="auto", choices=["auto", "fused", "two_phase"],
+                    help="tangent-matvec variant (auto: timed on the first solve)")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
-    ap.add_argument("--coarse-reuse", type=int, default=1,
-                    help="PCG solves one coarse-operator assembly serves (two-level / learned)")
+    ap.add_argument("--coarse-reuse", type=int, default=0,
+                    help="PCG solves one coarse-operator assembly serves (0: adaptive)")
     ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
     return ap.parse_args()
 
@@ -159,10 +161,11 @@ def measured_peaks():
 def learned_info(mesh, args):
     import ctypes as C
     from simul_b200 import _lib
-    st = (C.c_int64 * 2)()
+    st = (C.c_int64 * 4)()
     _lib.load().fem_learned_stats(mesh.ctx, st)
     return {"weights": os.path.relpath(args.weights, ROOT), "coarse_correction": bool(args.learned_coarse),
-            "fallbacks_to_jacobi_pcg": int(st[0]),
+            "fallbacks_to_jacobi_pcg": int(st[0]), "fpcg_steps": int(st[2]),
+            "steps_with_jacobi_direction": int(st[3]),
             "network": "4-layer message passing, width 64, BF16 tcgen05 dense layers, FP32 accumulation"}
 
 
@@ -249,6 +252,8 @@ def main():
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond)
     mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse)
+    if args.matvec_variant != "auto":
+        mesh.set_matvec_variant(args.matvec_variant)
     if args.precond == "learned":
         from simul_b200 import learned
         learned.set_weights(mesh, learned.load(args.weights))

@@ -152,8 +152,10 @@ enum {
    * the cube root of 5x the mean element volume, i.e. the voxel edge of
    * 5-tet voxel meshes); grown automatically past 4096 coarse nodes */
   FEM_OPT_COARSE_CELL = 2,
-  /* two-level preconditioner: PCG solves one coarse assembly serves
-   * (default 1: reassembled at every tangent) */
+  /* two-level preconditioner: PCG solves one coarse assembly serves; 0
+   * (default) = adaptive: the operator is rebuilt at the next tangent once a
+   * solve needs 1.5x the CG iterations per decade of residual reduction
+   * measured right after the last assembly */
   FEM_OPT_COARSE_REUSE = 3,
   /* learned preconditioner: 1 (default) adds the two-level coarse correction
    * to the network's output, 0 uses the network alone */
@@ -173,8 +175,10 @@ int fem_mpnn_get_weights(void* ctx, float* w, int64_t n);
 /* z = M(r) at the current tangent (caller order, N x 3 FP32 device arrays) */
 int fem_mpnn_forward(void* ctx, const float* r, float* z);
 /* out[0] flexible solves that fell back to Jacobi-based PCG, out[1] 1 if
- * weights are set */
-int fem_learned_stats(void* ctx, int64_t* out2);
+ * weights are set, out[2] flexible PCG steps so far, out[3] of which used the
+ * Jacobi (+ coarse) direction because the network's was not a descent
+ * direction (r.z_net <= 0.25 r.z_jacobi) */
+int fem_learned_stats(void* ctx, int64_t* out4);
 /* grad (host, 34,307 FP32) = d<gz, M(r)>/dw at the current tangent; r, gz:
  * caller order, N x 3 FP32 device arrays (network only, no coarse part) */
 int fem_mpnn_backward(void* ctx, const float* r, const float* gz, float* grad);
@@ -272,6 +276,22 @@ int fem_pcg(void* ctx, int32_t precond, const double* r, double* du, double rtol
  * solves in FP32 (mixed-precision iterative refinement). */
 int fem_newton_solve(void* ctx, const FemSolveParams* params, FemSolveResult* result);
 void fem_default_solve_params(FemSolveParams* p);
+
+/* Load stepping (the reference loops solve() with scaled loads, e.g.
+ * benchmark_spine_compression.py:413-415): prescribed values and external
+ * forces become s x the values last given to fem_set_bc. */
+int fem_set_load_scale(void* ctx, double s);
+
+/* Batched solves of independent contexts (no reference counterpart): each
+ * context, on its own stream, runs `load_steps` load steps (scale k/steps,
+ * fem_set_load_scale + fem_newton_solve) on a pool of n_threads host workers
+ * (0: one per context), so the instances' kernels overlap on the GPU.
+ * results[i] aggregates instance i (iterations summed, converged if every
+ * step converged), status[i] its status, wall_ms[i] (optional) its host wall
+ * time.  Contexts must be distinct and must not share a stream with other
+ * work.  Progress callbacks are ignored. */
+int fem_batch_solve(void** ctxs, int32_t n, const FemSolveParams* prm, int32_t load_steps,
+                    FemSolveResult* results, int32_t* status, double* wall_ms, int32_t n_threads);
 
 /* Kernel timing (no reference counterpart; the reference has only wall clocks,
  * framework/_adapters/fem_adapter.py:162-172).  Launches each hot kernel

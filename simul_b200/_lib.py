@@ -108,6 +108,9 @@ SIGNATURES = {
     "fem_mpnn_train": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.POINTER(FemTrainParams),
                                  C.POINTER(FemTrainResult)]),
     "fem_mpnn_eval": (C.c_int, [_VP, _VP, _VP, C.c_int32, _DP, _DP]),
+    "fem_set_load_scale": (C.c_int, [_VP, C.c_double]),
+    "fem_batch_solve": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.POINTER(FemSolveParams), C.c_int32,
+                                  C.POINTER(FemSolveResult), C.POINTER(C.c_int32), _DP, C.c_int32]),
     "fem_set_materials": (C.c_int, [_VP, C.POINTER(FemMaterial), C.c_int32, _VP, _VP]),
     "fem_set_bc": (C.c_int, [_VP, _VP, _VP, _VP]),
     "fem_apply_bc": (C.c_int, [_VP]),

@@ -1,0 +1,131 @@
+"""Batched uneven solves: many seeded vertebral bodies of different sizes and
+load cases solved concurrently on one GPU; reports solves/s and p50/p99
+per-instance solve time.
+
+    python -m simul_b200.batch_bench --instances 64 --n-min 32 --n-max 96
+
+Instances: grid sizes drawn uniformly from [n-min, n-max] voxels per axis,
+per-instance modulus fields (cortical shell 12 GPa, lognormal core), J2
+(yield 100 MPa, H = 0.02 E).  Load case per instance, drawn from: axial
+compression 1-3 % of the height (prescribed top-face displacement), or a
+7.5 N m (7,500 N mm) flexion / extension / lateral-bending / torsion moment.
+A moment is applied as an equivalent linear nodal force couple on the top-face
+nodes (a rigid top plate is not modelled); the bottom face is fixed.
+All data are seeded synthetic inputs.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import time
+from concurrent.futures import ProcessPoolExecutor, ThreadPoolExecutor
+
+import numpy as np
+
+CASES = ("axial", "flexion", "extension", "lateral_bending", "torsion")
+MOMENT = 7500.0  # N mm
+
+
+def _make_case(args):
+    """Host-side generation of one instance (runs in a worker process)."""
+    idx, n, seed, case, strain = args
+    from simul_b200 import meshgen
+    v = meshgen.vertebral_body(n=n, seed=seed, axial_strain=strain)
+    X = v.X
+    fixed = v.fixed_mask.copy()
+    vals = v.fixed_vals.copy()
+    f = np.zeros_like(X)
+    if case != "axial":
+        top = np.isclose(X[:, 2], X[:, 2].max())
+        fixed[top] = False
+        vals[top] = 0.0
+        xc, yc = X[top, 0] - X[top, 0].mean(), X[top, 1] - X[top, 1].mean()
+        ft = np.zeros((int(top.sum()), 3))
+        if case in ("flexion", "extension"):
+            sgn = 1.0 if case == "flexion" else -1.0
+            ft[:, 2] = -sgn * MOMENT * yc / np.sum(yc * yc)
+        elif case == "lateral_bending":
+            ft[:, 2] = -MOMENT * xc / np.sum(xc * xc)
+        else:
+            r2 = np.sum(xc * xc + yc * yc)
+            ft[:, 0] = -MOMENT * yc / r2
+            ft[:, 1] = MOMENT * xc / r2
+        f[top] = ft
+    return {"idx": idx, "n": n, "seed": seed, "case": case, "strain": strain, "X": X, "conn": v.conn,
+            "E": v.E, "fixed": fixed, "vals": vals, "f": f, "tets": int(v.n_elements)}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--n-min", type=int, default=32)
+    ap.add_argument("--n-max", type=int, default=96)
+    ap.add_argument("--load-steps", type=int, default=10)
+    ap.add_argument("--threads", type=int, default=0, help="host workers (0: one per instance)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precond", default="two_level", choices=["jacobi", "two_level"])
+    ap.add_argument("--sequential", action="store_true", help="also time the instances one after another")
+    ap.add_argument("--workers", type=int, default=16, help="host processes generating meshes")
+    args = ap.parse_args(argv)
+    rng = np.random.default_rng(args.seed)
+    specs = []
+    for i in range(args.instances):
+        n = int(rng.integers(args.n_min, args.n_max + 1))
+        case = CASES[int(rng.integers(0, len(CASES)))]
+        specs.append((i, n, 1000 + i, case, float(rng.uniform(0.01, 0.03))))
+    t0 = time.perf_counter()
+    with ProcessPoolExecutor(max_workers=args.workers, mp_context=mp.get_context("spawn")) as ex:
+        cases = sorted(ex.map(_make_case, specs), key=lambda d: d["idx"])
+    t_gen = time.perf_counter() - t0
+
+    import torch
+    from simul_b200 import batch
+    from simul_b200 import fem as B
+    dev = torch.device("cuda", 0)
+    torch.cuda.init()
+
+    def build(d):
+        mat = B.J2Plasticity(d["E"], 0.3, 100.0, hardening_modulus=0.02 * d["E"])
+        return batch.BatchInstance(d["X"], d["conn"], mat, d["fixed"], d["vals"], d["f"], device=dev)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        insts = list(ex.map(build, cases))
+    t_setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    out = batch.solve_batch(insts, load_steps=args.load_steps, precond=args.precond, n_threads=args.threads)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = np.array([r["wall_ms"] for r in out["instances"]])
+    res = {"instances": args.instances, "tets_total": int(sum(d["tets"] for d in cases)),
+           "tets_min": int(min(d["tets"] for d in cases)), "tets_max": int(max(d["tets"] for d in cases)),
+           "cases": {c: sum(1 for d in cases if d["case"] == c) for c in CASES},
+           "load_steps": args.load_steps, "precond": args.precond,
+           "all_converged": bool(all(r["converged"] for r in out["instances"])),
+           "batch_wall_s": wall, "solves_per_s": args.instances / wall,
+           "p50_instance_ms": float(np.percentile(ms, 50)), "p99_instance_ms": float(np.percentile(ms, 99)),
+           "newton_iterations": int(sum(r["newton_iterations"] for r in out["instances"])),
+           "cg_iterations": int(sum(r["cg_iterations"] for r in out["instances"])),
+           "host_generation_s": t_gen, "host_setup_s": t_setup}
+    if args.sequential:
+        import ctypes as C
+        from simul_b200 import _lib
+        for inst in insts:
+            inst.mesh.u.zero_()
+            torch.cuda.synchronize()
+            B._check(_lib.load().fem_set_displacement(inst.ctx, C.c_void_p(inst.mesh.u.data_ptr())), inst.ctx,
+                     "fem_set_displacement")
+            inst.material.reset_state()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out2 = batch.solve_batch(insts, load_steps=args.load_steps, precond=args.precond, n_threads=1)
+        torch.cuda.synchronize()
+        res["sequential_wall_s"] = time.perf_counter() - t0
+        res["sequential_solves_per_s"] = args.instances / res["sequential_wall_s"]
+        res["sequential_all_converged"] = bool(all(r["converged"] for r in out2["instances"]))
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

@@ -222,19 +222,24 @@ __global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
 
 // ───────────────────────── per-iteration application ─────────────────────────
 
-// cell_r[cell][3 corner + d] = sum over the cell's nodes of w_corner r_d
-__global__ void __launch_bounds__(kCellThreads) coarse_restrict_kernel(
+// cell_r[cell][3 corner + d] = sum over the cell's nodes of w_corner r_d.
+// One CTA of kRestrictThreads per cell: warp-shuffle sums, then the warps'
+// 24-value shares added in warp order (one barrier).
+constexpr int kRestrictThreads = 128;
+
+__global__ void __launch_bounds__(kRestrictThreads) coarse_restrict_kernel(
     const __grid_constant__ CoarseArgs a, const float* __restrict__ r, const CGState* cg) {
   if (cg && cg->done) return;
-  __shared__ float sh[kCellThreads / 32];
+  __shared__ float sw[kRestrictThreads / 32][24];
   const CoarseDev& c = a.c;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cell = blockIdx.x;
   const int3 ijk = c.cell_ijk[cell];
   const int n0 = c.cell_node_ptr[cell], n1 = c.cell_node_ptr[cell + 1];
   float acc[24];
 #pragma unroll
   for (int k = 0; k < 24; ++k) acc[k] = 0.f;
-  for (int i = n0 + threadIdx.x; i < n1; i += kCellThreads) {
+  for (int i = n0 + threadIdx.x; i < n1; i += kRestrictThreads) {
     const int node = __ldg(c.cell_nodes + i);
     const float4 X = __ldg(a.m.X32 + node);
     const float4 rv = reinterpret_cast<const float4*>(r)[node];
@@ -250,13 +255,23 @@ __global__ void __launch_bounds__(kCellThreads) coarse_restrict_kernel(
   }
 #pragma unroll
   for (int k = 0; k < 24; ++k) {
-    const float v = block_sum_f<kCellThreads>(acc[k], sh);
-    if (threadIdx.x == 0) c.cell_r[cell * 24 + k] = v;
+    float v = acc[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sw[warp][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 24) {
+    float v = 0.f;
+#pragma unroll
+    for (int w = 0; w < kRestrictThreads / 32; ++w) v += sw[w][threadIdx.x];
+    c.cell_r[cell * 24 + threadIdx.x] = v;
   }
 }
 
-// y_c = Ainv r_c; every CTA first gathers r_c from the cell partials (fixed
-// order), then one warp per row.
+// y_c = Ainv r_c.  Every CTA stages r_c in shared memory: r_c[I] adds its
+// cells' shares in the fixed order of cn_cells (the eight entries are loaded
+// together, then the shares); then one warp per row.
 constexpr int kCoarseMvThreads = 256;
 
 __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
@@ -266,12 +281,16 @@ __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
   const int n = c.n_dof;
   for (int I = threadIdx.x; I < n; I += kCoarseMvThreads) {
     const int nI = I / 3, dI = I - 3 * nI;
+    const int4* ep = reinterpret_cast<const int4*>(c.cn_cells + nI * 8);
+    const int4 e0 = __ldg(ep), e1 = __ldg(ep + 1);
+    const int ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+    float sh[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      sh[k] = ent[k] >= 0 ? __ldcg(c.cell_r + (ent[k] >> 3) * 24 + 3 * (ent[k] & 7) + dI) : 0.f;
     float v = 0.f;
-    for (int k = 0; k < 8; ++k) {
-      const int ent = c.cn_cells[nI * 8 + k];
-      if (ent < 0) break;
-      v += c.cell_r[(ent >> 3) * 24 + 3 * (ent & 7) + dI];
-    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v += sh[k];
     s_rc[I] = v;
   }
   __syncthreads();
@@ -279,8 +298,14 @@ __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
   const int row = blockIdx.x * (kCoarseMvThreads / 32) + warp;
   if (row >= n) return;
   const float* Arow = c.Ainv + (size_t)row * n;
-  float s = 0.f;
-  for (int j = lane; j < n; j += 32) s += __ldg(Arow + j) * s_rc[j];
+  float s0 = 0.f, s1 = 0.f;
+  int j = lane;
+  for (; j + 32 < n; j += 64) {
+    s0 += __ldg(Arow + j) * s_rc[j];
+    s1 += __ldg(Arow + j + 32) * s_rc[j + 32];
+  }
+  if (j < n) s0 += __ldg(Arow + j) * s_rc[j];
+  float s = s0 + s1;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if (lane == 0) c.yc[row] = s;
@@ -360,23 +385,38 @@ __global__ void __launch_bounds__(256) tl_pupdate_kernel(float* p, const float* 
   reinterpret_cast<float4*>(p)[i] = pv;
 }
 
-// Flexible PCG step around a nonlinear preconditioner output z (already in
-// `z`): optionally z += P yc (coarse correction), then rz = r.z and z.q.
-// INIT: p = z.  Otherwise Polak-Ribiere beta = z.(r_new - r_old) / rz_old
-// = -alpha z.q / rz_old, using r_new - r_old = -alpha q.
+// Flexible PCG step around the learned preconditioner.  z holds the
+// network's output (which already contains D^-1 r); the kernel adds the coarse
+// part P yc when COARSE, forms the Jacobi (+ coarse) alternative in zalt, and
+// reduces r.z, z.q for both.  The last block keeps the network's direction
+// unless it is not a descent direction relative to the alternative
+// (r.z_net <= kSafe r.z_alt, or not finite); then the alternative is used for
+// this iteration (cg->zsel = 1); after kLock such steps the network is
+// switched off for the rest of the solve (cg->locked; its kernels then exit at
+// entry) and the recursion restarts with beta = 0, so a network that does not
+// help costs a few steps, not a slower solve.  INIT: p = chosen z.  Otherwise
+// Polak-Ribiere beta = z.(r_new - r_old) / rz_old = -alpha z.q / rz_old,
+// r_new - r_old = -alpha q.
+constexpr double kSafe = 0.25;
+constexpr int kLock = 3;
+
 template <bool INIT, bool COARSE>
 __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ CoarseArgs a,
                                                         const float* __restrict__ r,
-                                                        const float* __restrict__ q, float* z, float* p,
-                                                        CGState* cg, Reduce red, int site) {
+                                                        const float* __restrict__ q,
+                                                        const float* __restrict__ dinv, float* z, float* zalt,
+                                                        float* p, CGState* cg, Reduce red, int site,
+                                                        int site2) {
   if (cg->done) return;
   __shared__ double sred[8];
   __shared__ bool am_last;
   const int i = blockIdx.x * 256 + threadIdx.x;
-  double rz = 0.0, zq = 0.0;
+  double rz = 0.0, zq = 0.0, rza = 0.0, zqa = 0.0;
   if (i < a.m.n_nodes) {
     const float4 rv = reinterpret_cast<const float4*>(r)[i];
+    const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
     float4 zv = reinterpret_cast<const float4*>(z)[i];
+    float4 av = make_float4(dv.x * rv.x, dv.y * rv.y, dv.z * rv.z, 0.f);
     if (COARSE) {
       const CoarseDev& c = a.c;
       const float4 X = __ldg(a.m.X32 + i);
@@ -397,32 +437,75 @@ __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ 
       zv.x = (fx & 1) ? 0.f : zv.x + cz[0];
       zv.y = (fx & 2) ? 0.f : zv.y + cz[1];
       zv.z = (fx & 4) ? 0.f : zv.z + cz[2];
-      zv.w = 0.f;
-      reinterpret_cast<float4*>(z)[i] = zv;
+      av.x = (fx & 1) ? 0.f : av.x + cz[0];
+      av.y = (fx & 2) ? 0.f : av.y + cz[1];
+      av.z = (fx & 4) ? 0.f : av.z + cz[2];
     }
-    if (INIT) reinterpret_cast<float4*>(p)[i] = zv;
+    zv.w = 0.f;
+    reinterpret_cast<float4*>(z)[i] = zv;
+    reinterpret_cast<float4*>(zalt)[i] = av;
     rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
+    rza = (double)rv.x * av.x + (double)rv.y * av.y + (double)rv.z * av.z;
     if (!INIT) {
       const float4 qv = reinterpret_cast<const float4*>(q)[i];
       zq = (double)zv.x * qv.x + (double)zv.y * qv.y + (double)zv.z * qv.z;
+      zqa = (double)av.x * qv.x + (double)av.y * qv.y + (double)av.z * qv.z;
     }
   }
-  double v[2];
+  double v[2], v2[2];
   v[0] = block_sum<256>(rz, sred);
   v[1] = block_sum<256>(zq, sred);
+  v2[0] = block_sum<256>(rza, sred);
+  v2[1] = block_sum<256>(zqa, sred);
+  if (threadIdx.x == 0) {
+    red.partials[(size_t)(site2 * 2) * red.max_blocks + blockIdx.x] = v2[0];
+    red.partials[(size_t)(site2 * 2 + 1) * red.max_blocks + blockIdx.x] = v2[1];
+  }
   if (publish_partial(red, site, 2, v, &am_last)) {
     const double trz = final_sum<256>(red, site, 0, sred);
     const double tzq = final_sum<256>(red, site, 1, sred);
+    const double arz = final_sum<256>(red, site2, 0, sred);
+    const double azq = final_sum<256>(red, site2, 1, sred);
     if (threadIdx.x == 0) {
-      cg->beta = INIT ? 0.0 : -cg->alpha * tzq / cg->rz;
-      cg->rz = trz;
-      if (!isfinite(trz) || !(trz > 0.0) || !isfinite(cg->beta)) {
+      const bool was_locked = cg->locked != 0;
+      const bool net_ok = !was_locked && isfinite(trz) && isfinite(tzq) && trz > kSafe * arz;
+      const double rzc = net_ok ? trz : arz;
+      const double zqc = net_ok ? tzq : azq;
+      cg->zsel = net_ok ? 0 : 1;
+      bool restart = false;
+      if (!net_ok) {
+        cg->n_alt += 1;
+        if (!was_locked && cg->n_alt >= kLock) {
+          cg->locked = 1;
+          restart = true;
+        }
+      }
+      cg->beta = (INIT || restart) ? 0.0 : -cg->alpha * zqc / cg->rz;
+      cg->rz = rzc;
+      if (!isfinite(rzc) || !(rzc > 0.0) || !isfinite(cg->beta)) {
         cg->done = 3;
         cg->status = 3;
       }
       red.counters[site] = 0u;
     }
   }
+}
+
+// p = z_sel + beta p (INIT: p = z_sel), z_sel the direction fpcg_dots kept
+__global__ void __launch_bounds__(256) fpcg_pupdate_kernel(float* p, const float* __restrict__ z,
+                                                           const float* __restrict__ zalt, int n_nodes,
+                                                           const CGState* cg, int init) {
+  if (cg->done) return;
+  const float beta = init ? 0.f : (float)cg->beta;
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i >= n_nodes) return;
+  const float4 zv = reinterpret_cast<const float4*>(cg->zsel ? zalt : z)[i];
+  float4 pv = init ? make_float4(0.f, 0.f, 0.f, 0.f) : reinterpret_cast<float4*>(p)[i];
+  pv.x = zv.x + beta * pv.x;
+  pv.y = zv.y + beta * pv.y;
+  pv.z = zv.z + beta * pv.z;
+  pv.w = 0.f;
+  reinterpret_cast<float4*>(p)[i] = pv;
 }
 
 // z += P yc on free DOFs (the coarse part of a composite preconditioner)
@@ -521,18 +604,17 @@ size_t coarse_cell_smem() { return sizeof(float) * kCellThreads * (144 + 32); }
 int coarse_cell_slices() { return kCellSlices; }
 
 void prepare_coarse_kernels(int model, int n_dof) {
-  const int smem = (int)coarse_cell_smem();
+  (void)n_dof;
   switch (model) {
-    case M_LE: cudaFuncSetAttribute(coarse_cell_kernel<M_LE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
-    case M_NH: cudaFuncSetAttribute(coarse_cell_kernel<M_NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
-    case M_MR: cudaFuncSetAttribute(coarse_cell_kernel<M_MR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
-    case M_J2: cudaFuncSetAttribute(coarse_cell_kernel<M_J2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
-    case M_TI: cudaFuncSetAttribute(coarse_cell_kernel<M_TI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
-    case M_FMR: cudaFuncSetAttribute(coarse_cell_kernel<M_FMR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
-    default: cudaFuncSetAttribute(coarse_cell_kernel<-1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem); break;
+    case M_LE: raise_smem_limit_k(coarse_cell_kernel<M_LE>); break;
+    case M_NH: raise_smem_limit_k(coarse_cell_kernel<M_NH>); break;
+    case M_MR: raise_smem_limit_k(coarse_cell_kernel<M_MR>); break;
+    case M_J2: raise_smem_limit_k(coarse_cell_kernel<M_J2>); break;
+    case M_TI: raise_smem_limit_k(coarse_cell_kernel<M_TI>); break;
+    case M_FMR: raise_smem_limit_k(coarse_cell_kernel<M_FMR>); break;
+    default: raise_smem_limit_k(coarse_cell_kernel<-1>); break;
   }
-  cudaFuncSetAttribute(coarse_mv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(sizeof(float) * (size_t)n_dof));
+  raise_smem_limit_k(coarse_mv_kernel);
 }
 
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s) {
@@ -557,7 +639,7 @@ void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s) {
 }
 
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
-  coarse_restrict_kernel<<<a.c.n_cells, kCellThreads, 0, s>>>(a, r, cg);
+  coarse_restrict_kernel<<<a.c.n_cells, kRestrictThreads, 0, s>>>(a, r, cg);
   const int rows_per_cta = kCoarseMvThreads / 32;
   coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(
       a.c, cg);
@@ -572,20 +654,26 @@ void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* d
     tl_rz_kernel<false><<<g, 256, 0, s>>>(a, r, dinv, z, p, cg, red, site);
 }
 
-void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q, float* z,
-                      float* p, CGState* cg, Reduce red, int site, cudaStream_t s) {
+void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q,
+                      const float* dinv, float* z, float* zalt, float* p, CGState* cg, Reduce red, int site,
+                      int site2, cudaStream_t s) {
   const int g = nblk(a.m.n_nodes, 256);
   if (init) {
     if (coarse)
-      fpcg_dots_kernel<true, true><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+      fpcg_dots_kernel<true, true><<<g, 256, 0, s>>>(a, r, q, dinv, z, zalt, p, cg, red, site, site2);
     else
-      fpcg_dots_kernel<true, false><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+      fpcg_dots_kernel<true, false><<<g, 256, 0, s>>>(a, r, q, dinv, z, zalt, p, cg, red, site, site2);
   } else {
     if (coarse)
-      fpcg_dots_kernel<false, true><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+      fpcg_dots_kernel<false, true><<<g, 256, 0, s>>>(a, r, q, dinv, z, zalt, p, cg, red, site, site2);
     else
-      fpcg_dots_kernel<false, false><<<g, 256, 0, s>>>(a, r, q, z, p, cg, red, site);
+      fpcg_dots_kernel<false, false><<<g, 256, 0, s>>>(a, r, q, dinv, z, zalt, p, cg, red, site, site2);
   }
+}
+
+void launch_fpcg_pupdate(float* p, const float* z, const float* zalt, int n_nodes, const CGState* cg, bool init,
+                         cudaStream_t s) {
+  fpcg_pupdate_kernel<<<nblk(n_nodes, 256), 256, 0, s>>>(p, z, zalt, n_nodes, cg, init ? 1 : 0);
 }
 
 void launch_tl_pupdate(float* p, const float* z, int n_nodes, const CGState* cg, cudaStream_t s) {

@@ -8,7 +8,10 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -25,11 +28,16 @@ namespace {
 
 thread_local std::string g_create_error;
 
-enum { SITE_RES = 0, SITE_MV = 1, SITE_CGI = 2, SITE_CGU = 3, SITE_AUX = 4, SITE_RZ = 5, N_SITES = 6 };
+enum { SITE_RES = 0, SITE_MV = 1, SITE_CGI = 2, SITE_CGU = 3, SITE_AUX = 4, SITE_RZ = 5, SITE_RZ2 = 6, N_SITES = 7 };
 // captured CG iteration graphs: Jacobi / identity preconditioner, two-level,
 // learned (flexible PCG)
 enum { GRAPH_JACOBI = 0, GRAPH_TWO_LEVEL = 1, GRAPH_LEARNED = 2, N_GRAPHS = 3 };
-constexpr int kCGBatch = 32;  // CG iterations per captured graph launch
+// CG iterations per captured graph launch (Jacobi needs hundreds per solve;
+// the two-level and learned preconditioners tens, so their graphs are shorter
+// and fewer early-exit iterations run after convergence)
+constexpr int kCGBatch = 32;
+constexpr int kCGBatchShort = 12;
+inline int cg_batch(int kind) { return kind == 0 ? kCGBatch : kCGBatchShort; }
 
 struct FemCtx {
   int device = 0;
@@ -57,6 +65,8 @@ struct FemCtx {
   int max_slots = 0;
   uint8_t* fixed = nullptr;
   double* fixed_vals = nullptr;
+  double* fixed_vals_full = nullptr;  // last values given to fem_set_bc (fem_set_load_scale scales them)
+  double* fext_full = nullptr;
   double* fext = nullptr;
   double* u = nullptr;
   double* u_base = nullptr;
@@ -108,6 +118,9 @@ struct FemCtx {
   float* cfeat = nullptr;
   std::vector<double> elem_modulus;  // internal element order
   int64_t n_fallbacks = 0;
+  int64_t n_alt_steps = 0;    // learned FPCG steps that used the Jacobi (+ coarse) direction
+  int64_t n_learned_steps = 0;
+  float* zalt = nullptr;      // [Nn] float4 alternative direction of learned FPCG
   int* h_err = nullptr;
   // training state: backward buffers, gradient, Adam moments, per-sample vectors
   MpnnTrain mtrain{};
@@ -123,7 +136,8 @@ struct FemCtx {
   bool coarse_built = false;
   bool coarse_valid = false;   // Ainv matches the current tangent policy
   int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
-  int coarse_reuse = 1;        // PCG solves one assembly serves
+  int coarse_reuse = 0;        // PCG solves one assembly serves; 0 = adaptive
+  double coarse_base_ipd = -1;  // CG iterations per decade right after the last assembly
   int coarse_uses = 0;
   double coarse_H = 0.0;
   int64_t n_coarse_assemblies = 0;
@@ -255,6 +269,7 @@ void free_ctx(FemCtx* c) {
   if (c->spos) cudaFree(c->spos);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
+                  c->fixed_vals_full, c->fext_full,
                   c->u, c->u_base, c->R, c->tmpd, c->payload, c->ep_c, c->epe_c, c->ep_t,
                   c->epe_t, c->r, c->x, c->p, c->y, c->dinv, c->tmpf, c->d_perm_node,
                   c->d_perm_elem, c->matD, c->matF, c->partials, c->counters, c->scalars, c->cg};
@@ -441,6 +456,8 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->fixed, (size_t)c->Nn))) return st;
   if ((st = dalloc(c, &c->fixed_vals, nd))) return st;
   if ((st = dalloc(c, &c->fext, nd))) return st;
+  if ((st = dalloc(c, &c->fixed_vals_full, nd))) return st;
+  if ((st = dalloc(c, &c->fext_full, nd))) return st;
   if ((st = dalloc(c, &c->u, nd))) return st;
   if ((st = dalloc(c, &c->u_base, nd))) return st;
   if ((st = dalloc(c, &c->R, nd))) return st;
@@ -575,9 +592,9 @@ void enqueue_cg_iter(FemCtx* c, int kind) {
     launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream, 0);
     launch_mpnn_forward(c->mdev, c->r, c->dinv, c->tmpf, c->cg, c->red(), SITE_RZ, c->stream);
     if (c->learned_coarse) launch_coarse_apply(ca, c->r, c->cg, c->stream);
-    launch_fpcg_dots(ca, false, c->learned_coarse, c->r, c->y, c->tmpf, c->p, c->cg, c->red(), SITE_RZ,
-                     c->stream);
-    launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
+    launch_fpcg_dots(ca, false, c->learned_coarse, c->r, c->y, c->dinv, c->tmpf, c->zalt, c->p, c->cg, c->red(),
+                     SITE_RZ, SITE_RZ2, c->stream);
+    launch_fpcg_pupdate(c->p, c->tmpf, c->zalt, c->Nn, c->cg, false, c->stream);
     return;
   }
   if (kind == GRAPH_TWO_LEVEL) {
@@ -671,7 +688,7 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   if (kind == GRAPH_LEARNED) prepare_mpnn_kernels();
   cudaGraph_t g;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < kCGBatch; ++i) enqueue_cg_iter(c, kind);
+  for (int i = 0; i < cg_batch(kind); ++i) enqueue_cg_iter(c, kind);
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
   e = cudaGraphInstantiate(&c->cg_graph[kind], g, 0);
@@ -880,7 +897,7 @@ int build_coarse(FemCtx* c) {
 int ensure_coarse(FemCtx* c) {
   int st;
   if (!c->coarse_built && (st = build_coarse(c))) return st;
-  if (c->coarse_valid && c->coarse_uses < c->coarse_reuse) {
+  if (c->coarse_valid && (c->coarse_reuse == 0 || c->coarse_uses < c->coarse_reuse)) {
     ++c->coarse_uses;
     return FEM_OK;
   }
@@ -923,6 +940,7 @@ int ensure_coarse(FemCtx* c) {
   ++c->n_coarse_assemblies;
   c->coarse_valid = true;
   c->coarse_uses = 1;
+  c->coarse_base_ipd = -1;
   return FEM_OK;
 }
 
@@ -995,6 +1013,7 @@ int ensure_mpnn(FemCtx* c) {
     m.scal = scal;
     m.err = err;
     if (!c->h_err) CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_err), sizeof(int)));
+    if ((st = mpnn_alloc(c, &c->zalt, 4 * (size_t)Nn))) return st;
     CK(cudaStreamSynchronize(c->stream));
     c->mpnn_built = true;
   }
@@ -1133,9 +1152,10 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     const CoarseArgs ca = coarse_args(c);
     launch_mpnn_forward(c->mdev, c->r, c->dinv, c->tmpf, c->cg, c->red(), SITE_RZ, c->stream);
     if (c->learned_coarse) launch_coarse_apply(ca, c->r, c->cg, c->stream);
-    launch_fpcg_dots(ca, true, c->learned_coarse, c->r, c->y, c->tmpf, c->p, c->cg, c->red(), SITE_RZ,
-                     c->stream);
-    c->n_launches += 6 + 1 + (c->learned_coarse ? 2 : 0);
+    launch_fpcg_dots(ca, true, c->learned_coarse, c->r, c->y, c->dinv, c->tmpf, c->zalt, c->p, c->cg, c->red(),
+                     SITE_RZ, SITE_RZ2, c->stream);
+    launch_fpcg_pupdate(c->p, c->tmpf, c->zalt, c->Nn, c->cg, true, c->stream);
+    c->n_launches += 6 + 2 + (c->learned_coarse ? 2 : 0);
     CKL();
   }
   if (tl) {
@@ -1145,7 +1165,7 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     c->n_launches += 3;
     CKL();
   }
-  const int max_batches = maxit / kCGBatch + 2;
+  const int max_batches = maxit / cg_batch(kind) + 2;
   CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   int batches = 0;
@@ -1158,10 +1178,29 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   }
   const CGState& h = *c->h_cg;
   c->n_cg_iters += h.iter;
+  if ((tl || (learned && c->learned_coarse)) && c->coarse_reuse == 0 && h.done == 1 && h.rr0 > 0 && h.rr > 0) {
+    // adaptive reuse: iterations per decade of residual reduction; once a
+    // solve needs 1.5x the rate measured right after the assembly, the coarse
+    // operator is rebuilt at the next tangent
+    const double decades = std::max(0.5 * std::log10(h.rr0 / h.rr), 0.25);
+    const double ipd = h.iter / decades;
+    if (c->coarse_base_ipd < 0)
+      c->coarse_base_ipd = ipd;
+    else if (ipd > 1.5 * c->coarse_base_ipd + 2.0)
+      c->coarse_valid = false;
+  }
   // kernels that did work: 3 (Jacobi), 6 (two-level) or 11 + 2 (learned,
   // + coarse) per CG iteration; the rest of a batch exits at entry
-  c->n_launches += (tl ? 6LL : (learned ? (11LL + (c->learned_coarse ? 2 : 0)) : 3LL)) * h.iter;
   if (learned) {
+    // the network's 6 kernels run until it is switched off (after 3 rejected steps)
+    const int64_t net_steps = std::max<int64_t>(0, (int64_t)h.iter - h.n_alt + std::min(h.n_alt, 3));
+    c->n_launches += (5LL + (c->learned_coarse ? 2 : 0)) * h.iter + 6LL * net_steps;
+  } else {
+    c->n_launches += (tl ? 6LL : 3LL) * h.iter;
+  }
+  if (learned) {
+    c->n_alt_steps += h.n_alt;
+    c->n_learned_steps += h.iter;
     CK(cudaMemcpyAsync(c->h_err, c->mdev.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (*c->h_err) return set_err(c, FEM_ERR_BUDGET, "learned preconditioner: tensor-core wait gave up");
@@ -1304,11 +1343,13 @@ int fem_ctx_stats(void* ctx, int64_t* out) {
   return FEM_OK;
 }
 
-int fem_learned_stats(void* ctx, int64_t* out2) {
+int fem_learned_stats(void* ctx, int64_t* out4) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
-  if (!c || !out2) return FEM_ERR_INVALID;
-  out2[0] = c->n_fallbacks;
-  out2[1] = c->mpnn_has_weights ? 1 : 0;
+  if (!c || !out4) return FEM_ERR_INVALID;
+  out4[0] = c->n_fallbacks;
+  out4[1] = c->mpnn_has_weights ? 1 : 0;
+  out4[2] = c->n_learned_steps;
+  out4[3] = c->n_alt_steps;
   return FEM_OK;
 }
 
@@ -1346,8 +1387,8 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       c->learned_coarse = value != 0;
       return FEM_OK;
     case FEM_OPT_COARSE_REUSE:
-      if (value < 1 || value > (1 << 20))
-        return set_err(c, FEM_ERR_INVALID, "coarse reuse count %lld not in [1, 2^20]", (long long)value);
+      if (value < 0 || value > (1 << 20))
+        return set_err(c, FEM_ERR_INVALID, "coarse reuse count %lld not in [0, 2^20]", (long long)value);
       c->coarse_reuse = (int)value;
       return FEM_OK;
     default:
@@ -1653,13 +1694,103 @@ int fem_set_bc(void* ctx, const uint8_t* fixed_mask, const double* fixed_values,
   if (fixed_values) {
     ++c->n_launches; launch_gather_d(fixed_values, c->fixed_vals, c->d_perm_node, c->Nn, c->stream);
     CKL();
+    CK(cudaMemcpyAsync(c->fixed_vals_full, c->fixed_vals, sizeof(double) * c->ndof, cudaMemcpyDeviceToDevice,
+                       c->stream));
   }
   if (f_ext) {
     ++c->n_launches; launch_gather_d(f_ext, c->fext, c->d_perm_node, c->Nn, c->stream);
     CKL();
+    CK(cudaMemcpyAsync(c->fext_full, c->fext, sizeof(double) * c->ndof, cudaMemcpyDeviceToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
   c->tangent_valid = false;
+  return FEM_OK;
+}
+
+int fem_set_load_scale(void* ctx, double s) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!std::isfinite(s)) return set_err(c, FEM_ERR_INVALID, "load scale must be finite");
+  ++c->n_launches; launch_scale_d(c->fixed_vals_full, s, c->fixed_vals, c->ndof, c->stream);
+  ++c->n_launches; launch_scale_d(c->fext_full, s, c->fext, c->ndof, c->stream);
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  c->tangent_valid = false;
+  return FEM_OK;
+}
+
+int fem_batch_solve(void** ctxs, int32_t n, const FemSolveParams* prm, int32_t load_steps,
+                    FemSolveResult* results, int32_t* status, double* wall_ms, int32_t n_threads) {
+  if (!ctxs || n <= 0 || !results || !status) return set_global_error(FEM_ERR_INVALID, "need contexts and outputs");
+  if (load_steps <= 0) return set_global_error(FEM_ERR_INVALID, "load_steps must be > 0");
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) return set_global_error(FEM_ERR_INVALID, "context %d is null", i);
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) return set_global_error(FEM_ERR_INVALID, "context %d repeats context %d", i, j);
+  }
+  FemSolveParams p;
+  if (prm)
+    p = *prm;
+  else
+    fem_default_solve_params(&p);
+  p.progress = nullptr;  // callbacks are not re-entrant across workers
+  const int workers = std::max(1, std::min<int>(n, n_threads > 0 ? n_threads : n));
+  // One thread first brings every instance to a solvable state: tangent at the
+  // current displacement, matvec variant, coarse operator and the captured CG
+  // graph.  Graph capture then never runs while other workers issue work.
+  for (int i = 0; i < n; ++i) {
+    FemCtx* c = static_cast<FemCtx*>(ctxs[i]);
+    int st;
+    if ((st = check_ctx(c))) return st;
+    if (!c->materials_set) return set_err(c, FEM_ERR_STATE, "materials not set");
+    if (!c->tangent_valid && (st = eval_residual(c, nullptr, nullptr))) return st;
+    const bool tl = p.precond == FEM_PRECOND_TWO_LEVEL;
+    const bool learned = p.precond == FEM_PRECOND_LEARNED;
+    if (learned && !c->mpnn_has_weights) return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights");
+    if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : p.precond))) return st;
+    if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
+    if (learned && (st = ensure_mpnn(c))) return st;
+    if ((st = ensure_cg_graph(c, learned ? GRAPH_LEARNED : (tl ? GRAPH_TWO_LEVEL : GRAPH_JACOBI)))) return st;
+  }
+  std::atomic<int> next{0};
+  auto work = [&]() {
+    cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+    cudaThreadExchangeStreamCaptureMode(&mode);
+    for (int i = next.fetch_add(1); i < n; i = next.fetch_add(1)) {
+      FemCtx* c = static_cast<FemCtx*>(ctxs[i]);
+      const auto t0 = std::chrono::steady_clock::now();
+      FemSolveResult agg;
+      std::memset(&agg, 0, sizeof(agg));
+      agg.converged = 1;
+      int st = FEM_OK;
+      for (int k = 1; k <= load_steps && (st == FEM_OK || st == FEM_NOT_CONVERGED); ++k) {
+        st = fem_set_load_scale(c, (double)k / load_steps);
+        if (st) break;
+        FemSolveResult r;
+        std::memset(&r, 0, sizeof(r));
+        st = fem_newton_solve(c, &p, &r);
+        agg.iterations += r.iterations;
+        agg.cg_iterations += r.cg_iterations;
+        agg.residual_evals += r.residual_evals;
+        agg.residual = r.residual;
+        agg.relative_residual = std::max(agg.relative_residual, r.relative_residual);
+        if (k == 1) agg.first_residual = r.first_residual;
+        if (!r.converged) agg.converged = 0;
+      }
+      results[i] = agg;
+      status[i] = st;
+      if (wall_ms)
+        wall_ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    cudaThreadExchangeStreamCaptureMode(&mode);
+  };
+  std::vector<std::thread> pool;
+  for (int w = 1; w < workers; ++w) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  for (int i = 0; i < n; ++i)
+    if (status[i] != FEM_OK && status[i] != FEM_NOT_CONVERGED) return status[i];
   return FEM_OK;
 }
 

@@ -49,6 +49,10 @@ struct Reduce {
 struct CGState {
   double rz, pAp, rr, rr0, tol2, alpha, beta, pad;
   int iter, max_iter, done, status;  // done: 0 running, 1 converged, 2 max iters, 3 breakdown
+  int zsel;                          // learned FPCG: 1 = this step used the Jacobi (+ coarse) direction
+  int n_alt;                         // learned FPCG: steps that used it
+  int locked;                        // learned FPCG: network switched off for the rest of the solve
+  int pad2;
 };
 
 struct ResArgs {
@@ -165,6 +169,17 @@ struct MpnnTrain {
   float* gpart;                 // [tiles][kMpnnParams] per-tile gradient shares
 };
 
+// Raises a kernel's dynamic shared-memory limit to the device's opt-in maximum
+// (minus the kernel's static shared memory), once per (device, kernel).  The
+// limit is process-wide state: setting it to what one mesh needs would fail
+// the launches of a larger mesh, or of another thread, so it is only ever
+// raised to the maximum (fem_smem.cu).
+void raise_smem_limit(const void* kernel);
+template <typename K>
+inline void raise_smem_limit_k(K kernel) {
+  raise_smem_limit(reinterpret_cast<const void*>(kernel));
+}
+
 // Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
 // returns `code`.
 int set_global_error(int code, const char* fmt, ...);
@@ -189,9 +204,13 @@ void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg,
 void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* dinv, float* z, float* p,
                   CGState* cg, Reduce red, int site, cudaStream_t s);
 void launch_tl_pupdate(float* p, const float* z, int n_nodes, const CGState* cg, cudaStream_t s);
-// flexible PCG: [z += P yc], rz = r.z, z.q; init: p = z; else Polak-Ribiere beta
-void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q, float* z,
-                      float* p, CGState* cg, Reduce red, int site, cudaStream_t s);
+// learned flexible PCG: [z += P yc], safeguard against the Jacobi (+ coarse)
+// direction zalt, rz and Polak-Ribiere beta (two reduction sites)
+void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q,
+                      const float* dinv, float* z, float* zalt, float* p, CGState* cg, Reduce red, int site,
+                      int site2, cudaStream_t s);
+void launch_fpcg_pupdate(float* p, const float* z, const float* zalt, int n_nodes, const CGState* cg, bool init,
+                         cudaStream_t s);
 
 // learned preconditioner (fem_mpnn.cu)
 void prepare_mpnn_kernels();
@@ -247,6 +266,8 @@ void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, 
 // u[3n+d] = u_base[3n+d] + alpha du[4n+d] for n < n_nodes
 void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int n_nodes,
                      cudaStream_t s);
+// out[i] = s in[i], i < n
+void launch_scale_d(const double* in, double s, double* out, int n, cudaStream_t st);
 // X32[n].w = fixed bits of node n
 void launch_x32_mask(float4* X32, const uint8_t* fixed, int n, cudaStream_t s);
 void launch_gather_d_masked(const double* in_user, double* out_int, const int* perm,

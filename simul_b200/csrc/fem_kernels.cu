@@ -518,6 +518,9 @@ __global__ void __launch_bounds__(kVecThreads) cg_init_kernel(const double* __re
       cg->pAp = 0.0;
       cg->iter = 0;
       cg->max_iter = maxit;
+      cg->zsel = 0;
+      cg->n_alt = 0;
+      cg->locked = 0;
       cg->status = isfinite(trr) ? 0 : 3;
       cg->done = (!isfinite(trr)) ? 3 : ((trr == 0.0 || (jac && !(trz > 0.0))) ? 1 : 0);
       red.counters[site] = 0u;
@@ -808,15 +811,12 @@ __global__ void rhs_minus_kernel(const double* R, const float* y, const uint8_t*
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
 
-// Raises a kernel's dynamic shared-memory limit to what the launch needs (the
-// default limit counts static + dynamic shared memory).  Skipped while the
-// stream is being captured: prepare_kernels sets the limit beforehand.
+// Every launch below raises its kernel's shared-memory limit to the device
+// maximum first (once per kernel; also before stream capture, in
+// prepare_kernels).
 template <typename K>
-static void allow_smem(K kernel, size_t smem, cudaStream_t s) {
-  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  cudaStreamIsCapturing(s, &cs);
-  if (cs != cudaStreamCaptureStatusNone) return;
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+static void allow_smem(K kernel, size_t, cudaStream_t) {
+  raise_smem_limit_k(kernel);
 }
 
 static size_t slots_smem(const MeshDev& m) { return sizeof(uint32_t) * (size_t)m.max_slots; }
@@ -899,7 +899,8 @@ void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
 
 template <int NB>
 static void prepare_nb(int model, size_t smem) {
-  auto set = [&](auto k) { cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); };
+  (void)smem;
+  auto set = [&](auto k) { raise_smem_limit_k(k); };
   switch (model) {
     case M_LE: set(matvec_kernel<NB, M_LE, true>); break;
     case M_NH: set(matvec_kernel<NB, M_NH, true>); break;
@@ -1004,6 +1005,15 @@ void launch_scatter_f2d(const float* in_int, double* out_user, const int* perm, 
                         cudaStream_t s) {
   scatter_f4_kernel<double><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
 }
+__global__ void scale_d_kernel(const double* in, double s, double* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = s * in[i];
+}
+
+void launch_scale_d(const double* in, double s, double* out, int n, cudaStream_t st) {
+  scale_d_kernel<<<nblk(n, 256), 256, 0, st>>>(in, s, out, n);
+}
+
 void launch_x32_mask(float4* X32, const uint8_t* fixed, int n, cudaStream_t s) {
   x32_mask_kernel<<<nblk(n, 256), 256, 0, s>>>(X32, fixed, n);
 }

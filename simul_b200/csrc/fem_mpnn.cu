@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(256) mpnn_scale_kernel(const __grid_constant__
                                                          const float* __restrict__ r,
                                                          const float* __restrict__ dinv, const CGState* cg,
                                                          Reduce red, int site) {
-  if (cg && cg->done) return;
+  if (cg && (cg->done || cg->locked)) return;
   __shared__ double sred[8];
   __shared__ bool am_last;
   const int i = blockIdx.x * 256 + threadIdx.x;
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(256) mpnn_scale_kernel(const __grid_constant__
 __global__ void __launch_bounds__(kTile) mpnn_encode_kernel(const __grid_constant__ MpnnDev m,
                                                             const float* __restrict__ r,
                                                             const float* __restrict__ dinv, const CGState* cg) {
-  if (cg && cg->done) return;
+  if (cg && (cg->done || cg->locked)) return;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(2 * kTile) mpnn_layer_kernel(const __grid_cons
                                                                const float* __restrict__ r,
                                                                const float* __restrict__ dinv, float* z,
                                                                const CGState* cg) {
-  if (cg && cg->done) return;
+  if (cg && (cg->done || cg->locked)) return;
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
@@ -657,10 +657,10 @@ constexpr size_t kEncSmem = 32 * 1024;
 constexpr size_t kLayerSmem = kTile * 2 * kHid * 2 + kHid * 2 * kHid * 2;  // 48 KB: <= 4 CTAs per SM
 
 void prepare_mpnn_kernels() {
-  cudaFuncSetAttribute(mpnn_layer_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
-  cudaFuncSetAttribute(mpnn_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEncSmem);
-  cudaFuncSetAttribute(mpnn_layer_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLayerSmem);
-  cudaFuncSetAttribute(mpnn_layer_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLayerSmem);
+  raise_smem_limit_k(mpnn_layer_bwd_kernel);
+  raise_smem_limit_k(mpnn_encode_kernel);
+  raise_smem_limit_k(mpnn_layer_kernel<false>);
+  raise_smem_limit_k(mpnn_layer_kernel<true>);
 }
 
 void launch_mpnn_pack(const float* w, __nv_bfloat16* We_p, __nv_bfloat16* Wl_p, __nv_bfloat16* WlT_p,

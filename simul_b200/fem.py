@@ -66,7 +66,7 @@ class FEMesh:
     """
 
     def __init__(self, n_nodes: int, n_elements: int, element_type: ElementType = ElementType.TET4,
-                 device=None, nodes_per_block: int = 0):
+                 device=None, nodes_per_block: int = 0, own_stream: bool = False):
         if element_type is not ElementType.TET4 and element_type != "C3D4":
             raise FEAValidationError(f"element type {element_type} is not supported by the B200 path "
                                      "(TET4 only)", parameter="element_type", value=element_type)
@@ -78,6 +78,9 @@ class FEMesh:
         self.n_gauss = 1
         self.device = _require_cuda(device)
         self.nodes_per_block = nodes_per_block
+        # own_stream: the library creates a private non-blocking stream for this
+        # mesh (batched solves); callers then synchronise torch work themselves
+        self.own_stream = bool(own_stream)
         self._ctx = None
         self._bound_material = None
         z = lambda *s, dt=torch.float64: torch.zeros(*s, dtype=dt, device=self.device)
@@ -109,7 +112,7 @@ class FEMesh:
             self.material_id = np.asarray(material_ids, dtype=np.int32).copy()
         lib = _lib.load()
         with torch.cuda.device(self.device):
-            stream = torch.cuda.current_stream(self.device).cuda_stream
+            stream = None if self.own_stream else torch.cuda.current_stream(self.device).cuda_stream
             desc = _lib.FemMeshDesc(self.n_nodes, self.n_elements,
                                     nodes.ctypes.data_as(C.POINTER(C.c_double)),
                                     elements.ctypes.data_as(C.POINTER(C.c_int32)),
@@ -161,7 +164,7 @@ class FEMesh:
 
     def set_coarse_options(self, cell=None, reuse=None):
         """Two-level preconditioner: lattice cell edge in mesh lengths and the
-        number of PCG solves one coarse assembly serves."""
+        number of PCG solves one coarse assembly serves (0: adaptive)."""
         lib = _lib.load()
         if cell is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_CELL, int(cell)), self.ctx, "fem_set_option")
@@ -216,6 +219,8 @@ class FEMesh:
 
     def _push_bc(self):
         mask = (self.fixed != 0).to(torch.uint8).contiguous()
+        if self.own_stream:
+            torch.cuda.current_stream(self.device).synchronize()
         _check(_lib.load().fem_set_bc(self.ctx, _ptr(mask), _ptr(self.fixed_value.contiguous()),
                                       _ptr(self.f_ext.contiguous())), self.ctx, "fem_set_bc")
         self._bc_dirty = False

@@ -269,9 +269,27 @@ __global__ void __launch_bounds__(kRestrictThreads) coarse_restrict_kernel(
   }
 }
 
-// y_c = Ainv r_c.  Every CTA stages r_c in shared memory: r_c[I] adds its
-// cells' shares in the fixed order of cn_cells (the eight entries are loaded
-// together, then the shares); then one warp per row.
+// rc[I] = sum of the cells' shares of coarse DOF I, in the fixed order of
+// cn_cells (the eight entries are loaded together, then the shares)
+__global__ void __launch_bounds__(256) coarse_rc_kernel(const __grid_constant__ CoarseDev c, const CGState* cg) {
+  if (cg && cg->done) return;
+  const int I = blockIdx.x * 256 + threadIdx.x;
+  if (I >= c.n_dof) return;
+  const int nI = I / 3, dI = I - 3 * nI;
+  const int4* ep = reinterpret_cast<const int4*>(c.cn_cells + nI * 8);
+  const int4 e0 = __ldg(ep), e1 = __ldg(ep + 1);
+  const int ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+  float sh[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    sh[k] = ent[k] >= 0 ? __ldcg(c.cell_r + (ent[k] >> 3) * 24 + 3 * (ent[k] & 7) + dI) : 0.f;
+  float v = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v += sh[k];
+  c.rc[I] = v;
+}
+
+// y_c = Ainv r_c: r_c staged in shared memory, one warp per row
 constexpr int kCoarseMvThreads = 256;
 
 __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
@@ -279,20 +297,7 @@ __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
   if (cg && cg->done) return;
   extern __shared__ __align__(16) float s_rc[];
   const int n = c.n_dof;
-  for (int I = threadIdx.x; I < n; I += kCoarseMvThreads) {
-    const int nI = I / 3, dI = I - 3 * nI;
-    const int4* ep = reinterpret_cast<const int4*>(c.cn_cells + nI * 8);
-    const int4 e0 = __ldg(ep), e1 = __ldg(ep + 1);
-    const int ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-    float sh[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-      sh[k] = ent[k] >= 0 ? __ldcg(c.cell_r + (ent[k] >> 3) * 24 + 3 * (ent[k] & 7) + dI) : 0.f;
-    float v = 0.f;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v += sh[k];
-    s_rc[I] = v;
-  }
+  for (int I = threadIdx.x; I < n; I += kCoarseMvThreads) s_rc[I] = __ldcg(c.rc + I);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * (kCoarseMvThreads / 32) + warp;
@@ -640,6 +645,7 @@ void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s) {
 
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
   coarse_restrict_kernel<<<a.c.n_cells, kRestrictThreads, 0, s>>>(a, r, cg);
+  coarse_rc_kernel<<<nblk(a.c.n_dof, 256), 256, 0, s>>>(a.c, cg);
   const int rows_per_cta = kCoarseMvThreads / 32;
   coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(
       a.c, cg);

@@ -867,6 +867,7 @@ int build_coarse(FemCtx* c) {
   if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
   if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * 24))) return st;
   if ((st = coarse_alloc(c, &cd.yc, nd))) return st;
+  if ((st = coarse_alloc(c, &cd.rc, nd))) return st;
   if (!c->solver) {
     if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS)
       return set_err(c, FEM_ERR_CUDA, "cusolverDnCreate failed");
@@ -1095,7 +1096,7 @@ void mpnn_apply(FemCtx* c, const float* r, float* z, bool coarse, bool base) {
     const CoarseArgs ca = coarse_args(c);
     launch_coarse_apply(ca, r, nullptr, c->stream);
     launch_coarse_add(ca, z, c->stream);
-    c->n_launches += 3;
+    c->n_launches += 4;
   }
 }
 
@@ -1155,14 +1156,14 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     launch_fpcg_dots(ca, true, c->learned_coarse, c->r, c->y, c->dinv, c->tmpf, c->zalt, c->p, c->cg, c->red(),
                      SITE_RZ, SITE_RZ2, c->stream);
     launch_fpcg_pupdate(c->p, c->tmpf, c->zalt, c->Nn, c->cg, true, c->stream);
-    c->n_launches += 6 + 2 + (c->learned_coarse ? 2 : 0);
+    c->n_launches += 6 + 2 + (c->learned_coarse ? 3 : 0);
     CKL();
   }
   if (tl) {
     const CoarseArgs ca = coarse_args(c);
     launch_coarse_apply(ca, c->r, c->cg, c->stream);
     launch_tl_rz(ca, true, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
-    c->n_launches += 3;
+    c->n_launches += 4;
     CKL();
   }
   const int max_batches = maxit / cg_batch(kind) + 2;
@@ -1194,9 +1195,9 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if (learned) {
     // the network's 6 kernels run until it is switched off (after 3 rejected steps)
     const int64_t net_steps = std::max<int64_t>(0, (int64_t)h.iter - h.n_alt + std::min(h.n_alt, 3));
-    c->n_launches += (5LL + (c->learned_coarse ? 2 : 0)) * h.iter + 6LL * net_steps;
+    c->n_launches += (5LL + (c->learned_coarse ? 3 : 0)) * h.iter + 6LL * net_steps;
   } else {
-    c->n_launches += (tl ? 6LL : 3LL) * h.iter;
+    c->n_launches += (tl ? 7LL : 3LL) * h.iter;
   }
   if (learned) {
     c->n_alt_steps += h.n_alt;

@@ -117,6 +117,7 @@ struct CoarseDev {
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
   float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric)
   float* cell_r;            // [n_cells][24] restricted residual per cell
+  float* rc;                // [n_dof] coarse residual P^T r
   float* yc;                // [n_dof] coarse correction
 };
 

@@ -326,8 +326,10 @@ __device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
   __stcg(a.stage + sp.w, make_float4(f[3][0], f[3][1], f[3][2], 0.f));
 }
 
+// 5 CTAs per SM: 48 registers (no spills) instead of 52 lift occupancy from
+// 50 % to 62.5 % for this latency-bound gather-compute-scatter kernel.
 template <int MODEL, bool CG>
-__global__ void __launch_bounds__(256) elem_mv_kernel(const __grid_constant__ MvArgs a) {
+__global__ void __launch_bounds__(256, 5) elem_mv_kernel(const __grid_constant__ MvArgs a) {
   if (CG) {
     if (a.cg->done) return;
   }

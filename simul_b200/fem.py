@@ -607,7 +607,7 @@ class TransverseIsotropic(MaterialBase):
 
 _LS = {"reference": _lib.FEM_LS_REFERENCE, "guarded": _lib.FEM_LS_GUARDED, "none": _lib.FEM_LS_NONE}
 _PC = {"jacobi": _lib.FEM_PRECOND_JACOBI, "none": _lib.FEM_PRECOND_NONE,
-       "two_level": _lib.FEM_PRECOND_TWO_LEVEL}
+       "two_level": _lib.FEM_PRECOND_TWO_LEVEL, "learned": _lib.FEM_PRECOND_LEARNED}
 
 
 class StaticSolver:
@@ -621,7 +621,7 @@ class StaticSolver:
     residual too; J2 history is committed once per converged ``solve()``.
     ``linear_solver`` is accepted for compatibility (the B200 path always
     uses PCG).  Extra keyword options: ``line_search`` ("guarded",
-    "reference", "none"), ``precond`` ("jacobi", "none"),
+    "reference", "none"), ``precond`` ("jacobi", "none", "two_level", "learned"),
     ``cg_max_iterations``, ``cg_rtol_min``, ``cg_rtol_max``.
     """
 

@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--n", type=int, default=64, help="voxels per axis of the vertebral grid")
+    ap.add_argument("--n", "--grid", dest="n", type=int, default=64, help="voxels per axis of the vertebral grid")
     ap.add_argument("--load-steps", type=int, default=20)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -62,6 +62,16 @@ def parse():
                     help="PCG solves one coarse-operator assembly serves (0: adaptive)")
     ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
     return ap.parse_args()
+
+
+def max_over_ranks(x: float, device, ws: int) -> float:
+    """Max of a per-rank timing over all ranks (any backend; identity at N=1)."""
+    if ws <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
 
 
 def world():
@@ -307,10 +317,7 @@ def main():
     launches = mesh.stats()["launches"] - launches0
     clk = clocks.stop()
     ms = float(np.mean(step_ms))
-    if ws > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dev, ws)
 
     # end to end through the public API: per-solve inputs from pinned host memory
     h_fixed = torch.from_numpy(v.fixed_vals).pin_memory()
@@ -341,10 +348,7 @@ def main():
     h2d = h_fixed.numel() * 8 + h_mask.numel() * 4 + h_fext.numel() * 8
     d2h = h_u.numel() * 8
     e2e_s = float(np.mean(e2e_ms)) / 1e3
-    if ws > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dev, ws)
 
     # the plain method timed beside the chosen one (same mesh, same clocks regime)
     jac = None
@@ -360,10 +364,7 @@ def main():
         e1.record(stream)
         e1.synchronize()
         jms = e0.elapsed_time(e1)
-        if ws > 1:
-            t = torch.tensor([jms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            jms = float(t.item())
+        jms = max_over_ranks(jms, dev, ws)
         jac = {"s": jms / 1e3, "newton_iterations": jl["newton"], "cg_iterations": jl["cg"],
                "all_converged": bool(jl["converged"]), "max_relative_residual": jl["max_rel"],
                "speedup_of_timed_method": jms / ms, "timed_once_after_one_warmup": True}
@@ -381,6 +382,7 @@ def main():
     variant = st["matvec_variant"]
     traffic = load_traffic().get(f"matvec_{variant}_j2_n{args.n}")
     line = {"metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "job_solves_per_s": ws / (ms / 1e3),
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 matvec / f64 residual+dots",
             "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),

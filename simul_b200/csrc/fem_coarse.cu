@@ -222,10 +222,12 @@ __global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
 
 // ───────────────────────── per-iteration application ─────────────────────────
 
-// cell_r[cell][3 corner + d] = sum over the cell's nodes of w_corner r_d.
-// One CTA of kRestrictThreads per cell: warp-shuffle sums, then the warps'
+// cell_r[cell][slice][3 corner + d] = sum over the slice's nodes of
+// w_corner r_d.  kRestrictSlices CTAs of kRestrictThreads per cell (slice s
+// takes the cell's nodes s, s + S, ...): warp-shuffle sums, then the warps'
 // 24-value shares added in warp order (one barrier).
 constexpr int kRestrictThreads = 128;
+constexpr int kRestrictSlices = 4;
 
 __global__ void __launch_bounds__(kRestrictThreads) coarse_restrict_kernel(
     const __grid_constant__ CoarseArgs a, const float* __restrict__ r, const CGState* cg) {
@@ -233,13 +235,13 @@ __global__ void __launch_bounds__(kRestrictThreads) coarse_restrict_kernel(
   __shared__ float sw[kRestrictThreads / 32][24];
   const CoarseDev& c = a.c;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cell = blockIdx.x;
+  const int cell = blockIdx.x / kRestrictSlices, slice = blockIdx.x - cell * kRestrictSlices;
   const int3 ijk = c.cell_ijk[cell];
   const int n0 = c.cell_node_ptr[cell], n1 = c.cell_node_ptr[cell + 1];
   float acc[24];
 #pragma unroll
   for (int k = 0; k < 24; ++k) acc[k] = 0.f;
-  for (int i = n0 + threadIdx.x; i < n1; i += kRestrictThreads) {
+  for (int i = n0 + slice + kRestrictSlices * (int)threadIdx.x; i < n1; i += kRestrictSlices * kRestrictThreads) {
     const int node = __ldg(c.cell_nodes + i);
     const float4 X = __ldg(a.m.X32 + node);
     const float4 rv = reinterpret_cast<const float4*>(r)[node];
@@ -265,7 +267,7 @@ __global__ void __launch_bounds__(kRestrictThreads) coarse_restrict_kernel(
     float v = 0.f;
 #pragma unroll
     for (int w = 0; w < kRestrictThreads / 32; ++w) v += sw[w][threadIdx.x];
-    c.cell_r[cell * 24 + threadIdx.x] = v;
+    c.cell_r[(size_t)blockIdx.x * 24 + threadIdx.x] = v;
   }
 }
 
@@ -279,13 +281,19 @@ __global__ void __launch_bounds__(256) coarse_rc_kernel(const __grid_constant__ 
   const int4* ep = reinterpret_cast<const int4*>(c.cn_cells + nI * 8);
   const int4 e0 = __ldg(ep), e1 = __ldg(ep + 1);
   const int ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-  float sh[8];
+  float sh[8][kRestrictSlices];
 #pragma unroll
   for (int k = 0; k < 8; ++k)
-    sh[k] = ent[k] >= 0 ? __ldcg(c.cell_r + (ent[k] >> 3) * 24 + 3 * (ent[k] & 7) + dI) : 0.f;
+#pragma unroll
+    for (int q = 0; q < kRestrictSlices; ++q)
+      sh[k][q] = ent[k] >= 0
+                     ? __ldcg(c.cell_r + ((size_t)(ent[k] >> 3) * kRestrictSlices + q) * 24 + 3 * (ent[k] & 7) + dI)
+                     : 0.f;
   float v = 0.f;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) v += sh[k];
+  for (int k = 0; k < 8; ++k)
+#pragma unroll
+    for (int q = 0; q < kRestrictSlices; ++q) v += sh[k][q];
   c.rc[I] = v;
 }
 
@@ -607,6 +615,7 @@ static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 size_t coarse_cell_smem() { return sizeof(float) * kCellThreads * (144 + 32); }
 int coarse_cell_slices() { return kCellSlices; }
+int coarse_restrict_slices() { return kRestrictSlices; }
 
 void prepare_coarse_kernels(int model, int n_dof) {
   (void)n_dof;
@@ -644,7 +653,7 @@ void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s) {
 }
 
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
-  coarse_restrict_kernel<<<a.c.n_cells, kRestrictThreads, 0, s>>>(a, r, cg);
+  coarse_restrict_kernel<<<a.c.n_cells * kRestrictSlices, kRestrictThreads, 0, s>>>(a, r, cg);
   coarse_rc_kernel<<<nblk(a.c.n_dof, 256), 256, 0, s>>>(a.c, cg);
   const int rows_per_cta = kCoarseMvThreads / 32;
   coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(

@@ -865,7 +865,7 @@ int build_coarse(FemCtx* c) {
   if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * coarse_cell_slices() * 576))) return st;
   if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
   if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
-  if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * 24))) return st;
+  if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * coarse_restrict_slices() * 24))) return st;
   if ((st = coarse_alloc(c, &cd.yc, nd))) return st;
   if ((st = coarse_alloc(c, &cd.rc, nd))) return st;
   if (!c->solver) {

@@ -116,7 +116,7 @@ struct CoarseDev {
   double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
   float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric)
-  float* cell_r;            // [n_cells][24] restricted residual per cell
+  float* cell_r;            // [n_cells][slices][24] restricted residual shares per cell
   float* rc;                // [n_dof] coarse residual P^T r
   float* yc;                // [n_dof] coarse correction
 };
@@ -194,6 +194,7 @@ void launch_diag(const DiagArgs& a, int model, cudaStream_t s);
 // coarse lattice (fem_coarse.cu)
 size_t coarse_cell_smem();
 int coarse_cell_slices();   // CTAs (and Galerkin block slots) per lattice cell
+int coarse_restrict_slices();  // CTAs (and restricted-residual slots) per lattice cell
 void prepare_coarse_kernels(int model, int n_dof);
 // cell Galerkin blocks + dense Ac (FP64, column-major)
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);

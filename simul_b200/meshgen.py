@@ -212,3 +212,82 @@ def vertebral_body(n=64, seed=0, a=15.0, b=12.0, height=25.0, extent=32.0,
                    info={"kind": "vertebral_body", "n": n, "h": h, "seed": seed, "nu": nu,
                          "n_voxels": int(mask.sum()), "height": float(top_z),
                          "shell_elements": int(np.sum(E == E_cortical))})
+
+
+def top_moment_forces(X: np.ndarray, top: np.ndarray, case: str, moment: float) -> np.ndarray:
+    """Nodal forces on the ``top`` nodes equivalent to a moment (N mm) about
+    the top face's centroid: a linear force couple (flexion / extension about
+    x, lateral bending about y) or a tangential couple (torsion about z).
+    No rigid plate is modelled."""
+    f = np.zeros_like(X)
+    xc = X[top, 0] - X[top, 0].mean()
+    yc = X[top, 1] - X[top, 1].mean()
+    ft = np.zeros((int(np.count_nonzero(top)), 3))
+    if case in ("flexion", "extension"):
+        sgn = 1.0 if case == "flexion" else -1.0
+        ft[:, 2] = -sgn * moment * yc / np.sum(yc * yc)
+    elif case == "lateral_bending":
+        ft[:, 2] = -moment * xc / np.sum(xc * xc)
+    elif case == "torsion":
+        r2 = np.sum(xc * xc + yc * yc)
+        ft[:, 0] = -moment * yc / r2
+        ft[:, 1] = moment * xc / r2
+    else:
+        raise ValueError(f"unknown moment case {case!r}")
+    f[top] = ft
+    return f
+
+
+def motion_segment(n=80, seed=0, a=15.0, b=12.0, body_height=25.0, disc_height=10.0, extent=32.0,
+                   E_cortical=12e3, E_core_median=300.0, core_sigma=0.3, smooth_voxels=3.0,
+                   shell_voxels=2, screw_radius=3.0, screw_length=45.0) -> TetMesh:
+    """Synthetic motion segment: two vertebral bodies (as ``vertebral_body``,
+    n voxels across ``extent``) joined by an intervertebral disc, with a
+    titanium pedicle-screw cylinder in the lower body.
+
+    Voxel spacing h = extent / n; the stack is body (z in [0, H)), disc
+    ([H, H + D)), body ([H + D, 2H + D)), all with the elliptic cross-section.
+    The screw (radius 3 mm, length 45 mm) runs along y through the lower
+    body's mid-height, its tip at the anterior surface; the part behind the
+    body (up to the grid's edge) stays screw material.  Material ids per element: 0 bone (per-element
+    modulus in ``E``), 1 disc, 2 screw.  Bottom face fixed; loads are left to
+    the caller (``top_moment_forces``).
+    """
+    from scipy import ndimage
+
+    h = extent / n
+    H, D = body_height, disc_height
+    nz = int(round((2 * H + D) / h))
+    c = (np.arange(n) + 0.5) * h - extent / 2.0
+    zc = (np.arange(nz) + 0.5) * h
+    Xv, Yv, Zv = np.meshgrid(c, c, zc, indexing="ij")
+    ell = (Xv / a) ** 2 + (Yv / b) ** 2 <= 1.0
+    lower = ell & (Zv < H)
+    disc = ell & (Zv >= H) & (Zv < H + D)
+    upper = ell & (Zv >= H + D) & (Zv < 2 * H + D)
+    # the screw's tip reaches the anterior surface (y = +b); the rest runs
+    # posteriorly, clipped to the voxel grid
+    y_tip = b
+    screw = ((Xv ** 2 + (Zv - H / 2.0) ** 2) <= screw_radius ** 2) & (Yv < y_tip) & (Yv >= y_tip - screw_length)
+    bone = (lower | upper) & ~screw
+    mask = bone | disc | screw
+    rng = np.random.default_rng(seed)
+    core = ndimage.binary_erosion(lower, iterations=shell_voxels) | ndimage.binary_erosion(upper, iterations=shell_voxels)
+    z = ndimage.gaussian_filter(rng.standard_normal(mask.shape), sigma=smooth_voxels)
+    zsel = z[core & bone]
+    z = (z - zsel.mean()) / zsel.std()
+    Evox = np.where(core, E_core_median * np.exp(core_sigma * z), E_cortical)
+    mid = np.zeros(mask.shape, dtype=np.int32)
+    mid[disc] = 1
+    mid[screw] = 2
+    X, conn, vox, (vi, vj, vk) = voxel_tets(mask, h, origin=(-extent / 2.0, -extent / 2.0, 0.0))
+    E = Evox[vi, vj, vk][vox]
+    ids = mid[vi, vj, vk][vox]
+    E = np.where(ids == 0, E, 1.0)
+    fixed = np.zeros((X.shape[0], 3), dtype=bool)
+    fixed[np.isclose(X[:, 2], 0.0)] = True
+    return TetMesh(X=X, conn=conn, E=E.astype(np.float64), fixed_mask=fixed, fixed_vals=np.zeros_like(X),
+                   f_ext=np.zeros_like(X),
+                   info={"kind": "motion_segment", "n": n, "h": h, "seed": seed, "material_ids": ids,
+                         "n_voxels": int(mask.sum()), "height": float(X[:, 2].max()),
+                         "disc_elements": int(np.sum(ids == 1)), "screw_elements": int(np.sum(ids == 2))})

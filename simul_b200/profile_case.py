@@ -5,7 +5,8 @@ plasticity, evaluates the FP64 residual at a plastic state (top face pushed
 ``--strain`` of the height, which yields the cortical shell), and launches each
 hot kernel ``--reps`` times through ``fem_profile_kernels``: the tangent matvec
 (the variant given by ``--variant``), the FP64 residual, the CG update and the
-CG direction update.  The per-launch CUDA-event times are printed as one JSON
+CG direction update; optionally the learned network's forward pass
+(``--learned weights.npz``) and one two-level PCG solve (``--two-level``).  The per-launch CUDA-event times are printed as one JSON
 line.  With ``--reps 3`` and ``-k``/``-c`` filters an ncu capture of one kernel
 ends in seconds.
 
@@ -27,6 +28,8 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--strain", type=float, default=0.004)
     ap.add_argument("--nodes-per-block", type=int, default=0)
+    ap.add_argument("--learned", default="", help="weights file: also run the network forward --reps times")
+    ap.add_argument("--two-level", action="store_true", help="also run one two-level PCG solve (rtol 1e-6)")
     args = ap.parse_args(argv)
 
     import torch
@@ -53,10 +56,36 @@ def main(argv=None):
     if rc != 0:
         raise RuntimeError(_lib.last_error(mesh.ctx))
     torch.cuda.synchronize()
+    extra = {}
+    if args.learned:
+        from simul_b200 import learned
+        learned.set_weights(mesh, learned.load(args.learned))
+        r = torch.randn(v.n_nodes, 3, dtype=torch.float32, device=mesh.device)
+        z = torch.empty_like(r)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.reps):
+            rc = _lib.load().fem_mpnn_forward(mesh.ctx, C.c_void_p(r.data_ptr()), C.c_void_p(z.data_ptr()))
+            if rc != 0:
+                raise RuntimeError(_lib.last_error(mesh.ctx))
+        e1.record()
+        e1.synchronize()
+        extra["mpnn_forward_ms"] = e0.elapsed_time(e1) / args.reps
+    if args.two_level:
+        rhs = torch.randn(v.n_nodes, 3, dtype=torch.float64, device=mesh.device)
+        du = torch.zeros_like(rhs)
+        it, rel = C.c_int32(), C.c_double()
+        rc = _lib.load().fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, C.c_void_p(rhs.data_ptr()),
+                                 C.c_void_p(du.data_ptr()), 1e-6, 5000, C.byref(it), C.byref(rel))
+        if rc not in (0, _lib.FEM_NOT_CONVERGED):
+            raise RuntimeError(_lib.last_error(mesh.ctx))
+        extra["two_level_iterations"] = it.value
+        extra["coarse"] = mesh.coarse_info()
     info = mesh.info()
     print(json.dumps({"n": args.n, "tets": info["n_elements"], "nodes": info["n_nodes"],
                       "variant": args.variant, "reps": args.reps,
-                      "ms": {"matvec": ms[0], "residual": ms[1], "cg_update": ms[2], "cg_direction": ms[3]}}))
+                      "ms": {"matvec": ms[0], "residual": ms[1], "cg_update": ms[2], "cg_direction": ms[3]},
+                      **extra}))
 
 
 if __name__ == "__main__":

@@ -239,6 +239,30 @@ class Material:
 
 
 @dataclass
+class MixedMaterial:
+    """Per-element choice among several Materials: element e uses
+    ``parts[ids[e]]`` (the reference's ``materials={id: material}`` with
+    ``material_id`` per element, static_solver.py:32-71; there every id's
+    residual uses the first material's tangent, quirk Q3 — here each element
+    uses its own).  Per-element array parameters of a part are indexed by the
+    global element number."""
+    parts: list
+    ids: np.ndarray
+
+    model = "mixed"
+    small_strain = False
+
+
+def _subset(mat: Material, sel, ne):
+    """The Material restricted to elements ``sel`` (array parameters sliced)."""
+    kw = {}
+    for name in ("E", "nu", "C10", "C01", "D1", "sigma_y", "H", "fiber_E"):
+        v = getattr(mat, name)
+        kw[name] = v[sel] if (v is not None and np.ndim(v) == 1 and np.size(v) == ne) else v
+    return Material(mat.model, C_voigt=mat.C_voigt, fiber_a=mat.fiber_a, **kw)
+
+
+@dataclass
 class J2State:
     """J2 history per Gauss point (j2_plasticity.py:103-123)."""
     ep: np.ndarray      # (Ne,3,3) plastic strain
@@ -286,8 +310,36 @@ def j2_return_map(F, ep, epe, E, nu, sigma_y, H):
     return sigma, ep_new, epe_new, (n, theta, gamma2, plastic)
 
 
+def _mixed_cauchy(mat: MixedMaterial, F, j2_state):
+    ne = F.shape[0]
+    sig = np.zeros((ne, 3, 3))
+    st = j2_state if j2_state is not None else J2State.zeros(ne)
+    new = st.copy()
+    n = np.zeros((ne, 3, 3))
+    theta = np.ones(ne)
+    gamma2 = np.zeros(ne)
+    plastic = np.zeros(ne, dtype=bool)
+    has_j2 = False
+    for k, part in enumerate(mat.parts):
+        m = np.asarray(mat.ids) == k
+        if not np.any(m):
+            continue
+        sub = _subset(part, m, ne)
+        if part.model == "j2":
+            s, (stk, tk) = cauchy_stress(sub, F[m], J2State(st.ep[m], st.epe[m]))
+            new.ep[m], new.epe[m] = stk.ep, stk.epe
+            n[m], theta[m], gamma2[m], plastic[m] = tk
+            has_j2 = True
+        else:
+            s, _ = cauchy_stress(sub, F[m])
+        sig[m] = s
+    return sig, ((new, (n, theta, gamma2, plastic)) if has_j2 else None)
+
+
 def cauchy_stress(mat: Material, F, j2_state: Optional[J2State] = None):
     """Cauchy stress per element.  Returns (sigma, aux)."""
+    if isinstance(mat, MixedMaterial):
+        return _mixed_cauchy(mat, F, j2_state)
     I = np.eye(3)[None]
     if mat.model == "neo_hookean":               # neo_hookean.py:99-129
         mu, lam = lame(mat.E, mat.nu)
@@ -351,6 +403,13 @@ def first_piola(mat: Material, F, sigma):
     Large strain (neo_hookean.py:169-180): P = J_safe sigma F^-T.
     Small strain (linear_elastic.py:142-173, j2_plasticity.py:366-393): sigma.
     """
+    if isinstance(mat, MixedMaterial):
+        out = np.zeros_like(sigma)
+        for k, part in enumerate(mat.parts):
+            m = np.asarray(mat.ids) == k
+            if np.any(m):
+                out[m] = first_piola(_subset(part, m, F.shape[0]), F[m], sigma[m])
+        return out
     if mat.small_strain:
         return sigma
     Js = np.maximum(np.linalg.det(F), J_FLOOR)
@@ -374,6 +433,15 @@ def scatter_forces(fe, conn, n_nodes):
 
 def dP_directional(mat: Material, F, dF, tang=None):
     """Directional derivative dP[F](dF) of the stress measure used in the force."""
+    if isinstance(mat, MixedMaterial):
+        out = np.zeros_like(dF)
+        for k, part in enumerate(mat.parts):
+            m = np.asarray(mat.ids) == k
+            if not np.any(m):
+                continue
+            tk = None if (tang is None or part.model != "j2") else tuple(t[m] for t in tang)
+            out[m] = dP_directional(_subset(part, m, F.shape[0]), F[m], dF[m], tk)
+        return out
     I = np.eye(3)[None]
     Ft = np.transpose(F, (0, 2, 1))
     if mat.model == "neo_hookean":

@@ -24,11 +24,14 @@ class BatchInstance:
     """A mesh + material on a private stream, with its loads pushed."""
 
     def __init__(self, X, conn, material, fixed_mask, fixed_vals=None, f_ext=None, device=0,
-                 coarse_cell: int = 8):
+                 coarse_cell: int = 8, material_ids=None):
+        """``material`` is one material, or a dict {id: material} with
+        ``material_ids`` giving each element's id (as StaticSolver's
+        ``materials=``)."""
         # the library owns a non-blocking stream per instance; torch work on the
         # mesh's tensors is synchronised before every library call below
         self.mesh = B.FEMesh(X.shape[0], conn.shape[0], device=device, own_stream=True)
-        self.mesh.initialize_from_numpy(X, conn)
+        self.mesh.initialize_from_numpy(X, conn, material_ids=material_ids)
         idx = np.where(np.asarray(fixed_mask).reshape(-1))[0]
         vals = None if fixed_vals is None else np.asarray(fixed_vals).reshape(-1)[idx]
         self.mesh.set_fixed_dofs(idx, vals)
@@ -37,7 +40,11 @@ class BatchInstance:
         self.material = material
         self.mesh.set_coarse_options(cell=coarse_cell)
         torch.cuda.synchronize(self.mesh.device)
-        material.compute_nodal_forces(self.mesh)   # binds the material, pushes the loads
+        if isinstance(material, dict):
+            # binds the material table through a solver object (no solve)
+            B.StaticSolver(self.mesh, materials=material)._bind()
+        else:
+            material.compute_nodal_forces(self.mesh)   # binds the material, pushes the loads
         torch.cuda.synchronize(self.mesh.device)
         self.mesh._push_bc()
         torch.cuda.synchronize(self.mesh.device)
@@ -46,9 +53,19 @@ class BatchInstance:
     def ctx(self):
         return self.mesh.ctx
 
+    def reset(self):
+        """Back to rest: u = 0 and no plastic history."""
+        lib = _lib.load()
+        self.mesh.u.zero_()
+        torch.cuda.synchronize(self.mesh.device)
+        B._check(lib.fem_set_displacement(self.ctx, C.c_void_p(self.mesh.u.data_ptr())), self.ctx,
+                 "fem_set_displacement")
+        B._check(lib.fem_reset_history(self.ctx), self.ctx, "fem_reset_history")
+
 
 def solve_batch(instances: Sequence[BatchInstance], load_steps: int = 10, precond: str = "two_level",
-                tol: float = 1e-8, max_iterations: int = 50, n_threads: int = 0) -> Dict:
+                tol: float = 1e-8, max_iterations: int = 50, n_threads: int = 0,
+                line_search: str = "guarded") -> Dict:
     """Solves every instance from its current state through ``load_steps``
     load steps; returns per-instance results and host wall times."""
     lib = _lib.load()
@@ -59,6 +76,7 @@ def solve_batch(instances: Sequence[BatchInstance], load_steps: int = 10, precon
     prm.tol = tol
     prm.max_iterations = max_iterations
     prm.precond = B._PC[precond]
+    prm.line_search = B._LS[line_search]
     res = (_lib.FemSolveResult * n)()
     status = (C.c_int32 * n)()
     wall = (C.c_double * n)()

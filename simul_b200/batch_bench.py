@@ -40,18 +40,7 @@ def _make_case(args):
         top = np.isclose(X[:, 2], X[:, 2].max())
         fixed[top] = False
         vals[top] = 0.0
-        xc, yc = X[top, 0] - X[top, 0].mean(), X[top, 1] - X[top, 1].mean()
-        ft = np.zeros((int(top.sum()), 3))
-        if case in ("flexion", "extension"):
-            sgn = 1.0 if case == "flexion" else -1.0
-            ft[:, 2] = -sgn * MOMENT * yc / np.sum(yc * yc)
-        elif case == "lateral_bending":
-            ft[:, 2] = -MOMENT * xc / np.sum(xc * xc)
-        else:
-            r2 = np.sum(xc * xc + yc * yc)
-            ft[:, 0] = -MOMENT * yc / r2
-            ft[:, 1] = MOMENT * xc / r2
-        f[top] = ft
+        f = meshgen.top_moment_forces(X, top, case, MOMENT)
     return {"idx": idx, "n": n, "seed": seed, "case": case, "strain": strain, "X": X, "conn": v.conn,
             "E": v.E, "fixed": fixed, "vals": vals, "f": f, "tets": int(v.n_elements)}
 
@@ -93,17 +82,10 @@ def main(argv=None):
     with ThreadPoolExecutor(max_workers=8) as ex:
         insts = list(ex.map(build, cases))
     t_setup = time.perf_counter() - t0
-    import ctypes as C
-    from simul_b200 import _lib
-
     def reset():
         """Every instance back to rest: u = 0, no plastic history."""
         for inst in insts:
-            inst.mesh.u.zero_()
-            torch.cuda.synchronize()
-            B._check(_lib.load().fem_set_displacement(inst.ctx, C.c_void_p(inst.mesh.u.data_ptr())), inst.ctx,
-                     "fem_set_displacement")
-            inst.material.reset_state()
+            inst.reset()
         torch.cuda.synchronize()
 
     # warm-up pass (graph capture, matvec-variant timing, coarse set-up), then reset

@@ -144,6 +144,7 @@ struct FemCtx {
   std::vector<uint8_t> fixed_host;  // last constraint pattern (internal order)
   double coarse_ms_last = 0.0;
   double coarse_ms_assembly = 0.0;   // of which cell blocks + dense assembly
+  cudaEvent_t coarse_ev[3] = {nullptr, nullptr, nullptr};
   std::vector<void*> coarse_bufs;
   cusolverDnHandle_t solver = nullptr;
   double* sol_work = nullptr;
@@ -184,6 +185,19 @@ struct FemCtx {
     rd.counters = counters;
     rd.max_blocks = max_blocks;
     return rd;
+  }
+};
+
+// Two CUDA events destroyed on every return path.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t create() {
+    cudaError_t e = cudaEventCreate(&a);
+    return e == cudaSuccess ? cudaEventCreate(&b) : e;
+  }
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
   }
 };
 
@@ -265,6 +279,8 @@ void free_ctx(FemCtx* c) {
   if (c->sol_info) cudaFree(c->sol_info);
   if (c->h_info) cudaFreeHost(c->h_info);
   if (c->solver) cusolverDnDestroy(c->solver);
+  for (cudaEvent_t ev : c->coarse_ev)
+    if (ev) cudaEventDestroy(ev);
   if (c->stage) cudaFree(c->stage);
   if (c->spos) cudaFree(c->spos);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
@@ -637,9 +653,9 @@ int choose_matvec_variant(FemCtx* c) {
   const CGState hs = endless_cg();
   CK(cudaMemcpyAsync(c->cg, &hs, sizeof(hs), cudaMemcpyHostToDevice, c->stream));
   launch_dinv_identity(c->p, c->fixed, c->Nn, c->stream);
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  EventPair ev;
+  CK(ev.create());
+  cudaEvent_t e0 = ev.a, e1 = ev.b;
   for (int v = 0; v < MV_N_VARIANTS; ++v) {
     MvArgs mv = make_mv(c);
     mv.variant = v;
@@ -663,8 +679,6 @@ int choose_matvec_variant(FemCtx* c) {
     c->mv_ns[v] = 1e6 * ms / kReps;
     c->n_launches += (v == MV_TWO_PHASE ? 2 : 1) * 13;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   c->mv_variant = c->mv_ns[MV_TWO_PHASE] < c->mv_ns[MV_FUSED] ? MV_TWO_PHASE : MV_FUSED;
   c->mv_tuned = true;
   c->mv_tuned_model = c->model_kind;
@@ -764,7 +778,7 @@ int build_coarse(FemCtx* c) {
   for (int attempt = 0; attempt < 64; ++attempt) {
     for (int d = 0; d < 3; ++d) g[d] = std::max(1, (int)std::ceil((hi[d] - lo[d]) / H - 1e-9));
     const int64_t ncell_lat = (int64_t)g[0] * g[1] * g[2];
-    if (ncell_lat > (1 << 26)) {
+    if (ncell_lat > (1 << 22)) {
       H *= 1.25;
       continue;
     }
@@ -902,17 +916,16 @@ int ensure_coarse(FemCtx* c) {
     ++c->coarse_uses;
     return FEM_OK;
   }
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  // timing events live as long as the context (no leak on the error returns)
+  for (cudaEvent_t& ev : c->coarse_ev)
+    if (!ev) CK(cudaEventCreate(&ev));
+  cudaEvent_t e0 = c->coarse_ev[0], em = c->coarse_ev[1], e1 = c->coarse_ev[2];
   CK(cudaEventRecord(e0, c->stream));
   prepare_coarse_kernels(c->model_kind, c->cdev.n_dof);
   const CoarseArgs ca = coarse_args(c);
   launch_coarse_assemble(ca, c->model_kind, c->stream);
   c->n_launches += 2;
   CKL();
-  cudaEvent_t em;
-  CK(cudaEventCreate(&em));
   CK(cudaEventRecord(em, c->stream));
   const int n = c->cdev.n_dof;
   if (cusolverDnDpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
@@ -933,9 +946,6 @@ int ensure_coarse(FemCtx* c) {
   float ms = 0.f, ms_asm = 0.f;
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventElapsedTime(&ms_asm, e0, em);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(em);
   c->coarse_ms_last = ms;
   c->coarse_ms_assembly = ms_asm;
   ++c->n_coarse_assemblies;
@@ -2106,9 +2116,9 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
   if ((st = check_ctx(c))) return st;
   if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
   if (reps <= 0 || !ms_out) return set_err(c, FEM_ERR_INVALID, "need reps > 0 and an output array");
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
+  EventPair ev;
+  CK(ev.create());
+  cudaEvent_t e0 = ev.a, e1 = ev.b;
   const int nn = c->Nn;
   const CGState hs = endless_cg();
   // a nonzero direction: p = 1 on free DOFs
@@ -2161,8 +2171,6 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
     CK(cudaEventElapsedTime(&ms, e0, e1));
     ms_out[k] = ms / reps;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   c->tangent_valid = true;
   return FEM_OK;
 }

@@ -51,3 +51,57 @@ def test_batch_rejects_duplicates_and_bad_steps(cuda):
     assert "repeats" in _lib.last_error(None)
     ctx1 = (C.c_void_p * 1)(inst.ctx.value)
     assert lib.fem_batch_solve(ctx1, 1, None, 0, res, st, None, 0) == _lib.FEM_ERR_INVALID
+
+
+def _ms_oracle_materials(ms):
+    from oracle import fem_oracle as O
+    fib = np.array([[np.cos(np.pi / 6), 0.0, np.sin(np.pi / 6)], [np.cos(np.pi / 6), 0.0, -np.sin(np.pi / 6)]])
+    mu = 2.0 * (0.18 + 0.045)
+    K = 2.0 * mu * (1.0 + 0.45) / (3.0 * (1.0 - 2.0 * 0.45))
+    parts = [O.Material("j2", E=ms.E, nu=0.3, sigma_y=100.0, H=0.02 * ms.E),
+             O.Material("ti_hyper", C10=0.18, C01=0.045, D1=2.0 / K, fiber_a=fib, fiber_E=500.0),
+             O.Material("linear_elastic", E=110e3, nu=0.3)]
+    return O.MixedMaterial(parts, ms.info["material_ids"])
+
+
+def test_motion_segment_mixed_materials_match_oracle(cuda):
+    """J2 bone + fibre-reinforced Mooney-Rivlin disc + elastic screw on one
+    mesh, flexion moment: converged displacements within 1e-6 relative L2 of
+    the FP64 oracle, with the Jacobi and the two-level preconditioner."""
+    from oracle import fem_oracle as O
+    from simul_b200 import motion_segment_bench as MSB
+    ms = meshgen.motion_segment(n=8)
+    top = np.isclose(ms.X[:, 2], ms.X[:, 2].max())
+    f = meshgen.top_moment_forces(ms.X, top, "flexion", 750.0)
+    m = O.Mesh(ms.X, ms.conn)
+    u_ref, info = O.consistent_newton(m, _ms_oracle_materials(ms), f, ms.fixed_mask, ms.fixed_vals,
+                                      j2_state=O.J2State.zeros(ms.n_elements), tol=1e-11, line_search=True)
+    assert info["converged"]
+    for pc in ("jacobi", "two_level"):
+        mesh = B.FEMesh(ms.n_nodes, ms.n_elements, device=cuda)
+        mesh.initialize_from_numpy(ms.X, ms.conn, material_ids=ms.info["material_ids"])
+        mesh.set_fixed_nodes(np.where(ms.fixed_mask[:, 0])[0])
+        mesh.set_nodal_forces(np.arange(ms.n_nodes), f)
+        res = B.StaticSolver(mesh, materials=MSB.materials(ms.E), tol=1e-10, precond=pc).solve(verbose=False)
+        assert res["converged"], (pc, res)
+        u = mesh.get_displacements()
+        assert np.linalg.norm(u - u_ref) / np.linalg.norm(u_ref) < 1e-6, pc
+
+
+def test_motion_segment_moment_cases_batch(cuda):
+    from simul_b200 import motion_segment_bench as MSB
+    ms = meshgen.motion_segment(n=8)
+    top = np.isclose(ms.X[:, 2], ms.X[:, 2].max())
+    insts = [batch.BatchInstance(ms.X, ms.conn, MSB.materials(ms.E), ms.fixed_mask, None,
+                                 meshgen.top_moment_forces(ms.X, top, c, 300.0), device=cuda,
+                                 material_ids=ms.info["material_ids"]) for c in MSB.CASES]
+    out = batch.solve_batch(insts, load_steps=2, precond="two_level")
+    assert all(r["converged"] for r in out["instances"]), out
+    torch.cuda.synchronize()
+    u = [i.mesh.u.cpu().numpy() for i in insts]
+    # flexion and extension are the same couple with opposite sign: the top
+    # face moves forward in one and backward in the other (the soft disc makes
+    # the response strongly nonlinear, so not exactly opposite)
+    uy = [x[top, 1].mean() for x in u]
+    assert uy[0] * uy[1] < 0, uy
+    assert all(np.abs(x).max() > 0 for x in u)

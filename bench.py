@@ -403,6 +403,8 @@ def main():
             "gpu_launches": int(launches // max(args.steps, 1)),
             "kernel_ms": {"matvec": kms[0], "residual": kms[1], "cg_update": kms[2], "cg_direction": kms[3]},
             "matvec_variant": {"chosen": variant, "ns_per_launch": st["matvec_ns"]},
+            "whole_solve_graphs": {"available": st["whole_solve_graph_available"],
+                                   "pcg_solves_as_one_launch": st["whole_solve_graphs"]},
             "roofline": {"bound": "hbm", "kernel": ("matvec_kernel<J2> (fused node-block)" if variant == "fused"
                                                     else "elem_mv_kernel<J2> + node_gather_kernel (two-phase)"),
                          "achieved": achieved, "peak": peak,

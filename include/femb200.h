@@ -138,8 +138,9 @@ int fem_ctx_info(void* ctx, int64_t* out6);
  * out[3] CG graph launches; matvec variant selection: out[4] variant in use
  * (0 fused node-block, 1 two-phase), out[5] / out[6] timed ns per launch of
  * the fused / two-phase variant (0 if not timed), out[7] 1 if the choice was
- * made by timing */
-int fem_ctx_stats(void* ctx, int64_t* out8);
+ * made by timing; out[8] PCG solves run as one whole-solve graph launch
+ * (conditional WHILE node), out[9] 1 if such graphs are available */
+int fem_ctx_stats(void* ctx, int64_t* out10);
 
 /* Option keys of fem_set_option (no reference counterpart: the reference has
  * one matvec formulation, backend/fea/fem/material/nonlinear/base.py:110-145). */

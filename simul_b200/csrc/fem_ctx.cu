@@ -62,6 +62,7 @@ struct FemCtx {
   int* node_row = nullptr;
   uint32_t* node_slots = nullptr;
   int4* spos = nullptr;
+  float4* geom = nullptr;
   int max_slots = 0;
   uint8_t* fixed = nullptr;
   double* fixed_vals = nullptr;
@@ -102,6 +103,12 @@ struct FemCtx {
   bool materials_set = false;
   bool tangent_valid = false;
   cudaGraphExec_t cg_graph[N_GRAPHS] = {nullptr, nullptr, nullptr};
+  // whole-solve graphs: a conditional WHILE node repeats kLoopIters CG
+  // iterations until the device-side CG state says done (null: not
+  // available, the batched graphs above are used)
+  cudaGraphExec_t loop_graph[N_GRAPHS] = {nullptr, nullptr, nullptr};
+  bool use_loop_graph = true;
+  int64_t n_loop_graphs = 0;   // PCG solves run as one whole-solve graph launch
   int cg_graph_model[N_GRAPHS] = {-2, -2, -2};
   int cg_graph_variant[N_GRAPHS] = {-1, -1, -1};
   int cg_graph_flags[N_GRAPHS] = {-1, -1, -1};
@@ -177,6 +184,7 @@ struct FemCtx {
     m.fixed = fixed;
     m.max_slots = max_slots;
     m.spos = spos;
+    m.geom = geom;
     return m;
   }
   Reduce red() const {
@@ -268,8 +276,10 @@ void free_ctx(FemCtx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (int k = 0; k < N_GRAPHS; ++k)
+  for (int k = 0; k < N_GRAPHS; ++k) {
     if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+    if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
+  }
   for (void* p : c->coarse_bufs)
     if (p) cudaFree(p);
   for (void* p : c->mpnn_bufs)
@@ -283,6 +293,7 @@ void free_ctx(FemCtx* c) {
     if (ev) cudaEventDestroy(ev);
   if (c->stage) cudaFree(c->stage);
   if (c->spos) cudaFree(c->spos);
+  if (c->geom) cudaFree(c->geom);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
                   c->fixed_vals_full, c->fext_full,
@@ -446,6 +457,7 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   if ((st = dalloc(c, &c->node_row, node_row.size()))) return st;
   if ((st = dalloc(c, &c->node_slots, node_slots.size()))) return st;
   if ((st = dalloc(c, &c->spos, (size_t)Ne))) return st;
+  if ((st = dalloc(c, &c->geom, 3 * (size_t)Ne))) return st;
   if ((st = dalloc(c, &c->d_perm_node, (size_t)Nn))) return st;
   if ((st = dalloc(c, &c->d_perm_elem, (size_t)Ne))) return st;
   CK(cudaMemcpyAsync(c->X64, X64.data(), X64.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -459,6 +471,8 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   CK(cudaMemcpyAsync(c->spos, spos.data(), spos.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_perm_node, c->perm_node.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_perm_elem, c->perm_elem.data(), Ne * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  launch_geom(c->X64, c->conn, c->geom, Ne, c->stream);
+  CKL();
   // the host vectors go out of scope: finish the copies first
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;
@@ -685,6 +699,46 @@ int choose_matvec_variant(FemCtx* c) {
   return FEM_OK;
 }
 
+// One graph for a whole PCG solve: a conditional WHILE node whose body holds
+// kLoopIters CG iterations and cg_loop_cond_kernel, which clears the
+// condition once the CG state is done (converged, out of iterations, broken
+// down) and also after max_iter / kLoopIters + 2 trips, so the loop ends
+// even if the state stopped advancing.  Returns false (and leaves nothing
+// behind) if the runtime cannot build it; the batched graphs are used then.
+constexpr int kLoopIters = 4;
+
+bool build_loop_graph(FemCtx* c, int kind) {
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+  bool ok = false;
+  do {
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+    cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &np) != cudaSuccess) break;
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+      break;
+    for (int i = 0; i < kLoopIters; ++i) enqueue_cg_iter(c, kind);
+    launch_cg_loop_cond(h, c->cg, kLoopIters, c->stream);
+    cudaGraph_t captured = nullptr;
+    if (cudaStreamEndCapture(c->stream, &captured) != cudaSuccess) break;
+    if (cudaGraphInstantiate(&c->loop_graph[kind], g, 0) != cudaSuccess) {
+      c->loop_graph[kind] = nullptr;
+      break;
+    }
+    ok = true;
+  } while (false);
+  cudaGraphDestroy(g);
+  cudaGetLastError();  // a refused build leaves no sticky error behind
+  return ok;
+}
+
 int ensure_cg_graph(FemCtx* c, int kind) {
   int st;
   if ((st = choose_matvec_variant(c))) return st;
@@ -695,6 +749,10 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   if (c->cg_graph[kind]) {
     cudaGraphExecDestroy(c->cg_graph[kind]);
     c->cg_graph[kind] = nullptr;
+  }
+  if (c->loop_graph[kind]) {
+    cudaGraphExecDestroy(c->loop_graph[kind]);
+    c->loop_graph[kind] = nullptr;
   }
   prepare_kernels(c->mesh(), c->model_kind);
   if (kind == GRAPH_TWO_LEVEL || (kind == GRAPH_LEARNED && c->learned_coarse))
@@ -708,6 +766,7 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   e = cudaGraphInstantiate(&c->cg_graph[kind], g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+  if (c->use_loop_graph && !build_loop_graph(c, kind)) c->use_loop_graph = false;
   c->cg_graph_model[kind] = c->model_kind;
   c->cg_graph_variant[kind] = c->mv_variant;
   c->cg_graph_flags[kind] = flags;
@@ -1180,6 +1239,14 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   int batches = 0;
+  if (!c->h_cg->done && c->loop_graph[kind]) {
+    CK(cudaGraphLaunch(c->loop_graph[kind], c->stream));
+    c->n_graphs++;
+    c->n_loop_graphs++;
+    CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    batches = max_batches;
+  }
   while (!c->h_cg->done && batches < max_batches) {
     CK(cudaGraphLaunch(c->cg_graph[kind], c->stream));
     c->n_graphs++;
@@ -1351,6 +1418,8 @@ int fem_ctx_stats(void* ctx, int64_t* out) {
   out[5] = (int64_t)std::llround(c->mv_ns[MV_FUSED]);
   out[6] = (int64_t)std::llround(c->mv_ns[MV_TWO_PHASE]);
   out[7] = c->mv_tuned ? 1 : 0;
+  out[8] = c->n_loop_graphs;
+  out[9] = c->use_loop_graph ? 1 : 0;
   return FEM_OK;
 }
 

@@ -32,6 +32,7 @@ struct MeshDev {
   const uint8_t* fixed;     // [Nn] bit d set = DOF d fixed
   int max_slots;            // largest slot-list range of one block (shared memory sizing)
   const int4* spos;         // [Ne] position of each (element, slot) in node_slots order
+  const float4* geom;       // [3 Ne] dN_1..3/dX (row-major 3x3) and volume per element
 };
 
 // Last-block reduction bookkeeping: one slot per reduction site.
@@ -52,7 +53,7 @@ struct CGState {
   int zsel;                          // learned FPCG: 1 = this step used the Jacobi (+ coarse) direction
   int n_alt;                         // learned FPCG: steps that used it
   int locked;                        // learned FPCG: network switched off for the rest of the solve
-  int pad2;
+  int trips;                         // whole-solve graph: trips through the loop body
 };
 
 struct ResArgs {
@@ -237,6 +238,10 @@ void launch_train_grad_z(const float* q, const float* r, const uint8_t* fixed, c
                          int n, cudaStream_t s);
 void launch_jacobi_apply(const float* r, const float* dinv, float* z, int n, cudaStream_t s);
 
+// whole-solve CG graph: clears the WHILE condition once cg->done is set, or
+// after cg->max_iter / iters_per_trip + 2 trips (then cg->done = 2)
+void launch_cg_loop_cond(cudaGraphConditionalHandle h, CGState* cg, int iters_per_trip, cudaStream_t s);
+
 // PCG vector kernels.  precond_in_update = 1: Jacobi z = D^-1 r is applied
 // inside cg_init / cg_update (rz, beta there); 0: an external preconditioner
 // kernel computes rz and beta.
@@ -268,6 +273,8 @@ void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, 
 // u[3n+d] = u_base[3n+d] + alpha du[4n+d] for n < n_nodes
 void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int n_nodes,
                      cudaStream_t s);
+// per-element shape-function gradients and volume (FP64 -> FP32 table)
+void launch_geom(const double* X, const int4* conn, float4* geom, int n, cudaStream_t s);
 // out[i] = s in[i], i < n
 void launch_scale_d(const double* in, double s, double* out, int n, cudaStream_t st);
 // X32[n].w = fixed bits of node n

@@ -149,11 +149,12 @@ class FEMesh:
                 "block_element_entries": out[3], "nodes_per_block": out[4], "device_bytes": out[5]}
 
     def stats(self) -> dict:
-        out = (C.c_int64 * 8)()
+        out = (C.c_int64 * 10)()
         _check(_lib.load().fem_ctx_stats(self.ctx, out), self.ctx, "fem_ctx_stats")
         return {"launches": out[0], "cg_iterations": out[1], "residual_evals": out[2], "cg_graphs": out[3],
                 "matvec_variant": _lib.MATVEC_VARIANTS.get(out[4], str(out[4])),
-                "matvec_ns": {"fused": out[5], "two_phase": out[6]}, "matvec_tuned": bool(out[7])}
+                "matvec_ns": {"fused": out[5], "two_phase": out[6]}, "matvec_tuned": bool(out[7]),
+                "whole_solve_graphs": out[8], "whole_solve_graph_available": bool(out[9])}
 
     def coarse_info(self) -> dict:
         out = (C.c_double * 8)()

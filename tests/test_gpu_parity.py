@@ -294,8 +294,10 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
         y = torch.empty_like(x)
         assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0
         ys[v] = y.cpu().numpy().astype(np.float64)
-    # both sum each node's slot vectors in the same order; only FMA contraction may differ
-    assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-6
+    # both sum each node's slot vectors in the same order; they differ in FMA
+    # contraction and in the element gradients (two-phase streams them from a
+    # table built in FP64, the fused kernel derives them in FP32)
+    assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-5
     # automatic choice: the first PCG solve times both variants and keeps the faster
     mesh.set_matvec_variant(None)
     mesh.u.zero_()
@@ -309,6 +311,8 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
     assert st["matvec_ns"]["fused"] > 0 and st["matvec_ns"]["two_phase"] > 0
     faster = min(st["matvec_ns"], key=st["matvec_ns"].get)
     assert st["matvec_variant"] == faster
+    # every PCG solve ran as one whole-solve graph launch (conditional WHILE node)
+    assert st["whole_solve_graph_available"] and st["whole_solve_graphs"] > 0
     assert _lib.load().fem_set_option(mesh.ctx, _lib.FEM_OPT_MATVEC_VARIANT, 7) == _lib.FEM_ERR_INVALID
     assert "matvec variant" in _lib.last_error(mesh.ctx)
 

@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="PCG solves one coarse-operator assembly serves (0: adaptive)")
     ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
+    ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
+    ap.add_argument("--cg-rtol-max", type=float, default=1e-1, help="inexact-Newton forcing term cap")
     return ap.parse_args()
 
 
@@ -261,7 +263,8 @@ def main():
     mesh = B.FEMesh(v.n_nodes, v.n_elements, device=local)
     mesh.initialize_from_numpy(v.X, v.conn)
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
-    solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond)
+    solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond, cg_rtol_min=args.cg_rtol_min,
+                            cg_rtol_max=args.cg_rtol_max)
     mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse)
     if args.matvec_variant != "auto":
         mesh.set_matvec_variant(args.matvec_variant)

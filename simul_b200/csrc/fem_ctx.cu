@@ -62,7 +62,6 @@ struct FemCtx {
   int* node_row = nullptr;
   uint32_t* node_slots = nullptr;
   int4* spos = nullptr;
-  float4* geom = nullptr;
   int max_slots = 0;
   uint8_t* fixed = nullptr;
   double* fixed_vals = nullptr;
@@ -184,7 +183,6 @@ struct FemCtx {
     m.fixed = fixed;
     m.max_slots = max_slots;
     m.spos = spos;
-    m.geom = geom;
     return m;
   }
   Reduce red() const {
@@ -293,7 +291,6 @@ void free_ctx(FemCtx* c) {
     if (ev) cudaEventDestroy(ev);
   if (c->stage) cudaFree(c->stage);
   if (c->spos) cudaFree(c->spos);
-  if (c->geom) cudaFree(c->geom);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
                   c->fixed_vals_full, c->fext_full,
@@ -457,7 +454,6 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   if ((st = dalloc(c, &c->node_row, node_row.size()))) return st;
   if ((st = dalloc(c, &c->node_slots, node_slots.size()))) return st;
   if ((st = dalloc(c, &c->spos, (size_t)Ne))) return st;
-  if ((st = dalloc(c, &c->geom, 3 * (size_t)Ne))) return st;
   if ((st = dalloc(c, &c->d_perm_node, (size_t)Nn))) return st;
   if ((st = dalloc(c, &c->d_perm_elem, (size_t)Ne))) return st;
   CK(cudaMemcpyAsync(c->X64, X64.data(), X64.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -471,8 +467,6 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   CK(cudaMemcpyAsync(c->spos, spos.data(), spos.size() * sizeof(int4), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_perm_node, c->perm_node.data(), Nn * sizeof(int), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->d_perm_elem, c->perm_elem.data(), Ne * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  launch_geom(c->X64, c->conn, c->geom, Ne, c->stream);
-  CKL();
   // the host vectors go out of scope: finish the copies first
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;

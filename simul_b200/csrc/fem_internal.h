@@ -32,7 +32,6 @@ struct MeshDev {
   const uint8_t* fixed;     // [Nn] bit d set = DOF d fixed
   int max_slots;            // largest slot-list range of one block (shared memory sizing)
   const int4* spos;         // [Ne] position of each (element, slot) in node_slots order
-  const float4* geom;       // [3 Ne] dN_1..3/dX (row-major 3x3) and volume per element
 };
 
 // Last-block reduction bookkeeping: one slot per reduction site.
@@ -273,8 +272,6 @@ void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, 
 // u[3n+d] = u_base[3n+d] + alpha du[4n+d] for n < n_nodes
 void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int n_nodes,
                      cudaStream_t s);
-// per-element shape-function gradients and volume (FP64 -> FP32 table)
-void launch_geom(const double* X, const int4* conn, float4* geom, int n, cudaStream_t s);
 // out[i] = s in[i], i < n
 void launch_scale_d(const double* in, double s, double* out, int n, cudaStream_t st);
 // X32[n].w = fixed bits of node n

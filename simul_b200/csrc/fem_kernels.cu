@@ -281,21 +281,17 @@ __device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
   const int4 cn = __ldg(m.conn + e);
   const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
   const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
-  // shape-function gradients G[k] = dN_{k+1}/dX and the volume, streamed from
-  // the per-element table (built once in FP64) instead of gathering the four
-  // vertices and re-deriving them
-  const float4 g0 = __ldg(m.geom + 3 * (size_t)e);
-  const float4 g1 = __ldg(m.geom + 3 * (size_t)e + 1);
-  const float4 g2 = __ldg(m.geom + 3 * (size_t)e + 2);
-  const float G[3][3] = {{g0.x, g0.y, g0.z}, {g0.w, g1.x, g1.y}, {g1.z, g1.w, g2.x}};
-  const float vol = g2.y;
-  float pv[4][3];
+  float xv[4][3], pv[4][3];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
+    const float4 X = __ldg(m.X32 + nid[k]);
     const float4 P = __ldg(xin + nid[k]);
+    xv[k][0] = X.x;
+    xv[k][1] = X.y;
+    xv[k][2] = X.z;
     // CG directions are zero on fixed DOFs already; only a standalone
     // matvec masks its input
-    const int fx = MASK ? (int)__ldg(m.fixed + nid[k]) : 0;
+    const int fx = MASK ? (int)X.w : 0;
     pv[k][0] = (fx & 1) ? 0.f : P.x;
     pv[k][1] = (fx & 2) ? 0.f : P.y;
     pv[k][2] = (fx & 4) ? 0.f : P.z;
@@ -311,27 +307,19 @@ __device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
       pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
   }
   const int4 sp = __ldg(m.spos + e);
+  TetGeom<float> g;
+  tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+  float D[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) D[k][d] = pv[k + 1][d] - pv[0][d];
   float dF[9];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j)
-      dF[3 * i + j] = (pv[1][i] - pv[0][i]) * G[0][j] + (pv[2][i] - pv[0][i]) * G[1][j] +
-                      (pv[3][i] - pv[0][i]) * G[2][j];
+  grad_from_diffs(D, g, dF);
   float dP[9];
   dP_any<MODEL>(mat, scl, pay, dF, dP);
   float f[4][3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    float acc0 = 0.f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const float v = vol * (dP[3 * i] * G[k][0] + dP[3 * i + 1] * G[k][1] + dP[3 * i + 2] * G[k][2]);
-      f[k + 1][i] = v;
-      acc0 += v;
-    }
-    f[0][i] = -acc0;
-  }
+  slot_vectors(dP, g, g.s6, f);
   __stcg(a.stage + sp.x, make_float4(f[0][0], f[0][1], f[0][2], 0.f));
   __stcg(a.stage + sp.y, make_float4(f[1][0], f[1][1], f[1][2], 0.f));
   __stcg(a.stage + sp.z, make_float4(f[2][0], f[2][1], f[2][2], 0.f));
@@ -1020,32 +1008,6 @@ void launch_scatter_f2d(const float* in_int, double* out_user, const int* perm, 
                         cudaStream_t s) {
   scatter_f4_kernel<double><<<nblk(n, 256), 256, 0, s>>>(in_int, out_user, perm, n);
 }
-// geom[3e..3e+2] = dN_1..3/dX (9 floats, row k = node k+1) and the element
-// volume, from the FP64 coordinates
-__global__ void geom_kernel(const double* __restrict__ X, const int4* __restrict__ conn, float4* geom, int n) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= n) return;
-  const int4 cn = conn[e];
-  const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
-  double xv[4][3];
-  for (int k = 0; k < 4; ++k)
-    for (int d = 0; d < 3; ++d) xv[k][d] = X[3 * nid[k] + d];
-  TetGeom<double> g;
-  tet_geom(xv[0], xv[1], xv[2], xv[3], g);
-  float G[9];
-  for (int k = 0; k < 3; ++k)
-    for (int j = 0; j < 3; ++j) G[3 * k + j] = (float)(g.c[k][j] * g.inv_det);
-  // slot vectors: s6 c_k = vol * G_k (vol carries the orientation's sign)
-  const float vol = (float)(g.s6 / g.inv_det);
-  geom[3 * (size_t)e] = make_float4(G[0], G[1], G[2], G[3]);
-  geom[3 * (size_t)e + 1] = make_float4(G[4], G[5], G[6], G[7]);
-  geom[3 * (size_t)e + 2] = make_float4(G[8], vol, 0.f, 0.f);
-}
-
-void launch_geom(const double* X, const int4* conn, float4* geom, int n, cudaStream_t s) {
-  geom_kernel<<<nblk(n, 256), 256, 0, s>>>(X, conn, geom, n);
-}
-
 __global__ void scale_d_kernel(const double* in, double s, double* out, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = s * in[i];

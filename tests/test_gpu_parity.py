@@ -294,10 +294,8 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
         y = torch.empty_like(x)
         assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0
         ys[v] = y.cpu().numpy().astype(np.float64)
-    # both sum each node's slot vectors in the same order; they differ in FMA
-    # contraction and in the element gradients (two-phase streams them from a
-    # table built in FP64, the fused kernel derives them in FP32)
-    assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-5
+    # both sum each node's slot vectors in the same order; only FMA contraction may differ
+    assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-6
     # automatic choice: the first PCG solve times both variants and keeps the faster
     mesh.set_matvec_variant(None)
     mesh.u.zero_()

@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="PCG solves one coarse-operator assembly serves (0: adaptive)")
     ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
+    ap.add_argument("--coarse-bf16", type=int, default=0, help="store the coarse inverse in BF16")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
     ap.add_argument("--cg-rtol-max", type=float, default=1e-1, help="inexact-Newton forcing term cap")
     return ap.parse_args()
@@ -265,7 +266,7 @@ def main():
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond, cg_rtol_min=args.cg_rtol_min,
                             cg_rtol_max=args.cg_rtol_max)
-    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse)
+    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16))
     if args.matvec_variant != "auto":
         mesh.set_matvec_variant(args.matvec_variant)
     if args.precond == "learned":
@@ -373,6 +374,29 @@ def main():
                "speedup_of_timed_method": jms / ms, "timed_once_after_one_warmup": True}
         del jsolver
 
+    # learned flexible PCG timed beside it (held-out trained weights), when available
+    lrn = None
+    if args.precond != "learned" and not args.no_jacobi_baseline and os.path.exists(args.weights):
+        from simul_b200 import learned as L
+        L.set_weights(mesh, L.load(args.weights))
+        L.set_coarse(mesh, bool(args.learned_coarse))
+        lsolver = B.StaticSolver(mesh, mat, tol=args.tol, precond="learned")
+        solve_all(lsolver)
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ll = solve_all(lsolver)
+        e1.record(stream)
+        e1.synchronize()
+        lms = max_over_ranks(e0.elapsed_time(e1), dev, ws)
+        lrn = {"s": lms / 1e3, "newton_iterations": ll["newton"], "cg_iterations": ll["cg"],
+               "all_converged": bool(ll["converged"]), "max_relative_residual": ll["max_rel"],
+               "vs_jacobi_pcg": (jac["s"] * 1e3 / lms) if jac else None, "timed_once_after_one_warmup": True,
+               **learned_info(mesh, args)}
+        del lsolver
+
     # roofline of the dominant kernel (tangent matvec), CUDA events on the solver stream
     kms = (C.c_double * 4)()
     rc = _lib.load().fem_profile_kernels(mesh.ctx, 200, kms)
@@ -393,10 +417,10 @@ def main():
                        "two_level": "Newton (FP64 residual) + two-level PCG: Jacobi + trilinear Galerkin "
                                     "coarse correction (FP32 matvec, FP64 dots)",
                        "jacobi": "Newton (FP64 residual) + Jacobi-PCG (FP32 matvec, FP64 dots)"}[args.precond],
-            "learned_fpcg_s": (ms / 1e3) if args.precond == "learned" else None,
-            "learned": (learned_info(mesh, args) if args.precond == "learned" else None),
+            "learned_fpcg_s": (ms / 1e3) if args.precond == "learned" else (lrn["s"] if lrn else None),
+            "learned": (learned_info(mesh, args) if args.precond == "learned" else lrn),
             "jacobi_pcg": jac,
-            "coarse": ({**mesh.coarse_info(), "reuse": args.coarse_reuse}
+            "coarse": ({**mesh.coarse_info(), "reuse": args.coarse_reuse, "inverse_dtype": "bf16" if args.coarse_bf16 else "f32"}
                        if args.precond in ("two_level", "learned") else None),
             "solve": {"newton_iterations": last["newton"], "cg_iterations": last["cg"],
                       "all_converged": bool(last["converged"]), "max_relative_residual": last["max_rel"],

@@ -160,7 +160,10 @@ enum {
   FEM_OPT_COARSE_REUSE = 3,
   /* learned preconditioner: 1 (default) adds the two-level coarse correction
    * to the network's output, 0 uses the network alone */
-  FEM_OPT_LEARNED_COARSE = 4
+  FEM_OPT_LEARNED_COARSE = 4,
+  /* two-level preconditioner: 1 stores the coarse inverse in BF16 (half the
+   * bytes per CG iteration; FP32 products), 0 (default) in FP32 */
+  FEM_OPT_COARSE_BF16 = 5
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

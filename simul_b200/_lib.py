@@ -40,6 +40,7 @@ FEM_OPT_MATVEC_VARIANT = 1
 FEM_OPT_COARSE_CELL = 2
 FEM_OPT_COARSE_REUSE = 3
 FEM_OPT_LEARNED_COARSE = 4
+FEM_OPT_COARSE_BF16 = 5
 MPNN_PARAMS = 34307
 MATVEC_VARIANTS = {0: "fused", 1: "two_phase"}
 

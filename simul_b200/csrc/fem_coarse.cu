@@ -28,12 +28,23 @@ __device__ __forceinline__ float tri_weight(float tx, float ty, float tz, int co
   return wx * wy * wz;
 }
 
-// local coordinates of a point in lattice cell ijk, clamped to [0, 1]
+// Local coordinate of a point along one lattice axis, clamped to [0, 1] and
+// snapped to the cell face within 1e-4: a mesh node on a face gets exactly 0
+// or 1, so a coarse node whose support holds only such nodes assembles an
+// exactly-zero row (decoupled) instead of a rounding-sized one.
+__device__ __forceinline__ float lattice_coord(float x, float lo, float inv_H, int i) {
+  float t = fminf(fmaxf((x - lo) * inv_H - (float)i, 0.f), 1.f);
+  if (t < 1e-4f) t = 0.f;
+  if (t > 1.f - 1e-4f) t = 1.f;
+  return t;
+}
+
+// local coordinates of a point in lattice cell ijk
 __device__ __forceinline__ void cell_local(const CoarseDev& c, int3 ijk, float x, float y, float z,
                                            float t[3]) {
-  t[0] = fminf(fmaxf((x - c.lo.x) * c.inv_H - (float)ijk.x, 0.f), 1.f);
-  t[1] = fminf(fmaxf((y - c.lo.y) * c.inv_H - (float)ijk.y, 0.f), 1.f);
-  t[2] = fminf(fmaxf((z - c.lo.z) * c.inv_H - (float)ijk.z, 0.f), 1.f);
+  t[0] = lattice_coord(x, c.lo.x, c.inv_H, ijk.x);
+  t[1] = lattice_coord(y, c.lo.y, c.inv_H, ijk.y);
+  t[2] = lattice_coord(z, c.lo.z, c.inv_H, ijk.z);
 }
 
 template <int NT>
@@ -209,15 +220,23 @@ __global__ void coarse_dense_kernel(const __grid_constant__ CoarseDev c) {
   c.Ac[q] = acc;
 }
 
-// FP32 symmetric copy of the inverse whose lower triangle potri wrote.
+// Symmetric FP32 (or BF16) copy of the inverse whose lower triangle potri
+// wrote.
 __global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = c.n_dof;
   if (q >= (int64_t)n * n) return;
   const int row = (int)(q / n), col = (int)(q % n);
   const int lo = max(row, col), hi = min(row, col);
-  // column-major lower triangle: element (lo, hi) at hi * n + lo
-  c.Ainv[q] = (float)c.Ac[(size_t)hi * n + lo];
+  // column-major lower triangle: element (lo, hi) at hi * n + lo; rows padded
+  // to an even length for the BF16 pair loads
+  const double v = c.Ac[(size_t)hi * n + lo];
+  if (c.Ainv16) {
+    c.Ainv16[(size_t)row * c.ld16 + col] = __float2bfloat16_rn((float)v);
+    // the pad column of an odd-length row must hold a finite value
+    if (col == n - 1 && c.ld16 > n) c.Ainv16[(size_t)row * c.ld16 + n] = __float2bfloat16_rn(0.f);
+  } else
+    c.Ainv[q] = (float)v;
 }
 
 // ───────────────────────── per-iteration application ─────────────────────────
@@ -297,7 +316,9 @@ __global__ void __launch_bounds__(256) coarse_rc_kernel(const __grid_constant__ 
   c.rc[I] = v;
 }
 
-// y_c = Ainv r_c: r_c staged in shared memory, one warp per row
+// y_c = Ainv r_c: r_c staged in shared memory, one warp per row.  The inverse
+// is FP32, or BF16 (half the bytes; rows padded to even length, pairs loaded
+// together; FP32 products and sums).
 constexpr int kCoarseMvThreads = 256;
 
 __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
@@ -306,18 +327,29 @@ __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
   extern __shared__ __align__(16) float s_rc[];
   const int n = c.n_dof;
   for (int I = threadIdx.x; I < n; I += kCoarseMvThreads) s_rc[I] = __ldcg(c.rc + I);
+  if (c.Ainv16 && threadIdx.x == 0 && (n & 1)) s_rc[n] = 0.f;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * (kCoarseMvThreads / 32) + warp;
   if (row >= n) return;
-  const float* Arow = c.Ainv + (size_t)row * n;
   float s0 = 0.f, s1 = 0.f;
-  int j = lane;
-  for (; j + 32 < n; j += 64) {
-    s0 += __ldg(Arow + j) * s_rc[j];
-    s1 += __ldg(Arow + j + 32) * s_rc[j + 32];
+  if (c.Ainv16) {
+    const __nv_bfloat162* Arow = reinterpret_cast<const __nv_bfloat162*>(c.Ainv16 + (size_t)row * c.ld16);
+    const int np = c.ld16 / 2;
+    for (int j = lane; j < np; j += 32) {
+      const float2 a2 = __bfloat1622float2(__ldg(Arow + j));
+      s0 += a2.x * s_rc[2 * j];
+      s1 += a2.y * s_rc[2 * j + 1];
+    }
+  } else {
+    const float* Arow = c.Ainv + (size_t)row * n;
+    int j = lane;
+    for (; j + 32 < n; j += 64) {
+      s0 += __ldg(Arow + j) * s_rc[j];
+      s1 += __ldg(Arow + j + 32) * s_rc[j + 32];
+    }
+    if (j < n) s0 += __ldg(Arow + j) * s_rc[j];
   }
-  if (j < n) s0 += __ldg(Arow + j) * s_rc[j];
   float s = s0 + s1;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -656,7 +688,7 @@ void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg,
   coarse_restrict_kernel<<<a.c.n_cells * kRestrictSlices, kRestrictThreads, 0, s>>>(a, r, cg);
   coarse_rc_kernel<<<nblk(a.c.n_dof, 256), 256, 0, s>>>(a.c, cg);
   const int rows_per_cta = kCoarseMvThreads / 32;
-  coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(
+  coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * ((size_t)a.c.n_dof + 1), s>>>(
       a.c, cg);
 }
 

@@ -142,6 +142,7 @@ struct FemCtx {
   bool coarse_built = false;
   bool coarse_valid = false;   // Ainv matches the current tangent policy
   int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
+  bool coarse_bf16 = false;    // store the coarse inverse in BF16
   int coarse_reuse = 0;        // PCG solves one assembly serves; 0 = adaptive
   double coarse_base_ipd = -1;  // CG iterations per decade right after the last assembly
   int coarse_uses = 0;
@@ -733,6 +734,25 @@ bool build_loop_graph(FemCtx* c, int kind) {
   return ok;
 }
 
+// Frees the coarse lattice and the graphs that captured its buffers (two-level
+// and learned); the next two-level / learned solve rebuilds them.
+int drop_coarse(FemCtx* c) {
+  CK(cudaStreamSynchronize(c->stream));
+  for (void* p : c->coarse_bufs)
+    if (p) cudaFree(p);
+  c->coarse_bufs.clear();
+  c->cdev = CoarseDev{};
+  c->coarse_built = false;
+  c->coarse_valid = false;
+  for (int k : {GRAPH_TWO_LEVEL, GRAPH_LEARNED}) {
+    if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+    if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
+    c->cg_graph[k] = nullptr;
+    c->loop_graph[k] = nullptr;
+  }
+  return FEM_OK;
+}
+
 int ensure_cg_graph(FemCtx* c, int kind) {
   int st;
   if ((st = choose_matvec_variant(c))) return st;
@@ -789,8 +809,12 @@ int coarse_alloc(FemCtx* c, T** dst, size_t n) {
 // Builds the coarse lattice: cell edge H = coarse_cell_voxels x the mesh
 // length (cube root of 5 x the mean element volume: the voxel edge on
 // 5-tet voxel meshes), grown by 25 % steps until at most kMaxCoarseNodes
-// coarse nodes remain.  Elements go to the cell of their centroid; a node to
-// the cell of its lowest-numbered element.
+// coarse nodes remain.  Along each axis the lattice overhangs the mesh by
+// less than one cell; the overhang is split between both ends in whole mesh
+// lengths, so no end cell holds a slab thinner than about H/2 (a thin end
+// slab leaves coarse nodes with almost no support and an ill-conditioned
+// coarse operator).  Elements go to the cell of their centroid; a node to the
+// cell of its lowest-numbered element.
 constexpr int kMaxCoarseNodes = 4096;
 
 int build_coarse(FemCtx* c) {
@@ -828,8 +852,13 @@ int build_coarse(FemCtx* c) {
   std::vector<int> ecell(Ne), cell_of_lin, act_lin, cn_of_lat;
   int g[3];
   int n_cells = 0, n_cn = 0;
+  double org[3] = {lo[0], lo[1], lo[2]};
   for (int attempt = 0; attempt < 64; ++attempt) {
-    for (int d = 0; d < 3; ++d) g[d] = std::max(1, (int)std::ceil((hi[d] - lo[d]) / H - 1e-9));
+    for (int d = 0; d < 3; ++d) {
+      g[d] = std::max(1, (int)std::ceil((hi[d] - lo[d]) / H - 1e-9));
+      const double overhang = g[d] * H - (hi[d] - lo[d]);
+      org[d] = lo[d] - std::floor(0.5 * overhang / hmesh + 1e-6) * hmesh;
+    }
     const int64_t ncell_lat = (int64_t)g[0] * g[1] * g[2];
     if (ncell_lat > (1 << 22)) {
       H *= 1.25;
@@ -839,7 +868,7 @@ int build_coarse(FemCtx* c) {
     for (int e = 0; e < Ne; ++e) {
       int ijk[3];
       for (int d = 0; d < 3; ++d)
-        ijk[d] = std::min(g[d] - 1, std::max(0, (int)std::floor((cen[3 * e + d] - lo[d]) / H)));
+        ijk[d] = std::min(g[d] - 1, std::max(0, (int)std::floor((cen[3 * e + d] - org[d]) / H)));
       const int lin = (ijk[0] * g[1] + ijk[1]) * g[2] + ijk[2];
       ecell[e] = lin;
       cell_of_lin[lin] = 0;
@@ -918,7 +947,7 @@ int build_coarse(FemCtx* c) {
   cd.n_cn = n_cn;
   cd.n_dof = 3 * n_cn;
   cd.inv_H = (float)(1.0 / H);
-  cd.lo = make_float3((float)lo[0], (float)lo[1], (float)lo[2]);
+  cd.lo = make_float3((float)org[0], (float)org[1], (float)org[2]);
   int st;
   if ((st = coarse_upload(c, &cd.cell_ijk, cell_ijk))) return st;
   if ((st = coarse_upload(c, &cd.cell_corner, cell_corner))) return st;
@@ -931,7 +960,14 @@ int build_coarse(FemCtx* c) {
   const size_t nd = (size_t)cd.n_dof;
   if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * coarse_cell_slices() * 576))) return st;
   if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
-  if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
+  cd.ld16 = (cd.n_dof + 1) & ~1;
+  cd.Ainv = nullptr;
+  cd.Ainv16 = nullptr;
+  if (c->coarse_bf16) {
+    if ((st = coarse_alloc(c, &cd.Ainv16, nd * (size_t)cd.ld16))) return st;
+  } else {
+    if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
+  }
   if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * coarse_restrict_slices() * 24))) return st;
   if ((st = coarse_alloc(c, &cd.yc, nd))) return st;
   if ((st = coarse_alloc(c, &cd.rc, nd))) return st;
@@ -960,7 +996,7 @@ int build_coarse(FemCtx* c) {
 }
 
 // Assembles Ac = P^T K_T P at the current tangent and inverts it (FP64
-// Cholesky + inverse, then an FP32 copy), unless the reuse policy keeps the
+// Cholesky + inverse, then an FP32 or BF16 copy), unless the reuse policy keeps the
 // previous one.
 int ensure_coarse(FemCtx* c) {
   int st;
@@ -1444,16 +1480,15 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       if (value < 1 || value > 64)
         return set_err(c, FEM_ERR_INVALID, "coarse cell edge %lld not in [1, 64] mesh lengths", (long long)value);
       if (value != c->coarse_cell_voxels) {
-        CK(cudaStreamSynchronize(c->stream));
-        for (void* p : c->coarse_bufs)
-          if (p) cudaFree(p);
-        c->coarse_bufs.clear();
         c->coarse_cell_voxels = (int)value;
-        c->coarse_built = false;
-        c->coarse_valid = false;
-        // the captured two-level graph holds the old coarse buffers
-        if (c->cg_graph[GRAPH_TWO_LEVEL]) cudaGraphExecDestroy(c->cg_graph[GRAPH_TWO_LEVEL]);
-        c->cg_graph[GRAPH_TWO_LEVEL] = nullptr;
+        return drop_coarse(c);
+      }
+      return FEM_OK;
+    case FEM_OPT_COARSE_BF16:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "coarse BF16 flag must be 0 or 1");
+      if ((value != 0) != c->coarse_bf16) {
+        c->coarse_bf16 = value != 0;
+        return drop_coarse(c);
       }
       return FEM_OK;
     case FEM_OPT_LEARNED_COARSE:

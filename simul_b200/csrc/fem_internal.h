@@ -115,7 +115,9 @@ struct CoarseDev {
   const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
   double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
-  float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric)
+  float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric), or null
+  __nv_bfloat16* Ainv16;    // [n_dof * ld16] BF16 inverse, or null
+  int ld16;                 // n_dof rounded up to even
   float* cell_r;            // [n_cells][slices][24] restricted residual shares per cell
   float* rc;                // [n_dof] coarse residual P^T r
   float* yc;                // [n_dof] coarse correction

@@ -163,10 +163,14 @@ class FEMesh:
                 "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5],
                 "last_assembly_kernels_ms": out[6], "reuse": int(out[7])}
 
-    def set_coarse_options(self, cell=None, reuse=None):
-        """Two-level preconditioner: lattice cell edge in mesh lengths and the
-        number of PCG solves one coarse assembly serves (0: adaptive)."""
+    def set_coarse_options(self, cell=None, reuse=None, bf16=None):
+        """Two-level preconditioner: lattice cell edge in mesh lengths, the
+        number of PCG solves one coarse assembly serves (0: adaptive), and
+        whether the coarse inverse is stored in BF16."""
         lib = _lib.load()
+        if bf16 is not None:
+            _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_BF16, 1 if bf16 else 0), self.ctx,
+                   "fem_set_option")
         if cell is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_CELL, int(cell)), self.ctx, "fem_set_option")
         if reuse is not None:

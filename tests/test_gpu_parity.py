@@ -189,15 +189,17 @@ def test_pcg_solves_tangent_system(cuda, bar):
     assert rc == 0 and it2.value > 0
 
 
-def test_two_level_pcg_matches_oracle_with_fewer_iterations(cuda, vox):
+@pytest.mark.parametrize("bf16", [False, True])
+def test_two_level_pcg_matches_oracle_with_fewer_iterations(cuda, vox, bf16):
     """Jacobi + trilinear Galerkin coarse correction: same solution as the
-    FP64 oracle, fewer CG iterations than Jacobi alone."""
+    FP64 oracle, fewer CG iterations than Jacobi alone; the coarse inverse
+    stored in FP32 or BF16."""
     mesh = make_mesh(vox.X, vox.conn, cuda)
     mat = B.LinearElastic(1e3, 0.3)
     idx = np.where(vox.fixed_mask.reshape(-1))[0]
     mesh.set_fixed_dofs(idx, np.zeros(idx.size))
     mat.compute_nodal_forces(mesh)
-    mesh.set_coarse_options(cell=4)         # 3x3x3 cells on this 12^3-voxel body
+    mesh.set_coarse_options(cell=4, bf16=bf16)   # 3x3x3 cells on this 12^3-voxel body
     lib = _lib.load()
     rng = np.random.default_rng(5)
     rhs = rng.standard_normal(vox.X.shape)

@@ -62,6 +62,8 @@ def parse():
                     help="PCG solves one coarse-operator assembly serves (0: adaptive)")
     ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
     ap.add_argument("--coarse-bf16", type=int, default=0, help="store the coarse inverse in BF16")
+    ap.add_argument("--fused-step", type=int, default=0,
+                    help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
     ap.add_argument("--cg-rtol-max", type=float, default=1e-1, help="inexact-Newton forcing term cap")
     return ap.parse_args()
@@ -269,6 +271,7 @@ def main():
     mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16))
     if args.matvec_variant != "auto":
         mesh.set_matvec_variant(args.matvec_variant)
+    mesh.set_fused_step(bool(args.fused_step))
     if args.precond == "learned":
         from simul_b200 import learned
         learned.set_weights(mesh, learned.load(args.weights))
@@ -430,6 +433,7 @@ def main():
             "gpu_launches": int(launches // max(args.steps, 1)),
             "kernel_ms": {"matvec": kms[0], "residual": kms[1], "cg_update": kms[2], "cg_direction": kms[3]},
             "matvec_variant": {"chosen": variant, "ns_per_launch": st["matvec_ns"]},
+            "fused_step": mesh.step_info(),
             "whole_solve_graphs": {"available": st["whole_solve_graph_available"],
                                    "pcg_solves_as_one_launch": st["whole_solve_graphs"]},
             "roofline": {"bound": "hbm", "kernel": ("matvec_kernel<J2> (fused node-block)" if variant == "fused"

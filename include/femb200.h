@@ -163,7 +163,17 @@ enum {
   FEM_OPT_LEARNED_COARSE = 4,
   /* two-level preconditioner: 1 stores the coarse inverse in BF16 (half the
    * bytes per CG iteration; FP32 products), 0 (default) in FP32 */
-  FEM_OPT_COARSE_BF16 = 5
+  FEM_OPT_COARSE_BF16 = 5,
+  /* 1: the CG work after each matvec (update, restriction, coarse product,
+   * preconditioner, direction) runs as one cooperative kernel with grid-wide
+   * barriers, where the runtime accepts it in a graph; 0 (default): as a
+   * chain of kernels.  Jacobi and two-level; batched solves use the chain. */
+  FEM_OPT_FUSED_STEP = 6,
+  /* 1 (default): a PCG solve runs as one graph launch (a conditional WHILE
+   * node); 0: as launches of fixed 12- or 32-iteration graphs with a host
+   * check between them (kernel profilers cannot attribute kernels inside
+   * conditional graphs) */
+  FEM_OPT_WHOLE_SOLVE_GRAPH = 7
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing
@@ -227,6 +237,10 @@ int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t
  * assembly + factorisation (CUDA events), [6] ms of its assembly part,
  * [7] PCG solves one assembly serves */
 int fem_coarse_info(void* ctx, double* out8);
+/* fused CG step: out[0] 1 while the option is on and the runtime accepted
+ * it, [1] the captured Jacobi CG graph uses it, [2] the two-level one does,
+ * [3] warps per lattice cell in its restriction phase */
+int fem_step_info(void* ctx, int64_t* out4);
 /* cudaStream_t of the context (as void*) */
 void* fem_ctx_stream(void* ctx);
 

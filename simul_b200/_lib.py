@@ -41,6 +41,8 @@ FEM_OPT_COARSE_CELL = 2
 FEM_OPT_COARSE_REUSE = 3
 FEM_OPT_LEARNED_COARSE = 4
 FEM_OPT_COARSE_BF16 = 5
+FEM_OPT_FUSED_STEP = 6
+FEM_OPT_WHOLE_SOLVE_GRAPH = 7
 MPNN_PARAMS = 34307
 MATVEC_VARIANTS = {0: "fused", 1: "two_phase"}
 
@@ -100,6 +102,7 @@ SIGNATURES = {
     "fem_ctx_stream": (C.c_void_p, [_VP]),
     "fem_set_option": (C.c_int, [_VP, C.c_int32, C.c_int64]),
     "fem_coarse_info": (C.c_int, [_VP, _DP]),
+    "fem_step_info": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "fem_selftest_umma": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32, _VP]),
     "fem_mpnn_set_weights": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int64]),
     "fem_mpnn_get_weights": (C.c_int, [_VP, C.POINTER(C.c_float), C.c_int64]),

@@ -38,6 +38,7 @@ enum { GRAPH_JACOBI = 0, GRAPH_TWO_LEVEL = 1, GRAPH_LEARNED = 2, N_GRAPHS = 3 };
 constexpr int kCGBatch = 32;
 constexpr int kCGBatchShort = 12;
 inline int cg_batch(int kind) { return kind == 0 ? kCGBatch : kCGBatchShort; }
+inline int step_chunks(int n_nodes) { return (n_nodes + kStepThreads - 1) / kStepThreads; }
 
 struct FemCtx {
   int device = 0;
@@ -111,6 +112,20 @@ struct FemCtx {
   int cg_graph_model[N_GRAPHS] = {-2, -2, -2};
   int cg_graph_variant[N_GRAPHS] = {-1, -1, -1};
   int cg_graph_flags[N_GRAPHS] = {-1, -1, -1};
+  // fused CG step (one cooperative kernel after each matvec; off by default:
+  // on B200 its four grid barriers and the cooperative launch cost more than
+  // the launch gaps of the kernel chain they replace): wanted by the
+  // option, still available (a refused capture turns it off), and not while
+  // fem_batch_solve runs several contexts at once (cooperative grids of
+  // concurrent contexts could wait on each other's SMs)
+  bool fused_step = false;
+  bool fused_ok = true;
+  bool in_batch = false;
+  unsigned int* step_bar = nullptr;  // [4] grid barrier words
+  double* jac_part = nullptr;        // [2 n_chunks] Jacobi step shares
+  float* cell_rf = nullptr;          // two-level step: [n_cells][tl_slices][24]
+  double* tl_part = nullptr;         // two-level step: [n_cells tl_slices + n_chunks]
+  int tl_slices = 1;
 
   // learned preconditioner: node graph, features, weights, activations
   MpnnDev mdev{};
@@ -297,7 +312,8 @@ void free_ctx(FemCtx* c) {
                   c->fixed_vals_full, c->fext_full,
                   c->u, c->u_base, c->R, c->tmpd, c->payload, c->ep_c, c->epe_c, c->ep_t,
                   c->epe_t, c->r, c->x, c->p, c->y, c->dinv, c->tmpf, c->d_perm_node,
-                  c->d_perm_elem, c->matD, c->matF, c->partials, c->counters, c->scalars, c->cg};
+                  c->d_perm_elem, c->matD, c->matF, c->partials, c->counters, c->scalars, c->cg,
+                  c->step_bar, c->jac_part};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_cg) cudaFreeHost(c->h_cg);
@@ -507,6 +523,8 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->counters, (size_t)N_SITES))) return st;
   if ((st = dalloc(c, &c->scalars, (size_t)8))) return st;
   if ((st = dalloc(c, &c->cg, (size_t)1))) return st;
+  if ((st = dalloc(c, &c->step_bar, (size_t)4))) return st;
+  if ((st = dalloc(c, &c->jac_part, 2 * (size_t)step_chunks(c->Nn)))) return st;
   CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_cg), sizeof(CGState)));
   CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_scalars), 8 * sizeof(double)));
   // default material: unit-scale linear elastic placeholder, every element id 0, scale 1
@@ -601,7 +619,40 @@ CoarseArgs coarse_args(const FemCtx* c) {
   return a;
 }
 
-void enqueue_cg_iter(FemCtx* c, int kind) {
+bool use_fused(const FemCtx* c, int kind) {
+  return kind != GRAPH_LEARNED && c->fused_step && c->fused_ok && !c->in_batch &&
+         (kind == GRAPH_JACOBI || c->cell_rf != nullptr);
+}
+
+StepArgs step_args(const FemCtx* c, int kind) {
+  StepArgs a;
+  a.m = c->mesh();
+  a.c = c->cdev;
+  a.x = c->x;
+  a.r = c->r;
+  a.p = c->p;
+  a.q = c->y;
+  a.dinv = c->dinv;
+  a.z = c->tmpf;
+  a.cg = c->cg;
+  a.part = kind == GRAPH_TWO_LEVEL ? c->tl_part : c->jac_part;
+  a.cell_rf = c->cell_rf;
+  a.slices = c->tl_slices;
+  a.n_chunks = step_chunks(c->Nn);
+  a.bar = c->step_bar;
+  return a;
+}
+
+// Kernels launched per CG iteration (matvec + the rest).
+int64_t kernels_per_iter(const FemCtx* c, int kind, bool fused) {
+  const int64_t mv = c->mv_variant == MV_TWO_PHASE ? 2 : 1;
+  if (fused) return mv + 1;
+  return mv + (kind == GRAPH_TWO_LEVEL ? 6 : 2);
+}
+
+// Enqueues one CG iteration; returns the first launch error (a refused
+// cooperative launch during capture).
+cudaError_t enqueue_cg_iter(FemCtx* c, int kind, bool fused) {
   MvArgs mv = make_mv(c);
   mv.matF = c->matF;
   mv.payload = c->payload;
@@ -620,7 +671,11 @@ void enqueue_cg_iter(FemCtx* c, int kind) {
     launch_fpcg_dots(ca, false, c->learned_coarse, c->r, c->y, c->dinv, c->tmpf, c->zalt, c->p, c->cg, c->red(),
                      SITE_RZ, SITE_RZ2, c->stream);
     launch_fpcg_pupdate(c->p, c->tmpf, c->zalt, c->Nn, c->cg, false, c->stream);
-    return;
+    return cudaSuccess;
+  }
+  if (fused) {
+    const StepArgs sa = step_args(c, kind);
+    return kind == GRAPH_TWO_LEVEL ? launch_tl_step(sa, c->stream) : launch_jacobi_step(sa, c->stream);
   }
   if (kind == GRAPH_TWO_LEVEL) {
     const CoarseArgs ca = coarse_args(c);
@@ -628,10 +683,11 @@ void enqueue_cg_iter(FemCtx* c, int kind) {
     launch_coarse_apply(ca, c->r, c->cg, c->stream);
     launch_tl_rz(ca, false, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
     launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
-    return;
+    return cudaSuccess;
   }
   launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream);
   launch_cg_pupdate(c->p, c->r, c->dinv, c->Nn, c->cg, c->stream);
+  return cudaSuccess;
 }
 
 // A CG state that never finishes, so the fused CG kernels do their full work
@@ -702,7 +758,7 @@ int choose_matvec_variant(FemCtx* c) {
 // behind) if the runtime cannot build it; the batched graphs are used then.
 constexpr int kLoopIters = 4;
 
-bool build_loop_graph(FemCtx* c, int kind) {
+bool build_loop_graph(FemCtx* c, int kind, bool fused) {
   cudaGraph_t g = nullptr;
   if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
   bool ok = false;
@@ -719,10 +775,14 @@ bool build_loop_graph(FemCtx* c, int kind) {
     if (cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
         cudaSuccess)
       break;
-    for (int i = 0; i < kLoopIters; ++i) enqueue_cg_iter(c, kind);
+    cudaError_t le = cudaSuccess;
+    for (int i = 0; i < kLoopIters; ++i) {
+      const cudaError_t e = enqueue_cg_iter(c, kind, fused);
+      if (le == cudaSuccess) le = e;
+    }
     launch_cg_loop_cond(h, c->cg, kLoopIters, c->stream);
     cudaGraph_t captured = nullptr;
-    if (cudaStreamEndCapture(c->stream, &captured) != cudaSuccess) break;
+    if (cudaStreamEndCapture(c->stream, &captured) != cudaSuccess || le != cudaSuccess) break;
     if (cudaGraphInstantiate(&c->loop_graph[kind], g, 0) != cudaSuccess) {
       c->loop_graph[kind] = nullptr;
       break;
@@ -742,6 +802,8 @@ int drop_coarse(FemCtx* c) {
     if (p) cudaFree(p);
   c->coarse_bufs.clear();
   c->cdev = CoarseDev{};
+  c->cell_rf = nullptr;
+  c->tl_part = nullptr;
   c->coarse_built = false;
   c->coarse_valid = false;
   for (int k : {GRAPH_TWO_LEVEL, GRAPH_LEARNED}) {
@@ -756,7 +818,8 @@ int drop_coarse(FemCtx* c) {
 int ensure_cg_graph(FemCtx* c, int kind) {
   int st;
   if ((st = choose_matvec_variant(c))) return st;
-  const int flags = kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0;
+  const bool fused = use_fused(c, kind);
+  const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0);
   if (c->cg_graph[kind] && c->cg_graph_model[kind] == c->model_kind &&
       c->cg_graph_variant[kind] == c->mv_variant && c->cg_graph_flags[kind] == flags)
     return FEM_OK;
@@ -772,15 +835,33 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   if (kind == GRAPH_TWO_LEVEL || (kind == GRAPH_LEARNED && c->learned_coarse))
     prepare_coarse_kernels(c->model_kind, c->cdev.n_dof);
   if (kind == GRAPH_LEARNED) prepare_mpnn_kernels();
-  cudaGraph_t g;
+  if (fused) prepare_step_kernels(kind == GRAPH_TWO_LEVEL ? 1 : 0, c->cdev.n_dof);
+  cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < cg_batch(kind); ++i) enqueue_cg_iter(c, kind);
+  cudaError_t le = cudaSuccess;
+  for (int i = 0; i < cg_batch(kind); ++i) {
+    const cudaError_t e1 = enqueue_cg_iter(c, kind, fused);
+    if (le == cudaSuccess) le = e1;
+  }
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (fused && (e != cudaSuccess || le != cudaSuccess)) {
+    // the runtime refused the cooperative step: capture the kernel chain
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    c->fused_ok = false;
+    return ensure_cg_graph(c, kind);
+  }
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
   e = cudaGraphInstantiate(&c->cg_graph[kind], g, 0);
   cudaGraphDestroy(g);
+  if (e != cudaSuccess && fused) {
+    c->cg_graph[kind] = nullptr;
+    cudaGetLastError();
+    c->fused_ok = false;
+    return ensure_cg_graph(c, kind);
+  }
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-  if (c->use_loop_graph && !build_loop_graph(c, kind)) c->use_loop_graph = false;
+  if (c->use_loop_graph && !build_loop_graph(c, kind, fused)) c->use_loop_graph = false;
   c->cg_graph_model[kind] = c->model_kind;
   c->cg_graph_variant[kind] = c->mv_variant;
   c->cg_graph_flags[kind] = flags;
@@ -971,6 +1052,11 @@ int build_coarse(FemCtx* c) {
   if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * coarse_restrict_slices() * 24))) return st;
   if ((st = coarse_alloc(c, &cd.yc, nd))) return st;
   if ((st = coarse_alloc(c, &cd.rc, nd))) return st;
+  // fused two-level step: per (cell, slice) restriction and ||r||^2 shares
+  c->tl_slices = step_slices(n_cells, cd.n_dof);
+  const size_t items = (size_t)n_cells * c->tl_slices;
+  if ((st = coarse_alloc(c, &c->cell_rf, items * 24))) return st;
+  if ((st = coarse_alloc(c, &c->tl_part, items + step_chunks(Nn)))) return st;
   if (!c->solver) {
     if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS)
       return set_err(c, FEM_ERR_CUDA, "cusolverDnCreate failed");
@@ -1244,6 +1330,8 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
   if (learned && (st = ensure_mpnn(c))) return st;
   if ((st = ensure_cg_graph(c, kind))) return st;
+  const bool fused = (c->cg_graph_flags[kind] & 2) != 0;
+  if (fused) CK(cudaMemsetAsync(c->step_bar, 0, 4 * sizeof(unsigned int), c->stream));
   if (learned) CK(cudaMemsetAsync(c->mdev.err, 0, sizeof(int), c->stream));
   ++c->n_launches; launch_cg_init(b_int, c->r, c->x, c->p, c->dinv, c->Nn, c->cg, rtol, maxit, c->red(), SITE_CGI,
                  c->stream, (tl || learned) ? 0 : 1);
@@ -1304,7 +1392,7 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     const int64_t net_steps = std::max<int64_t>(0, (int64_t)h.iter - h.n_alt + std::min(h.n_alt, 3));
     c->n_launches += (5LL + (c->learned_coarse ? 3 : 0)) * h.iter + 6LL * net_steps;
   } else {
-    c->n_launches += (tl ? 7LL : 3LL) * h.iter;
+    c->n_launches += kernels_per_iter(c, kind, fused) * h.iter;
   }
   if (learned) {
     c->n_alt_steps += h.n_alt;
@@ -1494,6 +1582,24 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
     case FEM_OPT_LEARNED_COARSE:
       if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "learned coarse flag must be 0 or 1");
       c->learned_coarse = value != 0;
+      return FEM_OK;
+    case FEM_OPT_WHOLE_SOLVE_GRAPH:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "whole-solve graph flag must be 0 or 1");
+      if ((value != 0) != c->use_loop_graph) {
+        CK(cudaStreamSynchronize(c->stream));
+        // recaptured on the next solve, with or without the loop graph
+        for (int k = 0; k < N_GRAPHS; ++k) {
+          if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+          if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
+          c->cg_graph[k] = nullptr;
+          c->loop_graph[k] = nullptr;
+        }
+        c->use_loop_graph = value != 0;
+      }
+      return FEM_OK;
+    case FEM_OPT_FUSED_STEP:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "fused step flag must be 0 or 1");
+      c->fused_step = value != 0;
       return FEM_OK;
     case FEM_OPT_COARSE_REUSE:
       if (value < 0 || value > (1 << 20))
@@ -1689,6 +1795,16 @@ int fem_coarse_info(void* ctx, double* out8) {
   return FEM_OK;
 }
 
+int fem_step_info(void* ctx, int64_t* out4) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  if (!c || !out4) return FEM_ERR_INVALID;
+  out4[0] = (c->fused_step && c->fused_ok) ? 1 : 0;
+  out4[1] = (c->cg_graph[GRAPH_JACOBI] && (c->cg_graph_flags[GRAPH_JACOBI] & 2)) ? 1 : 0;
+  out4[2] = (c->cg_graph[GRAPH_TWO_LEVEL] && (c->cg_graph_flags[GRAPH_TWO_LEVEL] & 2)) ? 1 : 0;
+  out4[3] = c->tl_slices;
+  return FEM_OK;
+}
+
 void* fem_ctx_stream(void* ctx) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   return c ? (void*)c->stream : nullptr;
@@ -1845,6 +1961,14 @@ int fem_batch_solve(void** ctxs, int32_t n, const FemSolveParams* prm, int32_t l
     fem_default_solve_params(&p);
   p.progress = nullptr;  // callbacks are not re-entrant across workers
   const int workers = std::max(1, std::min<int>(n, n_threads > 0 ? n_threads : n));
+  // contexts leave batch mode on every return path
+  struct BatchMode {
+    void** ctxs;
+    int n;
+    ~BatchMode() {
+      for (int i = 0; i < n; ++i) static_cast<FemCtx*>(ctxs[i])->in_batch = false;
+    }
+  } batch_mode{ctxs, n};
   // One thread first brings every instance to a solvable state: tangent at the
   // current displacement, matvec variant, coarse operator and the captured CG
   // graph.  Graph capture then never runs while other workers issue work.
@@ -1860,6 +1984,7 @@ int fem_batch_solve(void** ctxs, int32_t n, const FemSolveParams* prm, int32_t l
     if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : p.precond))) return st;
     if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
     if (learned && (st = ensure_mpnn(c))) return st;
+    c->in_batch = workers > 1;
     if ((st = ensure_cg_graph(c, learned ? GRAPH_LEARNED : (tl ? GRAPH_TWO_LEVEL : GRAPH_JACOBI)))) return st;
   }
   std::atomic<int> next{0};

@@ -130,6 +130,42 @@ struct CoarseArgs {
   const float* payload;
 };
 
+// Fused CG step (fem_step.cu): the work of one PCG iteration after the
+// tangent matvec, as one cooperative kernel whose phases are separated by
+// grid-wide barriers.  Two-level: x, r update + ||r||^2 + restriction |
+// coarse residual + convergence test | coarse product | z = D^-1 r + P y_c and
+// r.z | p = z + beta p.  Jacobi: x, r update + ||r||^2 + r.D^-1 r |
+// p = D^-1 r + beta p.
+constexpr int kStepThreads = 512;
+
+struct StepArgs {
+  MeshDev m;
+  CoarseDev c;
+  float* x;
+  float* r;
+  float* p;
+  const float* q;           // K p from the matvec
+  const float* dinv;
+  float* z;                 // two-level: preconditioned residual (scratch)
+  CGState* cg;
+  double* part;             // two-level: [n_cells * slices] ||r||^2 shares, then [n_chunks] r.z shares;
+                            // Jacobi: [2][n_chunks]
+  float* cell_rf;           // two-level: [n_cells][slices][24] restricted residual shares
+  int slices;               // two-level: warps per cell in the update + restriction phase
+  int n_chunks;             // ceil(n_nodes / kStepThreads)
+  unsigned int* bar;        // [2] grid barrier: arrivals, generation
+};
+
+// CTAs of a cooperative step launch on this device (0: not available);
+// kind 0 Jacobi, 1 two-level with an n_dof coarse space.
+int step_grid(int kind, int n_dof);
+// warps per lattice cell in the two-level step's restriction phase
+int step_slices(int n_cells, int n_dof);
+// raises the step kernels' shared-memory limit (before a capture)
+void prepare_step_kernels(int kind, int n_dof);
+cudaError_t launch_tl_step(const StepArgs& a, cudaStream_t s);
+cudaError_t launch_jacobi_step(const StepArgs& a, cudaStream_t s);
+
 // Learned preconditioner (fem_mpnn.cu).  Flat FP32 parameter order:
 // W_e [64][16], b_e [64], then per layer W_l [64][128], b_l [64], then
 // W_d [3][64], b_d [3].

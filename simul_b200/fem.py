@@ -176,6 +176,25 @@ class FEMesh:
         if reuse is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_REUSE, int(reuse)), self.ctx, "fem_set_option")
 
+    def set_fused_step(self, on: bool):
+        """Runs the CG work after each matvec as one cooperative kernel (True)
+        or as a chain of kernels (False, the default)."""
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_FUSED_STEP, 1 if on else 0), self.ctx,
+               "fem_set_option")
+
+    def set_whole_solve_graph(self, on: bool):
+        """One graph launch per PCG solve (True, the default) or fixed-size
+        iteration graphs with a host check between them (False; kernel
+        profilers cannot see inside the conditional graph)."""
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_WHOLE_SOLVE_GRAPH, 1 if on else 0), self.ctx,
+               "fem_set_option")
+
+    def step_info(self) -> dict:
+        out = (C.c_int64 * 4)()
+        _check(_lib.load().fem_step_info(self.ctx, out), self.ctx, "fem_step_info")
+        return {"available": bool(out[0]), "jacobi_graph_fused": bool(out[1]),
+                "two_level_graph_fused": bool(out[2]), "restriction_warps_per_cell": int(out[3])}
+
     def set_matvec_variant(self, variant):
         """Forces the tangent-matvec variant ("fused", "two_phase") or restores
         the timed choice (None)."""

@@ -228,6 +228,69 @@ def test_two_level_pcg_matches_oracle_with_fewer_iterations(cuda, vox, bf16):
         assert _rel_l2(sols[name], u_ref) < 1e-5, name
 
 
+def _pcg_fused_vs_chain(mesh, pc, rhs, cuda, rtol):
+    lib = _lib.load()
+    r = dev(rhs, cuda)
+    out = {}
+    for fused in (True, False):
+        mesh.set_fused_step(fused)
+        du = torch.zeros_like(r)
+        it = C.c_int32()
+        rel = C.c_double()
+        rc = lib.fem_pcg(mesh.ctx, pc, ptr(r), ptr(du), rtol, 20000, C.byref(it), C.byref(rel))
+        assert rc == 0, _lib.last_error(mesh.ctx)
+        assert rel.value <= rtol
+        info = mesh.step_info()
+        key = "two_level_graph_fused" if pc == _lib.FEM_PRECOND_TWO_LEVEL else "jacobi_graph_fused"
+        assert info[key] == fused, info
+        out[fused] = (du.cpu().numpy(), it.value)
+    return out
+
+
+@pytest.mark.parametrize("pc", ["jacobi", "two_level"])
+def test_fused_step_matches_kernel_chain(cuda, vox, pc):
+    """The cooperative fused CG step (one kernel after each matvec, grid-wide
+    barriers) and the chain of kernels solve to the same displacement in
+    about the same number of iterations; both match the FP64 oracle."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    mesh.set_coarse_options(cell=4)
+    rng = np.random.default_rng(11)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    code = {"jacobi": _lib.FEM_PRECOND_JACOBI, "two_level": _lib.FEM_PRECOND_TWO_LEVEL}[pc]
+    out = _pcg_fused_vs_chain(mesh, code, rhs, cuda, 1e-7)
+    (u_f, it_f), (u_c, it_c) = out[True], out[False]
+    assert abs(it_f - it_c) <= max(2, 0.05 * it_c), (it_f, it_c)
+    m = O.Mesh(vox.X, vox.conn)
+    F = O.deformation_gradient(np.zeros_like(vox.X), vox.conn.astype(np.int64), m.dNdX)
+    u_ref = O.solve_tangent(O.Material("linear_elastic", E=1e3, nu=0.3), F, None, m, rhs, vox.fixed_mask)
+    assert _rel_l2(u_f, u_ref) < 1e-5
+    assert _rel_l2(u_c, u_ref) < 1e-5
+
+
+def test_fused_step_grid_stride_on_larger_mesh(cuda):
+    """A mesh with more nodes than the fused step's grid has threads (every
+    vector phase loops): fused and chained two-level PCG agree."""
+    v = meshgen.vertebral_body(n=80, seed=3)
+    mesh = make_mesh(v.X, v.conn, cuda)
+    assert v.n_nodes > 2 * 148 * 512
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(v.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    rng = np.random.default_rng(12)
+    rhs = rng.standard_normal(v.X.shape)
+    rhs[v.fixed_mask] = 0.0
+    out = _pcg_fused_vs_chain(mesh, _lib.FEM_PRECOND_TWO_LEVEL, rhs, cuda, 1e-6)
+    (u_f, it_f), (u_c, it_c) = out[True], out[False]
+    assert abs(it_f - it_c) <= max(3, 0.05 * it_c), (it_f, it_c)
+    assert _rel_l2(u_f, u_c) < 1e-4
+
+
 @pytest.mark.parametrize("reuse", [0, 1])
 def test_newton_j2_two_level_matches_oracle(cuda, vox, reuse):
     """reuse 0: adaptive coarse-operator reuse; 1: rebuilt for every PCG solve."""

@@ -60,8 +60,10 @@ def parse():
     ap.add_argument("--no-jacobi-baseline", action="store_true")
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="PCG solves one coarse-operator assembly serves (0: adaptive)")
-    ap.add_argument("--coarse-cell", type=int, default=8, help="coarse lattice cell edge in voxels")
-    ap.add_argument("--coarse-bf16", type=int, default=0, help="store the coarse inverse in BF16")
+    ap.add_argument("--coarse-cell", type=int, default=4,
+                    help="coarse lattice cell edge in voxels (4: 7,728 coarse DOFs on the n = 64 body)")
+    ap.add_argument("--coarse-bf16", type=int, default=1,
+                    help="store the coarse inverse in BF16 (packed lower block triangle)")
     ap.add_argument("--fused-step", type=int, default=0,
                     help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")

@@ -14,6 +14,8 @@
 // spsolve / ILU-CG (backend/fea/fem/solver/static_solver.py:399-462).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fem_internal.h"
 #include "fem_lattice.cuh"
 #include "fem_reduce.cuh"
@@ -195,23 +197,45 @@ __global__ void coarse_dense_kernel(const __grid_constant__ CoarseDev c) {
   c.Ac[q] = acc;
 }
 
-// Symmetric FP32 (or BF16) copy of the inverse whose lower triangle potri
-// wrote.
+// Symmetric FP32 copy of the inverse whose lower triangle potri wrote
+// (column-major: element (lo, hi), lo >= hi, at hi * n + lo).
 __global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int n = c.n_dof;
   if (q >= (int64_t)n * n) return;
   const int row = (int)(q / n), col = (int)(q % n);
   const int lo = max(row, col), hi = min(row, col);
-  // column-major lower triangle: element (lo, hi) at hi * n + lo; rows padded
-  // to an even length for the BF16 pair loads
-  const double v = c.Ac[(size_t)hi * n + lo];
-  if (c.Ainv16) {
-    c.Ainv16[(size_t)row * c.ld16 + col] = __float2bfloat16_rn((float)v);
-    // the pad column of an odd-length row must hold a finite value
-    if (col == n - 1 && c.ld16 > n) c.Ainv16[(size_t)row * c.ld16 + n] = __float2bfloat16_rn(0.f);
-  } else
-    c.Ainv[q] = (float)v;
+  c.Ainv[q] = (float)c.Ac[(size_t)hi * n + lo];
+}
+
+constexpr int kTile = 64;
+constexpr int kTileElems = kTile * kTile;
+
+// Block-triangle index t = I (I + 1) / 2 + J -> (I, J), J <= I.
+__device__ __forceinline__ void tile_ij(int t, int& I, int& J) {
+  int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((i + 1) * (i + 2) / 2 <= t) ++i;
+  while (i * (i + 1) / 2 > t) --i;
+  I = i;
+  J = t - i * (i + 1) / 2;
+}
+
+// Packed BF16 copy: the lower block triangle of 64 x 64 tiles.
+__global__ void coarse_pack16_kernel(const __grid_constant__ CoarseDev c) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nt = c.nb16 * (c.nb16 + 1) / 2;
+  if (q >= (int64_t)nt * kTileElems) return;
+  const int t = (int)(q / kTileElems), e = (int)(q % kTileElems);
+  int I, J;
+  tile_ij(t, I, J);
+  const int row = I * kTile + e / kTile, col = J * kTile + e % kTile;
+  const int n = c.n_dof;
+  float v = 0.f;
+  if (row < n && col < n) {
+    const int lo = max(row, col), hi = min(row, col);
+    v = (float)c.Ac[(size_t)hi * n + lo];
+  }
+  c.Ainv16[q] = __float2bfloat16_rn(v);
 }
 
 // ───────────────────────── per-iteration application ─────────────────────────
@@ -291,9 +315,8 @@ __global__ void __launch_bounds__(256) coarse_rc_kernel(const __grid_constant__ 
   c.rc[I] = v;
 }
 
-// y_c = Ainv r_c: r_c staged in shared memory, one warp per row.  The inverse
-// is FP32, or BF16 (half the bytes; rows padded to even length, pairs loaded
-// together; FP32 products and sums).
+// y_c = Ainv r_c with the FP32 inverse: r_c staged in shared memory, one warp
+// per row.
 constexpr int kCoarseMvThreads = 256;
 
 __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
@@ -302,21 +325,12 @@ __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
   extern __shared__ __align__(16) float s_rc[];
   const int n = c.n_dof;
   for (int I = threadIdx.x; I < n; I += kCoarseMvThreads) s_rc[I] = __ldcg(c.rc + I);
-  if (c.Ainv16 && threadIdx.x == 0 && (n & 1)) s_rc[n] = 0.f;
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row = blockIdx.x * (kCoarseMvThreads / 32) + warp;
   if (row >= n) return;
   float s0 = 0.f, s1 = 0.f;
-  if (c.Ainv16) {
-    const __nv_bfloat162* Arow = reinterpret_cast<const __nv_bfloat162*>(c.Ainv16 + (size_t)row * c.ld16);
-    const int np = c.ld16 / 2;
-    for (int j = lane; j < np; j += 32) {
-      const float2 a2 = __bfloat1622float2(__ldg(Arow + j));
-      s0 += a2.x * s_rc[2 * j];
-      s1 += a2.y * s_rc[2 * j + 1];
-    }
-  } else {
+  {
     const float* Arow = c.Ainv + (size_t)row * n;
     int j = lane;
     for (; j + 32 < n; j += 64) {
@@ -329,6 +343,125 @@ __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
   if (lane == 0) c.yc[row] = s;
+}
+
+// y_c = Ainv r_c with the packed BF16 inverse, in two passes.
+//
+// Pass 1, one warp per stored tile (I, J), reading the tile once for both
+// products it feeds: u = A_IJ r_J (row block I) and, off the diagonal,
+// v = A_IJ^T r_I (row block J).  Lane l takes row quad position q = l / 8
+// and the 8 columns 8 (l % 8) ...; one 16-byte load per lane covers 4 tile
+// rows (512 contiguous bytes per warp), 16 loads the whole tile.  The row
+// sums of u are completed across the 8 lanes of a row by a butterfly
+// reduce-scatter (each lane ends with 2 rows); the column sums of v across
+// the 4 lanes of a column group likewise (each lane ends with 2 columns).
+// u goes to slot (I, J), v to slot (J, I): every slot (R, K) has exactly one
+// writer.  The product streams the packed half of the matrix once.
+//
+// Pass 2: y_c[64 R + i] = sum over K of slot (R, K), K ascending: a CTA per
+// (R, half of the rows), its 8 warps take K = w, w + 8, ... and the 8
+// partials are added in warp order.  Both passes are deterministic.
+constexpr int kTileWarps = 8;
+
+__device__ __forceinline__ void bf16x8_to_f32(const uint4 w, float a[8]) {
+  const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&w);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float2 f = __bfloat1622float2(h[k]);
+    a[2 * k] = f.x;
+    a[2 * k + 1] = f.y;
+  }
+}
+
+__global__ void __launch_bounds__(kTileWarps * 32, 3) coarse_tile_mv_kernel(
+    const __grid_constant__ CoarseDev c, const CGState* cg) {
+  if (cg && cg->done) return;
+  __shared__ float s_x[kTileWarps][2][kTile];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nb = c.nb16;
+  const int n_tiles = nb * (nb + 1) / 2;
+  const int q = lane >> 3, cg8 = lane & 7;
+  for (int t = blockIdx.x * kTileWarps + warp; t < n_tiles; t += gridDim.x * kTileWarps) {
+    int I, J;
+    tile_ij(t, I, J);
+    const bool offdiag = I != J;
+    __syncwarp();
+    reinterpret_cast<float2*>(s_x[warp][0])[lane] = __ldcg(reinterpret_cast<const float2*>(c.rc + J * kTile) + lane);
+    reinterpret_cast<float2*>(s_x[warp][1])[lane] = __ldcg(reinterpret_cast<const float2*>(c.rc + I * kTile) + lane);
+    __syncwarp();
+    float xj[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) xj[k] = s_x[warp][0][8 * cg8 + k];
+    const uint4* tile = reinterpret_cast<const uint4*>(c.Ainv16 + (size_t)t * kTileElems);
+    float u[16], v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int row = 4 * k + q;
+      float a[8];
+      bf16x8_to_f32(__ldg(tile + row * (kTile / 8) + cg8), a);
+      float s = 0.f;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) s += a[e] * xj[e];
+      u[k] = s;
+      const float xr = s_x[warp][1][row];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] += a[e] * xr;
+    }
+    // u: reduce-scatter over the 8 lanes of a row quad position (lane bits
+    // 2, 1, 0); lane keeps k = 2 cg8 + {0, 1}, i.e. rows 4 (2 cg8 + j) + q
+#pragma unroll
+    for (int o = 4, w = 8; o >= 1; o >>= 1, w >>= 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int k = 0; k < w; ++k) {
+        const float send = up ? u[k] : u[k + w];
+        const float keep = up ? u[k + w] : u[k];
+        u[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+    float* slot_u = c.yslots + ((size_t)I * nb + J) * kTile;
+    slot_u[4 * (2 * cg8) + q] = u[0];
+    slot_u[4 * (2 * cg8 + 1) + q] = u[1];
+    if (offdiag) {
+      // v: reduce-scatter over the 4 lanes of a column group (lane bits 4,
+      // 3); lane keeps columns 8 cg8 + 2 q + {0, 1}
+#pragma unroll
+      for (int o = 16, w = 4; o >= 8; o >>= 1, w >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < w; ++k) {
+          const float send = up ? v[k] : v[k + w];
+          const float keep = up ? v[k + w] : v[k];
+          v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      reinterpret_cast<float2*>(c.yslots + ((size_t)J * nb + I) * kTile + 8 * cg8 + 2 * q)[0] =
+          make_float2(v[0], v[1]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTileWarps * 32) coarse_slot_sum_kernel(
+    const __grid_constant__ CoarseDev c, const CGState* cg) {
+  if (cg && cg->done) return;
+  __shared__ float part[kTileWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int R = blockIdx.x >> 1, half = blockIdx.x & 1;
+  const int nb = c.nb16;
+  const float* src = c.yslots + (size_t)R * nb * kTile + 32 * half + lane;
+  float v = 0.f;
+  for (int K = warp; K < nb; K += kTileWarps) v += __ldcg(src + (size_t)K * kTile);
+  part[warp][lane] = v;
+  __syncthreads();
+  if (warp == 0) {
+    float y = 0.f;
+#pragma unroll
+    for (int w = 0; w < kTileWarps; ++w) y += part[w][lane];
+    const int row = R * kTile + 32 * half + lane;
+    if (row < c.n_dof) c.yc[row] = y;
+  }
 }
 
 // z = D^-1 r + P y_c (zero on fixed DOFs) and r.z.  INIT: p = z, rz set;
@@ -655,15 +788,41 @@ void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s) {
 }
 
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s) {
+  if (c.Ainv16) {
+    const int64_t ne = (int64_t)c.nb16 * (c.nb16 + 1) / 2 * kTileElems;
+    coarse_pack16_kernel<<<nblk(ne, 256), 256, 0, s>>>(c);
+    return;
+  }
   const int64_t nn = (int64_t)c.n_dof * c.n_dof;
   coarse_sym_kernel<<<nblk(nn, 256), 256, 0, s>>>(c);
+}
+
+int coarse_product_kernels(const CoarseDev& c) { return c.Ainv16 ? 2 : 1; }
+
+// Resident CTAs of the tile product on this device (one wave, tiles looped).
+int tile_mv_grid() {
+  static int grid = 0;
+  if (grid == 0) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, coarse_tile_mv_kernel, kTileWarps * 32, 0);
+    grid = std::max(1, sms * std::max(per_sm, 1));
+  }
+  return grid;
 }
 
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
   coarse_restrict_kernel<<<a.c.n_cells * kRestrictSlices, kRestrictThreads, 0, s>>>(a, r, cg);
   coarse_rc_kernel<<<nblk(a.c.n_dof, 256), 256, 0, s>>>(a.c, cg);
+  if (a.c.Ainv16) {
+    const int nt = a.c.nb16 * (a.c.nb16 + 1) / 2;
+    coarse_tile_mv_kernel<<<std::min(nblk(nt, kTileWarps), tile_mv_grid()), kTileWarps * 32, 0, s>>>(a.c, cg);
+    coarse_slot_sum_kernel<<<2 * a.c.nb16, kTileWarps * 32, 0, s>>>(a.c, cg);
+    return;
+  }
   const int rows_per_cta = kCoarseMvThreads / 32;
-  coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * ((size_t)a.c.n_dof + 1), s>>>(
+  coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(
       a.c, cg);
 }
 

@@ -621,7 +621,7 @@ CoarseArgs coarse_args(const FemCtx* c) {
 
 bool use_fused(const FemCtx* c, int kind) {
   return kind != GRAPH_LEARNED && c->fused_step && c->fused_ok && !c->in_batch &&
-         (kind == GRAPH_JACOBI || c->cell_rf != nullptr);
+         (kind == GRAPH_JACOBI || (c->cell_rf != nullptr && c->cdev.Ainv != nullptr));
 }
 
 StepArgs step_args(const FemCtx* c, int kind) {
@@ -647,7 +647,7 @@ StepArgs step_args(const FemCtx* c, int kind) {
 int64_t kernels_per_iter(const FemCtx* c, int kind, bool fused) {
   const int64_t mv = c->mv_variant == MV_TWO_PHASE ? 2 : 1;
   if (fused) return mv + 1;
-  return mv + (kind == GRAPH_TWO_LEVEL ? 6 : 2);
+  return mv + (kind == GRAPH_TWO_LEVEL ? 5 + coarse_product_kernels(c->cdev) : 2);
 }
 
 // Enqueues one CG iteration; returns the first launch error (a refused
@@ -1041,17 +1041,20 @@ int build_coarse(FemCtx* c) {
   const size_t nd = (size_t)cd.n_dof;
   if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * coarse_cell_slices() * 576))) return st;
   if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
-  cd.ld16 = (cd.n_dof + 1) & ~1;
+  cd.nb16 = (cd.n_dof + 63) / 64;
+  const size_t nb = (size_t)cd.nb16;
   cd.Ainv = nullptr;
   cd.Ainv16 = nullptr;
+  cd.yslots = nullptr;
   if (c->coarse_bf16) {
-    if ((st = coarse_alloc(c, &cd.Ainv16, nd * (size_t)cd.ld16))) return st;
+    if ((st = coarse_alloc(c, &cd.Ainv16, nb * (nb + 1) / 2 * 4096))) return st;
+    if ((st = coarse_alloc(c, &cd.yslots, nb * nb * 64))) return st;
   } else {
     if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
   }
   if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * coarse_restrict_slices() * 24))) return st;
-  if ((st = coarse_alloc(c, &cd.yc, nd))) return st;
-  if ((st = coarse_alloc(c, &cd.rc, nd))) return st;
+  if ((st = coarse_alloc(c, &cd.yc, nb * 64))) return st;
+  if ((st = coarse_alloc(c, &cd.rc, nb * 64))) return st;
   // fused two-level step: per (cell, slice) restriction and ||r||^2 shares
   c->tl_slices = step_slices(n_cells, cd.n_dof);
   const size_t items = (size_t)n_cells * c->tl_slices;
@@ -1281,7 +1284,7 @@ void mpnn_apply(FemCtx* c, const float* r, float* z, bool coarse, bool base) {
     const CoarseArgs ca = coarse_args(c);
     launch_coarse_apply(ca, r, nullptr, c->stream);
     launch_coarse_add(ca, z, c->stream);
-    c->n_launches += 4;
+    c->n_launches += 3 + coarse_product_kernels(c->cdev);
   }
 }
 
@@ -1343,14 +1346,14 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     launch_fpcg_dots(ca, true, c->learned_coarse, c->r, c->y, c->dinv, c->tmpf, c->zalt, c->p, c->cg, c->red(),
                      SITE_RZ, SITE_RZ2, c->stream);
     launch_fpcg_pupdate(c->p, c->tmpf, c->zalt, c->Nn, c->cg, true, c->stream);
-    c->n_launches += 6 + 2 + (c->learned_coarse ? 3 : 0);
+    c->n_launches += 6 + 2 + (c->learned_coarse ? 2 + coarse_product_kernels(c->cdev) : 0);
     CKL();
   }
   if (tl) {
     const CoarseArgs ca = coarse_args(c);
     launch_coarse_apply(ca, c->r, c->cg, c->stream);
     launch_tl_rz(ca, true, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
-    c->n_launches += 4;
+    c->n_launches += 3 + coarse_product_kernels(c->cdev);
     CKL();
   }
   const int max_batches = maxit / cg_batch(kind) + 2;
@@ -1390,7 +1393,7 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if (learned) {
     // the network's 6 kernels run until it is switched off (after 3 rejected steps)
     const int64_t net_steps = std::max<int64_t>(0, (int64_t)h.iter - h.n_alt + std::min(h.n_alt, 3));
-    c->n_launches += (5LL + (c->learned_coarse ? 3 : 0)) * h.iter + 6LL * net_steps;
+    c->n_launches += (5LL + (c->learned_coarse ? 2 + coarse_product_kernels(c->cdev) : 0)) * h.iter + 6LL * net_steps;
   } else {
     c->n_launches += kernels_per_iter(c, kind, fused) * h.iter;
   }

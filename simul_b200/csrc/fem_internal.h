@@ -116,11 +116,15 @@ struct CoarseDev {
   double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
   float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric), or null
-  __nv_bfloat16* Ainv16;    // [n_dof * ld16] BF16 inverse, or null
-  int ld16;                 // n_dof rounded up to even
+  // BF16 inverse, or null: the lower block triangle of 64 x 64 tiles, tile
+  // (I, J), I >= J, at index I (I + 1) / 2 + J, row-major inside the tile,
+  // zero beyond n_dof (a diagonal tile holds both of its triangles)
+  __nv_bfloat16* Ainv16;
+  int nb16;                 // tiles per side: ceil(n_dof / 64)
+  float* yslots;            // BF16 path: [nb16][nb16][64] slot (R, K) = Ainv_RK r_c,K
   float* cell_r;            // [n_cells][slices][24] restricted residual shares per cell
-  float* rc;                // [n_dof] coarse residual P^T r
-  float* yc;                // [n_dof] coarse correction
+  float* rc;                // [64 nb16] coarse residual P^T r (zero beyond n_dof)
+  float* yc;                // [64 nb16] coarse correction
 };
 
 struct CoarseArgs {
@@ -237,6 +241,8 @@ void prepare_coarse_kernels(int model, int n_dof);
 // cell Galerkin blocks + dense Ac (FP64, column-major)
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
 // Ainv = FP32 symmetric copy of the lower triangle left in Ac
+// kernels one coarse product launches (1 FP32, 2 packed BF16)
+int coarse_product_kernels(const CoarseDev& c);
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);
 // yc = Ainv P^T r (skipped once cg->done is set, when cg is non-null)
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s);

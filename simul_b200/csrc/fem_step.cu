@@ -215,22 +215,14 @@ __global__ void __launch_bounds__(kStepThreads) tl_step_kernel(const __grid_cons
   if (!grid_sync(a.bar, cg)) return;
   if (*(volatile int*)&cg->done) return;
 
-  // C: y_c = Ainv r_c, r_c staged in shared memory, one warp per row
+  // C: y_c = Ainv r_c (FP32 inverse), r_c staged in shared memory, one warp
+  // per row
   const int n = c.n_dof;
   for (int k = threadIdx.x; k < n; k += kStepThreads) s_rc[k] = __ldcg(c.rc + k);
-  if (threadIdx.x == 0 && (n & 1)) s_rc[n] = 0.f;
   __syncthreads();
   for (int row = gwarp; row < n; row += n_gwarps) {
     float s0 = 0.f, s1 = 0.f;
-    if (c.Ainv16) {
-      const __nv_bfloat162* Arow = reinterpret_cast<const __nv_bfloat162*>(c.Ainv16 + (size_t)row * c.ld16);
-      const int np = c.ld16 / 2;
-      for (int j = lane; j < np; j += 32) {
-        const float2 a2 = __bfloat1622float2(__ldg(Arow + j));
-        s0 += a2.x * s_rc[2 * j];
-        s1 += a2.y * s_rc[2 * j + 1];
-      }
-    } else {
+    {
       const float* Arow = c.Ainv + (size_t)row * n;
       int j = lane;
       for (; j + 32 < n; j += 64) {

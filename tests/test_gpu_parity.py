@@ -228,6 +228,41 @@ def test_two_level_pcg_matches_oracle_with_fewer_iterations(cuda, vox, bf16):
         assert _rel_l2(sols[name], u_ref) < 1e-5, name
 
 
+@pytest.mark.parametrize("cell", [3, 4])
+def test_bf16_packed_coarse_inverse_tracks_fp32(cuda, vox, cell):
+    """The packed BF16 coarse inverse (lower block triangle of 64 x 64 tiles,
+    both products from one read of a tile) preconditions like the FP32 one:
+    about as many PCG iterations, same solution.  Both lattices give coarse
+    DOF counts (240, 144) that leave the last tile row and column partly
+    padding."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    lib = _lib.load()
+    rng = np.random.default_rng(21)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    r = dev(rhs, cuda)
+    its, sols = {}, {}
+    for bf in (False, True):
+        mesh.set_coarse_options(cell=cell, bf16=bf)
+        for rep in range(2):
+            du = torch.zeros_like(r)
+            it = C.c_int32()
+            rel = C.c_double()
+            rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, ptr(r), ptr(du), 1e-7, 20000, C.byref(it),
+                             C.byref(rel))
+            assert rc == 0, _lib.last_error(mesh.ctx)
+            its[(bf, rep)] = it.value
+        sols[bf] = du.cpu().numpy()
+    assert mesh.coarse_info()["coarse_dofs"] % 64 != 0
+    assert its[(True, 0)] == its[(True, 1)]          # deterministic
+    assert its[(True, 0)] <= 1.15 * its[(False, 0)] + 2, its
+    assert _rel_l2(sols[True], sols[False]) < 1e-5
+
+
 def _pcg_fused_vs_chain(mesh, pc, rhs, cuda, rtol):
     lib = _lib.load()
     r = dev(rhs, cuda)

@@ -64,6 +64,8 @@ def parse():
                     help="coarse lattice cell edge in voxels (4: 7,728 coarse DOFs on the n = 64 body)")
     ap.add_argument("--coarse-bf16", type=int, default=1,
                     help="store the coarse inverse in BF16 (packed lower block triangle)")
+    ap.add_argument("--whole-solve-graph", type=int, default=1,
+                    help="1: one graph launch per PCG solve; 0: fixed-size iteration graphs (for kernel profilers)")
     ap.add_argument("--fused-step", type=int, default=0,
                     help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
@@ -274,6 +276,7 @@ def main():
     if args.matvec_variant != "auto":
         mesh.set_matvec_variant(args.matvec_variant)
     mesh.set_fused_step(bool(args.fused_step))
+    mesh.set_whole_solve_graph(bool(args.whole_solve_graph))
     if args.precond == "learned":
         from simul_b200 import learned
         learned.set_weights(mesh, learned.load(args.weights))

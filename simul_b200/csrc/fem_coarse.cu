@@ -240,79 +240,130 @@ __global__ void coarse_pack16_kernel(const __grid_constant__ CoarseDev c) {
 
 // ───────────────────────── per-iteration application ─────────────────────────
 
-// cell_r[cell][slice][3 corner + d] = sum over the slice's nodes of
-// w_corner r_d.  kRestrictSlices CTAs of kRestrictThreads per cell (slice s
-// takes the cell's nodes s, s + S, ...): warp-shuffle sums, then the warps'
-// 24-value shares added in warp order (one barrier).
-constexpr int kRestrictThreads = 128;
-constexpr int kRestrictSlices = 4;
+// Restriction, one warp per (cell, slice) item: slice s of a cell takes the
+// cell's nodes in runs of 32, runs s, s + S, ... (S = r_slices, chosen so the
+// items fill the GPU's warps); the item's 24 shares
+//   cell_r[cell][s][3 corner + d] = sum over its nodes of w_corner r_d
+// are completed by xor butterflies (lane k stores share k).  UPDATE fuses the
+// CG update in front: x += alpha p, r -= alpha q on the item's nodes (every
+// node belongs to exactly one cell), ||r||^2 per CTA (its warps' items in
+// order), and the last CTA runs the convergence test on the ordered total.
+constexpr int kRestrictWarps = 8;
+constexpr int kMaxRestrictSlices = 8;
 
-__global__ void __launch_bounds__(kRestrictThreads) coarse_restrict_kernel(
-    const __grid_constant__ CoarseArgs a, const float* __restrict__ r, const CGState* cg) {
+__device__ __forceinline__ float warp_allsum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool UPDATE>
+__global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
+    const __grid_constant__ CoarseArgs a, float* r, float* x, const float* __restrict__ p,
+    const float* __restrict__ q, CGState* cg, Reduce red, int site) {
   if (cg && cg->done) return;
-  __shared__ float sw[kRestrictThreads / 32][24];
+  __shared__ double s_rr[kRestrictWarps];
+  __shared__ double s_red[kRestrictWarps];
+  __shared__ bool am_last;
   const CoarseDev& c = a.c;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int cell = blockIdx.x / kRestrictSlices, slice = blockIdx.x - cell * kRestrictSlices;
-  const int3 ijk = c.cell_ijk[cell];
-  const int n0 = c.cell_node_ptr[cell], n1 = c.cell_node_ptr[cell + 1];
-  float acc[24];
+  const int S = c.r_slices;
+  const int n_items = c.n_cells * S;
+  const float alpha = UPDATE ? (float)cg->alpha : 0.f;
+  float4* r4 = reinterpret_cast<float4*>(r);
+  float4* x4 = reinterpret_cast<float4*>(x);
+  const float4* p4 = reinterpret_cast<const float4*>(p);
+  const float4* q4 = reinterpret_cast<const float4*>(q);
+  double rr_w = 0.0;
+  for (int item = blockIdx.x * kRestrictWarps + warp; item < n_items; item += gridDim.x * kRestrictWarps) {
+    const int cell = item / S, sl = item - cell * S;
+    const int3 ijk = c.cell_ijk[cell];
+    const int n0 = c.cell_node_ptr[cell], n1 = c.cell_node_ptr[cell + 1];
+    float acc[24];
 #pragma unroll
-  for (int k = 0; k < 24; ++k) acc[k] = 0.f;
-  for (int i = n0 + slice + kRestrictSlices * (int)threadIdx.x; i < n1; i += kRestrictSlices * kRestrictThreads) {
-    const int node = __ldg(c.cell_nodes + i);
-    const float4 X = __ldg(a.m.X32 + node);
-    const float4 rv = reinterpret_cast<const float4*>(r)[node];
-    float t[3];
-    cell_local(c, ijk, X.x, X.y, X.z, t);
+    for (int k = 0; k < 24; ++k) acc[k] = 0.f;
+    for (int i = n0 + 32 * sl + lane; i < n1; i += 32 * S) {
+      const int node = __ldg(c.cell_nodes + i);
+      const float4 X = __ldg(a.m.X32 + node);
+      float4 rv = r4[node];
+      if (UPDATE) {
+        float4 xv = x4[node];
+        const float4 pv = p4[node], qv = q4[node];
+        xv.x += alpha * pv.x; xv.y += alpha * pv.y; xv.z += alpha * pv.z;
+        rv.x -= alpha * qv.x; rv.y -= alpha * qv.y; rv.z -= alpha * qv.z;
+        x4[node] = xv;
+        r4[node] = rv;
+        rr_w += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
+      }
+      float t[3];
+      cell_local(c, ijk, X.x, X.y, X.z, t);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float wq = tri_weight(t[0], t[1], t[2], q);
-      acc[3 * q] += wq * rv.x;
-      acc[3 * q + 1] += wq * rv.y;
-      acc[3 * q + 2] += wq * rv.z;
+      for (int k = 0; k < 8; ++k) {
+        const float w = tri_weight(t[0], t[1], t[2], k);
+        acc[3 * k] += w * rv.x;
+        acc[3 * k + 1] += w * rv.y;
+        acc[3 * k + 2] += w * rv.z;
+      }
     }
-  }
+    float mine = 0.f;
 #pragma unroll
-  for (int k = 0; k < 24; ++k) {
-    float v = acc[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) sw[warp][k] = v;
+    for (int k = 0; k < 24; ++k) {
+      const float v = warp_allsum(acc[k]);
+      if (lane == k) mine = v;
+    }
+    if (lane < 24) c.cell_r[(size_t)item * 24 + lane] = mine;
   }
+  if (!UPDATE) return;
+  // ||r||^2: lanes, then warps in order, then CTAs in order (last CTA)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) rr_w += __shfl_xor_sync(0xffffffffu, rr_w, o);
+  if (lane == 0) s_rr[warp] = rr_w;
   __syncthreads();
-  if (threadIdx.x < 24) {
-    float v = 0.f;
-#pragma unroll
-    for (int w = 0; w < kRestrictThreads / 32; ++w) v += sw[w][threadIdx.x];
-    c.cell_r[(size_t)blockIdx.x * 24 + threadIdx.x] = v;
+  double v = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kRestrictWarps; ++w) v += s_rr[w];
+  if (publish_partial(red, site, 1, &v, &am_last)) {
+    const double trr = final_sum<kRestrictWarps * 32>(red, site, 0, s_red);
+    if (threadIdx.x == 0) {
+      cg->rr = trr;
+      cg->iter += 1;
+      if (!isfinite(trr)) {
+        cg->done = 3;
+        cg->status = 3;
+      } else if (trr <= cg->tol2) {
+        cg->done = 1;
+      } else if (cg->iter >= cg->max_iter) {
+        cg->done = 2;
+      }
+      red.counters[site] = 0u;
+    }
   }
 }
 
-// rc[I] = sum of the cells' shares of coarse DOF I, in the fixed order of
-// cn_cells (the eight entries are loaded together, then the shares)
+// r_c, one warp per coarse node: lane 4k + j adds the node's k-th cell share
+// (cn_cells order) over slices j, j + 4, ...; a fixed butterfly combines the
+// lanes (lanes 0..2 store the node's three DOFs).
 __global__ void __launch_bounds__(256) coarse_rc_kernel(const __grid_constant__ CoarseDev c, const CGState* cg) {
   if (cg && cg->done) return;
-  const int I = blockIdx.x * 256 + threadIdx.x;
-  if (I >= c.n_dof) return;
-  const int nI = I / 3, dI = I - 3 * nI;
-  const int4* ep = reinterpret_cast<const int4*>(c.cn_cells + nI * 8);
-  const int4 e0 = __ldg(ep), e1 = __ldg(ep + 1);
-  const int ent[8] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-  float sh[8][kRestrictSlices];
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-#pragma unroll
-    for (int q = 0; q < kRestrictSlices; ++q)
-      sh[k][q] = ent[k] >= 0
-                     ? __ldcg(c.cell_r + ((size_t)(ent[k] >> 3) * kRestrictSlices + q) * 24 + 3 * (ent[k] & 7) + dI)
-                     : 0.f;
-  float v = 0.f;
-#pragma unroll
-  for (int k = 0; k < 8; ++k)
-#pragma unroll
-    for (int q = 0; q < kRestrictSlices; ++q) v += sh[k][q];
-  c.rc[I] = v;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cn = blockIdx.x * 8 + warp;
+  if (cn >= c.n_cn) return;
+  const int S = c.r_slices;
+  const int ent = __ldg(c.cn_cells + cn * 8 + (lane >> 2));
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+  if (ent >= 0) {
+    const float* src = c.cell_r + (size_t)(ent >> 3) * S * 24 + 3 * (ent & 7);
+    for (int sl = lane & 3; sl < S; sl += 4) {
+      const float* q = src + (size_t)sl * 24;
+      v0 += __ldcg(q);
+      v1 += __ldcg(q + 1);
+      v2 += __ldcg(q + 2);
+    }
+  }
+  v0 = warp_allsum(v0);
+  v1 = warp_allsum(v1);
+  v2 = warp_allsum(v2);
+  if (lane < 3) c.rc[3 * cn + lane] = lane == 0 ? v0 : (lane == 1 ? v1 : v2);
 }
 
 // y_c = Ainv r_c with the FP32 inverse: r_c staged in shared memory, one warp
@@ -755,7 +806,13 @@ static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 size_t coarse_cell_smem() { return sizeof(float) * kCellThreads * (144 + 32); }
 int coarse_cell_slices() { return kCellSlices; }
-int coarse_restrict_slices() { return kRestrictSlices; }
+int coarse_restrict_slices(int n_cells) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int warps = std::max(sms, 1) * 32;
+  return std::max(1, std::min(kMaxRestrictSlices, (warps + std::max(n_cells, 1) - 1) / std::max(n_cells, 1)));
+}
 
 void prepare_coarse_kernels(int model, int n_dof) {
   (void)n_dof;
@@ -813,8 +870,20 @@ int tile_mv_grid() {
 }
 
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
-  coarse_restrict_kernel<<<a.c.n_cells * kRestrictSlices, kRestrictThreads, 0, s>>>(a, r, cg);
-  coarse_rc_kernel<<<nblk(a.c.n_dof, 256), 256, 0, s>>>(a.c, cg);
+  restrict_cells_kernel<false><<<nblk((int64_t)a.c.n_cells * a.c.r_slices, kRestrictWarps), kRestrictWarps * 32, 0,
+                                  s>>>(a, const_cast<float*>(r), nullptr, nullptr, nullptr, const_cast<CGState*>(cg),
+                                       Reduce{}, 0);
+  launch_coarse_solve(a, cg, s);
+}
+
+void launch_update_restrict(const CoarseArgs& a, float* x, float* r, const float* p, const float* q, CGState* cg,
+                            Reduce red, int site, cudaStream_t s) {
+  const int grid = std::min(nblk((int64_t)a.c.n_cells * a.c.r_slices, kRestrictWarps), red.max_blocks - 1);
+  restrict_cells_kernel<true><<<std::max(grid, 1), kRestrictWarps * 32, 0, s>>>(a, r, x, p, q, cg, red, site);
+}
+
+void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s) {
+  coarse_rc_kernel<<<nblk(a.c.n_cn, 8), 256, 0, s>>>(a.c, cg);
   if (a.c.Ainv16) {
     const int nt = a.c.nb16 * (a.c.nb16 + 1) / 2;
     coarse_tile_mv_kernel<<<std::min(nblk(nt, kTileWarps), tile_mv_grid()), kTileWarps * 32, 0, s>>>(a.c, cg);

@@ -123,9 +123,7 @@ struct FemCtx {
   bool in_batch = false;
   unsigned int* step_bar = nullptr;  // [4] grid barrier words
   double* jac_part = nullptr;        // [2 n_chunks] Jacobi step shares
-  float* cell_rf = nullptr;          // two-level step: [n_cells][tl_slices][24]
-  double* tl_part = nullptr;         // two-level step: [n_cells tl_slices + n_chunks]
-  int tl_slices = 1;
+  double* tl_part = nullptr;         // two-level step: [n_cells r_slices + n_chunks]
 
   // learned preconditioner: node graph, features, weights, activations
   MpnnDev mdev{};
@@ -621,7 +619,7 @@ CoarseArgs coarse_args(const FemCtx* c) {
 
 bool use_fused(const FemCtx* c, int kind) {
   return kind != GRAPH_LEARNED && c->fused_step && c->fused_ok && !c->in_batch &&
-         (kind == GRAPH_JACOBI || (c->cell_rf != nullptr && c->cdev.Ainv != nullptr));
+         (kind == GRAPH_JACOBI || (c->tl_part != nullptr && c->cdev.Ainv != nullptr));
 }
 
 StepArgs step_args(const FemCtx* c, int kind) {
@@ -636,8 +634,6 @@ StepArgs step_args(const FemCtx* c, int kind) {
   a.z = c->tmpf;
   a.cg = c->cg;
   a.part = kind == GRAPH_TWO_LEVEL ? c->tl_part : c->jac_part;
-  a.cell_rf = c->cell_rf;
-  a.slices = c->tl_slices;
   a.n_chunks = step_chunks(c->Nn);
   a.bar = c->step_bar;
   return a;
@@ -647,7 +643,7 @@ StepArgs step_args(const FemCtx* c, int kind) {
 int64_t kernels_per_iter(const FemCtx* c, int kind, bool fused) {
   const int64_t mv = c->mv_variant == MV_TWO_PHASE ? 2 : 1;
   if (fused) return mv + 1;
-  return mv + (kind == GRAPH_TWO_LEVEL ? 5 + coarse_product_kernels(c->cdev) : 2);
+  return mv + (kind == GRAPH_TWO_LEVEL ? 4 + coarse_product_kernels(c->cdev) : 2);
 }
 
 // Enqueues one CG iteration; returns the first launch error (a refused
@@ -679,8 +675,8 @@ cudaError_t enqueue_cg_iter(FemCtx* c, int kind, bool fused) {
   }
   if (kind == GRAPH_TWO_LEVEL) {
     const CoarseArgs ca = coarse_args(c);
-    launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream, 0);
-    launch_coarse_apply(ca, c->r, c->cg, c->stream);
+    launch_update_restrict(ca, c->x, c->r, c->p, c->y, c->cg, c->red(), SITE_CGU, c->stream);
+    launch_coarse_solve(ca, c->cg, c->stream);
     launch_tl_rz(ca, false, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
     launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
     return cudaSuccess;
@@ -802,7 +798,6 @@ int drop_coarse(FemCtx* c) {
     if (p) cudaFree(p);
   c->coarse_bufs.clear();
   c->cdev = CoarseDev{};
-  c->cell_rf = nullptr;
   c->tl_part = nullptr;
   c->coarse_built = false;
   c->coarse_valid = false;
@@ -1052,14 +1047,12 @@ int build_coarse(FemCtx* c) {
   } else {
     if ((st = coarse_alloc(c, &cd.Ainv, nd * nd))) return st;
   }
-  if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * coarse_restrict_slices() * 24))) return st;
+  cd.r_slices = coarse_restrict_slices(n_cells);
+  if ((st = coarse_alloc(c, &cd.cell_r, (size_t)n_cells * cd.r_slices * 24))) return st;
   if ((st = coarse_alloc(c, &cd.yc, nb * 64))) return st;
   if ((st = coarse_alloc(c, &cd.rc, nb * 64))) return st;
   // fused two-level step: per (cell, slice) restriction and ||r||^2 shares
-  c->tl_slices = step_slices(n_cells, cd.n_dof);
-  const size_t items = (size_t)n_cells * c->tl_slices;
-  if ((st = coarse_alloc(c, &c->cell_rf, items * 24))) return st;
-  if ((st = coarse_alloc(c, &c->tl_part, items + step_chunks(Nn)))) return st;
+  if ((st = coarse_alloc(c, &c->tl_part, (size_t)n_cells * cd.r_slices + step_chunks(Nn)))) return st;
   if (!c->solver) {
     if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS)
       return set_err(c, FEM_ERR_CUDA, "cusolverDnCreate failed");
@@ -1804,7 +1797,7 @@ int fem_step_info(void* ctx, int64_t* out4) {
   out4[0] = (c->fused_step && c->fused_ok) ? 1 : 0;
   out4[1] = (c->cg_graph[GRAPH_JACOBI] && (c->cg_graph_flags[GRAPH_JACOBI] & 2)) ? 1 : 0;
   out4[2] = (c->cg_graph[GRAPH_TWO_LEVEL] && (c->cg_graph_flags[GRAPH_TWO_LEVEL] & 2)) ? 1 : 0;
-  out4[3] = c->tl_slices;
+  out4[3] = c->cdev.r_slices;
   return FEM_OK;
 }
 

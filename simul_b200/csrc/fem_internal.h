@@ -122,7 +122,8 @@ struct CoarseDev {
   __nv_bfloat16* Ainv16;
   int nb16;                 // tiles per side: ceil(n_dof / 64)
   float* yslots;            // BF16 path: [nb16][nb16][64] slot (R, K) = Ainv_RK r_c,K
-  float* cell_r;            // [n_cells][slices][24] restricted residual shares per cell
+  float* cell_r;            // [n_cells][r_slices][24] restricted residual shares per cell
+  int r_slices;             // warps (node slices) per cell in the restriction
   float* rc;                // [64 nb16] coarse residual P^T r (zero beyond n_dof)
   float* yc;                // [64 nb16] coarse correction
 };
@@ -154,8 +155,6 @@ struct StepArgs {
   CGState* cg;
   double* part;             // two-level: [n_cells * slices] ||r||^2 shares, then [n_chunks] r.z shares;
                             // Jacobi: [2][n_chunks]
-  float* cell_rf;           // two-level: [n_cells][slices][24] restricted residual shares
-  int slices;               // two-level: warps per cell in the update + restriction phase
   int n_chunks;             // ceil(n_nodes / kStepThreads)
   unsigned int* bar;        // [2] grid barrier: arrivals, generation
 };
@@ -163,8 +162,6 @@ struct StepArgs {
 // CTAs of a cooperative step launch on this device (0: not available);
 // kind 0 Jacobi, 1 two-level with an n_dof coarse space.
 int step_grid(int kind, int n_dof);
-// warps per lattice cell in the two-level step's restriction phase
-int step_slices(int n_cells, int n_dof);
 // raises the step kernels' shared-memory limit (before a capture)
 void prepare_step_kernels(int kind, int n_dof);
 cudaError_t launch_tl_step(const StepArgs& a, cudaStream_t s);
@@ -236,7 +233,13 @@ void launch_diag(const DiagArgs& a, int model, cudaStream_t s);
 // coarse lattice (fem_coarse.cu)
 size_t coarse_cell_smem();
 int coarse_cell_slices();   // CTAs (and Galerkin block slots) per lattice cell
-int coarse_restrict_slices();  // CTAs (and restricted-residual slots) per lattice cell
+int coarse_restrict_slices(int n_cells);  // node slices (restriction warps) per lattice cell
+// x += alpha p, r -= alpha q, ||r||^2 + convergence test, and the restriction
+// of the new r into cell_r (one kernel)
+void launch_update_restrict(const CoarseArgs& a, float* x, float* r, const float* p, const float* q, CGState* cg,
+                            Reduce red, int site, cudaStream_t s);
+// r_c from cell_r, then y_c = Ainv r_c
+void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s);
 void prepare_coarse_kernels(int model, int n_dof);
 // cell Galerkin blocks + dense Ac (FP64, column-major)
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);

@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kStepThreads) tl_step_kernel(const __grid_cons
   float4* z4 = reinterpret_cast<float4*>(a.z);
   const float4* q4 = reinterpret_cast<const float4*>(a.q);
   const float4* d4 = reinterpret_cast<const float4*>(a.dinv);
-  const int S = a.slices;
+  const int S = c.r_slices;
   const int n_items = c.n_cells * S;
 
   // A: x += alpha p, r -= alpha q over each cell's nodes; per (cell, slice)
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kStepThreads) tl_step_kernel(const __grid_cons
       if (lane == k) mine = v;
     }
     rr = warp_sum_d(rr);
-    if (lane < 24) __stcg(a.cell_rf + (size_t)item * 24 + lane, mine);
+    if (lane < 24) __stcg(c.cell_r + (size_t)item * 24 + lane, mine);
     if (lane == 0) __stcg(a.part + item, rr);
   }
   if (!grid_sync(a.bar, cg)) return;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kStepThreads) tl_step_kernel(const __grid_cons
     const int ent = __ldg(c.cn_cells + cn * 8 + (lane >> 2));
     float v0 = 0.f, v1 = 0.f, v2 = 0.f;
     if (ent >= 0) {
-      const float* src = a.cell_rf + (size_t)(ent >> 3) * S * 24 + 3 * (ent & 7);
+      const float* src = c.cell_r + (size_t)(ent >> 3) * S * 24 + 3 * (ent & 7);
       for (int sl = lane & 3; sl < S; sl += 4) {
         const float* q = src + (size_t)sl * 24;
         v0 += __ldcg(q);
@@ -412,12 +412,6 @@ void prepare_step_kernels(int kind, int n_dof) {
   (void)n_dof;
 }
 
-int step_slices(int n_cells, int n_dof) {
-  const int g = step_grid(1, n_dof);
-  if (g <= 0 || n_cells <= 0) return 1;
-  const int warps = g * kStepWarps;
-  return std::max(1, std::min(kMaxSlices, (warps + n_cells - 1) / n_cells));
-}
 
 cudaError_t launch_tl_step(const StepArgs& a, cudaStream_t s) {
   const int g = step_grid(1, a.c.n_dof);

@@ -173,7 +173,12 @@ enum {
    * node); 0: as launches of fixed 12- or 32-iteration graphs with a host
    * check between them (kernel profilers cannot attribute kernels inside
    * conditional graphs) */
-  FEM_OPT_WHOLE_SOLVE_GRAPH = 7
+  FEM_OPT_WHOLE_SOLVE_GRAPH = 7,
+  /* 1 (default): inside the captured CG graphs each kernel of the iteration
+   * chain is launched as a programmatic dependent of the previous one (it is
+   * scheduled while the previous one drains and waits for its results on the
+   * device), where the runtime accepts it; 0: plain stream order */
+  FEM_OPT_PDL = 8
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing
@@ -237,10 +242,12 @@ int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t
  * assembly + factorisation (CUDA events), [6] ms of its assembly part,
  * [7] PCG solves one assembly serves */
 int fem_coarse_info(void* ctx, double* out8);
-/* fused CG step: out[0] 1 while the option is on and the runtime accepted
- * it, [1] the captured Jacobi CG graph uses it, [2] the two-level one does,
- * [3] warps per lattice cell in its restriction phase */
-int fem_step_info(void* ctx, int64_t* out4);
+/* CG iteration launch structure: out[0] 1 while the fused-step option is on
+ * and the runtime accepted it, [1] the captured Jacobi CG graph uses the
+ * fused step, [2] the two-level one does, [3] warps per lattice cell in the
+ * restriction, [4] the Jacobi CG graph uses programmatic dependent launches,
+ * [5] the two-level one does */
+int fem_step_info(void* ctx, int64_t* out6);
 /* cudaStream_t of the context (as void*) */
 void* fem_ctx_stream(void* ctx);
 

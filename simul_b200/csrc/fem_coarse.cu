@@ -261,6 +261,7 @@ template <bool UPDATE>
 __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
     const __grid_constant__ CoarseArgs a, float* r, float* x, const float* __restrict__ p,
     const float* __restrict__ q, CGState* cg, Reduce red, int site) {
+  chain_enter();
   if (cg && cg->done) return;
   __shared__ double s_rr[kRestrictWarps];
   __shared__ double s_red[kRestrictWarps];
@@ -344,6 +345,7 @@ __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
 // (cn_cells order) over slices j, j + 4, ...; a fixed butterfly combines the
 // lanes (lanes 0..2 store the node's three DOFs).
 __global__ void __launch_bounds__(256) coarse_rc_kernel(const __grid_constant__ CoarseDev c, const CGState* cg) {
+  chain_enter();
   if (cg && cg->done) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int cn = blockIdx.x * 8 + warp;
@@ -372,6 +374,7 @@ constexpr int kCoarseMvThreads = 256;
 
 __global__ void __launch_bounds__(kCoarseMvThreads) coarse_mv_kernel(
     const __grid_constant__ CoarseDev c, const CGState* cg) {
+  chain_enter();
   if (cg && cg->done) return;
   extern __shared__ __align__(16) float s_rc[];
   const int n = c.n_dof;
@@ -426,6 +429,7 @@ __device__ __forceinline__ void bf16x8_to_f32(const uint4 w, float a[8]) {
 
 __global__ void __launch_bounds__(kTileWarps * 32, 3) coarse_tile_mv_kernel(
     const __grid_constant__ CoarseDev c, const CGState* cg) {
+  chain_enter();
   if (cg && cg->done) return;
   __shared__ float s_x[kTileWarps][2][kTile];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -496,6 +500,7 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) coarse_tile_mv_kernel(
 
 __global__ void __launch_bounds__(kTileWarps * 32) coarse_slot_sum_kernel(
     const __grid_constant__ CoarseDev c, const CGState* cg) {
+  chain_enter();
   if (cg && cg->done) return;
   __shared__ float part[kTileWarps][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -503,6 +508,7 @@ __global__ void __launch_bounds__(kTileWarps * 32) coarse_slot_sum_kernel(
   const int nb = c.nb16;
   const float* src = c.yslots + (size_t)R * nb * kTile + 32 * half + lane;
   float v = 0.f;
+#pragma unroll 4
   for (int K = warp; K < nb; K += kTileWarps) v += __ldcg(src + (size_t)K * kTile);
   part[warp][lane] = v;
   __syncthreads();
@@ -523,6 +529,7 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
                                                     const float* __restrict__ r,
                                                     const float* __restrict__ dinv, float* z,
                                                     float* p, CGState* cg, Reduce red, int site) {
+  chain_enter();
   if (cg->done) return;
   __shared__ double sred[8];
   __shared__ bool am_last;
@@ -532,11 +539,8 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
   if (i < a.m.n_nodes) {
     const float4 rv = reinterpret_cast<const float4*>(r)[i];
     const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
-    const float4 X = __ldg(a.m.X32 + i);
-    const int cell = __ldg(c.node_cell + i);
-    const int3 ijk = c.cell_ijk[cell];
     float t[3];
-    cell_local(c, ijk, X.x, X.y, X.z, t);
+    const int cell = node_lattice(c, i, t);
     float cz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
@@ -577,6 +581,7 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
 // p = z + beta p
 __global__ void __launch_bounds__(256) tl_pupdate_kernel(float* p, const float* __restrict__ z,
                                                          int n_nodes, const CGState* cg) {
+  chain_enter();
   if (cg->done) return;
   const float beta = (float)cg->beta;
   const int i = blockIdx.x * 256 + threadIdx.x;
@@ -623,11 +628,8 @@ __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ 
     float4 av = make_float4(dv.x * rv.x, dv.y * rv.y, dv.z * rv.z, 0.f);
     if (COARSE) {
       const CoarseDev& c = a.c;
-      const float4 X = __ldg(a.m.X32 + i);
-      const int cell = __ldg(c.node_cell + i);
-      const int3 ijk = c.cell_ijk[cell];
       float t[3];
-      cell_local(c, ijk, X.x, X.y, X.z, t);
+      const int cell = node_lattice(c, i, t);
       float cz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -717,11 +719,8 @@ __global__ void __launch_bounds__(256) coarse_add_kernel(const __grid_constant__
   const int i = blockIdx.x * 256 + threadIdx.x;
   if (i >= a.m.n_nodes) return;
   const CoarseDev& c = a.c;
-  const float4 X = __ldg(a.m.X32 + i);
-  const int cell = __ldg(c.node_cell + i);
-  const int3 ijk = c.cell_ijk[cell];
   float t[3];
-  cell_local(c, ijk, X.x, X.y, X.z, t);
+  const int cell = node_lattice(c, i, t);
   float cz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -854,6 +853,21 @@ void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s) {
   coarse_sym_kernel<<<nblk(nn, 256), 256, 0, s>>>(c);
 }
 
+__global__ void coarse_node_lat_kernel(const __grid_constant__ MeshDev m, const __grid_constant__ CoarseDev c,
+                                       float4* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.n_nodes) return;
+  const float4 X = __ldg(m.X32 + i);
+  const int cell = c.node_cell[i];
+  float t[3];
+  cell_local(c, c.cell_ijk[cell], X.x, X.y, X.z, t);
+  out[i] = make_float4(t[0], t[1], t[2], __int_as_float(cell));
+}
+
+void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, cudaStream_t s) {
+  coarse_node_lat_kernel<<<nblk(m.n_nodes, 256), 256, 0, s>>>(m, c, out);
+}
+
 int coarse_product_kernels(const CoarseDev& c) { return c.Ainv16 ? 2 : 1; }
 
 // Resident CTAs of the tile product on this device (one wave, tiles looped).
@@ -879,20 +893,22 @@ void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg,
 void launch_update_restrict(const CoarseArgs& a, float* x, float* r, const float* p, const float* q, CGState* cg,
                             Reduce red, int site, cudaStream_t s) {
   const int grid = std::min(nblk((int64_t)a.c.n_cells * a.c.r_slices, kRestrictWarps), red.max_blocks - 1);
-  restrict_cells_kernel<true><<<std::max(grid, 1), kRestrictWarps * 32, 0, s>>>(a, r, x, p, q, cg, red, site);
+  launch_chain(restrict_cells_kernel<true>, std::max(grid, 1), kRestrictWarps * 32, 0, s, a, r, x, p, q, cg, red,
+               site);
 }
 
 void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s) {
-  coarse_rc_kernel<<<nblk(a.c.n_cn, 8), 256, 0, s>>>(a.c, cg);
+  launch_chain(coarse_rc_kernel, nblk(a.c.n_cn, 8), 256, 0, s, a.c, cg);
   if (a.c.Ainv16) {
     const int nt = a.c.nb16 * (a.c.nb16 + 1) / 2;
-    coarse_tile_mv_kernel<<<std::min(nblk(nt, kTileWarps), tile_mv_grid()), kTileWarps * 32, 0, s>>>(a.c, cg);
-    coarse_slot_sum_kernel<<<2 * a.c.nb16, kTileWarps * 32, 0, s>>>(a.c, cg);
+    launch_chain(coarse_tile_mv_kernel, std::min(nblk(nt, kTileWarps), tile_mv_grid()), kTileWarps * 32, 0, s, a.c,
+                 cg);
+    launch_chain(coarse_slot_sum_kernel, 2 * a.c.nb16, kTileWarps * 32, 0, s, a.c, cg);
     return;
   }
   const int rows_per_cta = kCoarseMvThreads / 32;
-  coarse_mv_kernel<<<nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof, s>>>(
-      a.c, cg);
+  launch_chain(coarse_mv_kernel, nblk(a.c.n_dof, rows_per_cta), kCoarseMvThreads, sizeof(float) * (size_t)a.c.n_dof,
+               s, a.c, cg);
 }
 
 void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* dinv, float* z, float* p,
@@ -901,7 +917,7 @@ void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* d
   if (init)
     tl_rz_kernel<true><<<g, 256, 0, s>>>(a, r, dinv, z, p, cg, red, site);
   else
-    tl_rz_kernel<false><<<g, 256, 0, s>>>(a, r, dinv, z, p, cg, red, site);
+    launch_chain(tl_rz_kernel<false>, g, 256, 0, s, a, r, dinv, z, p, cg, red, site);
 }
 
 void launch_fpcg_dots(const CoarseArgs& a, bool init, bool coarse, const float* r, const float* q,
@@ -927,7 +943,7 @@ void launch_fpcg_pupdate(float* p, const float* z, const float* zalt, int n_node
 }
 
 void launch_tl_pupdate(float* p, const float* z, int n_nodes, const CGState* cg, cudaStream_t s) {
-  tl_pupdate_kernel<<<nblk(n_nodes, 256), 256, 0, s>>>(p, z, n_nodes, cg);
+  launch_chain(tl_pupdate_kernel, nblk(n_nodes, 256), 256, 0, s, p, z, n_nodes, cg);
 }
 
 void launch_coarse_add(const CoarseArgs& a, float* z, cudaStream_t s) {

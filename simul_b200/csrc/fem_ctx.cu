@@ -120,6 +120,10 @@ struct FemCtx {
   // concurrent contexts could wait on each other's SMs)
   bool fused_step = false;
   bool fused_ok = true;
+  // programmatic dependent launch between the CG chain's kernels inside the
+  // captured graphs (a refused capture turns it off)
+  bool pdl = true;
+  bool pdl_ok = true;
   bool in_batch = false;
   unsigned int* step_bar = nullptr;  // [4] grid barrier words
   double* jac_part = nullptr;        // [2 n_chunks] Jacobi step shares
@@ -617,6 +621,15 @@ CoarseArgs coarse_args(const FemCtx* c) {
   return a;
 }
 
+bool use_pdl(const FemCtx* c, int kind) { return kind != GRAPH_LEARNED && c->pdl && c->pdl_ok; }
+
+// Sets chain_pdl() for the launches of one capture, restores it after.
+struct ChainPdl {
+  bool saved;
+  explicit ChainPdl(bool on) : saved(chain_pdl()) { chain_pdl() = on; }
+  ~ChainPdl() { chain_pdl() = saved; }
+};
+
 bool use_fused(const FemCtx* c, int kind) {
   return kind != GRAPH_LEARNED && c->fused_step && c->fused_ok && !c->in_batch &&
          (kind == GRAPH_JACOBI || (c->tl_part != nullptr && c->cdev.Ainv != nullptr));
@@ -754,7 +767,7 @@ int choose_matvec_variant(FemCtx* c) {
 // behind) if the runtime cannot build it; the batched graphs are used then.
 constexpr int kLoopIters = 4;
 
-bool build_loop_graph(FemCtx* c, int kind, bool fused) {
+bool build_loop_graph(FemCtx* c, int kind, bool fused, bool pdl) {
   cudaGraph_t g = nullptr;
   if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
   bool ok = false;
@@ -772,11 +785,14 @@ bool build_loop_graph(FemCtx* c, int kind, bool fused) {
         cudaSuccess)
       break;
     cudaError_t le = cudaSuccess;
-    for (int i = 0; i < kLoopIters; ++i) {
-      const cudaError_t e = enqueue_cg_iter(c, kind, fused);
-      if (le == cudaSuccess) le = e;
+    {
+      ChainPdl pdl_scope(pdl);
+      for (int i = 0; i < kLoopIters; ++i) {
+        const cudaError_t e = enqueue_cg_iter(c, kind, fused);
+        if (le == cudaSuccess) le = e;
+      }
+      launch_cg_loop_cond(h, c->cg, kLoopIters, c->stream);
     }
-    launch_cg_loop_cond(h, c->cg, kLoopIters, c->stream);
     cudaGraph_t captured = nullptr;
     if (cudaStreamEndCapture(c->stream, &captured) != cudaSuccess || le != cudaSuccess) break;
     if (cudaGraphInstantiate(&c->loop_graph[kind], g, 0) != cudaSuccess) {
@@ -814,7 +830,8 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   int st;
   if ((st = choose_matvec_variant(c))) return st;
   const bool fused = use_fused(c, kind);
-  const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0);
+  const bool pdl = use_pdl(c, kind);
+  const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0) | (pdl ? 4 : 0);
   if (c->cg_graph[kind] && c->cg_graph_model[kind] == c->model_kind &&
       c->cg_graph_variant[kind] == c->mv_variant && c->cg_graph_flags[kind] == flags)
     return FEM_OK;
@@ -834,29 +851,41 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t le = cudaSuccess;
-  for (int i = 0; i < cg_batch(kind); ++i) {
-    const cudaError_t e1 = enqueue_cg_iter(c, kind, fused);
-    if (le == cudaSuccess) le = e1;
+  {
+    ChainPdl pdl_scope(pdl);
+    for (int i = 0; i < cg_batch(kind); ++i) {
+      const cudaError_t e1 = enqueue_cg_iter(c, kind, fused);
+      if (le == cudaSuccess) le = e1;
+    }
+    if (le == cudaSuccess) le = cudaGetLastError();
   }
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-  if (fused && (e != cudaSuccess || le != cudaSuccess)) {
-    // the runtime refused the cooperative step: capture the kernel chain
+  if ((pdl || fused) && (e != cudaSuccess || le != cudaSuccess)) {
+    // the runtime refused programmatic launches or the cooperative step:
+    // capture again without them (programmatic launches first)
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
-    c->fused_ok = false;
+    if (pdl)
+      c->pdl_ok = false;
+    else
+      c->fused_ok = false;
     return ensure_cg_graph(c, kind);
   }
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
   e = cudaGraphInstantiate(&c->cg_graph[kind], g, 0);
   cudaGraphDestroy(g);
-  if (e != cudaSuccess && fused) {
+  if (e != cudaSuccess && (pdl || fused)) {
     c->cg_graph[kind] = nullptr;
     cudaGetLastError();
-    c->fused_ok = false;
+    if (pdl)
+      c->pdl_ok = false;
+    else
+      c->fused_ok = false;
     return ensure_cg_graph(c, kind);
   }
   if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-  if (c->use_loop_graph && !build_loop_graph(c, kind, fused)) c->use_loop_graph = false;
+  if (c->use_loop_graph && !build_loop_graph(c, kind, fused, pdl) && !(pdl && build_loop_graph(c, kind, fused, false)))
+    c->use_loop_graph = false;
   c->cg_graph_model[kind] = c->model_kind;
   c->cg_graph_variant[kind] = c->mv_variant;
   c->cg_graph_flags[kind] = flags;
@@ -1033,6 +1062,13 @@ int build_coarse(FemCtx* c) {
   if ((st = coarse_upload(c, &cd.cell_elems, cell_elems))) return st;
   if ((st = coarse_upload(c, &cd.node_cell, node_cell))) return st;
   if ((st = coarse_upload(c, &cd.cn_cells, cn_cells))) return st;
+  {
+    float4* lat = nullptr;
+    if ((st = coarse_alloc(c, &lat, (size_t)Nn))) return st;
+    cd.node_lat = lat;
+    launch_coarse_node_lat(c->mesh(), cd, lat, c->stream);
+    CKL();
+  }
   const size_t nd = (size_t)cd.n_dof;
   if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * coarse_cell_slices() * 576))) return st;
   if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
@@ -1593,6 +1629,10 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
         c->use_loop_graph = value != 0;
       }
       return FEM_OK;
+    case FEM_OPT_PDL:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "programmatic launch flag must be 0 or 1");
+      c->pdl = value != 0;
+      return FEM_OK;
     case FEM_OPT_FUSED_STEP:
       if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "fused step flag must be 0 or 1");
       c->fused_step = value != 0;
@@ -1791,9 +1831,12 @@ int fem_coarse_info(void* ctx, double* out8) {
   return FEM_OK;
 }
 
-int fem_step_info(void* ctx, int64_t* out4) {
+int fem_step_info(void* ctx, int64_t* out6) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
-  if (!c || !out4) return FEM_ERR_INVALID;
+  if (!c || !out6) return FEM_ERR_INVALID;
+  int64_t* out4 = out6;
+  out6[4] = (c->cg_graph[GRAPH_JACOBI] && (c->cg_graph_flags[GRAPH_JACOBI] & 4)) ? 1 : 0;
+  out6[5] = (c->cg_graph[GRAPH_TWO_LEVEL] && (c->cg_graph_flags[GRAPH_TWO_LEVEL] & 4)) ? 1 : 0;
   out4[0] = (c->fused_step && c->fused_ok) ? 1 : 0;
   out4[1] = (c->cg_graph[GRAPH_JACOBI] && (c->cg_graph_flags[GRAPH_JACOBI] & 2)) ? 1 : 0;
   out4[2] = (c->cg_graph[GRAPH_TWO_LEVEL] && (c->cg_graph_flags[GRAPH_TWO_LEVEL] & 2)) ? 1 : 0;

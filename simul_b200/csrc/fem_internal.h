@@ -9,6 +9,46 @@
 
 namespace femb200 {
 
+// Programmatic dependent launch for the kernels of the PCG iteration chain:
+// a kernel launched with it may be scheduled as its predecessor's CTAs
+// retire, and waits (griddepcontrol.wait) for the predecessor's results
+// before it touches memory.  For a kernel launched without it the wait does
+// nothing.
+__device__ __forceinline__ void chain_enter() {
+#if defined(__CUDA_ARCH__)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+// Whether launches from this host thread use programmatic dependent launch
+// (set around graph capture of the CG iteration chain).
+inline bool& chain_pdl() {
+  static thread_local bool on = false;
+  return on;
+}
+
+// Launches a chain kernel (one that starts with chain_enter()), with
+// programmatic dependent launch when chain_pdl() is set.
+template <typename... KArgs, typename... Args>
+inline void launch_chain(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                         Args... args) {
+  if (!chain_pdl()) {
+    k<<<grid, block, smem, s>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, static_cast<KArgs>(args)...);
+}
+
 // Node-block gather tables (device).  Internal node n belongs to block
 // n / nb.  Block b lists every element touching one of its nodes: its "home"
 // elements (contiguous internal ids, listed first) then the foreign ones.
@@ -112,6 +152,7 @@ struct CoarseDev {
   const int* cell_elem_ptr; // [n_cells + 1] into cell_elems (cell of the centroid)
   const int* cell_elems;
   const int* node_cell;     // [Nn]
+  const float4* node_lat;   // [Nn] local coordinates in the node's cell (xyz), the cell (w, int bits)
   const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
   double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
@@ -244,6 +285,8 @@ void prepare_coarse_kernels(int model, int n_dof);
 // cell Galerkin blocks + dense Ac (FP64, column-major)
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
 // Ainv = FP32 symmetric copy of the lower triangle left in Ac
+// fills node_lat from X32, node_cell and cell_ijk
+void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, cudaStream_t s);
 // kernels one coarse product launches (1 FP32, 2 packed BF16)
 int coarse_product_kernels(const CoarseDev& c);
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);

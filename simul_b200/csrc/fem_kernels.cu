@@ -170,6 +170,7 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
 
 template <int NB, int MODEL, bool CG>
 __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
   if (CG) {
     if (a.cg->done) return;
   }
@@ -330,6 +331,7 @@ __device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
 // 50 % to 62.5 % for this latency-bound gather-compute-scatter kernel.
 template <int MODEL, bool CG>
 __global__ void __launch_bounds__(256, 5) elem_mv_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
   if (CG) {
     if (a.cg->done) return;
   }
@@ -345,6 +347,7 @@ __global__ void __launch_bounds__(256, 5) elem_mv_kernel(const __grid_constant__
 // slot-list order.
 template <bool CG>
 __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
   if (CG) {
     if (a.cg->done) return;
   }
@@ -537,6 +540,7 @@ __global__ void __launch_bounds__(kVecThreads) cg_update_kernel(float* x, float*
                                                                 const float* __restrict__ dinv,
                                                                 int n_nodes, CGState* cg, Reduce red,
                                                                 int site, int jac) {
+  chain_enter();
   if (cg->done) return;
   __shared__ double sred[kVecThreads / 32];
   __shared__ bool am_last;
@@ -586,6 +590,7 @@ __global__ void __launch_bounds__(kVecThreads) cg_pupdate_kernel(float* p,
                                                                  const float* __restrict__ r,
                                                                  const float* __restrict__ dinv,
                                                                  int n_nodes, const CGState* cg) {
+  chain_enter();
   if (cg->done) return;
   const float beta = (float)cg->beta;
   const int i = blockIdx.x * kVecThreads + threadIdx.x;
@@ -856,7 +861,7 @@ template <int NB, int MODEL, bool CG>
 static void matvec_go(const MvArgs& a, cudaStream_t s) {
   const size_t smem = slots_smem(a.m);
   allow_smem(matvec_kernel<NB, MODEL, CG>, smem, s);
-  matvec_kernel<NB, MODEL, CG><<<a.m.n_blocks, NB, smem, s>>>(a);
+  launch_chain(matvec_kernel<NB, MODEL, CG>, a.m.n_blocks, NB, smem, s, a);
 }
 
 template <int NB, bool CG>
@@ -876,15 +881,15 @@ template <bool CG>
 static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
   const int ge = nblk(a.m.n_elems, 256);
   switch (model) {
-    case M_LE: elem_mv_kernel<M_LE, CG><<<ge, 256, 0, s>>>(a); break;
-    case M_NH: elem_mv_kernel<M_NH, CG><<<ge, 256, 0, s>>>(a); break;
-    case M_MR: elem_mv_kernel<M_MR, CG><<<ge, 256, 0, s>>>(a); break;
-    case M_J2: elem_mv_kernel<M_J2, CG><<<ge, 256, 0, s>>>(a); break;
-    case M_TI: elem_mv_kernel<M_TI, CG><<<ge, 256, 0, s>>>(a); break;
-    case M_FMR: elem_mv_kernel<M_FMR, CG><<<ge, 256, 0, s>>>(a); break;
-    default: elem_mv_kernel<-1, CG><<<ge, 256, 0, s>>>(a); break;
+    case M_LE: launch_chain(elem_mv_kernel<M_LE, CG>, ge, 256, 0, s, a); break;
+    case M_NH: launch_chain(elem_mv_kernel<M_NH, CG>, ge, 256, 0, s, a); break;
+    case M_MR: launch_chain(elem_mv_kernel<M_MR, CG>, ge, 256, 0, s, a); break;
+    case M_J2: launch_chain(elem_mv_kernel<M_J2, CG>, ge, 256, 0, s, a); break;
+    case M_TI: launch_chain(elem_mv_kernel<M_TI, CG>, ge, 256, 0, s, a); break;
+    case M_FMR: launch_chain(elem_mv_kernel<M_FMR, CG>, ge, 256, 0, s, a); break;
+    default: launch_chain(elem_mv_kernel<-1, CG>, ge, 256, 0, s, a); break;
   }
-  node_gather_kernel<CG><<<nblk(a.m.n_nodes, 256), 256, 0, s>>>(a);
+  launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, 256), 256, 0, s, a);
 }
 
 void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
@@ -962,13 +967,14 @@ void launch_cg_init(const double* b, float* r, float* x, float* p, const float* 
 void launch_cg_update(float* x, float* r, const float* p, const float* y, const float* dinv,
                       int n_nodes, CGState* cg, Reduce red, int site, cudaStream_t s,
                       int precond_in_update) {
-  cg_update_kernel<<<nblk(n_nodes, kVecThreads), kVecThreads, 0, s>>>(x, r, p, y, dinv, n_nodes, cg,
-                                                                    red, site, precond_in_update);
+  launch_chain(cg_update_kernel, nblk(n_nodes, kVecThreads), kVecThreads, 0, s, x, r, p, y, dinv, n_nodes, cg,
+               red, site, precond_in_update);
 }
 
 void launch_cg_pupdate(float* p, const float* r, const float* dinv, int n_nodes, CGState* cg,
                        cudaStream_t s) {
-  cg_pupdate_kernel<<<nblk(n_nodes, kVecThreads), kVecThreads, 0, s>>>(p, r, dinv, n_nodes, cg);
+  launch_chain(cg_pupdate_kernel, nblk(n_nodes, kVecThreads), kVecThreads, 0, s, p, r, dinv, n_nodes,
+               static_cast<const CGState*>(cg));
 }
 
 void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
@@ -1018,6 +1024,7 @@ void launch_scale_d(const double* in, double s, double* out, int n, cudaStream_t
 }
 
 __global__ void cg_loop_cond_kernel(cudaGraphConditionalHandle h, CGState* cg, int iters_per_trip) {
+  chain_enter();
   if (threadIdx.x != 0) return;
   const int trips = ++cg->trips;
   const int cap = cg->max_iter / iters_per_trip + 2;
@@ -1030,7 +1037,7 @@ __global__ void cg_loop_cond_kernel(cudaGraphConditionalHandle h, CGState* cg, i
 }
 
 void launch_cg_loop_cond(cudaGraphConditionalHandle h, CGState* cg, int iters_per_trip, cudaStream_t s) {
-  cg_loop_cond_kernel<<<1, 32, 0, s>>>(h, cg, iters_per_trip);
+  launch_chain(cg_loop_cond_kernel, 1, 32, 0, s, h, cg, iters_per_trip);
 }
 
 void launch_x32_mask(float4* X32, const uint8_t* fixed, int n, cudaStream_t s) {

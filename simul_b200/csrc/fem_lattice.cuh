@@ -33,4 +33,14 @@ __device__ __forceinline__ void cell_local(const CoarseDev& c, int3 ijk, float x
   t[2] = lattice_coord(z, c.lo.z, c.inv_H, ijk.z);
 }
 
+// The lattice cell of mesh node i and its local coordinates there, from the
+// per-node table built with the lattice (the same values cell_local gives).
+__device__ __forceinline__ int node_lattice(const CoarseDev& c, int i, float t[3]) {
+  const float4 v = __ldg(c.node_lat + i);
+  t[0] = v.x;
+  t[1] = v.y;
+  t[2] = v.z;
+  return __float_as_int(v.w);
+}
+
 }  // namespace femb200

@@ -248,11 +248,8 @@ __global__ void __launch_bounds__(kStepThreads) tl_step_kernel(const __grid_cons
     if (i < Nn) {
       const float4 rv = __ldcg(r4 + i);
       const float4 dv = __ldg(d4 + i);
-      const float4 X = __ldg(a.m.X32 + i);
-      const int cell = __ldg(c.node_cell + i);
-      const int3 ijk = c.cell_ijk[cell];
       float t[3];
-      cell_local(c, ijk, X.x, X.y, X.z, t);
+      const int cell = node_lattice(c, i, t);
       float cz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
       for (int k = 0; k < 8; ++k) {

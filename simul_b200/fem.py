@@ -189,11 +189,17 @@ class FEMesh:
         _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_WHOLE_SOLVE_GRAPH, 1 if on else 0), self.ctx,
                "fem_set_option")
 
+    def set_programmatic_launch(self, on: bool):
+        """Programmatic dependent launches between the CG iteration's kernels
+        inside the captured graphs (True, the default) or plain stream order."""
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_PDL, 1 if on else 0), self.ctx, "fem_set_option")
+
     def step_info(self) -> dict:
-        out = (C.c_int64 * 4)()
+        out = (C.c_int64 * 6)()
         _check(_lib.load().fem_step_info(self.ctx, out), self.ctx, "fem_step_info")
         return {"available": bool(out[0]), "jacobi_graph_fused": bool(out[1]),
-                "two_level_graph_fused": bool(out[2]), "restriction_warps_per_cell": int(out[3])}
+                "two_level_graph_fused": bool(out[2]), "restriction_warps_per_cell": int(out[3]),
+                "jacobi_graph_pdl": bool(out[4]), "two_level_graph_pdl": bool(out[5])}
 
     def set_matvec_variant(self, variant):
         """Forces the tangent-matvec variant ("fused", "two_phase") or restores

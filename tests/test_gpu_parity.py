@@ -263,6 +263,37 @@ def test_bf16_packed_coarse_inverse_tracks_fp32(cuda, vox, cell):
     assert _rel_l2(sols[True], sols[False]) < 1e-5
 
 
+@pytest.mark.parametrize("pc", ["jacobi", "two_level"])
+def test_programmatic_launch_is_bitwise_neutral(cuda, vox, pc):
+    """Programmatic dependent launches between the CG kernels change when a
+    kernel is scheduled, not what it computes: the same iterations and the
+    bitwise same solution with and without them."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    mesh.set_coarse_options(cell=4)
+    lib = _lib.load()
+    rng = np.random.default_rng(31)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    r = dev(rhs, cuda)
+    code = {"jacobi": _lib.FEM_PRECOND_JACOBI, "two_level": _lib.FEM_PRECOND_TWO_LEVEL}[pc]
+    out = {}
+    for on in (True, False):
+        mesh.set_programmatic_launch(on)
+        du = torch.zeros_like(r)
+        it = C.c_int32()
+        rel = C.c_double()
+        rc = lib.fem_pcg(mesh.ctx, code, ptr(r), ptr(du), 1e-7, 20000, C.byref(it), C.byref(rel))
+        assert rc == 0, _lib.last_error(mesh.ctx)
+        assert mesh.step_info()[f"{pc}_graph_pdl"] == on
+        out[on] = (du.cpu().numpy(), it.value)
+    assert out[True][1] == out[False][1]
+    assert np.array_equal(out[True][0], out[False][0])
+
+
 def _pcg_fused_vs_chain(mesh, pc, rhs, cuda, rtol):
     lib = _lib.load()
     r = dev(rhs, cuda)

@@ -520,7 +520,7 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
   // every reducing kernel's grid must fit: node blocks and node-parallel blocks
-  c->max_blocks = std::max(c->n_blocks, (c->Nn + 255) / 256) + 1;
+  c->max_blocks = std::max(c->n_blocks, (c->Nn + 63) / 64) + 1;  // node gather: 64 nodes per CTA
   if ((st = dalloc(c, &c->partials, (size_t)N_SITES * 2 * c->max_blocks))) return st;
   if ((st = dalloc(c, &c->counters, (size_t)N_SITES))) return st;
   if ((st = dalloc(c, &c->scalars, (size_t)8))) return st;

@@ -343,8 +343,14 @@ __global__ void __launch_bounds__(256, 5) elem_mv_kernel(const __grid_constant__
     elem_mv_one<MODEL, false>(a, e);
 }
 
-// One thread per node; batches of 8 independent loads in flight, summed in
-// slot-list order.
+// kGatherLanes lanes per node: lane k of a node's group adds slots k,
+// k + kGatherLanes, ... of its slot list (a node's slots are contiguous, so a
+// warp reads one contiguous stretch), then xor steps combine the group in a
+// fixed order.  Several lanes per node keep several times as many loads in
+// flight as one thread per node.
+constexpr int kGatherLanes = 4;
+constexpr int kGatherNodes = 256 / kGatherLanes;  // nodes per CTA
+
 template <bool CG>
 __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant__ MvArgs a) {
   chain_enter();
@@ -354,17 +360,18 @@ __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant_
   __shared__ double sred[8];
   __shared__ bool am_last;
   const MeshDev& m = a.m;
-  const int n = blockIdx.x * 256 + threadIdx.x;
+  const int n = blockIdx.x * kGatherNodes + threadIdx.x / kGatherLanes;
+  const int sub = threadIdx.x % kGatherLanes;
   double pap = 0.0;
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f;
   if (n < m.n_nodes) {
     const int j0 = __ldg(m.node_row + n), j1 = __ldg(m.node_row + n + 1);
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
     constexpr int kBatch = 8;
-    for (int j = j0; j < j1; j += kBatch) {
+    for (int j = j0 + sub; j < j1; j += kBatch * kGatherLanes) {
       float4 v[kBatch];
 #pragma unroll
       for (int k = 0; k < kBatch; ++k)
-        v[k] = (j + k < j1) ? __ldcg(a.stage + j + k) : make_float4(0.f, 0.f, 0.f, 0.f);
+        v[k] = (j + k * kGatherLanes < j1) ? __ldcg(a.stage + j + k * kGatherLanes) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
       for (int k = 0; k < kBatch; ++k) {
         a0 += v[k].x;
@@ -372,6 +379,14 @@ __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant_
         a2 += v[k].z;
       }
     }
+  }
+#pragma unroll
+  for (int o = 1; o < kGatherLanes; o <<= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+  }
+  if (n < m.n_nodes && sub == 0) {
     const uint8_t fx = m.fixed[n];
     const float4 yv = make_float4((fx & 1) ? 0.f : a0, (fx & 2) ? 0.f : a1, (fx & 4) ? 0.f : a2, 0.f);
     reinterpret_cast<float4*>(a.y)[n] = yv;
@@ -889,7 +904,7 @@ static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
     case M_FMR: launch_chain(elem_mv_kernel<M_FMR, CG>, ge, 256, 0, s, a); break;
     default: launch_chain(elem_mv_kernel<-1, CG>, ge, 256, 0, s, a); break;
   }
-  launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, 256), 256, 0, s, a);
+  launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
 }
 
 void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {

@@ -306,13 +306,23 @@ __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
         acc[3 * k + 2] += w * rv.z;
       }
     }
-    float mine = 0.f;
+    // reduce-scatter of the 24 shares (padded to 32) over the warp: after
+    // the step of width o each lane keeps the half whose bit o matches its
+    // own; lane k ends with the full share k (31 shuffles, not 24 x 5)
+    float u[32];
 #pragma unroll
-    for (int k = 0; k < 24; ++k) {
-      const float v = warp_allsum(acc[k]);
-      if (lane == k) mine = v;
+    for (int k = 0; k < 32; ++k) u[k] = k < 24 ? acc[k] : 0.f;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      const bool up = (lane & o) != 0;
+#pragma unroll
+      for (int k = 0; k < o; ++k) {
+        const float send = up ? u[k] : u[k + o];
+        const float keep = up ? u[k + o] : u[k];
+        u[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
     }
-    if (lane < 24) c.cell_r[(size_t)item * 24 + lane] = mine;
+    if (lane < 24) c.cell_r[(size_t)item * 24 + lane] = u[0];
   }
   if (!UPDATE) return;
   // ||r||^2: lanes, then warps in order, then CTAs in order (last CTA)

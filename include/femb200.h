@@ -178,7 +178,12 @@ enum {
    * chain is launched as a programmatic dependent of the previous one (it is
    * scheduled while the previous one drains and waits for its results on the
    * device), where the runtime accepts it; 0: plain stream order */
-  FEM_OPT_PDL = 8
+  FEM_OPT_PDL = 8,
+  /* 1 (default): two-level PCG with the two-phase matvec applies the matvec
+   * to z and forms the direction in its node gather by recurrence,
+   * p = z + beta p and K p = K z + beta K p_old, saving the direction-update
+   * kernel; 0: p = z + beta p in its own kernel, then K p */
+  FEM_OPT_DIRECTION_RECURRENCE = 9
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

@@ -566,7 +566,8 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
     zv.y = (fx & 2) ? 0.f : dv.y * rv.y + cz[1];
     zv.z = (fx & 4) ? 0.f : dv.z * rv.z + cz[2];
     zv.w = 0.f;
-    reinterpret_cast<float4*>(INIT ? p : z)[i] = zv;
+    reinterpret_cast<float4*>(z)[i] = zv;
+    if (INIT) reinterpret_cast<float4*>(p)[i] = zv;
     rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
   }
   double v = block_sum<256>(rz, sred);

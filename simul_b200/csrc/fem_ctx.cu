@@ -124,6 +124,8 @@ struct FemCtx {
   // captured graphs (a refused capture turns it off)
   bool pdl = true;
   bool pdl_ok = true;
+  // two-level CG: direction by recurrence in the matvec's node gather
+  bool direction_recurrence = true;
   bool in_batch = false;
   unsigned int* step_bar = nullptr;  // [4] grid barrier words
   double* jac_part = nullptr;        // [2 n_chunks] Jacobi step shares
@@ -630,6 +632,12 @@ struct ChainPdl {
   ~ChainPdl() { chain_pdl() = saved; }
 };
 
+// Two-level PCG with the two-phase matvec: the matvec acts on z and its node
+// gather forms p = z + beta p, q = K z + beta q (no direction-update kernel).
+bool recurrence(const FemCtx* c, int kind) {
+  return kind == GRAPH_TWO_LEVEL && c->mv_variant == MV_TWO_PHASE && c->direction_recurrence;
+}
+
 bool use_fused(const FemCtx* c, int kind) {
   return kind != GRAPH_LEARNED && c->fused_step && c->fused_ok && !c->in_batch &&
          (kind == GRAPH_JACOBI || (c->tl_part != nullptr && c->cdev.Ainv != nullptr));
@@ -656,7 +664,8 @@ StepArgs step_args(const FemCtx* c, int kind) {
 int64_t kernels_per_iter(const FemCtx* c, int kind, bool fused) {
   const int64_t mv = c->mv_variant == MV_TWO_PHASE ? 2 : 1;
   if (fused) return mv + 1;
-  return mv + (kind == GRAPH_TWO_LEVEL ? 4 + coarse_product_kernels(c->cdev) : 2);
+  if (kind == GRAPH_TWO_LEVEL) return mv + 3 + coarse_product_kernels(c->cdev) + (recurrence(c, kind) ? 0 : 1);
+  return mv + 2;
 }
 
 // Enqueues one CG iteration; returns the first launch error (a refused
@@ -666,6 +675,10 @@ cudaError_t enqueue_cg_iter(FemCtx* c, int kind, bool fused) {
   mv.matF = c->matF;
   mv.payload = c->payload;
   mv.x = c->p;
+  if (!fused && recurrence(c, kind)) {
+    mv.x = c->tmpf;  // z
+    mv.p_rec = c->p;
+  }
   mv.y = c->y;
   mv.cg = c->cg;
   mv.red = c->red();
@@ -691,7 +704,8 @@ cudaError_t enqueue_cg_iter(FemCtx* c, int kind, bool fused) {
     launch_update_restrict(ca, c->x, c->r, c->p, c->y, c->cg, c->red(), SITE_CGU, c->stream);
     launch_coarse_solve(ca, c->cg, c->stream);
     launch_tl_rz(ca, false, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
-    launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
+    // with the recurrence the next matvec forms the direction
+    if (!recurrence(c, kind)) launch_tl_pupdate(c->p, c->tmpf, c->Nn, c->cg, c->stream);
     return cudaSuccess;
   }
   launch_cg_update(c->x, c->r, c->p, c->y, c->dinv, c->Nn, c->cg, c->red(), SITE_CGU, c->stream);
@@ -831,7 +845,8 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   if ((st = choose_matvec_variant(c))) return st;
   const bool fused = use_fused(c, kind);
   const bool pdl = use_pdl(c, kind);
-  const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0) | (pdl ? 4 : 0);
+  const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0) | (pdl ? 4 : 0) |
+                    (!fused && recurrence(c, kind) ? 8 : 0);
   if (c->cg_graph[kind] && c->cg_graph_model[kind] == c->model_kind &&
       c->cg_graph_variant[kind] == c->mv_variant && c->cg_graph_flags[kind] == flags)
     return FEM_OK;
@@ -1628,6 +1643,10 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
         }
         c->use_loop_graph = value != 0;
       }
+      return FEM_OK;
+    case FEM_OPT_DIRECTION_RECURRENCE:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "direction recurrence flag must be 0 or 1");
+      c->direction_recurrence = value != 0;
       return FEM_OK;
     case FEM_OPT_PDL:
       if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "programmatic launch flag must be 0 or 1");

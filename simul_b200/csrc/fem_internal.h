@@ -124,6 +124,10 @@ struct MvArgs {
   int mask_input;           // 1: fixed DOFs of x read as zero (K_ff x); 0: K_f,all x
   int variant;              // MV_FUSED (node-block) or MV_TWO_PHASE (element pass + node gather)
   float4* stage;            // [4 Ne] slot vectors in node_slots order (two-phase scratch)
+  // two-phase inside CG, non-null: x holds the preconditioned residual z and
+  // the node gather forms the direction by recurrence, p = z + beta p and
+  // q = K z + beta q (q in y, p here), so no separate direction update runs
+  float* p_rec;
 };
 
 enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_N_VARIANTS = 2 };

@@ -388,11 +388,28 @@ __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant_
   }
   if (n < m.n_nodes && sub == 0) {
     const uint8_t fx = m.fixed[n];
-    const float4 yv = make_float4((fx & 1) ? 0.f : a0, (fx & 2) ? 0.f : a1, (fx & 4) ? 0.f : a2, 0.f);
-    reinterpret_cast<float4*>(a.y)[n] = yv;
-    if (CG) {
-      const float4 pv = reinterpret_cast<const float4*>(a.x)[n];
+    float4 yv = make_float4((fx & 1) ? 0.f : a0, (fx & 2) ? 0.f : a1, (fx & 4) ? 0.f : a2, 0.f);
+    if (CG && a.p_rec) {
+      // direction by recurrence: x = z, q = K z + beta q_old, p = z + beta p_old
+      // (beta = 0 after the start: plain copies, whatever the old vectors hold)
+      const double beta_d = a.cg->beta;
+      const float beta = (float)beta_d;
+      float4 pv = reinterpret_cast<const float4*>(a.x)[n];
+      if (beta_d != 0.0) {
+        const float4 qo = reinterpret_cast<const float4*>(a.y)[n];
+        const float4 po = reinterpret_cast<const float4*>(a.p_rec)[n];
+        yv.x += beta * qo.x; yv.y += beta * qo.y; yv.z += beta * qo.z;
+        pv.x += beta * po.x; pv.y += beta * po.y; pv.z += beta * po.z;
+      }
+      reinterpret_cast<float4*>(a.p_rec)[n] = pv;
+      reinterpret_cast<float4*>(a.y)[n] = yv;
       pap = (double)yv.x * pv.x + (double)yv.y * pv.y + (double)yv.z * pv.z;
+    } else {
+      reinterpret_cast<float4*>(a.y)[n] = yv;
+      if (CG) {
+        const float4 pv = reinterpret_cast<const float4*>(a.x)[n];
+        pap = (double)yv.x * pv.x + (double)yv.y * pv.y + (double)yv.z * pv.z;
+      }
     }
   }
   if (CG) {

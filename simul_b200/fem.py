@@ -194,6 +194,12 @@ class FEMesh:
         inside the captured graphs (True, the default) or plain stream order."""
         _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_PDL, 1 if on else 0), self.ctx, "fem_set_option")
 
+    def set_direction_recurrence(self, on: bool):
+        """Two-level PCG: form the search direction by recurrence inside the
+        matvec's node gather (True, the default) or in its own kernel."""
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_DIRECTION_RECURRENCE, 1 if on else 0), self.ctx,
+               "fem_set_option")
+
     def step_info(self) -> dict:
         out = (C.c_int64 * 6)()
         _check(_lib.load().fem_step_info(self.ctx, out), self.ctx, "fem_step_info")

@@ -6,8 +6,10 @@ plasticity, evaluates the FP64 residual at a plastic state (top face pushed
 hot kernel ``--reps`` times through ``fem_profile_kernels``: the tangent matvec
 (the variant given by ``--variant``), the FP64 residual, the CG update and the
 CG direction update; optionally the learned network's forward pass
-(``--learned weights.npz``) and one two-level PCG solve (``--two-level``).  The per-launch CUDA-event times are printed as one JSON
-line.  With ``--reps 3`` and ``-k``/``-c`` filters an ncu capture of one kernel
+(``--learned weights.npz``) and one two-level PCG solve (``--two-level``,
+4-voxel cells with the packed BF16 coarse inverse by default, run as
+fixed-size iteration graphs so a kernel profiler sees every launch).  The
+per-launch CUDA-event times are printed as one JSON line.  With ``--reps 3`` and ``-k``/``-c`` filters an ncu capture of one kernel
 ends in seconds.
 
     python -m simul_b200.profile_case --n 64 --variant fused --reps 3
@@ -30,6 +32,8 @@ def main(argv=None):
     ap.add_argument("--nodes-per-block", type=int, default=0)
     ap.add_argument("--learned", default="", help="weights file: also run the network forward --reps times")
     ap.add_argument("--two-level", action="store_true", help="also run one two-level PCG solve (rtol 1e-6)")
+    ap.add_argument("--coarse-cell", type=int, default=4, help="two-level: lattice cell edge in voxels")
+    ap.add_argument("--coarse-bf16", type=int, default=1, help="two-level: BF16 packed coarse inverse")
     args = ap.parse_args(argv)
 
     import torch
@@ -72,6 +76,8 @@ def main(argv=None):
         e1.synchronize()
         extra["mpnn_forward_ms"] = e0.elapsed_time(e1) / args.reps
     if args.two_level:
+        mesh.set_coarse_options(cell=args.coarse_cell, bf16=bool(args.coarse_bf16))
+        mesh.set_whole_solve_graph(False)   # kernel profilers cannot see into the conditional graph
         rhs = torch.randn(v.n_nodes, 3, dtype=torch.float64, device=mesh.device)
         du = torch.zeros_like(rhs)
         it, rel = C.c_int32(), C.c_double()

@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--whole-solve-graph", type=int, default=1,
                     help="1: one graph launch per PCG solve; 0: fixed-size iteration graphs (for kernel profilers)")
     ap.add_argument("--pdl", type=int, default=1, help="programmatic dependent launches in the CG graphs")
+    ap.add_argument("--block-smoother", type=int, default=1,
+                    help="two-level smoother: 1 nodal 3x3 block inverse, 0 diagonal inverse")
     ap.add_argument("--fused-step", type=int, default=0,
                     help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
@@ -279,6 +281,7 @@ def main():
     mesh.set_fused_step(bool(args.fused_step))
     mesh.set_whole_solve_graph(bool(args.whole_solve_graph))
     mesh.set_programmatic_launch(bool(args.pdl))
+    mesh.set_block_smoother(bool(args.block_smoother))
     if args.precond == "learned":
         from simul_b200 import learned
         learned.set_weights(mesh, learned.load(args.weights))

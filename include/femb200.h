@@ -183,7 +183,11 @@ enum {
    * to z and forms the direction in its node gather by recurrence,
    * p = z + beta p and K p = K z + beta K p_old, saving the direction-update
    * kernel; 0: p = z + beta p in its own kernel, then K p */
-  FEM_OPT_DIRECTION_RECURRENCE = 9
+  FEM_OPT_DIRECTION_RECURRENCE = 9,
+  /* two-level preconditioner smoother: 1 (default) the inverse of each
+   * node's 3 x 3 diagonal block of K_T (free DOFs), 0 the inverse of the
+   * diagonal */
+  FEM_OPT_BLOCK_JACOBI = 10
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

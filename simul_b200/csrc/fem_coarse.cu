@@ -561,10 +561,18 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
       cz[2] += wq * c.yc[3 * cnode + 2];
     }
     const int fx = (int)a.m.fixed[i];
+    float sm[3] = {dv.x * rv.x, dv.y * rv.y, dv.z * rv.z};
+    if (a.boff) {
+      // nodal block smoother: off-diagonals (01, 02, 12) of the block inverse
+      const float4 ov = __ldg(reinterpret_cast<const float4*>(a.boff) + i);
+      sm[0] += ov.x * rv.y + ov.y * rv.z;
+      sm[1] += ov.x * rv.x + ov.z * rv.z;
+      sm[2] += ov.y * rv.x + ov.z * rv.y;
+    }
     float4 zv;
-    zv.x = (fx & 1) ? 0.f : dv.x * rv.x + cz[0];
-    zv.y = (fx & 2) ? 0.f : dv.y * rv.y + cz[1];
-    zv.z = (fx & 4) ? 0.f : dv.z * rv.z + cz[2];
+    zv.x = (fx & 1) ? 0.f : sm[0] + cz[0];
+    zv.y = (fx & 2) ? 0.f : sm[1] + cz[1];
+    zv.z = (fx & 4) ? 0.f : sm[2] + cz[2];
     zv.w = 0.f;
     reinterpret_cast<float4*>(z)[i] = zv;
     if (INIT) reinterpret_cast<float4*>(p)[i] = zv;

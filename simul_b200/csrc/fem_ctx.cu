@@ -126,6 +126,9 @@ struct FemCtx {
   bool pdl_ok = true;
   // two-level CG: direction by recurrence in the matvec's node gather
   bool direction_recurrence = true;
+  // two-level smoother: nodal 3x3 block inverse instead of 1 / diag
+  bool block_jacobi = true;
+  float* boff = nullptr;  // [Nn] float4 off-diagonals (01, 02, 12) of the block inverse
   bool in_batch = false;
   unsigned int* step_bar = nullptr;  // [4] grid barrier words
   double* jac_part = nullptr;        // [2 n_chunks] Jacobi step shares
@@ -317,7 +320,7 @@ void free_ctx(FemCtx* c) {
                   c->u, c->u_base, c->R, c->tmpd, c->payload, c->ep_c, c->epe_c, c->ep_t,
                   c->epe_t, c->r, c->x, c->p, c->y, c->dinv, c->tmpf, c->d_perm_node,
                   c->d_perm_elem, c->matD, c->matF, c->partials, c->counters, c->scalars, c->cg,
-                  c->step_bar, c->jac_part};
+                  c->step_bar, c->jac_part, c->boff};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_cg) cudaFreeHost(c->h_cg);
@@ -518,6 +521,7 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->y, nf))) return st;
   if ((st = dalloc(c, &c->dinv, nf))) return st;
   if ((st = dalloc(c, &c->tmpf, nf))) return st;
+  if ((st = dalloc(c, &c->boff, nf))) return st;
   if ((st = dalloc(c, &c->stage, 4 * Ne))) return st;
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
@@ -597,13 +601,16 @@ int eval_residual(FemCtx* c, double* fneg_out_int, double* rnorm2) {
   return FEM_OK;
 }
 
-int compute_dinv(FemCtx* c, int precond) {
+// Jacobi scaling for the PCG solve: 1 / diag(K_T), or with `block` the
+// nodal 3 x 3 block inverse (diagonal in dinv, off-diagonals in boff).
+int compute_dinv(FemCtx* c, int precond, bool block = false) {
   if (precond == FEM_PRECOND_JACOBI) {
     DiagArgs a;
     a.m = c->mesh();
     a.matF = c->matF;
     a.payload = c->payload;
     a.dinv = c->dinv;
+    a.boff = block ? c->boff : nullptr;
     ++c->n_launches; launch_diag(a, c->model_kind, c->stream);
     CKL();
   } else {
@@ -620,6 +627,7 @@ CoarseArgs coarse_args(const FemCtx* c) {
   a.c = c->cdev;
   a.matF = c->matF;
   a.payload = c->payload;
+  a.boff = c->block_jacobi ? c->boff : nullptr;
   return a;
 }
 
@@ -640,7 +648,7 @@ bool recurrence(const FemCtx* c, int kind) {
 
 bool use_fused(const FemCtx* c, int kind) {
   return kind != GRAPH_LEARNED && c->fused_step && c->fused_ok && !c->in_batch &&
-         (kind == GRAPH_JACOBI || (c->tl_part != nullptr && c->cdev.Ainv != nullptr));
+         (kind == GRAPH_JACOBI || (c->tl_part != nullptr && c->cdev.Ainv != nullptr && !c->block_jacobi));
 }
 
 StepArgs step_args(const FemCtx* c, int kind) {
@@ -846,7 +854,7 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   const bool fused = use_fused(c, kind);
   const bool pdl = use_pdl(c, kind);
   const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0) | (pdl ? 4 : 0) |
-                    (!fused && recurrence(c, kind) ? 8 : 0);
+                    (!fused && recurrence(c, kind) ? 8 : 0) | (kind == GRAPH_TWO_LEVEL && c->block_jacobi ? 16 : 0);
   if (c->cg_graph[kind] && c->cg_graph_model[kind] == c->model_kind &&
       c->cg_graph_variant[kind] == c->mv_variant && c->cg_graph_flags[kind] == flags)
     return FEM_OK;
@@ -1373,7 +1381,7 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   const int kind = learned ? GRAPH_LEARNED : (tl ? GRAPH_TWO_LEVEL : GRAPH_JACOBI);
   if (learned && !c->mpnn_has_weights)
     return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights (fem_mpnn_set_weights)");
-  if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : precond))) return st;
+  if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : precond, tl && c->block_jacobi))) return st;
   if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
   if (learned && (st = ensure_mpnn(c))) return st;
   if ((st = ensure_cg_graph(c, kind))) return st;
@@ -1643,6 +1651,10 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
         }
         c->use_loop_graph = value != 0;
       }
+      return FEM_OK;
+    case FEM_OPT_BLOCK_JACOBI:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "block smoother flag must be 0 or 1");
+      c->block_jacobi = value != 0;
       return FEM_OK;
     case FEM_OPT_DIRECTION_RECURRENCE:
       if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "direction recurrence flag must be 0 or 1");
@@ -2039,7 +2051,7 @@ int fem_batch_solve(void** ctxs, int32_t n, const FemSolveParams* prm, int32_t l
     const bool tl = p.precond == FEM_PRECOND_TWO_LEVEL;
     const bool learned = p.precond == FEM_PRECOND_LEARNED;
     if (learned && !c->mpnn_has_weights) return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights");
-    if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : p.precond))) return st;
+    if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : p.precond, tl && c->block_jacobi))) return st;
     if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
     if (learned && (st = ensure_mpnn(c))) return st;
     c->in_batch = workers > 1;

@@ -137,6 +137,7 @@ struct DiagArgs {
   const DevMat<float>* matF;
   const float* payload;
   float* dinv;              // [Nn] float4: 1/diag(K) on free DOFs, 0 elsewhere
+  float* boff;              // non-null: nodal 3x3 block inverse, dinv its diagonal, boff (01, 02, 12)
 };
 
 // Coarse lattice of the two-level preconditioner (fem_coarse.cu).  Cells
@@ -178,6 +179,7 @@ struct CoarseArgs {
   CoarseDev c;
   const DevMat<float>* matF;
   const float* payload;
+  const float* boff;        // non-null: the smoother is the nodal 3x3 block inverse (dinv + these)
 };
 
 // Fused CG step (fem_step.cu): the work of one PCG iteration after the

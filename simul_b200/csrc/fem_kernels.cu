@@ -56,6 +56,23 @@ __device__ __forceinline__ void gather_chunk(const uint32_t* s_slots, const T (*
   }
 }
 
+// gather_chunk for W values per slot: sf[W * slot + k][thread]
+template <int NB, int W>
+__device__ __forceinline__ void gather_chunk_w(const uint32_t* s_slots, const float (*sf)[NB], int base, int& cur,
+                                               int end, float (&acc)[W]) {
+  const int lim = base + NB;
+  while (cur < end) {
+    const uint32_t ent = s_slots[cur];
+    const int li = (int)(ent >> 2);
+    if (li >= lim) break;
+    const int t = li - base;
+    const int s = (int)(ent & 3u);
+#pragma unroll
+    for (int k = 0; k < W; ++k) acc[k] += sf[W * s + k][t];
+    ++cur;
+  }
+}
+
 // ───────────────────────── residual (FP64) ─────────────────────────
 
 template <int NB, int MODEL>
@@ -433,12 +450,20 @@ __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant_
 }
 
 // ───────────────────────── Jacobi diagonal (FP32) ─────────────────────────
+//
+// BLOCK = false: dinv = 1 / diag(K_T) on free DOFs.  BLOCK = true: the
+// node's 3 x 3 diagonal block of K_T (6 entries per element slot, gathered
+// in the same fixed order), restricted to the free DOFs and inverted in
+// FP64: dinv = the inverse's diagonal, boff = its off-diagonals (01, 02, 12);
+// fixed rows and columns are zero.  A block that is not positive definite
+// falls back to the scalar inverse of its diagonal.
 
-template <int NB, int MODEL>
+template <int NB, int MODEL, bool BLOCK>
 __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagArgs a) {
+  constexpr int W = BLOCK ? 6 : 3;
   extern __shared__ __align__(16) unsigned char s_dyn[];
   uint32_t* s_slots = reinterpret_cast<uint32_t*>(s_dyn);
-  __shared__ float sf[12][NB];
+  __shared__ float sf[4 * W][NB];
   const MeshDev& m = a.m;
   const int b = blockIdx.x;
   const int tid = threadIdx.x;
@@ -446,7 +471,9 @@ __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagAr
   const bool has_node = node < m.n_nodes;
   int cur, end;
   load_block_slots<NB>(m, b, s_slots, cur, end);
-  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f;
+  float acc[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) acc[k] = 0.f;
   const int e0 = m.blk_ptr[b], e1 = m.blk_ptr[b + 1];
   for (int c0 = e0; c0 < e1; c0 += NB) {
     const int idx = c0 + tid;
@@ -492,24 +519,56 @@ __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagAr
           for (int j = 0; j < 3; ++j) dF[3 * i + j] = w[s][j] * g.inv_det;
           float dP[9];
           dP_any<MODEL>(mat, scale, pay, dF, dP);
-          sf[3 * s + i][tid] =
-              g.s6 * (dP[3 * i] * w[s][0] + dP[3 * i + 1] * w[s][1] + dP[3 * i + 2] * w[s][2]);
+          if (BLOCK) {
+            // force component k at the slot's node for a unit displacement in
+            // direction i: entries (i, k), k >= i -> 00 01 02 | 11 12 | 22
+#pragma unroll
+            for (int k = i; k < 3; ++k) {
+              const int ent = (i == 0) ? k : (i == 1 ? 2 + k : 5);
+              sf[W * s + ent][tid] =
+                  g.s6 * (dP[3 * k] * w[s][0] + dP[3 * k + 1] * w[s][1] + dP[3 * k + 2] * w[s][2]);
+            }
+          } else {
+            sf[W * s + i][tid] =
+                g.s6 * (dP[3 * i] * w[s][0] + dP[3 * i + 1] * w[s][1] + dP[3 * i + 2] * w[s][2]);
+          }
         }
       }
     }
     __syncthreads();
-    gather_chunk<NB>(s_slots, sf, c0 - e0, cur, end, acc0, acc1, acc2);
+    gather_chunk_w<NB, W>(s_slots, sf, c0 - e0, cur, end, acc);
     __syncthreads();
   }
-  if (has_node) {
-    const uint8_t fx = m.fixed[node];
-    const float accs[3] = {acc0, acc1, acc2};
+  if (!has_node) return;
+  const uint8_t fx = m.fixed[node];
+  if (!BLOCK) {
     float dv[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-      dv[d] = (((fx >> d) & 1) || !(accs[d] > 0.f)) ? 0.f : 1.f / accs[d];
+    for (int d = 0; d < 3; ++d) dv[d] = (((fx >> d) & 1) || !(acc[d] > 0.f)) ? 0.f : 1.f / acc[d];
     reinterpret_cast<float4*>(a.dinv)[node] = make_float4(dv[0], dv[1], dv[2], 0.f);
+    return;
   }
+  // acc: 00 01 02 11 12 22; fixed rows/columns replaced by the identity
+  const bool f0 = fx & 1, f1 = (fx >> 1) & 1, f2 = (fx >> 2) & 1;
+  const double k00 = f0 ? 1.0 : acc[0], k11 = f1 ? 1.0 : acc[3], k22 = f2 ? 1.0 : acc[5];
+  const double k01 = (f0 || f1) ? 0.0 : acc[1], k02 = (f0 || f2) ? 0.0 : acc[2], k12 = (f1 || f2) ? 0.0 : acc[4];
+  const double c00 = k11 * k22 - k12 * k12, c01 = k02 * k12 - k01 * k22, c02 = k01 * k12 - k02 * k11;
+  const double det = k00 * c00 + k01 * c01 + k02 * c02;
+  float4 dv, ov;
+  if (det > 0.0 && k00 > 0.0 && k00 * k11 - k01 * k01 > 0.0 && isfinite(det)) {
+    const double id = 1.0 / det;
+    const double i11 = (k00 * k22 - k02 * k02) * id, i22 = (k00 * k11 - k01 * k01) * id;
+    const double i12 = (k01 * k02 - k00 * k12) * id;
+    dv = make_float4(f0 ? 0.f : (float)(c00 * id), f1 ? 0.f : (float)i11, f2 ? 0.f : (float)i22, 0.f);
+    ov = make_float4((f0 || f1) ? 0.f : (float)(c01 * id), (f0 || f2) ? 0.f : (float)(c02 * id),
+                     (f1 || f2) ? 0.f : (float)i12, 0.f);
+  } else {
+    dv = make_float4((f0 || !(acc[0] > 0.f)) ? 0.f : 1.f / acc[0], (f1 || !(acc[3] > 0.f)) ? 0.f : 1.f / acc[3],
+                     (f2 || !(acc[5] > 0.f)) ? 0.f : 1.f / acc[5], 0.f);
+    ov = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  reinterpret_cast<float4*>(a.dinv)[node] = dv;
+  reinterpret_cast<float4*>(a.boff)[node] = ov;
 }
 
 // ───────────────────────── PCG vector kernels ─────────────────────────
@@ -963,8 +1022,13 @@ void prepare_kernels(const MeshDev& m, int model) {
 template <int NB, int MODEL>
 static void diag_go(const DiagArgs& a, cudaStream_t s) {
   const size_t smem = slots_smem(a.m);
-  allow_smem(diag_kernel<NB, MODEL>, smem, s);
-  diag_kernel<NB, MODEL><<<a.m.n_blocks, NB, smem, s>>>(a);
+  if (a.boff) {
+    allow_smem(diag_kernel<NB, MODEL, true>, smem, s);
+    diag_kernel<NB, MODEL, true><<<a.m.n_blocks, NB, smem, s>>>(a);
+    return;
+  }
+  allow_smem(diag_kernel<NB, MODEL, false>, smem, s);
+  diag_kernel<NB, MODEL, false><<<a.m.n_blocks, NB, smem, s>>>(a);
 }
 
 template <int NB>

@@ -200,6 +200,12 @@ class FEMesh:
         _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_DIRECTION_RECURRENCE, 1 if on else 0), self.ctx,
                "fem_set_option")
 
+    def set_block_smoother(self, on: bool):
+        """Two-level preconditioner smoother: nodal 3x3 block inverse (True,
+        the default) or the inverse of the diagonal (False)."""
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_BLOCK_JACOBI, 1 if on else 0), self.ctx,
+               "fem_set_option")
+
     def step_info(self) -> dict:
         out = (C.c_int64 * 6)()
         _check(_lib.load().fem_step_info(self.ctx, out), self.ctx, "fem_step_info")

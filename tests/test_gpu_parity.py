@@ -330,8 +330,56 @@ def test_direction_recurrence_matches_direction_kernel(cuda, vox):
         assert _rel_l2(out[on][0], u_ref) < 1e-5, on
 
 
+@pytest.mark.parametrize("material", ["le", "j2"])
+def test_block_smoother_matches_oracle_with_no_more_iterations(cuda, vox, material):
+    """Two-level PCG with the nodal 3x3 block-inverse smoother and with the
+    diagonal smoother reach the FP64 oracle's solution; the block smoother
+    needs no more iterations.  J2 at a plastic state checks the block of the
+    consistent elasto-plastic tangent."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    if material == "le":
+        mat = B.LinearElastic(1e3, 0.3)
+        mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+        mat.compute_nodal_forces(mesh)
+    else:
+        ref = np.load(G.path_of("vox12_j2_steps"))
+        mat = make_material("j2", E=vox.E)
+        lf = float(ref["load_factor"])
+        vals = vox.fixed_vals * lf / int(ref["n_total"])
+        mesh.set_fixed_dofs(idx, vals.reshape(-1)[idx])
+        res = B.StaticSolver(mesh, mat, tol=1e-10, precond="two_level").solve(verbose=False)
+        assert res["converged"], res
+        mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+        mat.compute_nodal_forces(mesh)
+    mesh.set_coarse_options(cell=4)
+    lib = _lib.load()
+    rng = np.random.default_rng(51)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    r = dev(rhs, cuda)
+    out = {}
+    for on in (True, False):
+        mesh.set_block_smoother(on)
+        du = torch.zeros_like(r)
+        it = C.c_int32()
+        rel = C.c_double()
+        rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, ptr(r), ptr(du), 1e-8, 20000, C.byref(it),
+                         C.byref(rel))
+        assert rc == 0, _lib.last_error(mesh.ctx)
+        out[on] = (du.cpu().numpy(), it.value)
+    assert out[True][1] <= out[False][1], (out[True][1], out[False][1])
+    assert _rel_l2(out[True][0], out[False][0]) < 1e-5
+    if material == "le":
+        m = O.Mesh(vox.X, vox.conn)
+        F = O.deformation_gradient(np.zeros_like(vox.X), vox.conn.astype(np.int64), m.dNdX)
+        u_ref = O.solve_tangent(O.Material("linear_elastic", E=1e3, nu=0.3), F, None, m, rhs, vox.fixed_mask)
+        assert _rel_l2(out[True][0], u_ref) < 1e-6
+
+
 def _pcg_fused_vs_chain(mesh, pc, rhs, cuda, rtol):
     lib = _lib.load()
+    mesh.set_block_smoother(False)   # the fused step applies the diagonal smoother
     r = dev(rhs, cuda)
     out = {}
     for fused in (True, False):

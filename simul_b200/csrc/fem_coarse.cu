@@ -244,10 +244,10 @@ __global__ void coarse_pack16_kernel(const __grid_constant__ CoarseDev c) {
 // cell's nodes in runs of 32, runs s, s + S, ... (S = r_slices, chosen so the
 // items fill the GPU's warps); the item's 24 shares
 //   cell_r[cell][s][3 corner + d] = sum over its nodes of w_corner r_d
-// are completed by xor butterflies (lane k stores share k).  UPDATE fuses the
-// CG update in front: x += alpha p, r -= alpha q on the item's nodes (every
-// node belongs to exactly one cell), ||r||^2 per CTA (its warps' items in
-// order), and the last CTA runs the convergence test on the ordered total.
+// are completed by a reduce-scatter (lane k stores share k).  UPDATE fuses
+// the CG update in front: x += alpha p, r -= alpha q on the item's nodes
+// (every node belongs to exactly one cell); ||r||^2 and the convergence test
+// run with r.z in tl_rz_kernel, so this kernel needs no grid reduction.
 constexpr int kRestrictWarps = 8;
 constexpr int kMaxRestrictSlices = 8;
 
@@ -260,12 +260,9 @@ __device__ __forceinline__ float warp_allsum(float v) {
 template <bool UPDATE>
 __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
     const __grid_constant__ CoarseArgs a, float* r, float* x, const float* __restrict__ p,
-    const float* __restrict__ q, CGState* cg, Reduce red, int site) {
+    const float* __restrict__ q, const CGState* cg) {
   chain_enter();
   if (cg && cg->done) return;
-  __shared__ double s_rr[kRestrictWarps];
-  __shared__ double s_red[kRestrictWarps];
-  __shared__ bool am_last;
   const CoarseDev& c = a.c;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int S = c.r_slices;
@@ -275,7 +272,6 @@ __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
   float4* x4 = reinterpret_cast<float4*>(x);
   const float4* p4 = reinterpret_cast<const float4*>(p);
   const float4* q4 = reinterpret_cast<const float4*>(q);
-  double rr_w = 0.0;
   for (int item = blockIdx.x * kRestrictWarps + warp; item < n_items; item += gridDim.x * kRestrictWarps) {
     const int cell = item / S, sl = item - cell * S;
     const int3 ijk = c.cell_ijk[cell];
@@ -294,7 +290,6 @@ __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
         rv.x -= alpha * qv.x; rv.y -= alpha * qv.y; rv.z -= alpha * qv.z;
         x4[node] = xv;
         r4[node] = rv;
-        rr_w += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
       }
       float t[3];
       cell_local(c, ijk, X.x, X.y, X.z, t);
@@ -323,31 +318,6 @@ __global__ void __launch_bounds__(kRestrictWarps * 32) restrict_cells_kernel(
       }
     }
     if (lane < 24) c.cell_r[(size_t)item * 24 + lane] = u[0];
-  }
-  if (!UPDATE) return;
-  // ||r||^2: lanes, then warps in order, then CTAs in order (last CTA)
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) rr_w += __shfl_xor_sync(0xffffffffu, rr_w, o);
-  if (lane == 0) s_rr[warp] = rr_w;
-  __syncthreads();
-  double v = 0.0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < kRestrictWarps; ++w) v += s_rr[w];
-  if (publish_partial(red, site, 1, &v, &am_last)) {
-    const double trr = final_sum<kRestrictWarps * 32>(red, site, 0, s_red);
-    if (threadIdx.x == 0) {
-      cg->rr = trr;
-      cg->iter += 1;
-      if (!isfinite(trr)) {
-        cg->done = 3;
-        cg->status = 3;
-      } else if (trr <= cg->tol2) {
-        cg->done = 1;
-      } else if (cg->iter >= cg->max_iter) {
-        cg->done = 2;
-      }
-      red.counters[site] = 0u;
-    }
   }
 }
 
@@ -532,8 +502,11 @@ __global__ void __launch_bounds__(kTileWarps * 32) coarse_slot_sum_kernel(
 }
 
 // z = D^-1 r + P y_c (zero on fixed DOFs) and r.z.  INIT: p = z, rz set;
-// otherwise beta = rz_new / rz_old (Fletcher-Reeves, exact for a fixed SPD
-// preconditioner) and rz replaced.
+// otherwise also ||r||^2 of the r the update kernel just wrote: the last
+// block runs the convergence test (iteration count, converged / out of
+// iterations / breakdown), then beta = rz_new / rz_old (Fletcher-Reeves,
+// exact for a fixed SPD preconditioner) and rz replaced.  The node's eight
+// corner coarse nodes come from the per-node table (one dependent load less).
 template <bool INIT>
 __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ CoarseArgs a,
                                                     const float* __restrict__ r,
@@ -545,16 +518,18 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
   __shared__ bool am_last;
   const CoarseDev& c = a.c;
   const int i = blockIdx.x * 256 + threadIdx.x;
-  double rz = 0.0;
+  double rz = 0.0, rr = 0.0;
   if (i < a.m.n_nodes) {
     const float4 rv = reinterpret_cast<const float4*>(r)[i];
     const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
     float t[3];
-    const int cell = node_lattice(c, i, t);
+    node_lattice(c, i, t);
+    const uint4 cw = __ldg(c.node_corners + i);
+    const uint32_t cpk[4] = {cw.x, cw.y, cw.z, cw.w};
     float cz[3] = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const int cnode = __ldg(c.cell_corner + cell * 8 + q);
+      const int cnode = (int)((cpk[q >> 1] >> (16 * (q & 1))) & 0xFFFFu);
       const float wq = tri_weight(t[0], t[1], t[2], q);
       cz[0] += wq * c.yc[3 * cnode];
       cz[1] += wq * c.yc[3 * cnode + 1];
@@ -577,18 +552,31 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
     reinterpret_cast<float4*>(z)[i] = zv;
     if (INIT) reinterpret_cast<float4*>(p)[i] = zv;
     rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
+    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
   }
-  double v = block_sum<256>(rz, sred);
-  if (publish_partial(red, site, 1, &v, &am_last)) {
+  double v[2];
+  v[0] = block_sum<256>(rz, sred);
+  v[1] = INIT ? 0.0 : block_sum<256>(rr, sred);
+  if (publish_partial(red, site, INIT ? 1 : 2, v, &am_last)) {
     const double trz = final_sum<256>(red, site, 0, sred);
+    const double trr = INIT ? 0.0 : final_sum<256>(red, site, 1, sred);
     if (threadIdx.x == 0) {
       if (INIT) {
         cg->beta = 0.0;
       } else {
         cg->beta = trz / cg->rz;
+        cg->rr = trr;
+        cg->iter += 1;
       }
       cg->rz = trz;
-      if (!isfinite(trz) || !(trz > 0.0)) {
+      if (!INIT && !isfinite(trr)) {
+        cg->done = 3;
+        cg->status = 3;
+      } else if (!INIT && trr <= cg->tol2) {
+        cg->done = 1;
+      } else if (!INIT && cg->iter >= cg->max_iter) {
+        cg->done = 2;
+      } else if (!isfinite(trz) || !(trz > 0.0)) {
         cg->done = 3;
         cg->status = 3;
       }
@@ -887,6 +875,24 @@ void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, c
   coarse_node_lat_kernel<<<nblk(m.n_nodes, 256), 256, 0, s>>>(m, c, out);
 }
 
+// node_corners[i] = the eight corner coarse nodes of node i's cell, 16 bits each
+__global__ void coarse_node_corners_kernel(const __grid_constant__ MeshDev m, const __grid_constant__ CoarseDev c,
+                                           uint4* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.n_nodes) return;
+  const int cell = c.node_cell[i];
+  uint32_t w[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    w[k] = ((uint32_t)c.cell_corner[cell * 8 + 2 * k] & 0xFFFFu) |
+           (((uint32_t)c.cell_corner[cell * 8 + 2 * k + 1] & 0xFFFFu) << 16);
+  out[i] = make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out, cudaStream_t s) {
+  coarse_node_corners_kernel<<<nblk(m.n_nodes, 256), 256, 0, s>>>(m, c, out);
+}
+
 int coarse_product_kernels(const CoarseDev& c) { return c.Ainv16 ? 2 : 1; }
 
 // Resident CTAs of the tile product on this device (one wave, tiles looped).
@@ -904,16 +910,14 @@ int tile_mv_grid() {
 
 void launch_coarse_apply(const CoarseArgs& a, const float* r, const CGState* cg, cudaStream_t s) {
   restrict_cells_kernel<false><<<nblk((int64_t)a.c.n_cells * a.c.r_slices, kRestrictWarps), kRestrictWarps * 32, 0,
-                                  s>>>(a, const_cast<float*>(r), nullptr, nullptr, nullptr, const_cast<CGState*>(cg),
-                                       Reduce{}, 0);
+                                  s>>>(a, const_cast<float*>(r), nullptr, nullptr, nullptr, cg);
   launch_coarse_solve(a, cg, s);
 }
 
 void launch_update_restrict(const CoarseArgs& a, float* x, float* r, const float* p, const float* q, CGState* cg,
-                            Reduce red, int site, cudaStream_t s) {
-  const int grid = std::min(nblk((int64_t)a.c.n_cells * a.c.r_slices, kRestrictWarps), red.max_blocks - 1);
-  launch_chain(restrict_cells_kernel<true>, std::max(grid, 1), kRestrictWarps * 32, 0, s, a, r, x, p, q, cg, red,
-               site);
+                            cudaStream_t s) {
+  launch_chain(restrict_cells_kernel<true>, nblk((int64_t)a.c.n_cells * a.c.r_slices, kRestrictWarps),
+               kRestrictWarps * 32, 0, s, a, r, x, p, q, static_cast<const CGState*>(cg));
 }
 
 void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s) {

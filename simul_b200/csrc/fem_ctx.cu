@@ -709,7 +709,7 @@ cudaError_t enqueue_cg_iter(FemCtx* c, int kind, bool fused) {
   }
   if (kind == GRAPH_TWO_LEVEL) {
     const CoarseArgs ca = coarse_args(c);
-    launch_update_restrict(ca, c->x, c->r, c->p, c->y, c->cg, c->red(), SITE_CGU, c->stream);
+    launch_update_restrict(ca, c->x, c->r, c->p, c->y, c->cg, c->stream);
     launch_coarse_solve(ca, c->cg, c->stream);
     launch_tl_rz(ca, false, c->r, c->dinv, c->tmpf, c->p, c->cg, c->red(), SITE_RZ, c->stream);
     // with the recurrence the next matvec forms the direction
@@ -944,6 +944,7 @@ int coarse_alloc(FemCtx* c, T** dst, size_t n) {
 // coarse operator).  Elements go to the cell of their centroid; a node to the
 // cell of its lowest-numbered element.
 constexpr int kMaxCoarseNodes = 4096;
+static_assert(kMaxCoarseNodes <= 65535, "node_corners packs coarse node ids in 16 bits");
 
 int build_coarse(FemCtx* c) {
   const int Nn = c->Nn, Ne = c->Ne;
@@ -1090,6 +1091,11 @@ int build_coarse(FemCtx* c) {
     if ((st = coarse_alloc(c, &lat, (size_t)Nn))) return st;
     cd.node_lat = lat;
     launch_coarse_node_lat(c->mesh(), cd, lat, c->stream);
+    CKL();
+    uint4* corners = nullptr;
+    if ((st = coarse_alloc(c, &corners, (size_t)Nn))) return st;
+    cd.node_corners = corners;
+    launch_coarse_node_corners(c->mesh(), cd, corners, c->stream);
     CKL();
   }
   const size_t nd = (size_t)cd.n_dof;

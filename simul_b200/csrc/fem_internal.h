@@ -158,6 +158,7 @@ struct CoarseDev {
   const int* cell_elems;
   const int* node_cell;     // [Nn]
   const float4* node_lat;   // [Nn] local coordinates in the node's cell (xyz), the cell (w, int bits)
+  const uint4* node_corners;  // [Nn] the cell's 8 corner coarse nodes, 16 bits each (n_cn <= 65535)
   const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
   double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
@@ -281,10 +282,10 @@ void launch_diag(const DiagArgs& a, int model, cudaStream_t s);
 size_t coarse_cell_smem();
 int coarse_cell_slices();   // CTAs (and Galerkin block slots) per lattice cell
 int coarse_restrict_slices(int n_cells);  // node slices (restriction warps) per lattice cell
-// x += alpha p, r -= alpha q, ||r||^2 + convergence test, and the restriction
-// of the new r into cell_r (one kernel)
+// x += alpha p, r -= alpha q and the restriction of the new r into cell_r
+// (one kernel; ||r||^2 and the convergence test follow in tl_rz)
 void launch_update_restrict(const CoarseArgs& a, float* x, float* r, const float* p, const float* q, CGState* cg,
-                            Reduce red, int site, cudaStream_t s);
+                            cudaStream_t s);
 // r_c from cell_r, then y_c = Ainv r_c
 void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s);
 void prepare_coarse_kernels(int model, int n_dof);
@@ -293,6 +294,8 @@ void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
 // Ainv = FP32 symmetric copy of the lower triangle left in Ac
 // fills node_lat from X32, node_cell and cell_ijk
 void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, cudaStream_t s);
+// fills node_corners from node_cell and cell_corner
+void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out, cudaStream_t s);
 // kernels one coarse product launches (1 FP32, 2 packed BF16)
 int coarse_product_kernels(const CoarseDev& c);
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);

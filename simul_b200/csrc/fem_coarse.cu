@@ -554,6 +554,7 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
     rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
     rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
   }
+  chain_release();
   double v[2];
   v[0] = block_sum<256>(rz, sred);
   v[1] = INIT ? 0.0 : block_sum<256>(rr, sred);

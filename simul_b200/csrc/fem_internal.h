@@ -20,6 +20,14 @@ __device__ __forceinline__ void chain_enter() {
 #endif
 }
 
+// Lets the next chain kernel be scheduled: called once a kernel's memory
+// traffic is issued and only its block reduction is left.
+__device__ __forceinline__ void chain_release() {
+#if defined(__CUDA_ARCH__)
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
 // Whether launches from this host thread use programmatic dependent launch
 // (set around graph capture of the CG iteration chain).
 inline bool& chain_pdl() {

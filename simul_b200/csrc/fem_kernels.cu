@@ -430,6 +430,7 @@ __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant_
     }
   }
   if (CG) {
+    chain_release();
     double bsum = block_sum<256>(pap, sred);
     if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
       double tot = final_sum<256>(a.red, a.red_site, 0, sred);

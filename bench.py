@@ -59,9 +59,9 @@ def parse():
                     help="tangent-matvec variant (auto: timed on the first solve)")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
     ap.add_argument("--coarse-reuse", type=int, default=0,
-                    help="PCG solves one coarse-operator assembly serves (0: adaptive)")
-    ap.add_argument("--coarse-cell", type=int, default=4,
-                    help="coarse lattice cell edge in voxels (4: 7,728 coarse DOFs on the n = 64 body)")
+                    help="coarse operator rebuilds: 0 once per solve from rest, k every k PCG solves, -1 adaptive")
+    ap.add_argument("--coarse-cell", type=int, default=5,
+                    help="coarse lattice cell edge in voxels (5: 4,323 coarse DOFs on the n = 64 body)")
     ap.add_argument("--coarse-bf16", type=int, default=1,
                     help="store the coarse inverse in BF16 (packed lower block triangle)")
     ap.add_argument("--whole-solve-graph", type=int, default=1,

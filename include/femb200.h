@@ -153,10 +153,13 @@ enum {
    * the cube root of 5x the mean element volume, i.e. the voxel edge of
    * 5-tet voxel meshes); grown automatically past 4096 coarse nodes */
   FEM_OPT_COARSE_CELL = 2,
-  /* two-level preconditioner: PCG solves one coarse assembly serves; 0
-   * (default) = adaptive: the operator is rebuilt at the next tangent once a
-   * solve needs 1.5x the CG iterations per decade of residual reduction
-   * measured right after the last assembly */
+  /* two-level preconditioner: when the coarse operator is rebuilt.  0
+   * (default): once per state - at the first two-level solve after a history
+   * reset, a materials change or a new constraint pattern, then kept for the
+   * whole load path; k >= 1: every k PCG solves; -1: adaptive - rebuilt at
+   * the next tangent once a solve needs 1.5x the CG iterations per decade of
+   * residual reduction measured right after the last assembly, until a
+   * rebuild fails to cut that rate by 20 % */
   FEM_OPT_COARSE_REUSE = 3,
   /* learned preconditioner: 1 (default) adds the two-level coarse correction
    * to the network's output, 0 uses the network alone */
@@ -349,6 +352,8 @@ int fem_dot_f64_noalloc(const double* a, const double* b, int64_t n, double* res
 
 /* ---- J2 history (j2_plasticity.py:103-123, 513-520) ---- */
 int fem_commit_history(void* ctx);
+/* back to rest: zero history; also discards the two-level coarse operator
+ * (the next two-level solve assembles one for the new tangent) */
 int fem_reset_history(void* ctx);
 /* plastic strain (n_elements,3,3) and equivalent plastic strain (n_elements),
  * committed state; either may be NULL. */

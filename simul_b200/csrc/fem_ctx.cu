@@ -165,8 +165,10 @@ struct FemCtx {
   bool coarse_valid = false;   // Ainv matches the current tangent policy
   int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
   bool coarse_bf16 = false;    // store the coarse inverse in BF16
-  int coarse_reuse = 0;        // PCG solves one assembly serves; 0 = adaptive
+  int coarse_reuse = 0;        // PCG solves one assembly serves; 0 = once per state, -1 = adaptive
   double coarse_base_ipd = -1;  // CG iterations per decade right after the last assembly
+  double coarse_trigger_ipd = -1;  // the rate that triggered the last adaptive refresh
+  bool coarse_refresh_off = false; // a refresh did not help: keep the operator until the next reset
   int coarse_uses = 0;
   double coarse_H = 0.0;
   int64_t n_coarse_assemblies = 0;
@@ -839,6 +841,8 @@ int drop_coarse(FemCtx* c) {
   c->tl_part = nullptr;
   c->coarse_built = false;
   c->coarse_valid = false;
+  c->coarse_trigger_ipd = -1;
+  c->coarse_refresh_off = false;
   for (int k : {GRAPH_TWO_LEVEL, GRAPH_LEARNED}) {
     if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
     if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
@@ -846,6 +850,15 @@ int drop_coarse(FemCtx* c) {
     c->loop_graph[k] = nullptr;
   }
   return FEM_OK;
+}
+
+// The coarse operator no longer matches the problem (new state, materials
+// or constraints): the next two-level solve assembles one, and the adaptive
+// refresh starts over.
+void invalidate_coarse(FemCtx* c) {
+  c->coarse_valid = false;
+  c->coarse_trigger_ipd = -1;
+  c->coarse_refresh_off = false;
 }
 
 int ensure_cg_graph(FemCtx* c, int kind) {
@@ -1148,7 +1161,7 @@ int build_coarse(FemCtx* c) {
 int ensure_coarse(FemCtx* c) {
   int st;
   if (!c->coarse_built && (st = build_coarse(c))) return st;
-  if (c->coarse_valid && (c->coarse_reuse == 0 || c->coarse_uses < c->coarse_reuse)) {
+  if (c->coarse_valid && (c->coarse_reuse <= 0 || c->coarse_uses < c->coarse_reuse)) {
     ++c->coarse_uses;
     return FEM_OK;
   }
@@ -1435,16 +1448,24 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   }
   const CGState& h = *c->h_cg;
   c->n_cg_iters += h.iter;
-  if ((tl || (learned && c->learned_coarse)) && c->coarse_reuse == 0 && h.done == 1 && h.rr0 > 0 && h.rr > 0) {
+  if ((tl || (learned && c->learned_coarse)) && c->coarse_reuse < 0 && h.done == 1 && h.rr0 > 0 && h.rr > 0) {
     // adaptive reuse: iterations per decade of residual reduction; once a
     // solve needs 1.5x the rate measured right after the assembly, the coarse
-    // operator is rebuilt at the next tangent
+    // operator is rebuilt at the next tangent.  A refresh that does not bring
+    // the rate down by 20 % switches refreshing off until the next reset
+    // (state, materials or constraint pattern): on the vertebral body the
+    // operator of the first, elastic tangent serves the whole plastic load
+    // path as well as fresh ones.
     const double decades = std::max(0.5 * std::log10(h.rr0 / h.rr), 0.25);
     const double ipd = h.iter / decades;
-    if (c->coarse_base_ipd < 0)
+    if (c->coarse_base_ipd < 0) {
       c->coarse_base_ipd = ipd;
-    else if (ipd > 1.5 * c->coarse_base_ipd + 2.0)
+      if (c->coarse_trigger_ipd > 0 && ipd > 0.8 * c->coarse_trigger_ipd) c->coarse_refresh_off = true;
+      c->coarse_trigger_ipd = -1;
+    } else if (!c->coarse_refresh_off && ipd > 1.5 * c->coarse_base_ipd + 2.0) {
       c->coarse_valid = false;
+      c->coarse_trigger_ipd = ipd;
+    }
   }
   // kernels that did work: 3 (Jacobi), 6 (two-level) or 11 + 2 (learned,
   // + coarse) per CG iteration; the rest of a batch exits at entry
@@ -1675,8 +1696,8 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       c->fused_step = value != 0;
       return FEM_OK;
     case FEM_OPT_COARSE_REUSE:
-      if (value < 0 || value > (1 << 20))
-        return set_err(c, FEM_ERR_INVALID, "coarse reuse count %lld not in [0, 2^20]", (long long)value);
+      if (value < -1 || value > (1 << 20))
+        return set_err(c, FEM_ERR_INVALID, "coarse reuse count %lld not in [-1, 2^20]", (long long)value);
       c->coarse_reuse = (int)value;
       return FEM_OK;
     default:
@@ -1969,7 +1990,7 @@ int fem_set_materials(void* ctx, const FemMaterial* table, int32_t n, const uint
   c->has_j2 = has_j2;
   c->materials_set = true;
   c->tangent_valid = false;
-  c->coarse_valid = false;
+  invalidate_coarse(c);
   return FEM_OK;
 }
 
@@ -1989,7 +2010,7 @@ int fem_set_bc(void* ctx, const uint8_t* fixed_mask, const double* fixed_values,
     CK(cudaStreamSynchronize(c->stream));
     if (now != c->fixed_host) {
       c->fixed_host.swap(now);
-      c->coarse_valid = false;
+      invalidate_coarse(c);
     }
   }
   if (fixed_values) {
@@ -2494,6 +2515,9 @@ int fem_reset_history(void* ctx) {
   CK(cudaMemsetAsync(c->epe_t, 0, (size_t)c->Ne * sizeof(double), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->tangent_valid = false;
+  // back to rest: the coarse operator was built on a deformed, plastic
+  // tangent; the next two-level solve assembles a fresh one
+  invalidate_coarse(c);
   return FEM_OK;
 }
 

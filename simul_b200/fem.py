@@ -164,9 +164,10 @@ class FEMesh:
                 "last_assembly_kernels_ms": out[6], "reuse": int(out[7])}
 
     def set_coarse_options(self, cell=None, reuse=None, bf16=None):
-        """Two-level preconditioner: lattice cell edge in mesh lengths, the
-        number of PCG solves one coarse assembly serves (0: adaptive), and
-        whether the coarse inverse is stored in BF16."""
+        """Two-level preconditioner: lattice cell edge in mesh lengths, when
+        the coarse operator is rebuilt (0: once per state - after a history
+        reset, materials or constraint change; k >= 1: every k PCG solves;
+        -1: adaptive), and whether the coarse inverse is stored in BF16."""
         lib = _lib.load()
         if bf16 is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_BF16, 1 if bf16 else 0), self.ctx,

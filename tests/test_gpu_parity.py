@@ -441,9 +441,10 @@ def test_fused_step_grid_stride_on_larger_mesh(cuda):
     assert _rel_l2(u_f, u_c) < 1e-4
 
 
-@pytest.mark.parametrize("reuse", [0, 1])
+@pytest.mark.parametrize("reuse", [0, 1, -1])
 def test_newton_j2_two_level_matches_oracle(cuda, vox, reuse):
-    """reuse 0: adaptive coarse-operator reuse; 1: rebuilt for every PCG solve."""
+    """reuse 0: one coarse operator for the whole load path; 1: rebuilt for
+    every PCG solve; -1: adaptive refresh."""
     ref = np.load(G.path_of("vox12_j2_steps"))
     mesh = make_mesh(vox.X, vox.conn, cuda)
     mesh.set_coarse_options(reuse=reuse)
@@ -460,6 +461,8 @@ def test_newton_j2_two_level_matches_oracle(cuda, vox, reuse):
         assert _rel_l2(mesh.get_displacements(), ref["u_steps"][k]) < 1e-6
     n_asm = mesh.coarse_info()["assemblies"]
     assert n_asm >= (ref["u_steps"].shape[0] if reuse == 1 else 1)
+    if reuse == 0:
+        assert n_asm == 1
 
 
 def test_newton_bar_matches_oracle(cuda, bar):

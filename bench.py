@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--whole-solve-graph", type=int, default=1,
                     help="1: one graph launch per PCG solve; 0: fixed-size iteration graphs (for kernel profilers)")
     ap.add_argument("--pdl", type=int, default=1, help="programmatic dependent launches in the CG graphs")
+    ap.add_argument("--coarse-inverse", default="trsm_syrk", choices=["trsm_syrk", "potri"],
+                    help="coarse inverse from the Cholesky factor")
     ap.add_argument("--block-smoother", type=int, default=1,
                     help="two-level smoother: 1 nodal 3x3 block inverse, 0 diagonal inverse")
     ap.add_argument("--fused-step", type=int, default=0,
@@ -275,7 +277,8 @@ def main():
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond, cg_rtol_min=args.cg_rtol_min,
                             cg_rtol_max=args.cg_rtol_max)
-    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16))
+    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16),
+                            inverse=args.coarse_inverse)
     if args.matvec_variant != "auto":
         mesh.set_matvec_variant(args.matvec_variant)
     mesh.set_fused_step(bool(args.fused_step))

@@ -190,7 +190,11 @@ enum {
   /* two-level preconditioner smoother: 1 (default) the inverse of each
    * node's 3 x 3 diagonal block of K_T (free DOFs), 0 the inverse of the
    * diagonal */
-  FEM_OPT_BLOCK_JACOBI = 10
+  FEM_OPT_BLOCK_JACOBI = 10,
+  /* two-level coarse inverse from the FP64 Cholesky factor L: 1 (default)
+   * W = L^-1 by a triangular solve against the identity, then the lower
+   * triangle of W^T W (cuBLAS trsm + syrk); 0 cuSOLVER potri */
+  FEM_OPT_COARSE_INVERSE = 11
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

@@ -46,6 +46,7 @@ FEM_OPT_WHOLE_SOLVE_GRAPH = 7
 FEM_OPT_PDL = 8
 FEM_OPT_DIRECTION_RECURRENCE = 9
 FEM_OPT_BLOCK_JACOBI = 10
+FEM_OPT_COARSE_INVERSE = 11
 MPNN_PARAMS = 34307
 MATVEC_VARIANTS = {0: "fused", 1: "two_phase"}
 

@@ -896,6 +896,16 @@ void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out
 
 int coarse_product_kernels(const CoarseDev& c) { return c.Ainv16 ? 2 : 1; }
 
+__global__ void identity_d_kernel(double* w, int n) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (int64_t)n * n) return;
+  w[q] = (q / n == q % n) ? 1.0 : 0.0;
+}
+
+void launch_identity_d(double* w, int n, cudaStream_t s) {
+  identity_d_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(w, n);
+}
+
 // Resident CTAs of the tile product on this device (one wave, tiles looped).
 int tile_mv_grid() {
   static int grid = 0;

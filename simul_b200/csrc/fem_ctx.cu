@@ -5,6 +5,7 @@
 // element kernels use.  Callers keep their own numbering: every per-call array
 // is permuted on entry and exit.
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
 #include <algorithm>
@@ -179,6 +180,12 @@ struct FemCtx {
   std::vector<void*> coarse_bufs;
   cusolverDnHandle_t solver = nullptr;
   double* sol_work = nullptr;
+  // coarse inverse from the Cholesky factor: 1 (default) W = L^-1 by a
+  // triangular solve with n right-hand sides, then Ac^-1 = W^T W (cuBLAS
+  // trsm + syrk, GEMM-rich); 0 cuSOLVER potri
+  int coarse_inverse = 1;
+  cublasHandle_t blas = nullptr;
+  double* coarse_w = nullptr;  // [n_dof^2] W = L^-1
   int sol_lwork = 0;
   int* sol_info = nullptr;
   int* h_info = nullptr;
@@ -309,6 +316,8 @@ void free_ctx(FemCtx* c) {
     if (p) cudaFree(p);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->sol_work) cudaFree(c->sol_work);
+  if (c->coarse_w) cudaFree(c->coarse_w);
+  if (c->blas) cublasDestroy(c->blas);
   if (c->sol_info) cudaFree(c->sol_info);
   if (c->h_info) cudaFreeHost(c->h_info);
   if (c->solver) cusolverDnDestroy(c->solver);
@@ -839,6 +848,8 @@ int drop_coarse(FemCtx* c) {
   c->coarse_bufs.clear();
   c->cdev = CoarseDev{};
   c->tl_part = nullptr;
+  if (c->coarse_w) cudaFree(c->coarse_w);
+  c->coarse_w = nullptr;
   c->coarse_built = false;
   c->coarse_valid = false;
   c->coarse_trigger_ipd = -1;
@@ -1184,9 +1195,26 @@ int ensure_coarse(FemCtx* c) {
   CK(cudaStreamSynchronize(c->stream));
   if (*c->h_info != 0)
     return set_err(c, FEM_ERR_NAN, "coarse operator is not positive definite (potrf info %d)", *c->h_info);
-  if (cusolverDnDpotri(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
-                       c->sol_info) != CUSOLVER_STATUS_SUCCESS)
+  if (c->coarse_inverse == 1) {
+    // W = L^-1 (L W = I), then the lower triangle of W^T W = Ac^-1 into Ac
+    if (!c->blas) {
+      if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return set_err(c, FEM_ERR_CUDA, "cublasCreate failed");
+    }
+    cublasSetStream(c->blas, c->stream);
+    if (!c->coarse_w) CK(cudaMalloc(reinterpret_cast<void**>(&c->coarse_w), sizeof(double) * (size_t)n * n));
+    launch_identity_d(c->coarse_w, n, c->stream);
+    CKL();
+    const double one = 1.0, zero = 0.0;
+    if (cublasDtrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n, &one,
+                    c->cdev.Ac, n, c->coarse_w, n) != CUBLAS_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cublasDtrsm failed to launch");
+    if (cublasDsyrk(c->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &one, c->coarse_w, n, &zero, c->cdev.Ac,
+                    n) != CUBLAS_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cublasDsyrk failed to launch");
+  } else if (cusolverDnDpotri(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
+                              c->sol_info) != CUSOLVER_STATUS_SUCCESS) {
     return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotri failed to launch");
+  }
   launch_coarse_symmetrize(c->cdev, c->stream);
   ++c->n_launches;
   CKL();
@@ -1678,6 +1706,10 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
         }
         c->use_loop_graph = value != 0;
       }
+      return FEM_OK;
+    case FEM_OPT_COARSE_INVERSE:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "coarse inverse method must be 0 or 1");
+      c->coarse_inverse = (int)value;
       return FEM_OK;
     case FEM_OPT_BLOCK_JACOBI:
       if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "block smoother flag must be 0 or 1");

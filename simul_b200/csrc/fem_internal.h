@@ -304,6 +304,8 @@ void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
 void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, cudaStream_t s);
 // fills node_corners from node_cell and cell_corner
 void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out, cudaStream_t s);
+// w = the n x n identity (FP64, column-major)
+void launch_identity_d(double* w, int n, cudaStream_t s);
 // kernels one coarse product launches (1 FP32, 2 packed BF16)
 int coarse_product_kernels(const CoarseDev& c);
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);

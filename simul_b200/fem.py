@@ -163,12 +163,16 @@ class FEMesh:
                 "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5],
                 "last_assembly_kernels_ms": out[6], "reuse": int(out[7])}
 
-    def set_coarse_options(self, cell=None, reuse=None, bf16=None):
+    def set_coarse_options(self, cell=None, reuse=None, bf16=None, inverse=None):
         """Two-level preconditioner: lattice cell edge in mesh lengths, when
         the coarse operator is rebuilt (0: once per state - after a history
         reset, materials or constraint change; k >= 1: every k PCG solves;
-        -1: adaptive), and whether the coarse inverse is stored in BF16."""
+        -1: adaptive), whether the coarse inverse is stored in BF16, and how
+        it is formed from the Cholesky factor ("trsm_syrk" or "potri")."""
         lib = _lib.load()
+        if inverse is not None:
+            code = {"potri": 0, "trsm_syrk": 1}[inverse]
+            _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_INVERSE, code), self.ctx, "fem_set_option")
         if bf16 is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_BF16, 1 if bf16 else 0), self.ctx,
                    "fem_set_option")

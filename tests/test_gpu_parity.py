@@ -377,6 +377,34 @@ def test_block_smoother_matches_oracle_with_no_more_iterations(cuda, vox, materi
         assert _rel_l2(out[True][0], u_ref) < 1e-6
 
 
+def test_coarse_inverse_methods_agree(cuda, vox):
+    """The coarse inverse formed as W^T W with W = L^-1 (cuBLAS trsm + syrk)
+    and by cuSOLVER potri precondition alike: the same solution, iteration
+    counts within one."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    lib = _lib.load()
+    rng = np.random.default_rng(61)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    r = dev(rhs, cuda)
+    out = {}
+    for method in ("potri", "trsm_syrk"):
+        mesh.set_coarse_options(cell=3, bf16=False, inverse=method, reuse=1)
+        du = torch.zeros_like(r)
+        it = C.c_int32()
+        rel = C.c_double()
+        rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, ptr(r), ptr(du), 1e-8, 20000, C.byref(it),
+                         C.byref(rel))
+        assert rc == 0, _lib.last_error(mesh.ctx)
+        out[method] = (du.cpu().numpy(), it.value)
+    assert abs(out["potri"][1] - out["trsm_syrk"][1]) <= 1, out
+    assert _rel_l2(out["potri"][0], out["trsm_syrk"][0]) < 1e-6
+
+
 def _pcg_fused_vs_chain(mesh, pc, rhs, cuda, rtol):
     lib = _lib.load()
     mesh.set_block_smoother(False)   # the fused step applies the diagonal smoother

@@ -60,14 +60,15 @@ def parse():
     ap.add_argument("--no-jacobi-baseline", action="store_true")
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="coarse operator rebuilds: 0 once per solve from rest, k every k PCG solves, -1 adaptive")
-    ap.add_argument("--coarse-cell", type=int, default=5,
-                    help="coarse lattice cell edge in voxels (5: 4,323 coarse DOFs on the n = 64 body)")
+    ap.add_argument("--coarse-cell", type=int, default=4,
+                    help="coarse lattice cell edge in voxels (4: 7,728 coarse DOFs on the n = 64 body)")
     ap.add_argument("--coarse-bf16", type=int, default=1,
                     help="store the coarse inverse in BF16 (packed lower block triangle)")
     ap.add_argument("--whole-solve-graph", type=int, default=1,
                     help="1: one graph launch per PCG solve; 0: fixed-size iteration graphs (for kernel profilers)")
     ap.add_argument("--pdl", type=int, default=1, help="programmatic dependent launches in the CG graphs")
-    ap.add_argument("--coarse-inverse", default="trsm_syrk", choices=["trsm_syrk", "potri"],
+    ap.add_argument("--coarse-inverse", default="trsm_syrk_tf32",
+                    choices=["trsm_syrk", "potri", "trsm_syrk_f32", "trsm_syrk_tf32"],
                     help="coarse inverse from the Cholesky factor")
     ap.add_argument("--block-smoother", type=int, default=1,
                     help="two-level smoother: 1 nodal 3x3 block inverse, 0 diagonal inverse")

@@ -191,9 +191,11 @@ enum {
    * node's 3 x 3 diagonal block of K_T (free DOFs), 0 the inverse of the
    * diagonal */
   FEM_OPT_BLOCK_JACOBI = 10,
-  /* two-level coarse inverse from the FP64 Cholesky factor L: 1 (default)
+  /* two-level coarse inverse from the Cholesky factor L: 1 (default) FP64,
    * W = L^-1 by a triangular solve against the identity, then the lower
-   * triangle of W^T W (cuBLAS trsm + syrk); 0 cuSOLVER potri */
+   * triangle of W^T W (cuBLAS trsm + syrk); 0 FP64 cuSOLVER potri; 2 the
+   * same as 1 in FP32; 3 FP32 factor, trsm and syrk on TF32 tensor cores
+   * (for the BF16 inverse, whose rounding is coarser than TF32's) */
   FEM_OPT_COARSE_INVERSE = 11
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);

@@ -205,7 +205,7 @@ __global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
   if (q >= (int64_t)n * n) return;
   const int row = (int)(q / n), col = (int)(q % n);
   const int lo = max(row, col), hi = min(row, col);
-  c.Ainv[q] = (float)c.Ac[(size_t)hi * n + lo];
+  c.Ainv[q] = c.Ac32 ? c.Ac32[(size_t)hi * n + lo] : (float)c.Ac[(size_t)hi * n + lo];
 }
 
 constexpr int kTile = 64;
@@ -233,7 +233,7 @@ __global__ void coarse_pack16_kernel(const __grid_constant__ CoarseDev c) {
   float v = 0.f;
   if (row < n && col < n) {
     const int lo = max(row, col), hi = min(row, col);
-    v = (float)c.Ac[(size_t)hi * n + lo];
+    v = c.Ac32 ? c.Ac32[(size_t)hi * n + lo] : (float)c.Ac[(size_t)hi * n + lo];
   }
   c.Ainv16[q] = __float2bfloat16_rn(v);
 }
@@ -904,6 +904,27 @@ __global__ void identity_d_kernel(double* w, int n) {
 
 void launch_identity_d(double* w, int n, cudaStream_t s) {
   identity_d_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(w, n);
+}
+
+__global__ void identity_f_kernel(float* w, int n) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (int64_t)n * n) return;
+  w[q] = (q / n == q % n) ? 1.f : 0.f;
+}
+
+void launch_identity_f(float* w, int n, cudaStream_t s) {
+  identity_f_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(w, n);
+}
+
+__global__ void lower_to_f32_kernel(const double* a, float* out, int n) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (int64_t)n * n) return;
+  const int col = (int)(q / n), row = (int)(q % n);
+  out[q] = row >= col ? (float)a[q] : 0.f;
+}
+
+void launch_lower_to_f32(const double* a, float* out, int n, cudaStream_t s) {
+  lower_to_f32_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(a, out, n);
 }
 
 // Resident CTAs of the tile product on this device (one wave, tiles looped).

@@ -182,7 +182,8 @@ struct FemCtx {
   double* sol_work = nullptr;
   // coarse inverse from the Cholesky factor: 1 (default) W = L^-1 by a
   // triangular solve with n right-hand sides, then Ac^-1 = W^T W (cuBLAS
-  // trsm + syrk, GEMM-rich); 0 cuSOLVER potri
+  // trsm + syrk, GEMM-rich); 0 cuSOLVER potri; 2 / 3 as 1 in FP32 / with
+  // TF32 tensor cores
   int coarse_inverse = 1;
   cublasHandle_t blas = nullptr;
   double* coarse_w = nullptr;  // [n_dof^2] W = L^-1
@@ -1188,6 +1189,63 @@ int ensure_coarse(FemCtx* c) {
   CKL();
   CK(cudaEventRecord(em, c->stream));
   const int n = c->cdev.n_dof;
+  c->cdev.Ac32 = nullptr;
+  if (c->coarse_inverse >= 2) {
+    // FP32: Cholesky, W = L^-1, W^T W, all in single precision (the inverse
+    // is rounded to BF16 or FP32 afterwards anyway)
+    if (!c->blas) {
+      if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return set_err(c, FEM_ERR_CUDA, "cublasCreate failed");
+    }
+    cublasSetStream(c->blas, c->stream);
+    if (!c->coarse_w) CK(cudaMalloc(reinterpret_cast<void**>(&c->coarse_w), sizeof(double) * (size_t)n * n));
+    float* a32 = reinterpret_cast<float*>(c->coarse_w);
+    float* w32 = a32 + (size_t)n * n;
+    launch_lower_to_f32(c->cdev.Ac, a32, n, c->stream);
+    launch_identity_f(w32, n, c->stream);
+    CKL();
+    int lws = 0;
+    if (cusolverDnSpotrf_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, n, a32, n, &lws) != CUSOLVER_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cusolverDnSpotrf_bufferSize failed");
+    if ((lws + 1) / 2 > c->sol_lwork) {
+      CK(cudaStreamSynchronize(c->stream));
+      if (c->sol_work) cudaFree(c->sol_work);
+      c->sol_work = nullptr;
+      c->sol_lwork = (lws + 1) / 2;
+      CK(cudaMalloc(reinterpret_cast<void**>(&c->sol_work), sizeof(double) * (size_t)c->sol_lwork));
+    }
+    if (cusolverDnSpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, a32, n, reinterpret_cast<float*>(c->sol_work), lws,
+                         c->sol_info) != CUSOLVER_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cusolverDnSpotrf failed to launch");
+    CK(cudaMemcpyAsync(c->h_info, c->sol_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (*c->h_info != 0)
+      return set_err(c, FEM_ERR_NAN, "coarse operator is not positive definite in FP32 (potrf info %d)", *c->h_info);
+    const float one = 1.f, zero = 0.f;
+    // method 3: the triangular solve and the product on TF32 tensor cores
+    cublasSetMathMode(c->blas, c->coarse_inverse == 3 ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_DEFAULT_MATH);
+    if (cublasStrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n, &one,
+                    a32, n, w32, n) != CUBLAS_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cublasStrsm failed to launch");
+    if (cublasSsyrk(c->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &one, w32, n, &zero, a32, n) !=
+        CUBLAS_STATUS_SUCCESS)
+      return set_err(c, FEM_ERR_CUDA, "cublasSsyrk failed to launch");
+    c->cdev.Ac32 = a32;
+    launch_coarse_symmetrize(c->cdev, c->stream);
+    ++c->n_launches;
+    CKL();
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f, ms_asm = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventElapsedTime(&ms_asm, e0, em);
+    c->coarse_ms_last = ms;
+    c->coarse_ms_assembly = ms_asm;
+    ++c->n_coarse_assemblies;
+    c->coarse_valid = true;
+    c->coarse_uses = 1;
+    c->coarse_base_ipd = -1;
+    return FEM_OK;
+  }
   if (cusolverDnDpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
                        c->sol_info) != CUSOLVER_STATUS_SUCCESS)
     return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotrf failed to launch");
@@ -1708,7 +1766,7 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       }
       return FEM_OK;
     case FEM_OPT_COARSE_INVERSE:
-      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "coarse inverse method must be 0 or 1");
+      if (value < 0 || value > 3) return set_err(c, FEM_ERR_INVALID, "coarse inverse method must be 0 to 3");
       c->coarse_inverse = (int)value;
       return FEM_OK;
     case FEM_OPT_BLOCK_JACOBI:

@@ -170,6 +170,7 @@ struct CoarseDev {
   const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
   double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
+  const float* Ac32;        // non-null: the inverse's lower triangle is here in FP32 instead (FP32 inversion)
   float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric), or null
   // BF16 inverse, or null: the lower block triangle of 64 x 64 tiles, tile
   // (I, J), I >= J, at index I (I + 1) / 2 + J, row-major inside the tile,
@@ -306,6 +307,10 @@ void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, c
 void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out, cudaStream_t s);
 // w = the n x n identity (FP64, column-major)
 void launch_identity_d(double* w, int n, cudaStream_t s);
+// w = the n x n identity (FP32, column-major)
+void launch_identity_f(float* w, int n, cudaStream_t s);
+// out = the lower triangle of the FP64 column-major a, rounded to FP32
+void launch_lower_to_f32(const double* a, float* out, int n, cudaStream_t s);
 // kernels one coarse product launches (1 FP32, 2 packed BF16)
 int coarse_product_kernels(const CoarseDev& c);
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);

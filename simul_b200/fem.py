@@ -168,10 +168,11 @@ class FEMesh:
         the coarse operator is rebuilt (0: once per state - after a history
         reset, materials or constraint change; k >= 1: every k PCG solves;
         -1: adaptive), whether the coarse inverse is stored in BF16, and how
-        it is formed from the Cholesky factor ("trsm_syrk" or "potri")."""
+        it is formed from the Cholesky factor ("trsm_syrk", "potri", or
+        "trsm_syrk_f32" in single precision)."""
         lib = _lib.load()
         if inverse is not None:
-            code = {"potri": 0, "trsm_syrk": 1}[inverse]
+            code = {"potri": 0, "trsm_syrk": 1, "trsm_syrk_f32": 2, "trsm_syrk_tf32": 3}[inverse]
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_INVERSE, code), self.ctx, "fem_set_option")
         if bf16 is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_BF16, 1 if bf16 else 0), self.ctx,

@@ -205,7 +205,7 @@ def cpu_leg(args, v, gpu_cg_total, threads):
     t = time.perf_counter()
     info = s.solve(v.fixed_mask, v.fixed_vals / args.load_steps, v.f_ext, tol=args.tol)
     dt = time.perf_counter() - t
-    return s.n_threads, dt, info
+    return s.n_threads, dt, info, s.u.copy()
 
 
 def reference_arm(args, rank, ws):
@@ -461,7 +461,20 @@ def main():
                          if rc == 0 else None}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = args.cpu_threads or os.cpu_count() or 1
-        nthr, dt, cinfo = cpu_leg(args, v, last["cg"], threads)
+        nthr, dt, cinfo, u_cpu = cpu_leg(args, v, last["cg"], threads)
+        # accuracy: the first load step from rest on the GPU (timed method)
+        # against the FP64 CPU restatement's solution of the same step
+        mesh.u.zero_()
+        mat.reset_state()
+        mesh.fixed.copy_(fixed_mask)
+        mesh.fixed_value.copy_(fixed_full * (1.0 / args.load_steps))
+        mesh._bc_dirty = True
+        r1 = solver.solve(verbose=False)
+        u_gpu = mesh.get_displacements()
+        line["accuracy"] = {"load_step": 1, "reference": "oracle/cpu_fem.cpp (FP64 Newton + PCG to the same tol)",
+                            "u_rel_l2": float(np.linalg.norm(u_gpu - u_cpu) / max(np.linalg.norm(u_cpu), 1e-300)),
+                            "gpu_relative_residual": r1["relative_residual"],
+                            "cpu_relative_residual": cinfo["relative_residual"]}
         # the port restates the plain method (Jacobi-PCG); scale its first load
         # step by the plain method's CG count on the GPU for the same solve
         ref_cg = jac["cg_iterations"] if jac else last["cg"]

@@ -305,6 +305,12 @@ int fem_compute_stress(void* ctx, const double* u, double* F_out, double* sigma_
  * residual of static_solver.py:161-172. */
 int fem_element_forces(void* ctx, const double* u, double* f_out, double* residual_out,
                        double* rnorm);
+/* Nodal von Mises stress (n_nodes, device) at displacement u (NULL = context
+ * u): per node the von Mises stress of every element on it, added in a fixed
+ * order (no atomics); average = 0 keeps the sum, as compute_mises_stress
+ * leaves it (core/mesh.py:459-492, returned by StaticSolver.get_mises_stress,
+ * static_solver.py:512-515), average = 1 divides by the element count. */
+int fem_nodal_mises(void* ctx, const double* u, double* mises_out, int32_t average);
 /* y = K_T x with the consistent tangent at the last fem_element_forces state;
  * fixed DOFs of x are ignored and of y zeroed (FP32).  Matrix-free
  * replacement of _assemble_tangent_stiffness (static_solver.py:349-397,

@@ -799,6 +799,25 @@ def consistent_newton(mesh: Mesh, mat: Material, f_ext, fixed_mask, fixed_vals, 
                "relative_residual": rel, "history": history}
 
 
+def nodal_mises(mesh: Mesh, mat: Material, u, j2_state=None, average=False):
+    """core/mesh.py:459-492: per node the von Mises stress of each element on
+    it, summed (the reference never divides; ``average`` divides by the
+    element count)."""
+    F, sigma, P, f, aux = internal_state(mesh, mat, u, j2_state)
+    s = sigma
+    vm = np.sqrt(0.5 * ((s[:, 0, 0] - s[:, 1, 1]) ** 2 + (s[:, 1, 1] - s[:, 2, 2]) ** 2 +
+                        (s[:, 2, 2] - s[:, 0, 0]) ** 2 +
+                        6.0 * (s[:, 0, 1] ** 2 + s[:, 1, 2] ** 2 + s[:, 0, 2] ** 2)))
+    conn = np.asarray(mesh.conn, dtype=np.int64)
+    out = np.zeros(mesh.X.shape[0])
+    np.add.at(out, conn.reshape(-1), np.repeat(vm, 4))
+    if average:
+        cnt = np.zeros(mesh.X.shape[0])
+        np.add.at(cnt, conn.reshape(-1), 1.0)
+        out = out / np.maximum(cnt, 1.0)
+    return out
+
+
 def strain_energy(mesh: Mesh, mat: Material, u):
     """Total strain energy for NH / LE (neo_hookean.py:193-226, energy_balance)."""
     F = deformation_gradient(u, mesh.conn, mesh.dNdX)

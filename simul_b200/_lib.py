@@ -128,6 +128,7 @@ SIGNATURES = {
     "fem_compute_stress": (C.c_int, [_VP, _VP, _VP, _VP]),
     "fem_element_forces": (C.c_int, [_VP, _VP, _VP, _VP, _DP]),
     "fem_tangent_matvec": (C.c_int, [_VP, _VP, _VP]),
+    "fem_nodal_mises": (C.c_int, [_VP, _VP, _VP, C.c_int32]),
     "fem_pcg": (C.c_int, [_VP, C.c_int32, _VP, _VP, C.c_double, C.c_int32,
                           C.POINTER(C.c_int32), _DP]),
     "fem_newton_solve": (C.c_int, [_VP, C.POINTER(FemSolveParams), C.POINTER(FemSolveResult)]),

@@ -2274,6 +2274,30 @@ int fem_compute_stress(void* ctx, const double* u, double* F_out, double* sigma_
   return FEM_OK;
 }
 
+int fem_nodal_mises(void* ctx, const double* u, double* mises_out, int32_t average) {
+  FemCtx* c = static_cast<FemCtx*>(ctx);
+  int st;
+  if ((st = check_ctx(c))) return st;
+  if (!mises_out) return set_err(c, FEM_ERR_INVALID, "mises_out is null");
+  if (average != 0 && average != 1) return set_err(c, FEM_ERR_INVALID, "average must be 0 or 1");
+  if (!c->materials_set) return set_err(c, FEM_ERR_STATE, "materials not set");
+  if (u) {
+    ++c->n_launches; launch_gather_d(u, c->u, c->d_perm_node, c->Nn, c->stream);
+    CKL();
+  }
+  double* sig = nullptr;
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&sig), sizeof(double) * 9 * (size_t)c->Ne, c->stream));
+  ++c->n_launches; launch_stress(c->mesh(), c->matD, c->model_kind, c->u, c->ep_c, c->epe_c, c->d_perm_elem,
+                                 nullptr, sig, c->stream);
+  ++c->n_launches; launch_nodal_mises(c->mesh(), c->d_perm_elem, c->d_perm_node, sig, average, mises_out,
+                                      c->stream);
+  const cudaError_t e = cudaGetLastError();
+  cudaFreeAsync(sig, c->stream);
+  if (e != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "nodal Mises kernels failed: %s", cudaGetErrorString(e));
+  CK(cudaStreamSynchronize(c->stream));
+  return FEM_OK;
+}
+
 int fem_element_forces(void* ctx, const double* u, double* f_out, double* residual_out, double* rnorm) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   int st;

@@ -369,6 +369,9 @@ void launch_cg_pupdate(float* p, const float* r, const float* dinv, int n_nodes,
 void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
                    const double* ep_c, const double* epe_c, const int* perm_elem, double* F_out,
                    double* sig_out, cudaStream_t s);
+// nodal von Mises from caller-order element stresses (sum, or average)
+void launch_nodal_mises(const MeshDev& m, const int* perm_elem, const int* perm_node, const double* sig_user,
+                        int average, double* out_user, cudaStream_t s);
 void launch_refq(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol,
                  cudaStream_t s);
 // out[n*3+d] (internal) = in[perm[n]*3+d] (caller order) and back

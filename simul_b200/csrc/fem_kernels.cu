@@ -756,6 +756,31 @@ __global__ void stress_kernel(const MeshDev m, const DevMat<double>* matD, const
   }
 }
 
+// Nodal von Mises stress: per node, the von Mises stress of each element on
+// it (from the elements' Cauchy stresses in caller order) added in the
+// node's fixed slot order; average = 1 divides by the number of elements.
+// Written in caller node order.  core/mesh.py:459-492 accumulates the sum
+// with atomics and never divides (its average step is a comment).
+__global__ void nodal_mises_kernel(const MeshDev m, const int* perm_elem, const int* perm_node,
+                                   const double* sig_user, int average, double* out_user) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= m.n_nodes) return;
+  const int b = n / m.nb;
+  const int base = m.blk_ptr[b];
+  const int j0 = m.node_row[n], j1 = m.node_row[n + 1];
+  double acc = 0.0;
+  for (int j = j0; j < j1; ++j) {
+    const int li = (int)(m.node_slots[j] >> 2);
+    const int e = m.blk_elems[base + li];
+    const double* s = sig_user + (size_t)9 * perm_elem[e];
+    const double s11 = s[0], s22 = s[4], s33 = s[8], s12 = s[1], s23 = s[5], s13 = s[2];
+    acc += sqrt(0.5 * ((s11 - s22) * (s11 - s22) + (s22 - s33) * (s22 - s33) + (s33 - s11) * (s33 - s11) +
+                       6.0 * (s12 * s12 + s23 * s23 + s13 * s13)));
+  }
+  if (average && j1 > j0) acc /= (double)(j1 - j0);
+  out_user[perm_node[n]] = acc;
+}
+
 __global__ void refq_kernel(const MeshDev m, const int* perm_elem, double* dNdX, double* vol) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= m.n_elems) return;
@@ -1084,6 +1109,11 @@ void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, cons
     case M_J2: stress_kernel<M_J2><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
     default: stress_kernel<-1><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
   }
+}
+
+void launch_nodal_mises(const MeshDev& m, const int* perm_elem, const int* perm_node, const double* sig_user,
+                        int average, double* out_user, cudaStream_t s) {
+  nodal_mises_kernel<<<nblk(m.n_nodes, 256), 256, 0, s>>>(m, perm_elem, perm_node, sig_user, average, out_user);
 }
 
 void launch_refq(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol,

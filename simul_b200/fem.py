@@ -316,6 +316,19 @@ class FEMesh:
     def get_stress(self) -> np.ndarray:
         return self.stress.detach().cpu().numpy()
 
+    def compute_mises_stress(self, average: bool = False):
+        """Nodal von Mises stress into ``self.mises`` (core/mesh.py:459-492):
+        per node the von Mises stress of every element on it, added in a
+        fixed order.  The reference leaves the sum (its averaging step is a
+        comment); ``average=True`` divides by the element count."""
+        if self._bound_material is None:
+            raise FEAValidationError("bind a material first (compute_stress / compute_nodal_forces)",
+                                     parameter="material")
+        if getattr(self, "mises", None) is None:
+            self.mises = torch.zeros(self.n_nodes, dtype=torch.float64, device=self.device)
+        _check(_lib.load().fem_nodal_mises(self.ctx, _ptr(self.u.contiguous()), _ptr(self.mises), int(average)),
+               self.ctx, "fem_nodal_mises")
+
 
 # ───────────────────────── materials ─────────────────────────
 
@@ -761,6 +774,13 @@ class StaticSolver:
         if res.cancelled:
             out["cancelled"] = True
         return out
+
+    def get_mises_stress(self) -> np.ndarray:
+        """Nodal von Mises stress (static_solver.py:512-515, summed as the
+        reference leaves it)."""
+        self._bind()
+        self.mesh.compute_mises_stress()
+        return self.mesh.mises.cpu().numpy()
 
     def get_total_energy(self) -> float:
         raise NotImplementedError("strain energy is not part of the B200 path")

@@ -44,3 +44,19 @@ def test_nodal_mises_j2_through_static_solver(cuda):
     want = O.nodal_mises(O.Mesh(vox.X, vox.conn), om, ref["u"])
     # the return map rounds a little differently on each side near the yield surface
     assert np.max(np.abs(got - want)) <= 1e-8 * np.max(np.abs(want))
+
+
+def test_export_mesh_result_writes_gpu_fields(cuda, tmp_path):
+    import xml.etree.ElementTree as ET
+    from simul_b200.vtk_export import export_mesh_result
+    bar = meshgen.cantilever_bar(nx=4, ny=2, nz=2)
+    mesh = B.FEMesh(bar.n_nodes, bar.n_elements, device=cuda)
+    mesh.initialize_from_numpy(bar.X, bar.conn)
+    mat = B.NeoHookean(17e3, 0.3)
+    u = np.random.default_rng(8).standard_normal(bar.X.shape) * 0.01
+    mesh.u.copy_(torch.from_numpy(u))
+    path = export_mesh_result(str(tmp_path / "bar"), mesh, mat, binary=False)
+    arrays = {el.get("Name"): el for el in ET.parse(path).getroot().iter("DataArray")}
+    vm = np.array(arrays["von_mises"].text.split(), dtype=np.float64)
+    ref = O.nodal_mises(O.Mesh(bar.X, bar.conn), O.Material("neo_hookean", E=17e3, nu=0.3), u)
+    assert np.max(np.abs(vm - ref)) <= 1e-9 * np.max(np.abs(ref))

@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--coarse-inverse", default="trsm_syrk_tf32",
                     choices=["trsm_syrk", "potri", "trsm_syrk_f32", "trsm_syrk_tf32"],
                     help="coarse inverse from the Cholesky factor")
+    ap.add_argument("--coarse-max-nodes", type=int, default=6144, help="cap on the coarse lattice's nodes")
     ap.add_argument("--block-smoother", type=int, default=1,
                     help="two-level smoother: 1 nodal 3x3 block inverse, 0 diagonal inverse")
     ap.add_argument("--fused-step", type=int, default=0,
@@ -279,7 +280,7 @@ def main():
     solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond, cg_rtol_min=args.cg_rtol_min,
                             cg_rtol_max=args.cg_rtol_max)
     mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16),
-                            inverse=args.coarse_inverse)
+                            inverse=args.coarse_inverse, max_nodes=args.coarse_max_nodes)
     if args.matvec_variant != "auto":
         mesh.set_matvec_variant(args.matvec_variant)
     mesh.set_fused_step(bool(args.fused_step))

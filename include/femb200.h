@@ -196,7 +196,10 @@ enum {
    * triangle of W^T W (cuBLAS trsm + syrk); 0 FP64 cuSOLVER potri; 2 the
    * same as 1 in FP32; 3 FP32 factor, trsm and syrk on TF32 tensor cores
    * (for the BF16 inverse, whose rounding is coarser than TF32's) */
-  FEM_OPT_COARSE_INVERSE = 11
+  FEM_OPT_COARSE_INVERSE = 11,
+  /* two-level: at most this many coarse nodes (default 4096, up to 16384);
+   * the lattice cell grows by 25 % steps until the lattice fits */
+  FEM_OPT_COARSE_MAX_NODES = 12
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

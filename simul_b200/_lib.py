@@ -47,6 +47,7 @@ FEM_OPT_PDL = 8
 FEM_OPT_DIRECTION_RECURRENCE = 9
 FEM_OPT_BLOCK_JACOBI = 10
 FEM_OPT_COARSE_INVERSE = 11
+FEM_OPT_COARSE_MAX_NODES = 12
 MPNN_PARAMS = 34307
 MATVEC_VARIANTS = {0: "fused", 1: "two_phase"}
 

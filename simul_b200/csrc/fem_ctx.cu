@@ -166,6 +166,7 @@ struct FemCtx {
   bool coarse_valid = false;   // Ainv matches the current tangent policy
   int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
   bool coarse_bf16 = false;    // store the coarse inverse in BF16
+  int coarse_max_nodes = 4096; // the lattice cell grows until at most this many coarse nodes remain
   int coarse_reuse = 0;        // PCG solves one assembly serves; 0 = once per state, -1 = adaptive
   double coarse_base_ipd = -1;  // CG iterations per decade right after the last assembly
   double coarse_trigger_ipd = -1;  // the rate that triggered the last adaptive refresh
@@ -961,15 +962,15 @@ int coarse_alloc(FemCtx* c, T** dst, size_t n) {
 
 // Builds the coarse lattice: cell edge H = coarse_cell_voxels x the mesh
 // length (cube root of 5 x the mean element volume: the voxel edge on
-// 5-tet voxel meshes), grown by 25 % steps until at most kMaxCoarseNodes
+// 5-tet voxel meshes), grown by 25 % steps until at most coarse_max_nodes
 // coarse nodes remain.  Along each axis the lattice overhangs the mesh by
 // less than one cell; the overhang is split between both ends in whole mesh
 // lengths, so no end cell holds a slab thinner than about H/2 (a thin end
 // slab leaves coarse nodes with almost no support and an ill-conditioned
 // coarse operator).  Elements go to the cell of their centroid; a node to the
 // cell of its lowest-numbered element.
-constexpr int kMaxCoarseNodes = 4096;
-static_assert(kMaxCoarseNodes <= 65535, "node_corners packs coarse node ids in 16 bits");
+constexpr int kMaxCoarseNodesLimit = 16384;
+static_assert(kMaxCoarseNodesLimit <= 65535, "node_corners packs coarse node ids in 16 bits");
 
 int build_coarse(FemCtx* c) {
   const int Nn = c->Nn, Ne = c->Ne;
@@ -1049,11 +1050,11 @@ int build_coarse(FemCtx* c) {
     n_cn = 0;
     for (int64_t l = 0; l < nlat; ++l)
       if (cn_of_lat[l] == 0) cn_of_lat[l] = n_cn++;
-    if (n_cn <= kMaxCoarseNodes) break;
+    if (n_cn <= c->coarse_max_nodes) break;
     H *= 1.25;
   }
-  if (n_cn > kMaxCoarseNodes)
-    return set_err(c, FEM_ERR_INVALID, "coarse lattice: could not reach %d coarse nodes", kMaxCoarseNodes);
+  if (n_cn > c->coarse_max_nodes)
+    return set_err(c, FEM_ERR_INVALID, "coarse lattice: could not reach %d coarse nodes", c->coarse_max_nodes);
   // tables
   std::vector<int3> cell_ijk(n_cells);
   std::vector<int> cell_corner(8 * (size_t)n_cells);
@@ -1763,6 +1764,15 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
           c->loop_graph[k] = nullptr;
         }
         c->use_loop_graph = value != 0;
+      }
+      return FEM_OK;
+    case FEM_OPT_COARSE_MAX_NODES:
+      if (value < 8 || value > kMaxCoarseNodesLimit)
+        return set_err(c, FEM_ERR_INVALID, "coarse node cap %lld not in [8, %d]", (long long)value,
+                       kMaxCoarseNodesLimit);
+      if (value != c->coarse_max_nodes) {
+        c->coarse_max_nodes = (int)value;
+        return drop_coarse(c);
       }
       return FEM_OK;
     case FEM_OPT_COARSE_INVERSE:

@@ -163,7 +163,7 @@ class FEMesh:
                 "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5],
                 "last_assembly_kernels_ms": out[6], "reuse": int(out[7])}
 
-    def set_coarse_options(self, cell=None, reuse=None, bf16=None, inverse=None):
+    def set_coarse_options(self, cell=None, reuse=None, bf16=None, inverse=None, max_nodes=None):
         """Two-level preconditioner: lattice cell edge in mesh lengths, when
         the coarse operator is rebuilt (0: once per state - after a history
         reset, materials or constraint change; k >= 1: every k PCG solves;
@@ -171,6 +171,9 @@ class FEMesh:
         it is formed from the Cholesky factor ("trsm_syrk", "potri", or
         "trsm_syrk_f32" in single precision)."""
         lib = _lib.load()
+        if max_nodes is not None:
+            _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_MAX_NODES, int(max_nodes)), self.ctx,
+                   "fem_set_option")
         if inverse is not None:
             code = {"potri": 0, "trsm_syrk": 1, "trsm_syrk_f32": 2, "trsm_syrk_tf32": 3}[inverse]
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_INVERSE, code), self.ctx, "fem_set_option")

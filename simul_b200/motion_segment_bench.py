@@ -44,6 +44,11 @@ def main(argv=None):
     ap.add_argument("--precond", default="two_level", choices=["jacobi", "two_level"])
     ap.add_argument("--line-search", default="reference", choices=["reference", "guarded", "none"])
     ap.add_argument("--max-iterations", type=int, default=50)
+    ap.add_argument("--coarse-cell", type=int, default=8)
+    ap.add_argument("--coarse-reuse", type=int, default=-1,
+                    help="coarse operator: 0 once per state, -1 adaptive refresh, k every k PCG solves")
+    ap.add_argument("--recurrence", type=int, default=1, help="two-level CG direction by recurrence")
+    ap.add_argument("--block-smoother", type=int, default=1, help="two-level nodal block smoother")
     args = ap.parse_args(argv)
     from simul_b200 import batch, meshgen
     import torch
@@ -56,7 +61,11 @@ def main(argv=None):
     t0 = time.perf_counter()
     insts = [batch.BatchInstance(ms.X, ms.conn, materials(ms.E), ms.fixed_mask, None,
                                  meshgen.top_moment_forces(ms.X, top, case, args.moment), device=dev,
-                                 material_ids=ids) for case in CASES]
+                                 material_ids=ids, coarse_cell=args.coarse_cell) for case in CASES]
+    for inst in insts:
+        inst.mesh.set_coarse_options(reuse=args.coarse_reuse)
+        inst.mesh.set_direction_recurrence(bool(args.recurrence))
+        inst.mesh.set_block_smoother(bool(args.block_smoother))
     t_setup = time.perf_counter() - t0
     kw = dict(precond=args.precond, line_search=args.line_search, max_iterations=args.max_iterations)
     batch.solve_batch(insts, load_steps=1, **kw)      # warm-up
@@ -70,6 +79,8 @@ def main(argv=None):
     res = {"tets": int(ms.n_elements), "nodes": int(ms.n_nodes), "disc_tets": ms.info["disc_elements"],
            "screw_tets": ms.info["screw_elements"], "moment_N_mm": args.moment, "load_steps": args.load_steps,
            "precond": args.precond, "line_search": args.line_search, "batch_wall_s": wall,
+           "coarse": {"cell_voxels": args.coarse_cell, "reuse": args.coarse_reuse},
+           "direction_recurrence": bool(args.recurrence), "block_smoother": bool(args.block_smoother),
            "host_generation_s": t_gen, "host_setup_s": t_setup,
            "cases": {}}
     for case, inst, r in zip(CASES, insts, out["instances"]):

@@ -59,7 +59,8 @@ def parse():
                     help="tangent-matvec variant (auto: timed on the first solve)")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
     ap.add_argument("--coarse-reuse", type=int, default=0,
-                    help="coarse operator rebuilds: 0 once per solve from rest, k every k PCG solves, -1 adaptive")
+                    help="coarse operator rebuilds: 0 once per solve from rest (this small-strain J2 path: "
+                         "the first operator serves the whole load path), k every k PCG solves, -1 adaptive")
     ap.add_argument("--coarse-cell", type=int, default=4,
                     help="coarse lattice cell edge in voxels (4: 7,728 coarse DOFs on the n = 64 body)")
     ap.add_argument("--coarse-bf16", type=int, default=1,

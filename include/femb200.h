@@ -153,13 +153,13 @@ enum {
    * the cube root of 5x the mean element volume, i.e. the voxel edge of
    * 5-tet voxel meshes); grown automatically past 4096 coarse nodes */
   FEM_OPT_COARSE_CELL = 2,
-  /* two-level preconditioner: when the coarse operator is rebuilt.  0
-   * (default): once per state - at the first two-level solve after a history
-   * reset, a materials change or a new constraint pattern, then kept for the
-   * whole load path; k >= 1: every k PCG solves; -1: adaptive - rebuilt at
-   * the next tangent once a solve needs 1.5x the CG iterations per decade of
-   * residual reduction measured right after the last assembly, until a
-   * rebuild fails to cut that rate by 20 % */
+  /* two-level preconditioner: when the coarse operator is rebuilt.  -1
+   * (default): adaptive - rebuilt at the next tangent once a solve needs
+   * 1.5x the CG iterations per decade of residual reduction measured right
+   * after the last assembly; 0: once per state - at the first two-level
+   * solve after a history reset, a materials change or a new constraint
+   * pattern, then kept for the whole load path; k >= 1: every k PCG solves.
+   * Any mode assembles afresh after such a reset or change. */
   FEM_OPT_COARSE_REUSE = 3,
   /* learned preconditioner: 1 (default) adds the two-level coarse correction
    * to the network's output, 0 uses the network alone */

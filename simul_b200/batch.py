@@ -24,7 +24,7 @@ class BatchInstance:
     """A mesh + material on a private stream, with its loads pushed."""
 
     def __init__(self, X, conn, material, fixed_mask, fixed_vals=None, f_ext=None, device=0,
-                 coarse_cell: int = 8, material_ids=None, coarse_bf16: bool = False):
+                 coarse_cell: int = 8, material_ids=None, coarse_bf16: bool = False, coarse_reuse=None):
         """``material`` is one material, or a dict {id: material} with
         ``material_ids`` giving each element's id (as StaticSolver's
         ``materials=``)."""
@@ -38,7 +38,7 @@ class BatchInstance:
         if f_ext is not None:
             self.mesh.set_nodal_forces(np.arange(X.shape[0]), f_ext)
         self.material = material
-        self.mesh.set_coarse_options(cell=coarse_cell, bf16=coarse_bf16)
+        self.mesh.set_coarse_options(cell=coarse_cell, bf16=coarse_bf16, reuse=coarse_reuse)
         torch.cuda.synchronize(self.mesh.device)
         if isinstance(material, dict):
             # binds the material table through a solver object (no solve)

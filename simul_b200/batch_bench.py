@@ -58,6 +58,8 @@ def main(argv=None):
     ap.add_argument("--workers", type=int, default=16, help="host processes generating meshes")
     ap.add_argument("--coarse-cell", type=int, default=4, help="two-level lattice cell edge in voxels")
     ap.add_argument("--coarse-bf16", type=int, default=1, help="packed BF16 coarse inverse")
+    ap.add_argument("--coarse-reuse", type=int, default=0,
+                    help="coarse operator: 0 once per solve from rest (small-strain J2), -1 adaptive")
     args = ap.parse_args(argv)
     rng = np.random.default_rng(args.seed)
     specs = []
@@ -79,7 +81,8 @@ def main(argv=None):
     def build(d):
         mat = B.J2Plasticity(d["E"], 0.3, 100.0, hardening_modulus=0.02 * d["E"])
         return batch.BatchInstance(d["X"], d["conn"], mat, d["fixed"], d["vals"], d["f"], device=dev,
-                                   coarse_cell=args.coarse_cell, coarse_bf16=bool(args.coarse_bf16))
+                                   coarse_cell=args.coarse_cell, coarse_bf16=bool(args.coarse_bf16),
+                                   coarse_reuse=args.coarse_reuse)
 
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=8) as ex:
@@ -103,7 +106,8 @@ def main(argv=None):
            "tets_min": int(min(d["tets"] for d in cases)), "tets_max": int(max(d["tets"] for d in cases)),
            "cases": {c: sum(1 for d in cases if d["case"] == c) for c in CASES},
            "load_steps": args.load_steps, "precond": args.precond,
-           "coarse": {"cell_voxels": args.coarse_cell, "inverse": "bf16" if args.coarse_bf16 else "f32"},
+           "coarse": {"cell_voxels": args.coarse_cell, "inverse": "bf16" if args.coarse_bf16 else "f32",
+                      "reuse": args.coarse_reuse},
            "all_converged": bool(all(r["converged"] for r in out["instances"])),
            "batch_wall_s": wall, "solves_per_s": args.instances / wall,
            "p50_instance_ms": float(np.percentile(ms, 50)), "p99_instance_ms": float(np.percentile(ms, 99)),

@@ -164,13 +164,13 @@ struct FemCtx {
   CoarseDev cdev{};
   bool coarse_built = false;
   bool coarse_valid = false;   // Ainv matches the current tangent policy
+  bool coarse_have_inverse = false;  // an inverse of this lattice has been formed
+  int64_t n_coarse_kept = 0;   // refreshes whose operator was not SPD (the last inverse kept)
   int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
   bool coarse_bf16 = false;    // store the coarse inverse in BF16
   int coarse_max_nodes = 4096; // the lattice cell grows until at most this many coarse nodes remain
-  int coarse_reuse = 0;        // PCG solves one assembly serves; 0 = once per state, -1 = adaptive
+  int coarse_reuse = -1;       // PCG solves one assembly serves; 0 = once per state, -1 = adaptive
   double coarse_base_ipd = -1;  // CG iterations per decade right after the last assembly
-  double coarse_trigger_ipd = -1;  // the rate that triggered the last adaptive refresh
-  bool coarse_refresh_off = false; // a refresh did not help: keep the operator until the next reset
   int coarse_uses = 0;
   double coarse_H = 0.0;
   int64_t n_coarse_assemblies = 0;
@@ -849,13 +849,12 @@ int drop_coarse(FemCtx* c) {
     if (p) cudaFree(p);
   c->coarse_bufs.clear();
   c->cdev = CoarseDev{};
+  c->coarse_have_inverse = false;
   c->tl_part = nullptr;
   if (c->coarse_w) cudaFree(c->coarse_w);
   c->coarse_w = nullptr;
   c->coarse_built = false;
   c->coarse_valid = false;
-  c->coarse_trigger_ipd = -1;
-  c->coarse_refresh_off = false;
   for (int k : {GRAPH_TWO_LEVEL, GRAPH_LEARNED}) {
     if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
     if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
@@ -866,13 +865,8 @@ int drop_coarse(FemCtx* c) {
 }
 
 // The coarse operator no longer matches the problem (new state, materials
-// or constraints): the next two-level solve assembles one, and the adaptive
-// refresh starts over.
-void invalidate_coarse(FemCtx* c) {
-  c->coarse_valid = false;
-  c->coarse_trigger_ipd = -1;
-  c->coarse_refresh_off = false;
-}
+// or constraints): the next two-level solve assembles one.
+void invalidate_coarse(FemCtx* c) { c->coarse_valid = false; }
 
 int ensure_cg_graph(FemCtx* c, int kind) {
   int st;
@@ -1168,6 +1162,20 @@ int build_coarse(FemCtx* c) {
   return FEM_OK;
 }
 
+// A refreshed coarse operator that is not positive definite (a tangent off
+// the stable path, e.g. an arc-length predictor): keep applying the last
+// inverse, which is still a symmetric positive definite preconditioner;
+// without one the solve fails.
+int keep_previous_coarse(FemCtx* c, int info) {
+  if (!c->coarse_have_inverse)
+    return set_err(c, FEM_ERR_NAN, "coarse operator is not positive definite (potrf info %d)", info);
+  ++c->n_coarse_kept;
+  c->coarse_valid = true;
+  c->coarse_uses = 1;
+  c->coarse_base_ipd = -1;
+  return FEM_OK;
+}
+
 // Assembles Ac = P^T K_T P at the current tangent and inverts it (FP64
 // Cholesky + inverse, then an FP32 or BF16 copy), unless the reuse policy keeps the
 // previous one.
@@ -1219,8 +1227,7 @@ int ensure_coarse(FemCtx* c) {
       return set_err(c, FEM_ERR_CUDA, "cusolverDnSpotrf failed to launch");
     CK(cudaMemcpyAsync(c->h_info, c->sol_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (*c->h_info != 0)
-      return set_err(c, FEM_ERR_NAN, "coarse operator is not positive definite in FP32 (potrf info %d)", *c->h_info);
+    if (*c->h_info != 0) return keep_previous_coarse(c, *c->h_info);
     const float one = 1.f, zero = 0.f;
     // method 3: the triangular solve and the product on TF32 tensor cores
     cublasSetMathMode(c->blas, c->coarse_inverse == 3 ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_DEFAULT_MATH);
@@ -1242,6 +1249,7 @@ int ensure_coarse(FemCtx* c) {
     c->coarse_ms_last = ms;
     c->coarse_ms_assembly = ms_asm;
     ++c->n_coarse_assemblies;
+    c->coarse_have_inverse = true;
     c->coarse_valid = true;
     c->coarse_uses = 1;
     c->coarse_base_ipd = -1;
@@ -1252,8 +1260,7 @@ int ensure_coarse(FemCtx* c) {
     return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotrf failed to launch");
   CK(cudaMemcpyAsync(c->h_info, c->sol_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (*c->h_info != 0)
-    return set_err(c, FEM_ERR_NAN, "coarse operator is not positive definite (potrf info %d)", *c->h_info);
+  if (*c->h_info != 0) return keep_previous_coarse(c, *c->h_info);
   if (c->coarse_inverse == 1) {
     // W = L^-1 (L W = I), then the lower triangle of W^T W = Ac^-1 into Ac
     if (!c->blas) {
@@ -1285,6 +1292,7 @@ int ensure_coarse(FemCtx* c) {
   c->coarse_ms_last = ms;
   c->coarse_ms_assembly = ms_asm;
   ++c->n_coarse_assemblies;
+  c->coarse_have_inverse = true;
   c->coarse_valid = true;
   c->coarse_uses = 1;
   c->coarse_base_ipd = -1;
@@ -1538,21 +1546,13 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if ((tl || (learned && c->learned_coarse)) && c->coarse_reuse < 0 && h.done == 1 && h.rr0 > 0 && h.rr > 0) {
     // adaptive reuse: iterations per decade of residual reduction; once a
     // solve needs 1.5x the rate measured right after the assembly, the coarse
-    // operator is rebuilt at the next tangent.  A refresh that does not bring
-    // the rate down by 20 % switches refreshing off until the next reset
-    // (state, materials or constraint pattern): on the vertebral body the
-    // operator of the first, elastic tangent serves the whole plastic load
-    // path as well as fresh ones.
+    // operator is rebuilt at the next tangent
     const double decades = std::max(0.5 * std::log10(h.rr0 / h.rr), 0.25);
     const double ipd = h.iter / decades;
-    if (c->coarse_base_ipd < 0) {
+    if (c->coarse_base_ipd < 0)
       c->coarse_base_ipd = ipd;
-      if (c->coarse_trigger_ipd > 0 && ipd > 0.8 * c->coarse_trigger_ipd) c->coarse_refresh_off = true;
-      c->coarse_trigger_ipd = -1;
-    } else if (!c->coarse_refresh_off && ipd > 1.5 * c->coarse_base_ipd + 2.0) {
+    else if (ipd > 1.5 * c->coarse_base_ipd + 2.0)
       c->coarse_valid = false;
-      c->coarse_trigger_ipd = ipd;
-    }
   }
   // kernels that did work: 3 (Jacobi), 6 (two-level) or 11 + 2 (learned,
   // + coarse) per CG iteration; the rest of a batch exits at entry

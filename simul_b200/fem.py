@@ -165,9 +165,9 @@ class FEMesh:
 
     def set_coarse_options(self, cell=None, reuse=None, bf16=None, inverse=None, max_nodes=None):
         """Two-level preconditioner: lattice cell edge in mesh lengths, when
-        the coarse operator is rebuilt (0: once per state - after a history
-        reset, materials or constraint change; k >= 1: every k PCG solves;
-        -1: adaptive), whether the coarse inverse is stored in BF16, and how
+        the coarse operator is rebuilt (-1, the default: adaptive; 0: once per
+        state - after a history reset, materials or constraint change; k >= 1:
+        every k PCG solves), whether the coarse inverse is stored in BF16, and how
         it is formed from the Cholesky factor ("trsm_syrk", "potri", or
         "trsm_syrk_f32" in single precision)."""
         lib = _lib.load()

@@ -1523,16 +1523,19 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     CKL();
   }
   const int max_batches = maxit / cg_batch(kind) + 2;
-  CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
   int batches = 0;
-  if (!c->h_cg->done && c->loop_graph[kind]) {
+  if (c->loop_graph[kind]) {
+    // no host check first: a state that is done already makes the body's
+    // kernels exit at entry and the condition kernel end the loop
     CK(cudaGraphLaunch(c->loop_graph[kind], c->stream));
     c->n_graphs++;
     c->n_loop_graphs++;
     CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     batches = max_batches;
+  } else {
+    CK(cudaMemcpyAsync(c->h_cg, c->cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
   }
   while (!c->h_cg->done && batches < max_batches) {
     CK(cudaGraphLaunch(c->cg_graph[kind], c->stream));

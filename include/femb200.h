@@ -261,8 +261,11 @@ int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t
 /* two-level preconditioner state: out[0] lattice cells, [1] coarse nodes,
  * [2] coarse DOFs, [3] cell edge, [4] assemblies so far, [5] ms of the last
  * assembly + factorisation (CUDA events), [6] ms of its assembly part,
- * [7] PCG solves one assembly serves */
-int fem_coarse_info(void* ctx, double* out8);
+ * [7] the rebuild policy (FEM_OPT_COARSE_REUSE), [8] refreshes whose
+ * operator was not positive definite (the last inverse kept), [9] two-level
+ * solves run as Jacobi-PCG because no positive definite coarse operator
+ * existed yet */
+int fem_coarse_info(void* ctx, double* out10);
 /* CG iteration launch structure: out[0] 1 while the fused-step option is on
  * and the runtime accepted it, [1] the captured Jacobi CG graph uses the
  * fused step, [2] the two-level one does, [3] warps per lattice cell in the

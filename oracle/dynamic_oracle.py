@@ -78,6 +78,13 @@ class DynamicOracle:
             return
         self._bc()
 
+    def natural_frequencies(self, n_modes=5):
+        """dynamic_solver.py:372-413 with the assembled K (fixed DOFs removed)."""
+        from scipy.sparse.linalg import eigsh
+        f = self.free
+        vals, _ = eigsh(self.K[f][:, f].tocsc(), k=n_modes, M=sparse.diags(self.M[f]), sigma=0, which="LM")
+        return np.sort(np.sqrt(np.abs(vals)) / (2 * np.pi))
+
     def energy(self):
         """Kinetic + strain energy of the linear system, 1/2 v'Mv + 1/2 u'Ku."""
         return 0.5 * float(np.sum(self.M * self.v ** 2)) + 0.5 * float(self.u @ (self.K @ self.u))

@@ -166,6 +166,7 @@ struct FemCtx {
   bool coarse_valid = false;   // Ainv matches the current tangent policy
   bool coarse_have_inverse = false;  // an inverse of this lattice has been formed
   int64_t n_coarse_kept = 0;   // refreshes whose operator was not SPD (the last inverse kept)
+  int64_t n_coarse_fallbacks = 0;  // two-level solves run as Jacobi-PCG (no SPD coarse operator)
   int coarse_cell_voxels = 8;  // lattice cell edge in mesh lengths
   bool coarse_bf16 = false;    // store the coarse inverse in BF16
   int coarse_max_nodes = 4096; // the lattice cell grows until at most this many coarse nodes remain
@@ -1496,7 +1497,15 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
   if (learned && !c->mpnn_has_weights)
     return set_err(c, FEM_ERR_STATE, "learned preconditioner has no weights (fem_mpnn_set_weights)");
   if ((st = compute_dinv(c, (tl || learned) ? FEM_PRECOND_JACOBI : precond, tl && c->block_jacobi))) return st;
-  if ((tl || (learned && c->learned_coarse)) && (st = ensure_coarse(c))) return st;
+  if (tl && (st = ensure_coarse(c))) {
+    // no positive definite coarse operator on this lattice yet (e.g. cells
+    // finer than the elements of an anisotropic mesh): this solve runs as
+    // Jacobi-PCG instead of failing
+    if (st != FEM_ERR_NAN) return st;
+    ++c->n_coarse_fallbacks;
+    return run_pcg(c, b_int, FEM_PRECOND_JACOBI, rtol, maxit, iters, rel);
+  }
+  if (learned && c->learned_coarse && (st = ensure_coarse(c))) return st;
   if (learned && (st = ensure_mpnn(c))) return st;
   if ((st = ensure_cg_graph(c, kind))) return st;
   const bool fused = (c->cg_graph_flags[kind] & 2) != 0;
@@ -1977,10 +1986,13 @@ int fem_mpnn_train(void* ctx, const float* R, const float* E, int32_t n_pairs, c
   return FEM_OK;
 }
 
-int fem_coarse_info(void* ctx, double* out8) {
+int fem_coarse_info(void* ctx, double* out10) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
-  if (!c || !out8) return FEM_ERR_INVALID;
-  double* out6 = out8;
+  if (!c || !out10) return FEM_ERR_INVALID;
+  double* out8 = out10;
+  double* out6 = out10;
+  out10[8] = (double)c->n_coarse_kept;
+  out10[9] = (double)c->n_coarse_fallbacks;
   out8[6] = c->coarse_ms_assembly;
   out8[7] = (double)c->coarse_reuse;
   out6[0] = c->cdev.n_cells;

@@ -157,11 +157,12 @@ class FEMesh:
                 "whole_solve_graphs": out[8], "whole_solve_graph_available": bool(out[9])}
 
     def coarse_info(self) -> dict:
-        out = (C.c_double * 8)()
+        out = (C.c_double * 10)()
         _check(_lib.load().fem_coarse_info(self.ctx, out), self.ctx, "fem_coarse_info")
         return {"cells": int(out[0]), "coarse_nodes": int(out[1]), "coarse_dofs": int(out[2]),
                 "cell_edge": out[3], "assemblies": int(out[4]), "last_assembly_ms": out[5],
-                "last_assembly_kernels_ms": out[6], "reuse": int(out[7])}
+                "last_assembly_kernels_ms": out[6], "reuse": int(out[7]), "refreshes_kept": int(out[8]),
+                "jacobi_fallbacks": int(out[9])}
 
     def set_coarse_options(self, cell=None, reuse=None, bf16=None, inverse=None, max_nodes=None):
         """Two-level preconditioner: lattice cell edge in mesh lengths, when

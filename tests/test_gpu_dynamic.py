@@ -45,3 +45,16 @@ def test_dynamic_solver_matches_oracle(cuda, method, formulation, steps):
     assert _rel(dyn.v.cpu().numpy(), ora.v) < 2e-5
     assert dyn.get_kinetic_energy() > 0.0
     assert np.allclose(dyn.get_displacements(), mesh.get_displacements())
+
+
+def test_natural_frequencies_match_oracle(cuda):
+    bar = meshgen.cantilever_bar(nx=8, ny=2, nz=2)
+    mesh = B.FEMesh(bar.n_nodes, bar.n_elements, device=cuda)
+    mesh.initialize_from_numpy(bar.X, bar.conn)
+    mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
+    dyn = DynamicSolver(mesh, B.LinearElastic(1000.0, 0.3), density=1e-3)
+    got = dyn.get_natural_frequencies(5)
+    ora = DynamicOracle(O.Mesh(bar.X, bar.conn), O.Material("linear_elastic", E=1000.0, nu=0.3), 1000.0, 0.3,
+                        bar.fixed_mask, density=1e-3)
+    want = ora.natural_frequencies(5)
+    assert np.all(np.abs(got - want) <= 1e-4 * want), (got, want)

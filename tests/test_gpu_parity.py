@@ -405,6 +405,42 @@ def test_coarse_inverse_methods_agree(cuda, vox):
     assert _rel_l2(out["potri"][0], out["trsm_syrk"][0]) < 1e-6
 
 
+@pytest.mark.parametrize("inverse", ["trsm_syrk_f32", "trsm_syrk_tf32"])
+def test_single_precision_coarse_inverse_tracks_fp64(cuda, vox, inverse):
+    """The coarse inverse formed in FP32 (and with TF32 tensor-core trsm /
+    syrk) for the BF16 packed copy preconditions like the FP64 one: the same
+    solution, iterations within 10 %; the node cap bounds the lattice."""
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mat = B.LinearElastic(1e3, 0.3)
+    idx = np.where(vox.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, np.zeros(idx.size))
+    mat.compute_nodal_forces(mesh)
+    lib = _lib.load()
+    rng = np.random.default_rng(81)
+    rhs = rng.standard_normal(vox.X.shape)
+    rhs[vox.fixed_mask] = 0.0
+    r = dev(rhs, cuda)
+    out = {}
+    for method in ("trsm_syrk", inverse):
+        mesh.set_coarse_options(cell=3, bf16=True, inverse=method, reuse=1)
+        du = torch.zeros_like(r)
+        it = C.c_int32()
+        rel = C.c_double()
+        rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, ptr(r), ptr(du), 1e-8, 20000, C.byref(it),
+                         C.byref(rel))
+        assert rc == 0, _lib.last_error(mesh.ctx)
+        out[method] = (du.cpu().numpy(), it.value)
+    assert out[inverse][1] <= 1.1 * out["trsm_syrk"][1] + 1, out
+    assert _rel_l2(out[inverse][0], out["trsm_syrk"][0]) < 1e-6
+    mesh.set_coarse_options(cell=1, max_nodes=64)
+    du = torch.zeros_like(r)
+    it, rel = C.c_int32(), C.c_double()
+    assert lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, ptr(r), ptr(du), 1e-8, 20000, C.byref(it),
+                       C.byref(rel)) == 0
+    info = mesh.coarse_info()
+    assert 0 < info["coarse_nodes"] <= 64 and info["cell_edge"] > 1.0
+
+
 def test_two_level_without_spd_coarse_operator_falls_back_to_jacobi(cuda):
     """Lattice cells finer than the elements of an anisotropic mesh (1.25 mm
     hexes, ~1 mm cells) give a singular coarse operator: the two-level solve

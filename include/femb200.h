@@ -69,16 +69,21 @@ enum {
 
 #define FEM_MAX_MATERIALS 16
 
-/* Mesh description: replaces FEMesh(n_nodes, n_elements, TET4) +
+/* Mesh description: replaces FEMesh(n_nodes, n_elements, TET4 | HEX8) +
  * initialize_from_numpy (core/mesh.py:25-121).  HOST pointers. */
 typedef struct {
   int64_t n_nodes;
   int64_t n_elements;
   const double* X;        /* (n_nodes, 3) reference coordinates */
-  const int32_t* conn;    /* (n_elements, 4) TET4 connectivity */
+  const int32_t* conn;    /* (n_elements, nodes_per_elem) connectivity */
   int32_t device;         /* CUDA device ordinal */
   int32_t nodes_per_block;/* 0 = default (256); 128 / 256 / 512 accepted */
   void* stream;           /* cudaStream_t; NULL = a context-owned stream */
+  int32_t nodes_per_elem; /* 0 or 4: TET4 (one Gauss point); 8: HEX8, vertex order of
+                             core/element.py:297-315, 2 x 2 x 2 Gauss points.  HEX8
+                             contexts solve with Jacobi / nodal block-Jacobi PCG: a
+                             two-level or learned request runs Jacobi-PCG and is counted
+                             in fem_coarse_info's jacobi_fallbacks */
 } FemMeshDesc;
 
 /* One material of the table: replaces the MaterialBase subclasses'
@@ -294,10 +299,11 @@ int fem_set_displacement(void* ctx, const double* u);
 int fem_get_displacement(void* ctx, double* u_out);
 
 /* ---- kernels ---- */
-/* dN/dX (n_elements,4,3) and Gauss volumes (n_elements) —
- * _compute_reference_quantities (core/mesh.py:123-151).  Either may be NULL. */
+/* dN/dX (n_points,npe,3) and Gauss volumes (n_points) —
+ * _compute_reference_quantities (core/mesh.py:123-151).  Either may be NULL.
+ * n_points = n_elements (TET4) or 8 n_elements (HEX8, point e * 8 + g). */
 int fem_reference_quantities(void* ctx, double* dNdX_out, double* vol_out);
-/* F (n_elements,3,3) and Cauchy stress (n_elements,3,3) at displacement u
+/* F (n_points,3,3) and Cauchy stress (n_points,3,3) at displacement u
  * (NULL = context u) — compute_deformation_gradient (core/mesh.py:293-313)
  * + MaterialBase.compute_stress (e.g. neo_hookean.py:91-129,
  * j2_plasticity.py:159-249; J2 starts from the committed history). */
@@ -312,7 +318,8 @@ int fem_compute_stress(void* ctx, const double* u, double* F_out, double* sigma_
 int fem_element_forces(void* ctx, const double* u, double* f_out, double* residual_out,
                        double* rnorm);
 /* Nodal von Mises stress (n_nodes, device) at displacement u (NULL = context
- * u): per node the von Mises stress of every element on it, added in a fixed
+ * u): per node the von Mises stress of every element on it (of the element's
+ * Gauss-point mean stress for HEX8), added in a fixed
  * order (no atomics); average = 0 keeps the sum, as compute_mises_stress
  * leaves it (core/mesh.py:459-492, returned by StaticSolver.get_mises_stress,
  * static_solver.py:512-515), average = 1 divides by the element count. */
@@ -373,7 +380,7 @@ int fem_commit_history(void* ctx);
 /* back to rest: zero history; also discards the two-level coarse operator
  * (the next two-level solve assembles one for the new tangent) */
 int fem_reset_history(void* ctx);
-/* plastic strain (n_elements,3,3) and equivalent plastic strain (n_elements),
+/* plastic strain (n_points,3,3) and equivalent plastic strain (n_points),
  * committed state; either may be NULL. */
 int fem_get_history(void* ctx, double* ep_out, double* epe_out);
 

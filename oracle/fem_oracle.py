@@ -1,11 +1,14 @@
-"""FP64 CPU oracle for the TET4 FEM static-solve path (TEST INFRASTRUCTURE ONLY).
+"""FP64 CPU oracle for the TET4 / HEX8 FEM static-solve path (TEST INFRASTRUCTURE ONLY).
 
 This module is the checker, never the product: only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference legs may
 import it.  The shipped solver (``simul_b200``) never routes through it.
 
 It restates, in NumPy FP64, the arithmetic of the reference's FEM hot path
-(monostylegc/simul, ``backend/fea/fem``) for 4-node tetrahedra:
+(monostylegc/simul, ``backend/fea/fem``) for 4-node tetrahedra (one Gauss
+point) and 8-node hexahedra (2 x 2 x 2 Gauss points, ``core/mesh.py:182-200,
+240-260``; every per-point array is ordered e * 8 + g as the reference's
+``gp_idx``):
 
 * reference quantities       ``core/mesh.py:123-151`` (+ ``:153-291`` for TET4)
 * deformation gradient       ``core/mesh.py:293-313``
@@ -58,6 +61,28 @@ DN_DXI_TET4 = np.array([[-1.0, -1.0, -1.0],
                         [0.0, 0.0, 1.0]])
 TET4_WEIGHT = 1.0 / 6.0  # one-point rule at (1/4, 1/4, 1/4), core/mesh.py:166-168
 J_FLOOR = 1e-8           # J_safe clamp, material/neo_hookean.py:119, :176-180
+# HEX8 natural node coordinates (core/element.py:297-315); the 2x2x2 Gauss
+# points carry the same sign pattern in the same order (core/mesh.py:182-200),
+# at the reference's rounded 1/sqrt(3) and weight 1.
+HEX8_SIGNS = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                       [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=np.float64)
+HEX8_GP = 0.5773502691896257
+
+
+def hex8_dN_dxi(xi):
+    """dN_a/d(xi, eta, zeta) at one natural point (core/mesh.py:240-260), (8,3)."""
+    s = HEX8_SIGNS
+    f = 1.0 + s * np.asarray(xi, dtype=np.float64)[None, :]
+    out = np.empty((8, 3))
+    out[:, 0] = 0.125 * s[:, 0] * f[:, 1] * f[:, 2]
+    out[:, 1] = 0.125 * f[:, 0] * s[:, 1] * f[:, 2]
+    out[:, 2] = 0.125 * f[:, 0] * f[:, 1] * s[:, 2]
+    return out
+
+
+def hex8_N(xi):
+    """Trilinear shape functions at one natural point, (8,)."""
+    return 0.125 * np.prod(1.0 + HEX8_SIGNS * np.asarray(xi, dtype=np.float64)[None, :], axis=1)
 PENALTY = 1e30           # solver/static_solver.py:501
 
 
@@ -73,11 +98,20 @@ class OracleConvergenceError(RuntimeError):
 # ─────────────────────────── geometry / kinematics ───────────────────────────
 
 def reference_quantities(X: np.ndarray, conn: np.ndarray):
-    """dN/dX (Ne,4,3) and Gauss volumes (Ne,) — core/mesh.py:123-151.
+    """dN/dX and Gauss volumes — core/mesh.py:123-151.  TET4: (Ne,4,3) and
+    (Ne,); HEX8: (Ne*8,8,3) and (Ne*8,), point e * 8 + g.
 
     J = sum_a X_a (x) dN_a/dxi, dNdX = dNdxi . J^-1, vol = w |det J|.
     """
-    Xe = X[conn]                                       # (Ne,4,3)
+    Xe = X[conn]                                       # (Ne,npe,3)
+    if conn.shape[1] == 8:
+        dN, vol = [], []
+        for g in range(8):
+            d = hex8_dN_dxi(HEX8_GP * HEX8_SIGNS[g])
+            J = np.einsum("eai,aj->eij", Xe, d)
+            dN.append(np.einsum("aj,ejk->eak", d, np.linalg.inv(J)))
+            vol.append(np.abs(np.linalg.det(J)))
+        return (np.stack(dN, axis=1).reshape(-1, 8, 3), np.stack(vol, axis=1).reshape(-1))
     J = np.einsum("eai,aj->eij", Xe, DN_DXI_TET4)
     detJ = np.linalg.det(J)
     Jinv = np.linalg.inv(J)
@@ -515,23 +549,25 @@ def tangent_A(mat, F, tang=None):
 
 
 def element_stiffness(A, dNdX, vol):
-    """K_e[(a,i),(b,k)] = sum_jl dN_a,j A_ijkl dN_b,l vol, (Ne,12,12)."""
+    """K_e[(a,i),(b,k)] = sum_jl dN_a,j A_ijkl dN_b,l vol, (Ne, 3 npe, 3 npe)."""
     Ke = np.einsum("eaj,eijkl,ebl,e->eaibk", dNdX, A, dNdX, vol)
-    return Ke.reshape(-1, 12, 12)
+    nd = 3 * dNdX.shape[1]
+    return Ke.reshape(-1, nd, nd)
 
 
 def assemble(Ke, conn, n_nodes):
-    dofs = (conn[:, :, None] * 3 + np.arange(3)[None, None, :]).reshape(-1, 12)
-    rows = np.repeat(dofs, 12, axis=1).ravel()
-    cols = np.tile(dofs, (1, 12)).ravel()
+    nd = Ke.shape[1]
+    dofs = (conn[:, :, None] * 3 + np.arange(3)[None, None, :]).reshape(-1, nd)
+    rows = np.repeat(dofs, nd, axis=1).ravel()
+    cols = np.tile(dofs, (1, nd)).ravel()
     return sp.coo_matrix((Ke.reshape(-1), (rows, cols)), shape=(3 * n_nodes, 3 * n_nodes)).tocsr()
 
 
 def solve_tangent(mat, F, tang, mesh, rhs, fixed_mask):
     """Direct FP64 solve of K_ff x_f = rhs_f (x = 0 on fixed DOFs): the exact
     answer the GPU PCG paths approximate."""
-    K = assemble(element_stiffness(tangent_A(mat, F, tang), mesh.dNdX, mesh.vol),
-                 np.asarray(mesh.conn, dtype=np.int64), mesh.X.shape[0])
+    K = assemble(element_stiffness(tangent_A(mesh.qmat(mat), F, tang), mesh.dNdX, mesh.vol),
+                 np.asarray(mesh.qconn, dtype=np.int64), mesh.X.shape[0])
     free = ~np.asarray(fixed_mask, dtype=bool).reshape(-1)
     x = np.zeros(K.shape[0])
     x[free] = spsolve(K[free][:, free].tocsc(), np.asarray(rhs, dtype=np.float64).reshape(-1)[free])
@@ -558,7 +594,12 @@ class Mesh:
     def __post_init__(self):
         self.X = np.asarray(self.X, dtype=np.float64)
         self.conn = np.asarray(self.conn, dtype=np.int64)
+        if self.conn.shape[1] not in (4, 8):
+            raise ValueError(f"elements must have 4 (TET4) or 8 (HEX8) nodes, got {self.conn.shape}")
         self.dNdX, self.vol = reference_quantities(self.X, self.conn)
+        self.ngp = 1 if self.conn.shape[1] == 4 else 8
+        # connectivity per integration point (point q = e * ngp + g)
+        self.qconn = self.conn if self.ngp == 1 else np.repeat(self.conn, self.ngp, axis=0)
 
     @property
     def n_nodes(self):
@@ -568,13 +609,36 @@ class Mesh:
     def n_elements(self):
         return self.conn.shape[0]
 
+    @property
+    def n_points(self):
+        """Integration points (the rows of F, stress and the J2 history)."""
+        return self.conn.shape[0] * self.ngp
+
+    @property
+    def elem_vol(self):
+        return self.vol.reshape(-1, self.ngp).sum(axis=1)
+
+    def qmat(self, mat):
+        """``mat`` with per-element arrays repeated for every integration point."""
+        if self.ngp == 1:
+            return mat
+        ne = self.n_elements
+        if isinstance(mat, MixedMaterial):
+            return MixedMaterial([self.qmat(p) for p in mat.parts], np.repeat(np.asarray(mat.ids), self.ngp))
+        kw = {}
+        for name in ("E", "nu", "C10", "C01", "D1", "sigma_y", "H", "fiber_E"):
+            v = getattr(mat, name)
+            kw[name] = np.repeat(v, self.ngp) if (v is not None and np.ndim(v) == 1 and np.size(v) == ne) else v
+        return Material(mat.model, C_voigt=mat.C_voigt, fiber_a=mat.fiber_a, **kw)
+
 
 def internal_state(mesh: Mesh, mat: Material, u, j2_state=None):
-    """F, sigma, P, negative internal force f (Nn,3), J2 aux."""
-    F = deformation_gradient(u, mesh.conn, mesh.dNdX)
+    """F, sigma, P (per integration point), negative internal force f (Nn,3), J2 aux."""
+    mat = mesh.qmat(mat)
+    F = deformation_gradient(u, mesh.qconn, mesh.dNdX)
     sigma, aux = cauchy_stress(mat, F, j2_state)
     P = first_piola(mat, F, sigma)
-    f = scatter_forces(element_forces(P, mesh.dNdX, mesh.vol), mesh.conn, mesh.n_nodes)
+    f = scatter_forces(element_forces(P, mesh.dNdX, mesh.vol), mesh.qconn, mesh.n_nodes)
     return F, sigma, P, f, aux
 
 
@@ -591,9 +655,9 @@ def residual(mesh, mat, u, f_ext, fixed_mask, j2_state=None):
 def reference_K_material(mesh: Mesh, C):
     """assembly.py:92-169 — ke = vol B^T C B with B rows [xx,yy,zz,xy,yz,xz]."""
     d = mesh.dNdX
-    ne = mesh.n_elements
-    B = np.zeros((ne, 6, 12))
-    for a in range(4):
+    ne, npe = d.shape[0], d.shape[1]
+    B = np.zeros((ne, 6, 3 * npe))
+    for a in range(npe):
         B[:, 0, 3 * a] = d[:, a, 0]
         B[:, 1, 3 * a + 1] = d[:, a, 1]
         B[:, 2, 3 * a + 2] = d[:, a, 2]
@@ -610,17 +674,19 @@ def reference_K_material(mesh: Mesh, C):
 def reference_K_geometric(mesh: Mesh, sigma):
     """assembly.py:220-287 — K_geo[a*3+d, b*3+d] = vol dN_a^T sigma dN_b."""
     kg = np.einsum("e,eai,eij,ebj->eab", mesh.vol, mesh.dNdX, sigma, mesh.dNdX)
-    Ke = np.zeros((mesh.n_elements, 12, 12))
+    nd = 3 * mesh.dNdX.shape[1]
+    Ke = np.zeros((mesh.dNdX.shape[0], nd, nd))
     for dd in range(3):
         Ke[:, dd::3, dd::3] = kg
     return _assemble_filtered(Ke, mesh)
 
 
 def _assemble_filtered(Ke, mesh):
-    conn = mesh.conn
-    dofs = (conn[:, :, None] * 3 + np.arange(3)[None, None, :]).reshape(-1, 12)
-    rows = np.repeat(dofs, 12, axis=1).ravel()
-    cols = np.tile(dofs, (1, 12)).ravel()
+    conn = getattr(mesh, "qconn", mesh.conn)
+    nd = Ke.shape[1]
+    dofs = (conn[:, :, None] * 3 + np.arange(3)[None, None, :]).reshape(-1, nd)
+    rows = np.repeat(dofs, nd, axis=1).ravel()
+    cols = np.tile(dofs, (1, nd)).ravel()
     vals = Ke.reshape(-1)
     m = np.abs(vals) > 1e-20
     n = 3 * mesh.n_nodes
@@ -641,14 +707,16 @@ def reference_newton(mesh: Mesh, mat: Material, f_ext, fixed_mask, fixed_vals, u
     fixed_dofs = np.where(fixed_mask.reshape(-1))[0]
     fext = f_ext.reshape(-1)
 
+    qmat = mesh.qmat(mat)
+
     def eval_state(uu):
-        F = deformation_gradient(uu, mesh.conn, mesh.dNdX)
-        sigma, aux = cauchy_stress(mat, F, j2_state)
+        F = deformation_gradient(uu, mesh.qconn, mesh.dNdX)
+        sigma, aux = cauchy_stress(qmat, F, j2_state)
         if aux is not None:                           # Q1: in-place history update
             j2_state.ep[...] = aux[0].ep
             j2_state.epe[...] = aux[0].epe
-        P = first_piola(mat, F, sigma)
-        f = scatter_forces(element_forces(P, mesh.dNdX, mesh.vol), mesh.conn, mesh.n_nodes)
+        P = first_piola(qmat, F, sigma)
+        f = scatter_forces(element_forces(P, mesh.dNdX, mesh.vol), mesh.qconn, mesh.n_nodes)
         return sigma, f.reshape(-1)
 
     ref = None
@@ -702,7 +770,9 @@ def _multi_material_K(mesh, C_map, material_ids):
         if not np.any(sel):
             continue
         sub = Mesh.__new__(Mesh)
-        sub.X, sub.conn, sub.dNdX, sub.vol = mesh.X, mesh.conn[sel], mesh.dNdX[sel], mesh.vol[sel]
+        qsel = np.repeat(sel, mesh.ngp)
+        sub.X, sub.conn, sub.dNdX, sub.vol = mesh.X, mesh.conn[sel], mesh.dNdX[qsel], mesh.vol[qsel]
+        sub.qconn = mesh.qconn[qsel]
         Kp = reference_K_material(sub, C)
         K = Kp if K is None else K + Kp
     return K
@@ -730,19 +800,21 @@ def consistent_newton(mesh: Mesh, mat: Material, f_ext, fixed_mask, fixed_vals, 
     free = np.where(~fixed_mask.reshape(-1))[0]
     base = j2_state.copy() if j2_state is not None else None
 
+    qmat = mesh.qmat(mat)
+
     def evaluate(uu):
-        F = deformation_gradient(uu, mesh.conn, mesh.dNdX)
-        sigma, aux = cauchy_stress(mat, F, base)
-        P = first_piola(mat, F, sigma)
-        f = scatter_forces(element_forces(P, mesh.dNdX, mesh.vol), mesh.conn, mesh.n_nodes)
+        F = deformation_gradient(uu, mesh.qconn, mesh.dNdX)
+        sigma, aux = cauchy_stress(qmat, F, base)
+        P = first_piola(qmat, F, sigma)
+        f = scatter_forces(element_forces(P, mesh.dNdX, mesh.vol), mesh.qconn, mesh.n_nodes)
         R = f_ext + f
         R[fixed_mask] = 0.0
         return R, F, aux
 
     def tangent(F, aux):
         tang = aux[1] if aux is not None else None
-        return assemble(element_stiffness(tangent_A(mat, F, tang), mesh.dNdX, mesh.vol),
-                        mesh.conn, mesh.n_nodes)
+        return assemble(element_stiffness(tangent_A(qmat, F, tang), mesh.dNdX, mesh.vol),
+                        mesh.qconn, mesh.n_nodes)
 
     dc = np.zeros_like(u)
     dc[fixed_mask] = fixed_vals[fixed_mask] - u[fixed_mask]
@@ -801,16 +873,16 @@ def consistent_newton(mesh: Mesh, mat: Material, f_ext, fixed_mask, fixed_vals, 
 
 def nodal_mises(mesh: Mesh, mat: Material, u, j2_state=None, average=False):
     """core/mesh.py:459-492: per node the von Mises stress of each element on
-    it, summed (the reference never divides; ``average`` divides by the
-    element count)."""
+    it (of the element's Gauss-point mean stress), summed (the reference never
+    divides; ``average`` divides by the element count)."""
     F, sigma, P, f, aux = internal_state(mesh, mat, u, j2_state)
-    s = sigma
+    s = sigma.reshape(-1, mesh.ngp, 3, 3).sum(axis=1) / float(mesh.ngp)
     vm = np.sqrt(0.5 * ((s[:, 0, 0] - s[:, 1, 1]) ** 2 + (s[:, 1, 1] - s[:, 2, 2]) ** 2 +
                         (s[:, 2, 2] - s[:, 0, 0]) ** 2 +
                         6.0 * (s[:, 0, 1] ** 2 + s[:, 1, 2] ** 2 + s[:, 0, 2] ** 2)))
     conn = np.asarray(mesh.conn, dtype=np.int64)
     out = np.zeros(mesh.X.shape[0])
-    np.add.at(out, conn.reshape(-1), np.repeat(vm, 4))
+    np.add.at(out, conn.reshape(-1), np.repeat(vm, conn.shape[1]))
     if average:
         cnt = np.zeros(mesh.X.shape[0])
         np.add.at(cnt, conn.reshape(-1), 1.0)
@@ -820,7 +892,8 @@ def nodal_mises(mesh: Mesh, mat: Material, u, j2_state=None, average=False):
 
 def strain_energy(mesh: Mesh, mat: Material, u):
     """Total strain energy for NH / LE (neo_hookean.py:193-226, energy_balance)."""
-    F = deformation_gradient(u, mesh.conn, mesh.dNdX)
+    F = deformation_gradient(u, mesh.qconn, mesh.dNdX)
+    mat = mesh.qmat(mat)
     mu, lam = lame(mat.E, mat.nu)
     if mat.model == "neo_hookean":
         J = np.maximum(np.linalg.det(F), J_FLOOR)

@@ -56,7 +56,7 @@ class FemMeshDesc(C.Structure):
     _fields_ = [("n_nodes", C.c_int64), ("n_elements", C.c_int64),
                 ("X", C.POINTER(C.c_double)), ("conn", C.POINTER(C.c_int32)),
                 ("device", C.c_int32), ("nodes_per_block", C.c_int32),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("nodes_per_elem", C.c_int32)]
 
 
 class FemMaterial(C.Structure):

@@ -46,6 +46,10 @@ struct FemCtx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int Nn = 0, Ne = 0, nb = 256, n_blocks = 0;
+  int npe = 4;                 // nodes per element: 4 TET4, 8 HEX8
+  int ngp = 1;                 // Gauss points per element: 1 TET4, 8 HEX8
+  size_t Nq = 0;               // integration points Ne * ngp (payload and J2 history rows)
+  double* stage_d = nullptr;   // HEX8 residual: element slot forces in node_slots order
   int ndof = 0, ndof_pad = 0;
   int64_t blk_entries = 0;
   size_t bytes = 0;
@@ -218,6 +222,8 @@ struct FemCtx {
     m.fixed = fixed;
     m.max_slots = max_slots;
     m.spos = spos;
+    m.npe = npe;
+    m.slot_shift = npe == 8 ? 3 : 2;
     return m;
   }
   Reduce red() const {
@@ -327,6 +333,7 @@ void free_ctx(FemCtx* c) {
   for (cudaEvent_t ev : c->coarse_ev)
     if (ev) cudaEventDestroy(ev);
   if (c->stage) cudaFree(c->stage);
+  if (c->stage_d) cudaFree(c->stage_d);
   if (c->spos) cudaFree(c->spos);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
@@ -370,13 +377,16 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   // elements: home block = block of the lowest internal node, then Morton of centroid
   std::vector<int> home(Ne);
   std::vector<uint32_t> ecode(Ne);
+  const int npe = c->npe;
+  const int sh = npe == 8 ? 3 : 2;              // slot bits in the (element, slot) codes
+  const uint32_t smask = (1u << sh) - 1u;
   for (int e = 0; e < Ne; ++e) {
     int mn = Nn;
     double cen[3] = {0, 0, 0};
-    for (int k = 0; k < 4; ++k) {
-      const int nu = conn_user[4 * e + k];
+    for (int k = 0; k < npe; ++k) {
+      const int nu = conn_user[npe * e + k];
       mn = std::min(mn, iperm[nu]);
-      for (int d = 0; d < 3; ++d) cen[d] += 0.25 * X[3 * nu + d];
+      for (int d = 0; d < 3; ++d) cen[d] += X[3 * nu + d] / npe;
     }
     home[e] = mn / nb;
     ecode[e] = qz.code(cen);
@@ -387,26 +397,28 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
     if (home[a] != home[b]) return home[a] < home[b];
     return ecode[a] < ecode[b];
   });
-  std::vector<int4> conn(Ne);
+  // npe / 4 int4 per element (HEX8: vertices 0-3, then 4-7)
+  const int cw = npe / 4;
+  std::vector<int4> conn((size_t)cw * Ne);
   std::vector<int> ehome(Ne);
   for (int e = 0; e < Ne; ++e) {
     const int eu = c->perm_elem[e];
-    conn[e] = make_int4(iperm[conn_user[4 * eu]], iperm[conn_user[4 * eu + 1]],
-                        iperm[conn_user[4 * eu + 2]], iperm[conn_user[4 * eu + 3]]);
+    int* cn = &conn[(size_t)cw * e].x;
+    for (int k = 0; k < npe; ++k) cn[k] = iperm[conn_user[(size_t)npe * eu + k]];
     ehome[e] = home[eu];
   }
   // node -> (element, slot) adjacency, sorted by element id
   std::vector<int> arow(Nn + 1, 0);
   for (int e = 0; e < Ne; ++e) {
-    const int* cn = &conn[e].x;
-    for (int k = 0; k < 4; ++k) arow[cn[k] + 1]++;
+    const int* cn = &conn[(size_t)cw * e].x;
+    for (int k = 0; k < npe; ++k) arow[cn[k] + 1]++;
   }
   for (int i = 0; i < Nn; ++i) arow[i + 1] += arow[i];
   std::vector<int> acol(arow[Nn]);
   std::vector<int> fill(arow.begin(), arow.end() - 1);
   for (int e = 0; e < Ne; ++e) {
-    const int* cn = &conn[e].x;
-    for (int k = 0; k < 4; ++k) acol[fill[cn[k]]++] = (e << 2) | k;
+    const int* cn = &conn[(size_t)cw * e].x;
+    for (int k = 0; k < npe; ++k) acol[fill[cn[k]]++] = (e << sh) | k;
   }
   // blocks
   const int nblkn = (Nn + nb - 1) / nb;
@@ -424,8 +436,8 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   std::vector<uint32_t> node_slots(arow[Nn]);
   blk_elems.reserve((size_t)Ne * 3 / 2);
   std::vector<int> foreign;
-  std::vector<std::pair<uint32_t, int>> ents;  // (li << 2 | slot, element)
-  std::vector<int4> spos(Ne);
+  std::vector<std::pair<uint32_t, int>> ents;  // (li << sh | slot, element)
+  std::vector<int4> spos((size_t)cw * Ne);
   int max_slots = 0;
   for (int b = 0; b < nblkn; ++b) {
     const int n0 = b * nb, n1 = std::min(Nn, n0 + nb);
@@ -433,7 +445,7 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
     foreign.clear();
     for (int n = n0; n < n1; ++n)
       for (int j = arow[n]; j < arow[n + 1]; ++j) {
-        const int e = acol[j] >> 2;
+        const int e = acol[j] >> sh;
         if (ehome[e] != b) foreign.push_back(e);
       }
     std::sort(foreign.begin(), foreign.end());
@@ -445,21 +457,21 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
     for (int n = n0; n < n1; ++n) {
       ents.clear();
       for (int j = arow[n]; j < arow[n + 1]; ++j) {
-        const int e = acol[j] >> 2, s = acol[j] & 3;
+        const int e = acol[j] >> sh, s = acol[j] & (int)smask;
         int li;
         if (ehome[e] == b) {
           li = e - h0;
         } else {
           li = (h1 - h0) + (int)(std::lower_bound(foreign.begin(), foreign.end(), e) - foreign.begin());
         }
-        ents.push_back({((uint32_t)li << 2) | (uint32_t)s, e});
+        ents.push_back({((uint32_t)li << sh) | (uint32_t)s, e});
       }
       std::sort(ents.begin(), ents.end());
       node_row[n + 1] = node_row[n] + (int)ents.size();
       for (size_t k = 0; k < ents.size(); ++k) {
         const int pos = node_row[n] + (int)k;
         node_slots[pos] = ents[k].first;
-        (&spos[ents[k].second].x)[ents[k].first & 3] = pos;
+        (&spos[(size_t)cw * ents[k].second].x)[ents[k].first & smask] = pos;
       }
     }
     max_slots = std::max(max_slots, node_row[n1] - node_row[n0]);
@@ -467,7 +479,7 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   c->max_slots = max_slots;
   // the fused residual kernel stages 12 NB doubles plus the block's slot list
   const size_t smem_need = sizeof(double) * 12 * (size_t)nb + sizeof(uint32_t) * (size_t)max_slots;
-  if (smem_need > 200u * 1024u)
+  if (npe == 4 && smem_need > 200u * 1024u)
     return set_err(nullptr, FEM_ERR_INVALID,
                    "node block of %d nodes needs %zu bytes of shared memory (max 204800): use a smaller block",
                    nb, smem_need);
@@ -485,13 +497,13 @@ int build_tables(FemCtx* c, const double* X, const int32_t* conn_user) {
   int st;
   if ((st = dalloc(c, &c->X64, X64.size()))) return st;
   if ((st = dalloc(c, &c->X32, (size_t)Nn))) return st;
-  if ((st = dalloc(c, &c->conn, (size_t)Ne))) return st;
+  if ((st = dalloc(c, &c->conn, conn.size()))) return st;
   if ((st = dalloc(c, &c->blk_ptr, blk_ptr.size()))) return st;
   if ((st = dalloc(c, &c->blk_home, blk_home.size()))) return st;
   if ((st = dalloc(c, &c->blk_elems, blk_elems.size()))) return st;
   if ((st = dalloc(c, &c->node_row, node_row.size()))) return st;
   if ((st = dalloc(c, &c->node_slots, node_slots.size()))) return st;
-  if ((st = dalloc(c, &c->spos, (size_t)Ne))) return st;
+  if ((st = dalloc(c, &c->spos, spos.size()))) return st;
   if ((st = dalloc(c, &c->d_perm_node, (size_t)Nn))) return st;
   if ((st = dalloc(c, &c->d_perm_elem, (size_t)Ne))) return st;
   CK(cudaMemcpyAsync(c->X64, X64.data(), X64.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -524,11 +536,12 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->u_base, nd))) return st;
   if ((st = dalloc(c, &c->R, nd))) return st;
   if ((st = dalloc(c, &c->tmpd, nd))) return st;
-  if ((st = dalloc(c, &c->payload, Ne * kPay))) return st;
-  if ((st = dalloc(c, &c->ep_c, Ne * 6))) return st;
-  if ((st = dalloc(c, &c->epe_c, Ne))) return st;
-  if ((st = dalloc(c, &c->ep_t, Ne * 6))) return st;
-  if ((st = dalloc(c, &c->epe_t, Ne))) return st;
+  const size_t Nq = c->Nq;
+  if ((st = dalloc(c, &c->payload, Nq * kPay))) return st;
+  if ((st = dalloc(c, &c->ep_c, Nq * 6))) return st;
+  if ((st = dalloc(c, &c->epe_c, Nq))) return st;
+  if ((st = dalloc(c, &c->ep_t, Nq * 6))) return st;
+  if ((st = dalloc(c, &c->epe_t, Nq))) return st;
   if ((st = dalloc(c, &c->r, nf))) return st;
   if ((st = dalloc(c, &c->x, nf))) return st;
   if ((st = dalloc(c, &c->p, nf))) return st;
@@ -536,7 +549,9 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->dinv, nf))) return st;
   if ((st = dalloc(c, &c->tmpf, nf))) return st;
   if ((st = dalloc(c, &c->boff, nf))) return st;
-  if ((st = dalloc(c, &c->stage, 4 * Ne))) return st;
+  // slot vectors of the two-phase passes; HEX8 diagonal blocks take 2 per slot
+  if ((st = dalloc(c, &c->stage, c->npe == 8 ? 16 * Ne : 4 * Ne))) return st;
+  if (c->npe == 8 && (st = dalloc(c, &c->stage_d, 24 * Ne))) return st;
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
   // every reducing kernel's grid must fit: node blocks and node-parallel blocks
@@ -606,7 +621,9 @@ int eval_residual(FemCtx* c, double* fneg_out_int, double* rnorm2) {
   a.rnorm2 = c->scalars;
   a.red = c->red();
   a.red_site = SITE_RES;
-  ++c->n_launches; launch_residual(a, c->model_kind, c->stream);
+  a.stage_d = c->stage_d;
+  c->n_launches += c->npe == 8 ? 2 : 1;
+  launch_residual(a, c->model_kind, c->stream);
   CKL();
   CK(cudaMemcpyAsync(c->h_scalars, c->scalars, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -625,7 +642,9 @@ int compute_dinv(FemCtx* c, int precond, bool block = false) {
     a.payload = c->payload;
     a.dinv = c->dinv;
     a.boff = block ? c->boff : nullptr;
-    ++c->n_launches; launch_diag(a, c->model_kind, c->stream);
+    a.stage = c->stage;
+    c->n_launches += c->npe == 8 ? 2 : 1;
+    launch_diag(a, c->model_kind, c->stream);
     CKL();
   } else {
     // identity on free DOFs: dinv = 1 where not fixed
@@ -755,6 +774,11 @@ CGState endless_cg() {
 // with CUDA events as they run inside CG (3 warm-up + 10 timed launches each,
 // p = 1 on free DOFs).  The CG state is reset by cg_init afterwards.
 int choose_matvec_variant(FemCtx* c) {
+  if (c->npe == 8) {
+    // HEX8 has the two-phase pass only
+    c->mv_variant = MV_TWO_PHASE;
+    return FEM_OK;
+  }
   if (c->mv_forced >= 0) {
     c->mv_variant = c->mv_forced;
     return FEM_OK;
@@ -1491,6 +1515,12 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
             double* rel) {
   if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
   int st;
+  if (c->npe == 8 && (precond == FEM_PRECOND_TWO_LEVEL || precond == FEM_PRECOND_LEARNED)) {
+    // the coarse lattice's Galerkin blocks and the learned network are built
+    // for TET4: a HEX8 context runs these solves as Jacobi-PCG
+    ++c->n_coarse_fallbacks;
+    precond = FEM_PRECOND_JACOBI;
+  }
   const bool tl = precond == FEM_PRECOND_TWO_LEVEL;
   const bool learned = precond == FEM_PRECOND_LEARNED;
   const int kind = learned ? GRAPH_LEARNED : (tl ? GRAPH_TWO_LEVEL : GRAPH_JACOBI);
@@ -1644,14 +1674,20 @@ int fem_ctx_create(const FemMeshDesc* desc, void** ctx_out) {
   const int nb = desc->nodes_per_block == 0 ? 256 : desc->nodes_per_block;
   if (nb != 128 && nb != 256 && nb != 512)
     return set_err(nullptr, FEM_ERR_INVALID, "nodes_per_block must be 128, 256 or 512");
-  for (int64_t i = 0; i < 4 * desc->n_elements; ++i)
+  const int npe = desc->nodes_per_elem == 0 ? 4 : desc->nodes_per_elem;
+  if (npe != 4 && npe != 8)
+    return set_err(nullptr, FEM_ERR_INVALID, "nodes_per_elem must be 4 (TET4) or 8 (HEX8), got %d",
+                   desc->nodes_per_elem);
+  if (npe == 8 && desc->n_elements > (1LL << 27))
+    return set_err(nullptr, FEM_ERR_INVALID, "HEX8 mesh too large for 32-bit slot tables");
+  for (int64_t i = 0; i < npe * desc->n_elements; ++i)
     if (desc->conn[i] < 0 || desc->conn[i] >= desc->n_nodes)
       return set_err(nullptr, FEM_ERR_INVALID, "connectivity entry %lld = %d out of range [0, %lld)",
                      (long long)i, desc->conn[i], (long long)desc->n_nodes);
   for (int64_t e = 0; e < desc->n_elements; ++e) {
-    const int32_t* cn = desc->conn + 4 * e;
-    for (int a = 0; a < 4; ++a)
-      for (int b = a + 1; b < 4; ++b)
+    const int32_t* cn = desc->conn + npe * e;
+    for (int a = 0; a < npe; ++a)
+      for (int b = a + 1; b < npe; ++b)
         if (cn[a] == cn[b])
           return set_err(nullptr, FEM_ERR_INVALID, "element %lld repeats node %d", (long long)e, cn[a]);
   }
@@ -1664,6 +1700,9 @@ int fem_ctx_create(const FemMeshDesc* desc, void** ctx_out) {
   c->device = desc->device;
   c->Nn = (int)desc->n_nodes;
   c->Ne = (int)desc->n_elements;
+  c->npe = npe;
+  c->ngp = npe == 8 ? kHexGauss : 1;
+  c->Nq = (size_t)c->Ne * c->ngp;
   c->nb = nb;
   c->ndof = 3 * c->Nn;
   c->ndof_pad = (c->ndof + 3) / 4 * 4;
@@ -2311,7 +2350,7 @@ int fem_nodal_mises(void* ctx, const double* u, double* mises_out, int32_t avera
     CKL();
   }
   double* sig = nullptr;
-  CK(cudaMallocAsync(reinterpret_cast<void**>(&sig), sizeof(double) * 9 * (size_t)c->Ne, c->stream));
+  CK(cudaMallocAsync(reinterpret_cast<void**>(&sig), sizeof(double) * 9 * c->Nq, c->stream));
   ++c->n_launches; launch_stress(c->mesh(), c->matD, c->model_kind, c->u, c->ep_c, c->epe_c, c->d_perm_elem,
                                  nullptr, sig, c->stream);
   ++c->n_launches; launch_nodal_mises(c->mesh(), c->d_perm_elem, c->d_perm_node, sig, average, mises_out,
@@ -2557,8 +2596,8 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     }
   }
   if (converged && c->has_j2 && prm.auto_commit) {
-    CK(cudaMemcpyAsync(c->ep_c, c->ep_t, (size_t)6 * c->Ne * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->epe_c, c->epe_t, (size_t)c->Ne * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->ep_c, c->ep_t, 6 * c->Nq * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->epe_c, c->epe_t, c->Nq * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   }
   CK(cudaStreamSynchronize(c->stream));
   out.converged = converged ? 1 : 0;
@@ -2638,8 +2677,8 @@ int fem_commit_history(void* ctx) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   int st;
   if ((st = check_ctx(c))) return st;
-  CK(cudaMemcpyAsync(c->ep_c, c->ep_t, (size_t)6 * c->Ne * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->epe_c, c->epe_t, (size_t)c->Ne * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->ep_c, c->ep_t, 6 * c->Nq * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->epe_c, c->epe_t, c->Nq * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return FEM_OK;
 }
@@ -2648,10 +2687,10 @@ int fem_reset_history(void* ctx) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   int st;
   if ((st = check_ctx(c))) return st;
-  CK(cudaMemsetAsync(c->ep_c, 0, (size_t)6 * c->Ne * sizeof(double), c->stream));
-  CK(cudaMemsetAsync(c->epe_c, 0, (size_t)c->Ne * sizeof(double), c->stream));
-  CK(cudaMemsetAsync(c->ep_t, 0, (size_t)6 * c->Ne * sizeof(double), c->stream));
-  CK(cudaMemsetAsync(c->epe_t, 0, (size_t)c->Ne * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->ep_c, 0, 6 * c->Nq * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->epe_c, 0, c->Nq * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->ep_t, 0, 6 * c->Nq * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->epe_t, 0, c->Nq * sizeof(double), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->tangent_valid = false;
   // back to rest: the coarse operator was built on a deformed, plastic
@@ -2664,22 +2703,26 @@ int fem_get_history(void* ctx, double* ep_out, double* epe_out) {
   FemCtx* c = static_cast<FemCtx*>(ctx);
   int st;
   if ((st = check_ctx(c))) return st;
-  std::vector<double> ep((size_t)6 * c->Ne), epe(c->Ne);
+  std::vector<double> ep(6 * c->Nq), epe(c->Nq);
   CK(cudaMemcpyAsync(ep.data(), c->ep_c, ep.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(epe.data(), c->epe_c, epe.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   // internal SoA (xx,yy,zz,yz,xz,xy) -> caller (Ne,3,3) / (Ne)
-  std::vector<double> full((size_t)9 * c->Ne), e1(c->Ne);
+  // HEX8: caller point e * 8 + g (the reference's gp_idx), internal g * Ne + e
+  std::vector<double> full(9 * c->Nq), e1(c->Nq);
   for (int e = 0; e < c->Ne; ++e) {
     const int eu = c->perm_elem[e];
-    double s[6];
-    for (int k = 0; k < 6; ++k) s[k] = ep[(size_t)k * c->Ne + e];
-    double* F = &full[(size_t)9 * eu];
-    F[0] = s[0]; F[4] = s[1]; F[8] = s[2];
-    F[5] = F[7] = s[3];
-    F[2] = F[6] = s[4];
-    F[1] = F[3] = s[5];
-    e1[eu] = epe[e];
+    for (int g = 0; g < c->ngp; ++g) {
+      const size_t q = (size_t)g * c->Ne + e, qu = (size_t)eu * c->ngp + g;
+      double s[6];
+      for (int k = 0; k < 6; ++k) s[k] = ep[(size_t)k * c->Nq + q];
+      double* F = &full[9 * qu];
+      F[0] = s[0]; F[4] = s[1]; F[8] = s[2];
+      F[5] = F[7] = s[3];
+      F[2] = F[6] = s[4];
+      F[1] = F[3] = s[5];
+      e1[qu] = epe[q];
+    }
   }
   if (ep_out) CK(cudaMemcpyAsync(ep_out, full.data(), full.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (epe_out) CK(cudaMemcpyAsync(epe_out, e1.data(), e1.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));

@@ -483,4 +483,42 @@ __host__ __device__ __forceinline__ int model_pay_words(int model) {
   return model == M_NH ? 10 : (model == M_J2 ? 8 : ((model == M_MR || model == M_FMR) ? 9 : 0));
 }
 
+// Jacobi diagonal of one node from its summed element entries acc (BLOCK:
+// the 3 x 3 diagonal block 00 01 02 11 12 22; else the 3 diagonal entries):
+// dinv = 1 / diag on free DOFs, or (BLOCK) the inverse of the block
+// restricted to the free DOFs, computed in FP64, with its diagonal in dinv
+// and its off-diagonals (01, 02, 12) in boff.  A block that is not positive
+// definite falls back to the scalar inverse of its diagonal.
+template <bool BLOCK>
+__device__ __forceinline__ void diag_store(const float* acc, uint8_t fx, int node, float* dinv, float* boff) {
+  if (!BLOCK) {
+    float dv[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dv[d] = (((fx >> d) & 1) || !(acc[d] > 0.f)) ? 0.f : 1.f / acc[d];
+    reinterpret_cast<float4*>(dinv)[node] = make_float4(dv[0], dv[1], dv[2], 0.f);
+    return;
+  }
+  // acc: 00 01 02 11 12 22; fixed rows/columns replaced by the identity
+  const bool f0 = fx & 1, f1 = (fx >> 1) & 1, f2 = (fx >> 2) & 1;
+  const double k00 = f0 ? 1.0 : acc[0], k11 = f1 ? 1.0 : acc[3], k22 = f2 ? 1.0 : acc[5];
+  const double k01 = (f0 || f1) ? 0.0 : acc[1], k02 = (f0 || f2) ? 0.0 : acc[2], k12 = (f1 || f2) ? 0.0 : acc[4];
+  const double c00 = k11 * k22 - k12 * k12, c01 = k02 * k12 - k01 * k22, c02 = k01 * k12 - k02 * k11;
+  const double det = k00 * c00 + k01 * c01 + k02 * c02;
+  float4 dv, ov;
+  if (det > 0.0 && k00 > 0.0 && k00 * k11 - k01 * k01 > 0.0 && isfinite(det)) {
+    const double id = 1.0 / det;
+    const double i11 = (k00 * k22 - k02 * k02) * id, i22 = (k00 * k11 - k01 * k01) * id;
+    const double i12 = (k01 * k02 - k00 * k12) * id;
+    dv = make_float4(f0 ? 0.f : (float)(c00 * id), f1 ? 0.f : (float)i11, f2 ? 0.f : (float)i22, 0.f);
+    ov = make_float4((f0 || f1) ? 0.f : (float)(c01 * id), (f0 || f2) ? 0.f : (float)(c02 * id),
+                     (f1 || f2) ? 0.f : (float)i12, 0.f);
+  } else {
+    dv = make_float4((f0 || !(acc[0] > 0.f)) ? 0.f : 1.f / acc[0], (f1 || !(acc[3] > 0.f)) ? 0.f : 1.f / acc[3],
+                     (f2 || !(acc[5] > 0.f)) ? 0.f : 1.f / acc[5], 0.f);
+    ov = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  reinterpret_cast<float4*>(dinv)[node] = dv;
+  reinterpret_cast<float4*>(boff)[node] = ov;
+}
+
 }  // namespace femb200

@@ -80,7 +80,14 @@ struct MeshDev {
   const uint8_t* fixed;     // [Nn] bit d set = DOF d fixed
   int max_slots;            // largest slot-list range of one block (shared memory sizing)
   const int4* spos;         // [Ne] position of each (element, slot) in node_slots order
+                            // (HEX8: [2 Ne], slots 0-3 then 4-7 of each element)
+  int npe;                  // nodes per element: 4 (TET4) or 8 (HEX8; conn holds 2 int4 per element)
+  int slot_shift;           // node_slots entries are local element << slot_shift | slot
 };
+
+// HEX8 elements carry 8 Gauss points; per-point arrays (tangent payload, J2
+// history) are SoA over points q = g * Ne + e: word k of point q at k * Nq + q.
+constexpr int kHexGauss = 8;
 
 // Last-block reduction bookkeeping: one slot per reduction site.
 struct Reduce {
@@ -118,6 +125,7 @@ struct ResArgs {
   double* rnorm2;           // [1] ||R||^2 (free DOFs)
   Reduce red;
   int red_site;
+  double* stage_d;          // HEX8: [3 * 8 Ne] element slot forces in node_slots order
 };
 
 struct MvArgs {
@@ -146,6 +154,7 @@ struct DiagArgs {
   const float* payload;
   float* dinv;              // [Nn] float4: 1/diag(K) on free DOFs, 0 elsewhere
   float* boff;              // non-null: nodal 3x3 block inverse, dinv its diagonal, boff (01, 02, 12)
+  float4* stage;            // HEX8: [2 * 8 Ne] per slot the 6 block entries (or 3 diagonal entries)
 };
 
 // Coarse lattice of the two-level preconditioner (fem_coarse.cu).  Cells
@@ -374,6 +383,17 @@ void launch_nodal_mises(const MeshDev& m, const int* perm_elem, const int* perm_
                         int average, double* out_user, cudaStream_t s);
 void launch_refq(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol,
                  cudaStream_t s);
+// HEX8 (fem_hex8.cu): element pass writing slot vectors in node_slots order
+// plus a fixed-order node gather, like the two-phase TET4 matvec
+void launch_residual_hex(const ResArgs& a, int model, cudaStream_t s);
+void launch_matvec_hex(const MvArgs& a, int model, cudaStream_t s);
+void launch_diag_hex(const DiagArgs& a, int model, cudaStream_t s);
+void launch_stress_hex(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
+                       const double* ep_c, const double* epe_c, const int* perm_elem, double* F_out,
+                       double* sig_out, cudaStream_t s);
+void launch_refq_hex(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol, cudaStream_t s);
+// the node gather of the two-phase matvec (fem_kernels.cu)
+void launch_node_gather(const MvArgs& a, cudaStream_t s);
 // out[n*3+d] (internal) = in[perm[n]*3+d] (caller order) and back
 void launch_gather_d(const double* in_user, double* out_int, const int* perm, int n, cudaStream_t s);
 void launch_scatter_d(const double* in_int, double* out_user, const int* perm, int n,

@@ -541,35 +541,7 @@ __global__ void __launch_bounds__(NB) diag_kernel(const __grid_constant__ DiagAr
     __syncthreads();
   }
   if (!has_node) return;
-  const uint8_t fx = m.fixed[node];
-  if (!BLOCK) {
-    float dv[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) dv[d] = (((fx >> d) & 1) || !(acc[d] > 0.f)) ? 0.f : 1.f / acc[d];
-    reinterpret_cast<float4*>(a.dinv)[node] = make_float4(dv[0], dv[1], dv[2], 0.f);
-    return;
-  }
-  // acc: 00 01 02 11 12 22; fixed rows/columns replaced by the identity
-  const bool f0 = fx & 1, f1 = (fx >> 1) & 1, f2 = (fx >> 2) & 1;
-  const double k00 = f0 ? 1.0 : acc[0], k11 = f1 ? 1.0 : acc[3], k22 = f2 ? 1.0 : acc[5];
-  const double k01 = (f0 || f1) ? 0.0 : acc[1], k02 = (f0 || f2) ? 0.0 : acc[2], k12 = (f1 || f2) ? 0.0 : acc[4];
-  const double c00 = k11 * k22 - k12 * k12, c01 = k02 * k12 - k01 * k22, c02 = k01 * k12 - k02 * k11;
-  const double det = k00 * c00 + k01 * c01 + k02 * c02;
-  float4 dv, ov;
-  if (det > 0.0 && k00 > 0.0 && k00 * k11 - k01 * k01 > 0.0 && isfinite(det)) {
-    const double id = 1.0 / det;
-    const double i11 = (k00 * k22 - k02 * k02) * id, i22 = (k00 * k11 - k01 * k01) * id;
-    const double i12 = (k01 * k02 - k00 * k12) * id;
-    dv = make_float4(f0 ? 0.f : (float)(c00 * id), f1 ? 0.f : (float)i11, f2 ? 0.f : (float)i22, 0.f);
-    ov = make_float4((f0 || f1) ? 0.f : (float)(c01 * id), (f0 || f2) ? 0.f : (float)(c02 * id),
-                     (f1 || f2) ? 0.f : (float)i12, 0.f);
-  } else {
-    dv = make_float4((f0 || !(acc[0] > 0.f)) ? 0.f : 1.f / acc[0], (f1 || !(acc[3] > 0.f)) ? 0.f : 1.f / acc[3],
-                     (f2 || !(acc[5] > 0.f)) ? 0.f : 1.f / acc[5], 0.f);
-    ov = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  reinterpret_cast<float4*>(a.dinv)[node] = dv;
-  reinterpret_cast<float4*>(a.boff)[node] = ov;
+  diag_store<BLOCK>(acc, m.fixed[node], node, a.dinv, a.boff);
 }
 
 // ───────────────────────── PCG vector kernels ─────────────────────────
@@ -769,10 +741,18 @@ __global__ void nodal_mises_kernel(const MeshDev m, const int* perm_elem, const 
   const int base = m.blk_ptr[b];
   const int j0 = m.node_row[n], j1 = m.node_row[n + 1];
   double acc = 0.0;
+  const int ngp = m.npe == 8 ? kHexGauss : 1;
   for (int j = j0; j < j1; ++j) {
-    const int li = (int)(m.node_slots[j] >> 2);
+    const int li = (int)(m.node_slots[j] >> m.slot_shift);
     const int e = m.blk_elems[base + li];
-    const double* s = sig_user + (size_t)9 * perm_elem[e];
+    // the element's Gauss-point mean stress (core/mesh.py:470-474)
+    const double* sp = sig_user + (size_t)9 * ngp * perm_elem[e];
+    double s[9];
+    for (int k = 0; k < 9; ++k) s[k] = sp[k];
+    for (int g = 1; g < ngp; ++g)
+      for (int k = 0; k < 9; ++k) s[k] += sp[9 * g + k];
+    if (ngp > 1)
+      for (int k = 0; k < 9; ++k) s[k] /= (double)ngp;
     const double s11 = s[0], s22 = s[4], s33 = s[8], s12 = s[1], s23 = s[5], s13 = s[2];
     acc += sqrt(0.5 * ((s11 - s22) * (s11 - s22) + (s22 - s33) * (s22 - s33) + (s33 - s11) * (s33 - s11) +
                        6.0 * (s12 * s12 + s23 * s23 + s13 * s13)));
@@ -967,6 +947,10 @@ static void residual_nb(const ResArgs& a, int model, cudaStream_t s) {
 }
 
 void launch_residual(const ResArgs& a, int model, cudaStream_t s) {
+  if (a.m.npe == 8) {
+    launch_residual_hex(a, model, s);
+    return;
+  }
   switch (a.m.nb) {
     case 128: residual_nb<128>(a, model, s); break;
     case 512: residual_nb<512>(a, model, s); break;
@@ -1009,7 +993,18 @@ static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
   launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
 }
 
+void launch_node_gather(const MvArgs& a, cudaStream_t s) {
+  if (a.cg)
+    launch_chain(node_gather_kernel<true>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
+  else
+    launch_chain(node_gather_kernel<false>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
+}
+
 void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
+  if (a.m.npe == 8) {
+    launch_matvec_hex(a, model, s);
+    return;
+  }
   const bool cg = a.cg != nullptr;
   if (a.variant == MV_TWO_PHASE) {
     cg ? two_phase<true>(a, model, s) : two_phase<false>(a, model, s);
@@ -1071,6 +1066,10 @@ static void diag_nb(const DiagArgs& a, int model, cudaStream_t s) {
 }
 
 void launch_diag(const DiagArgs& a, int model, cudaStream_t s) {
+  if (a.m.npe == 8) {
+    launch_diag_hex(a, model, s);
+    return;
+  }
   switch (a.m.nb) {
     case 128: diag_nb<128>(a, model, s); break;
     case 512: diag_nb<512>(a, model, s); break;
@@ -1102,6 +1101,10 @@ void launch_cg_pupdate(float* p, const float* r, const float* dinv, int n_nodes,
 void launch_stress(const MeshDev& m, const DevMat<double>* matD, int model, const double* u,
                    const double* ep_c, const double* epe_c, const int* perm_elem, double* F_out,
                    double* sig_out, cudaStream_t s) {
+  if (m.npe == 8) {
+    launch_stress_hex(m, matD, model, u, ep_c, epe_c, perm_elem, F_out, sig_out, s);
+    return;
+  }
   const int t = 128;
   switch (model) {
     case M_LE: stress_kernel<M_LE><<<nblk(m.n_elems, t), t, 0, s>>>(m, matD, u, ep_c, epe_c, perm_elem, F_out, sig_out); break;
@@ -1118,6 +1121,10 @@ void launch_nodal_mises(const MeshDev& m, const int* perm_elem, const int* perm_
 
 void launch_refq(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol,
                  cudaStream_t s) {
+  if (m.npe == 8) {
+    launch_refq_hex(m, perm_elem, dNdX, vol, s);
+    return;
+  }
   refq_kernel<<<nblk(m.n_elems, 128), 128, 0, s>>>(m, perm_elem, dNdX, vol);
 }
 

@@ -84,7 +84,8 @@ class DynamicSolver:
         vol = self.mesh.elem_vol
         conn = torch.as_tensor(self.mesh.elements, dtype=torch.int64, device=self.mesh.device)
         node_mass = torch.zeros(self.mesh.n_nodes, dtype=torch.float64, device=self.mesh.device)
-        node_mass.index_add_(0, conn.reshape(-1), (density * vol / 4.0).repeat_interleave(4))
+        npe = self.mesh.nodes_per_elem
+        node_mass.index_add_(0, conn.reshape(-1), (density * vol / float(npe)).repeat_interleave(npe))
         return node_mass.repeat_interleave(3)
 
     def _estimate_stable_dt(self) -> float:

@@ -30,8 +30,10 @@ from .validation import (FEAConvergenceError, FEAValidationError, logger,
 
 
 class ElementType(enum.Enum):
-    """Element types (core/element.py:12-33); the B200 path implements TET4."""
+    """Element types (core/element.py:12-33); the B200 path implements TET4
+    (one Gauss point) and HEX8 (2 x 2 x 2 Gauss points)."""
     TET4 = "C3D4"
+    HEX8 = "C3D8"
 
 
 def _ptr(t: Optional[torch.Tensor]):
@@ -58,24 +60,28 @@ def _require_cuda(device) -> torch.device:
 
 
 class FEMesh:
-    """TET4 mesh on one GPU (core/mesh.py:18-86).
+    """TET4 or HEX8 mesh on one GPU (core/mesh.py:18-86).
 
     Field tensors (torch, float64, on the mesh's device): ``u``, ``f``,
-    ``f_ext``, ``fixed`` (int32 per DOF), ``fixed_value``; per element
-    ``F``/``stress`` after ``compute_stress`` and ``material_id``.
+    ``f_ext``, ``fixed`` (int32 per DOF), ``fixed_value``; per Gauss point
+    (point e * n_gauss + g, as the reference's ``gp_idx``) ``F``/``stress``
+    after ``compute_stress``; per element ``material_id``.  HEX8 meshes solve
+    with Jacobi or nodal block-Jacobi PCG (a two-level or learned request runs
+    Jacobi-PCG and counts a fallback in ``coarse_info``).
     """
 
     def __init__(self, n_nodes: int, n_elements: int, element_type: ElementType = ElementType.TET4,
                  device=None, nodes_per_block: int = 0, own_stream: bool = False):
-        if element_type is not ElementType.TET4 and element_type != "C3D4":
+        et = getattr(element_type, "value", element_type)
+        if et not in ("C3D4", "C3D8"):
             raise FEAValidationError(f"element type {element_type} is not supported by the B200 path "
-                                     "(TET4 only)", parameter="element_type", value=element_type)
+                                     "(TET4, HEX8)", parameter="element_type", value=element_type)
         self.n_nodes = int(n_nodes)
         self.n_elements = int(n_elements)
-        self.element_type = ElementType.TET4
+        self.element_type = ElementType(et)
         self.dim = 3
-        self.nodes_per_elem = 4
-        self.n_gauss = 1
+        self.nodes_per_elem = 4 if et == "C3D4" else 8
+        self.n_gauss = 1 if et == "C3D4" else 8
         self.device = _require_cuda(device)
         self.nodes_per_block = nodes_per_block
         # own_stream: the library creates a private non-blocking stream for this
@@ -89,8 +95,8 @@ class FEMesh:
         self.f_ext = z(self.n_nodes, 3)
         self.fixed = z(self.n_nodes, 3, dt=torch.int32)
         self.fixed_value = z(self.n_nodes, 3)
-        self.F = z(self.n_elements, 3, 3)
-        self.stress = z(self.n_elements, 3, 3)
+        self.F = z(self.n_elements * self.n_gauss, 3, 3)
+        self.stress = z(self.n_elements * self.n_gauss, 3, 3)
         self.material_id = np.zeros(self.n_elements, dtype=np.int32)
         self.X = None
         self.elements = None
@@ -103,9 +109,9 @@ class FEMesh:
         if nodes.shape != (self.n_nodes, 3):
             raise FEAValidationError(f"nodes must be ({self.n_nodes}, 3), got {nodes.shape}",
                                      parameter="nodes")
-        if elements.shape != (self.n_elements, 4):
-            raise FEAValidationError(f"elements must be ({self.n_elements}, 4), got {elements.shape}",
-                                     parameter="elements")
+        if elements.shape != (self.n_elements, self.nodes_per_elem):
+            raise FEAValidationError(f"elements must be ({self.n_elements}, {self.nodes_per_elem}), "
+                                     f"got {elements.shape}", parameter="elements")
         self.X = nodes
         self.elements = elements
         if material_ids is not None:
@@ -116,7 +122,8 @@ class FEMesh:
             desc = _lib.FemMeshDesc(self.n_nodes, self.n_elements,
                                     nodes.ctypes.data_as(C.POINTER(C.c_double)),
                                     elements.ctypes.data_as(C.POINTER(C.c_int32)),
-                                    self.device.index, int(self.nodes_per_block), C.c_void_p(stream))
+                                    self.device.index, int(self.nodes_per_block), C.c_void_p(stream),
+                                    self.nodes_per_elem)
             ctx = C.c_void_p()
             _check(lib.fem_ctx_create(C.byref(desc), C.byref(ctx)), None, "fem_ctx_create")
         self._ctx = ctx
@@ -284,8 +291,9 @@ class FEMesh:
 
     # ---- kinematics / outputs ----
     def _reference_quantities(self):
-        dN = torch.empty(self.n_elements, 4, 3, dtype=torch.float64, device=self.device)
-        vol = torch.empty(self.n_elements, dtype=torch.float64, device=self.device)
+        nq = self.n_elements * self.n_gauss
+        dN = torch.empty(nq, self.nodes_per_elem, 3, dtype=torch.float64, device=self.device)
+        vol = torch.empty(nq, dtype=torch.float64, device=self.device)
         _check(_lib.load().fem_reference_quantities(self.ctx, _ptr(dN), _ptr(vol)), self.ctx,
                "fem_reference_quantities")
         return dN, vol
@@ -300,7 +308,8 @@ class FEMesh:
 
     @property
     def elem_vol(self) -> torch.Tensor:
-        return self._reference_quantities()[1]
+        """Element volume: the sum of its Gauss volumes (core/mesh.py:147-151)."""
+        return self._reference_quantities()[1].view(self.n_elements, self.n_gauss).sum(dim=1)
 
     def compute_deformation_gradient(self):
         """F = I + sum_a u_a (x) dN_a/dX into ``self.F`` (core/mesh.py:293-313)."""
@@ -513,14 +522,16 @@ class J2Plasticity(LinearElastic):
     def get_plastic_strain(self) -> np.ndarray:
         if self._mesh is None:
             return np.array([])
-        epe = torch.empty(self._mesh.n_elements, dtype=torch.float64, device=self._mesh.device)
+        nq = self._mesh.n_elements * self._mesh.n_gauss
+        epe = torch.empty(nq, dtype=torch.float64, device=self._mesh.device)
         _check(_lib.load().fem_get_history(self._mesh.ctx, None, _ptr(epe)), self._mesh.ctx, "fem_get_history")
         return epe.cpu().numpy()
 
     def get_plastic_strain_tensor(self) -> np.ndarray:
         if self._mesh is None:
             return np.array([])
-        ep = torch.empty(self._mesh.n_elements, 3, 3, dtype=torch.float64, device=self._mesh.device)
+        nq = self._mesh.n_elements * self._mesh.n_gauss
+        ep = torch.empty(nq, 3, 3, dtype=torch.float64, device=self._mesh.device)
         _check(_lib.load().fem_get_history(self._mesh.ctx, _ptr(ep), None), self._mesh.ctx, "fem_get_history")
         return ep.cpu().numpy()
 

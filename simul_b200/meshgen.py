@@ -1,4 +1,4 @@
-"""Deterministic TET4 input generators for the static-solve workloads.
+"""Deterministic TET4 and HEX8 input generators for the static-solve workloads.
 
 * ``cantilever_bar``  — structured hex grid, every hex split into 6 Kuhn tets
   along its (0,0,0)->(1,1,1) diagonal; tip traction turned into consistent
@@ -10,9 +10,11 @@
   lognormal cancellous core (median 300 MPa).
 
 The reference builds HEX8 grids (``framework/_adapters/fem_adapter.py:41-70``)
-and voxel HEX8 meshes (``preprocessing/voxel_to_hex.py:11-68``); these
-generators produce the tetrahedral equivalents the TET4 hot path consumes.
-All arrays are NumPy; units are mm, N, MPa.
+and voxel HEX8 meshes (``preprocessing/voxel_to_hex.py:11-68``):
+``structured_hex8`` and ``voxels_to_hex_mesh`` restate those two (same node and
+element numbering), ``vertebral_body(..., element="hex8")`` builds the
+vertebral body from one HEX8 per voxel; the other generators produce the
+tetrahedral equivalents.  All arrays are NumPy; units are mm, N, MPa.
 """
 from __future__ import annotations
 
@@ -38,11 +40,60 @@ _FIVE_ODD = ((0b100, 0b010, 0b001, 0b111),
              (0b011, 0b010, 0b001, 0b111))
 
 
+# HEX8 vertex offsets in the reference's order (preprocessing/voxel_to_hex.py:38-50,
+# core/element.py:297-315): bottom face counter-clockwise, then the top face.
+HEX8_CORNERS = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                         [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=np.float64)
+
+
+def structured_hex8(nx, ny, nz, L=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0)):
+    """Structured HEX8 grid numbered as the reference's FEMAdapter builds it
+    (framework/_adapters/fem_adapter.py:41-70): node i + j (nx+1) + k (nx+1)(ny+1)
+    at origin + (i dx, j dy, k dz); elements x fastest, then y, then z."""
+    dx, dy, dz = L[0] / nx, L[1] / ny, L[2] / nz
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    X = np.stack([origin[0] + i.ravel() * dx, origin[1] + j.ravel() * dy, origin[2] + k.ravel() * dz],
+                 axis=1).astype(np.float64)
+    ez, ey, ex = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    n0 = (ex + ey * (nx + 1) + ez * (nx + 1) * (ny + 1)).ravel()
+    n3 = n0 + (nx + 1)
+    n4 = n0 + (nx + 1) * (ny + 1)
+    n7 = n4 + (nx + 1)
+    conn = np.stack([n0, n0 + 1, n3 + 1, n3, n4, n4 + 1, n7 + 1, n7], axis=1)
+    return X, conn.astype(np.int32)
+
+
+def voxels_to_hex_mesh(voxel_centers: np.ndarray, spacing) -> tuple:
+    """Voxel centres -> HEX8 mesh (preprocessing/voxel_to_hex.py:11-68): the
+    8 corners of every voxel, merged where their coordinates agree on a grid
+    of min(spacing) * 1e-4; nodes in ascending order of that rounded key
+    (lexicographic x, y, z), elements (n_voxels, 8) int64."""
+    centers = np.asarray(voxel_centers, dtype=np.float64).reshape(-1, 3)
+    spacing = np.asarray(spacing, dtype=np.float64).reshape(3)
+    if centers.shape[0] == 0:
+        return np.empty((0, 3)), np.empty((0, 8), dtype=np.int64)
+    verts = (centers[:, None, :] + HEX8_CORNERS[None, :, :] * (0.5 * spacing)[None, None, :]).reshape(-1, 3)
+    key = np.round(verts / (np.min(spacing) * 1e-4)).astype(np.int64)
+    _, first, inverse = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    return verts[first], inverse.reshape(-1, 8).astype(np.int64)
+
+
+def voxel_hex8(mask: np.ndarray, h: float, origin=(0.0, 0.0, 0.0)):
+    """One HEX8 per True voxel of ``mask`` (indexed [i,j,k] = x,y,z), through
+    ``voxels_to_hex_mesh``.  Returns nodes, connectivity (int32) and the voxel
+    indices in element order."""
+    vi, vj, vk = np.nonzero(mask)
+    centers = np.stack([origin[0] + (vi + 0.5) * h, origin[1] + (vj + 0.5) * h, origin[2] + (vk + 0.5) * h],
+                       axis=1)
+    X, conn = voxels_to_hex_mesh(centers, (h, h, h))
+    return X, conn.astype(np.int32), (vi, vj, vk)
+
+
 @dataclass
 class TetMesh:
-    """A TET4 mesh with boundary data, in the caller's (generator) order."""
+    """A TET4 (or HEX8) mesh with boundary data, in the caller's (generator) order."""
     X: np.ndarray                    # (Nn,3) float64
-    conn: np.ndarray                 # (Ne,4) int32, positively oriented
+    conn: np.ndarray                 # (Ne,4) int32, positively oriented (HEX8: (Ne,8))
     E: Optional[np.ndarray] = None   # (Ne,) per-element Young's modulus
     fixed_mask: Optional[np.ndarray] = None   # (Nn,3) bool
     fixed_vals: Optional[np.ndarray] = None   # (Nn,3) float64 (full-load value)
@@ -176,13 +227,17 @@ def voxel_tets(mask: np.ndarray, h: float, origin=(0.0, 0.0, 0.0)):
 def vertebral_body(n=64, seed=0, a=15.0, b=12.0, height=25.0, extent=32.0,
                    E_cortical=12e3, E_core_median=300.0, core_sigma=0.3,
                    smooth_voxels=3.0, shell_voxels=2, nu=0.3,
-                   axial_strain=0.02) -> TetMesh:
+                   axial_strain=0.02, element="tet4") -> TetMesh:
     """Synthetic vertebral body of the plain-method workload.
 
     Voxel (i,j,k) of spacing h = extent/n is inside when its centre satisfies
     (x/a)^2 + (y/b)^2 <= 1 and 0 <= z < height.  Bottom face fixed; the top
     face gets u_z = -axial_strain*height (full load; callers step it).
+    ``element="hex8"`` makes every voxel one HEX8 (``voxel_hex8``) instead of
+    five tets.
     """
+    if element not in ("tet4", "hex8"):
+        raise ValueError(f"element must be 'tet4' or 'hex8', got {element!r}")
     from scipy import ndimage
 
     h = extent / n
@@ -197,8 +252,12 @@ def vertebral_body(n=64, seed=0, a=15.0, b=12.0, height=25.0, extent=32.0,
     zc_ = z[core]
     z = (z - zc_.mean()) / zc_.std()
     Evox = np.where(core, E_core_median * np.exp(core_sigma * z), E_cortical)
-    X, conn, vox, (vi, vj, vk) = voxel_tets(mask, h, origin=(-extent / 2.0, -extent / 2.0, 0.0))
-    E = Evox[vi, vj, vk][vox]
+    if element == "hex8":
+        X, conn, (vi, vj, vk) = voxel_hex8(mask, h, origin=(-extent / 2.0, -extent / 2.0, 0.0))
+        E = Evox[vi, vj, vk]
+    else:
+        X, conn, vox, (vi, vj, vk) = voxel_tets(mask, h, origin=(-extent / 2.0, -extent / 2.0, 0.0))
+        E = Evox[vi, vj, vk][vox]
     top_z = X[:, 2].max()
     fixed = np.zeros((X.shape[0], 3), dtype=bool)
     fixed_vals = np.zeros_like(X)
@@ -209,7 +268,7 @@ def vertebral_body(n=64, seed=0, a=15.0, b=12.0, height=25.0, extent=32.0,
     fixed_vals[top, 2] = -axial_strain * top_z
     return TetMesh(X=X, conn=conn, E=E.astype(np.float64), fixed_mask=fixed,
                    fixed_vals=fixed_vals, f_ext=np.zeros_like(X),
-                   info={"kind": "vertebral_body", "n": n, "h": h, "seed": seed, "nu": nu,
+                   info={"kind": "vertebral_body", "element": element, "n": n, "h": h, "seed": seed, "nu": nu,
                          "n_voxels": int(mask.sum()), "height": float(top_z),
                          "shell_elements": int(np.sum(E == E_cortical))})
 

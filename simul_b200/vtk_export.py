@@ -148,5 +148,7 @@ def export_mesh_result(filename: str, mesh, material=None, binary: bool = True, 
         material.compute_stress(mesh)
     mesh.compute_mises_stress(average=average_mises)
     fields = {"displacement": mesh.get_displacements(), "von_mises": mesh.mises.cpu().numpy()}
-    cell = {"stress": mesh.get_stress()}
-    return export_vtk(filename, mesh.X, mesh.elements, 3, 4, fields, cell, binary)
+    st = mesh.get_stress()
+    # HEX8: the element's Gauss-point mean stress as its cell value
+    cell = {"stress": st.reshape(mesh.n_elements, mesh.n_gauss, 3, 3).mean(axis=1)}
+    return export_vtk(filename, mesh.X, mesh.elements, 3, mesh.nodes_per_elem, fields, cell, binary)

@@ -189,8 +189,8 @@ __global__ void coarse_dense_kernel(const __grid_constant__ CoarseDev c) {
       if (c.cell_corner[cell * 8 + t] == nJ) cJ = t;
     if (cJ >= 0) {
       const size_t off = (size_t)(3 * cI + dI) * 24 + 3 * cJ + dJ;
-      for (int sl = 0; sl < kCellSlices; ++sl)
-        acc += c.blocks[((size_t)cell * kCellSlices + sl) * kCellEntries + off];
+      for (int sl = 0; sl < c.cell_slices; ++sl)
+        acc += c.blocks[((size_t)cell * c.cell_slices + sl) * kCellEntries + off];
     }
   }
   if (I == J && !(acc > 0.0)) acc = 1.0;
@@ -812,7 +812,7 @@ __global__ void jacobi_apply_kernel(const float* __restrict__ r, const float* __
 static inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 size_t coarse_cell_smem() { return sizeof(float) * kCellThreads * (144 + 32); }
-int coarse_cell_slices() { return kCellSlices; }
+int coarse_cell_slices(int npe) { return npe == 8 ? kCellSlices * 4 : kCellSlices; }
 int coarse_restrict_slices(int n_cells) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -838,7 +838,8 @@ void prepare_coarse_kernels(int model, int n_dof) {
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s) {
   const size_t smem = coarse_cell_smem();
   const int g = a.c.n_cells * kCellSlices;
-  switch (model) {
+  if (a.m.npe == 8) launch_coarse_cells_hex(a, model, s);
+  else switch (model) {
     case M_LE: coarse_cell_kernel<M_LE><<<g, kCellThreads, smem, s>>>(a); break;
     case M_NH: coarse_cell_kernel<M_NH><<<g, kCellThreads, smem, s>>>(a); break;
     case M_MR: coarse_cell_kernel<M_MR><<<g, kCellThreads, smem, s>>>(a); break;

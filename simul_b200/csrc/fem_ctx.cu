@@ -992,9 +992,9 @@ constexpr int kMaxCoarseNodesLimit = 16384;
 static_assert(kMaxCoarseNodesLimit <= 65535, "node_corners packs coarse node ids in 16 bits");
 
 int build_coarse(FemCtx* c) {
-  const int Nn = c->Nn, Ne = c->Ne;
+  const int Nn = c->Nn, Ne = c->Ne, npe = c->npe, cw = npe / 4;
   std::vector<double> X(3 * (size_t)Nn);
-  std::vector<int4> conn(Ne);
+  std::vector<int4> conn((size_t)cw * Ne);
   CK(cudaMemcpyAsync(X.data(), c->X64, X.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(conn.data(), c->conn, conn.size() * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1008,20 +1008,26 @@ int build_coarse(FemCtx* c) {
   }
   double vsum = 0.0;
   std::vector<double> cen(3 * (size_t)Ne);
+  // TET4: the three edges at vertex 0 span 6 x the volume; HEX8: vertices
+  // 1, 3 and 4 are vertex 0's edge neighbours (the box volume for a voxel)
+  const int ea = 1, eb = npe == 8 ? 3 : 2, ec = npe == 8 ? 4 : 3;
   for (int e = 0; e < Ne; ++e) {
-    const int* cn = &conn[e].x;
+    const int* cn = &conn[(size_t)cw * e].x;
     double a[3], b[3], cc[3];
     for (int d = 0; d < 3; ++d) {
-      a[d] = X[3 * cn[1] + d] - X[3 * cn[0] + d];
-      b[d] = X[3 * cn[2] + d] - X[3 * cn[0] + d];
-      cc[d] = X[3 * cn[3] + d] - X[3 * cn[0] + d];
-      cen[3 * e + d] = 0.25 * (X[3 * cn[0] + d] + X[3 * cn[1] + d] + X[3 * cn[2] + d] + X[3 * cn[3] + d]);
+      a[d] = X[3 * cn[ea] + d] - X[3 * cn[0] + d];
+      b[d] = X[3 * cn[eb] + d] - X[3 * cn[0] + d];
+      cc[d] = X[3 * cn[ec] + d] - X[3 * cn[0] + d];
+      double s = 0.0;
+      for (int k = 0; k < npe; ++k) s += X[3 * cn[k] + d];
+      cen[3 * e + d] = s / npe;
     }
     const double det = a[0] * (b[1] * cc[2] - b[2] * cc[1]) - a[1] * (b[0] * cc[2] - b[2] * cc[0]) +
                        a[2] * (b[0] * cc[1] - b[1] * cc[0]);
-    vsum += std::fabs(det) / 6.0;
+    vsum += std::fabs(det) / (npe == 8 ? 1.0 : 6.0);
   }
-  const double hmesh = std::cbrt(5.0 * vsum / std::max(Ne, 1));
+  // mesh length: the edge of a voxel (5 tets, or one hexahedron)
+  const double hmesh = std::cbrt((npe == 8 ? 1.0 : 5.0) * vsum / std::max(Ne, 1));
   double H = c->coarse_cell_voxels * hmesh;
   std::vector<int> ecell(Ne), cell_of_lin, act_lin, cn_of_lat;
   int g[3];
@@ -1102,8 +1108,8 @@ int build_coarse(FemCtx* c) {
     for (int e = 0; e < Ne; ++e) {
       const int cl = cell_of_lin[ecell[e]];
       cell_elems[fill[cl]++] = e;
-      const int* cn = &conn[e].x;
-      for (int k = 0; k < 4; ++k)
+      const int* cn = &conn[(size_t)cw * e].x;
+      for (int k = 0; k < npe; ++k)
         if (node_cell[cn[k]] < 0) node_cell[cn[k]] = cl;
     }
   }
@@ -1144,7 +1150,8 @@ int build_coarse(FemCtx* c) {
     CKL();
   }
   const size_t nd = (size_t)cd.n_dof;
-  if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * coarse_cell_slices() * 576))) return st;
+  cd.cell_slices = coarse_cell_slices(c->npe);
+  if ((st = coarse_alloc(c, &cd.blocks, (size_t)n_cells * cd.cell_slices * 576))) return st;
   if ((st = coarse_alloc(c, &cd.Ac, nd * nd))) return st;
   cd.nb16 = (cd.n_dof + 63) / 64;
   const size_t nb = (size_t)cd.nb16;
@@ -1515,9 +1522,9 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
             double* rel) {
   if (!c->tangent_valid) return set_err(c, FEM_ERR_STATE, "no tangent state: evaluate forces first");
   int st;
-  if (c->npe == 8 && (precond == FEM_PRECOND_TWO_LEVEL || precond == FEM_PRECOND_LEARNED)) {
-    // the coarse lattice's Galerkin blocks and the learned network are built
-    // for TET4: a HEX8 context runs these solves as Jacobi-PCG
+  if (c->npe == 8 && precond == FEM_PRECOND_LEARNED) {
+    // the learned network is trained on TET4 graphs: a HEX8 context runs
+    // these solves as Jacobi-PCG
     ++c->n_coarse_fallbacks;
     precond = FEM_PRECOND_JACOBI;
   }
@@ -2646,6 +2653,7 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
   ra.rnorm2 = c->scalars + 2;
   ra.red = c->red();
   ra.red_site = SITE_RES;
+  ra.stage_d = c->stage_d;
   for (int k = 0; k < 4; ++k) {
     CK(reset_cg());
     for (int w = 0; w < 2; ++w) {

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "fem_internal.h"
+#include "fem_lattice.cuh"
 #include "fem_reduce.cuh"
 
 namespace femb200 {
@@ -456,9 +457,122 @@ __global__ void hex_refq_kernel(const MeshDev m, const int* perm_elem, double* d
   }
 }
 
+// ───────────────────────── two-level coarse operator ─────────────────────────
+// Galerkin block of a lattice cell, W^T K_e W summed over the cell's
+// elements (W: the trilinear weights of the element's vertices in the cell;
+// fixed rows and columns of K_e zeroed), as the TET4 cell kernel, here one
+// warp per element: lane l < 24 forms column l = 3 c2 + d2 of K_e W as the
+// element's tangent action on the field w_b(c2) e_d2 and contracts it with
+// W for the 24 rows.  Each warp keeps its share of the cell's 24 x 24 block
+// in registers (element order, FP32 products, FP64 accumulation) and writes
+// it to its own slot; the dense kernel adds the slots in order.
+constexpr int kHexCellCtas = 8;   // CTAs per cell (4 warps each): 32 block shares
+
+template <int MODEL>
+__global__ void __launch_bounds__(128) coarse_cell_hex_kernel(const __grid_constant__ CoarseArgs a) {
+  __shared__ float sW[4][64];     // per warp: W[vertex][corner]
+  __shared__ int sfx[4][8];
+  const MeshDev& m = a.m;
+  const CoarseDev& c = a.c;
+  const int cell = blockIdx.x / kHexCellCtas;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nsl = kHexCellCtas * 4;
+  const int slice = (blockIdx.x - cell * kHexCellCtas) * 4 + warp;
+  const int3 ijk = c.cell_ijk[cell];
+  const int e0 = c.cell_elem_ptr[cell], e1 = c.cell_elem_ptr[cell + 1];
+  const size_t Ne = (size_t)m.n_elems, Nq = kHexGauss * Ne;
+  const int c2 = lane / 3, d2 = lane - 3 * (lane / 3);
+  double acc[24];
+#pragma unroll
+  for (int r = 0; r < 24; ++r) acc[r] = 0.0;
+  for (int idx = e0 + slice; idx < e1; idx += nsl) {
+    const int e = __ldg(c.cell_elems + idx);
+    int nid[8];
+    hex_nodes(m, e, nid);
+    __syncwarp();
+    if (lane < 8) {
+      const float4 X = __ldg(m.X32 + nid[lane]);
+      float t[3];
+      cell_local(c, ijk, X.x, X.y, X.z, t);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) sW[warp][lane * 8 + q] = tri_weight(t[0], t[1], t[2], q);
+      sfx[warp][lane] = (int)m.fixed[nid[lane]];
+    }
+    __syncwarp();
+    if (lane < 24) {
+      float xr[8][3], wcol[8], f[8][3];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float4 X = __ldg(m.X32 + nid[k]);
+        xr[k][0] = X.x;
+        xr[k][1] = X.y;
+        xr[k][2] = X.z;
+        wcol[k] = ((sfx[warp][k] >> d2) & 1) ? 0.f : sW[warp][k * 8 + c2];
+        f[k][0] = f[k][1] = f[k][2] = 0.f;
+      }
+#pragma unroll
+      for (int k = 7; k >= 0; --k)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) xr[k][d] -= xr[0][d];
+      const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
+      const float scale = __ldg(m.scale + e);
+      const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
+#pragma unroll 1
+      for (int g = 0; g < kHexGauss; ++g) {
+        const size_t q = (size_t)g * Ne + e;
+        float dN[8][3], vol;
+        hex_point(xr, g, dN, vol);
+        float dF[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) dF[k] = 0.f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          float s = 0.f;
+#pragma unroll
+          for (int b = 0; b < 8; ++b) s += wcol[b] * dN[b][j];
+          dF[3 * d2 + j] = s;
+        }
+        float pay[kPay];
+#pragma unroll
+        for (int k = 0; k < kPay; ++k) pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * Nq + q) : 0.f;
+        float dP[9];
+        dP_any<MODEL>(mat, scale, pay, dF, dP);
+        hex_add_slots(dP, dN, vol, f);
+      }
+#pragma unroll
+      for (int r = 0; r < 24; ++r) {
+        const int c1 = r / 3, d1 = r - 3 * (r / 3);
+        float s = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          if (!((sfx[warp][k] >> d1) & 1)) s += sW[warp][k * 8 + c1] * f[k][d1];
+        acc[r] += (double)s;
+      }
+    }
+  }
+  if (lane < 24) {
+    double* out = c.blocks + ((size_t)cell * nsl + slice) * 576;
+#pragma unroll
+    for (int r = 0; r < 24; ++r) out[r * 24 + lane] = acc[r];
+  }
+}
+
 inline int nblk(int n, int t) { return (n + t - 1) / t; }
 
 }  // namespace
+
+void launch_coarse_cells_hex(const CoarseArgs& a, int model, cudaStream_t s) {
+  const int g = a.c.n_cells * kHexCellCtas;
+  switch (model) {
+    case M_LE: coarse_cell_hex_kernel<M_LE><<<g, 128, 0, s>>>(a); break;
+    case M_NH: coarse_cell_hex_kernel<M_NH><<<g, 128, 0, s>>>(a); break;
+    case M_MR: coarse_cell_hex_kernel<M_MR><<<g, 128, 0, s>>>(a); break;
+    case M_J2: coarse_cell_hex_kernel<M_J2><<<g, 128, 0, s>>>(a); break;
+    case M_TI: coarse_cell_hex_kernel<M_TI><<<g, 128, 0, s>>>(a); break;
+    case M_FMR: coarse_cell_hex_kernel<M_FMR><<<g, 128, 0, s>>>(a); break;
+    default: coarse_cell_hex_kernel<-1><<<g, 128, 0, s>>>(a); break;
+  }
+}
 
 void launch_residual_hex(const ResArgs& a, int model, cudaStream_t s) {
   const int ge = nblk(a.m.n_elems, 128);

@@ -177,7 +177,8 @@ struct CoarseDev {
   const float4* node_lat;   // [Nn] local coordinates in the node's cell (xyz), the cell (w, int bits)
   const uint4* node_corners;  // [Nn] the cell's 8 corner coarse nodes, 16 bits each (n_cn <= 65535)
   const int* cn_cells;      // [n_cn * 8] cell * 8 + corner, ascending cell, -1 padded
-  double* blocks;           // [n_cells][slices][24 * 24] Galerkin block shares of each cell
+  double* blocks;           // [n_cells][cell_slices][24 * 24] Galerkin block shares of each cell
+  int cell_slices;          // block shares per cell (coarse_cell_slices)
   double* Ac;               // [n_dof * n_dof] column-major; factorised / inverted in place
   const float* Ac32;        // non-null: the inverse's lower triangle is here in FP32 instead (FP32 inversion)
   float* Ainv;              // [n_dof * n_dof] FP32 inverse (symmetric), or null
@@ -298,7 +299,8 @@ void prepare_kernels(const MeshDev& m, int model);
 void launch_diag(const DiagArgs& a, int model, cudaStream_t s);
 // coarse lattice (fem_coarse.cu)
 size_t coarse_cell_smem();
-int coarse_cell_slices();   // CTAs (and Galerkin block slots) per lattice cell
+// Galerkin block slots per lattice cell (TET4: one per CTA; HEX8: one per warp)
+int coarse_cell_slices(int npe);
 int coarse_restrict_slices(int n_cells);  // node slices (restriction warps) per lattice cell
 // x += alpha p, r -= alpha q and the restriction of the new r into cell_r
 // (one kernel; ||r||^2 and the convergence test follow in tl_rz)
@@ -309,6 +311,8 @@ void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s)
 void prepare_coarse_kernels(int model, int n_dof);
 // cell Galerkin blocks + dense Ac (FP64, column-major)
 void launch_coarse_assemble(const CoarseArgs& a, int model, cudaStream_t s);
+// HEX8 cells' Galerkin block shares (fem_hex8.cu); launch_coarse_assemble calls it
+void launch_coarse_cells_hex(const CoarseArgs& a, int model, cudaStream_t s);
 // Ainv = FP32 symmetric copy of the lower triangle left in Ac
 // fills node_lat from X32, node_cell and cell_ijk
 void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, cudaStream_t s);

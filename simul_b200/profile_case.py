@@ -1,6 +1,7 @@
 """Small, self-terminating workload for kernel profiling (ncu) and timing.
 
-Builds the synthetic vertebral body at ``--n`` voxels per axis, binds J2
+Builds the synthetic vertebral body at ``--n`` voxels per axis (five TET4
+per voxel, or one HEX8 per voxel with ``--element hex8``), binds J2
 plasticity, evaluates the FP64 residual at a plastic state (top face pushed
 ``--strain`` of the height, which yields the cortical shell), and launches each
 hot kernel ``--reps`` times through ``fem_profile_kernels``: the tangent matvec
@@ -27,6 +28,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=64)
     ap.add_argument("--variant", default="fused", choices=["fused", "two_phase"])
+    ap.add_argument("--element", default="tet4", choices=["tet4", "hex8"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--strain", type=float, default=0.004)
     ap.add_argument("--nodes-per-block", type=int, default=0)
@@ -41,8 +43,9 @@ def main(argv=None):
     from simul_b200 import _lib, meshgen
     from simul_b200 import fem as B
 
-    v = meshgen.vertebral_body(n=args.n, seed=0)
-    mesh = B.FEMesh(v.n_nodes, v.n_elements, device=0, nodes_per_block=args.nodes_per_block)
+    v = meshgen.vertebral_body(n=args.n, seed=0, element=args.element)
+    et = B.ElementType.HEX8 if args.element == "hex8" else B.ElementType.TET4
+    mesh = B.FEMesh(v.n_nodes, v.n_elements, et, device=0, nodes_per_block=args.nodes_per_block)
     mesh.initialize_from_numpy(v.X, v.conn)
     mesh.set_matvec_variant(args.variant)
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
@@ -88,8 +91,9 @@ def main(argv=None):
         extra["two_level_iterations"] = it.value
         extra["coarse"] = mesh.coarse_info()
     info = mesh.info()
-    print(json.dumps({"n": args.n, "tets": info["n_elements"], "nodes": info["n_nodes"],
-                      "variant": args.variant, "reps": args.reps,
+    print(json.dumps({"n": args.n, "element": args.element, "elements": info["n_elements"],
+                      "nodes": info["n_nodes"], "variant": "two_phase" if args.element == "hex8" else args.variant,
+                      "reps": args.reps,
                       "ms": {"matvec": ms[0], "residual": ms[1], "cg_update": ms[2], "cg_direction": ms[3]},
                       **extra}))
 

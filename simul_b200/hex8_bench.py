@@ -31,6 +31,8 @@ def main(argv=None):
     ap.add_argument("--precond", nargs="+", default=["two_level", "jacobi"],
                     choices=["two_level", "jacobi"])
     ap.add_argument("--coarse-cell", type=int, default=4)
+    ap.add_argument("--whole-solve-graph", type=int, default=1,
+                    help="0: fixed-size iteration graphs (kernel profilers cannot see into the conditional graph)")
     args = ap.parse_args(argv)
 
     import torch
@@ -46,6 +48,7 @@ def main(argv=None):
         mesh.initialize_from_numpy(v.X, v.conn)
         mesh.set_coarse_options(cell=args.coarse_cell, bf16=True, reuse=0, inverse="trsm_syrk_tf32",
                                 max_nodes=6144)
+        mesh.set_whole_solve_graph(bool(args.whole_solve_graph))
         mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
         solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=pc)
         idx = np.where(v.fixed_mask.reshape(-1))[0]

@@ -89,6 +89,47 @@ def voxel_hex8(mask: np.ndarray, h: float, origin=(0.0, 0.0, 0.0)):
     return X, conn.astype(np.int32), (vi, vj, vk)
 
 
+def labelmap_voxel_centers(label_volume: np.ndarray, spacing, origin=(0.0, 0.0, 0.0), label: int = 1):
+    """Physical centres of the voxels carrying ``label`` (preprocessing/assembly.py:82-90):
+    ijk * spacing + origin + spacing / 2, voxels in C order of (i, j, k)."""
+    spacing = np.asarray(spacing, dtype=np.float64).reshape(3)
+    origin = np.asarray(origin, dtype=np.float64).reshape(3)
+    ijk = np.argwhere(np.asarray(label_volume) == label)
+    return ijk.astype(np.float64) * spacing + origin + spacing / 2.0
+
+
+def labelmap_bodies(label_volume: np.ndarray, spacing, origin=(0.0, 0.0, 0.0), min_voxels: int = 10) -> dict:
+    """One HEX8 body per non-zero label with at least ``min_voxels`` voxels,
+    as the labelmap assembly builds its FEM bodies (preprocessing/assembly.py:73-99,
+    207-249): label -> (nodes, elements) from ``voxels_to_hex_mesh``.  The
+    scene, contacts and particle bodies around them are not built here."""
+    out = {}
+    labels = np.unique(label_volume)
+    for label in labels[labels != 0]:
+        centers = labelmap_voxel_centers(label_volume, spacing, origin, int(label))
+        if centers.shape[0] < min_voxels:
+            continue
+        out[int(label)] = voxels_to_hex_mesh(centers, spacing)
+    return out
+
+
+def labelmap_hex8(label_volume: np.ndarray, spacing, origin=(0.0, 0.0, 0.0), labels=None):
+    """All voxels of ``labels`` (default: every non-zero label) as one
+    conforming HEX8 mesh: neighbouring voxels of different labels share their
+    face nodes (bonded bodies).  Returns nodes, connectivity (int32) and the
+    label of every element, for a per-label material table."""
+    lv = np.asarray(label_volume)
+    if labels is None:
+        labels = [int(v) for v in np.unique(lv) if v != 0]
+    centers, elabel = [], []
+    for label in labels:
+        c = labelmap_voxel_centers(lv, spacing, origin, label)
+        centers.append(c)
+        elabel.append(np.full(c.shape[0], label, dtype=np.int32))
+    X, conn = voxels_to_hex_mesh(np.concatenate(centers) if centers else np.empty((0, 3)), spacing)
+    return X, conn.astype(np.int32), (np.concatenate(elabel) if elabel else np.empty(0, dtype=np.int32))
+
+
 @dataclass
 class TetMesh:
     """A TET4 (or HEX8) mesh with boundary data, in the caller's (generator) order."""

@@ -230,3 +230,32 @@ def test_hex8_invalid_connectivity_raises(cuda):
         mesh.initialize_from_numpy(X, bad)
     with pytest.raises(B.FEAValidationError):
         mesh.initialize_from_numpy(X, conn[:, :4])
+
+
+def test_labelmap_bonded_stack_on_gpu(cuda):
+    # a two-label labelmap as one conforming HEX8 mesh, modulus by label:
+    # the interface displacement of the series stack (nu = 0, rollers)
+    lv = np.zeros((6, 5, 7), dtype=np.int16)
+    lv[1:5, 1:4, 0:3] = 1
+    lv[1:5, 1:4, 3:5] = 2
+    X, conn, lab = meshgen.labelmap_hex8(lv, [1.0, 1.0, 1.0])
+    E = np.where(lab == 1, 1000.0, 250.0)
+    mesh = hex_mesh(X, conn, cuda)
+    fixed = np.zeros_like(X, dtype=bool)
+    vals = np.zeros_like(X)
+    for d in range(3):
+        fixed[np.isclose(X[:, d], X[:, d].min()), d] = True
+    top = np.isclose(X[:, 2], X[:, 2].max())
+    fixed[top, 2] = True
+    vals[top, 2] = -0.05
+    idx = np.where(fixed.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, vals.reshape(-1)[idx])
+    res = B.StaticSolver(mesh, B.LinearElastic(E, 0.0), tol=1e-10, precond="two_level").solve(verbose=False)
+    assert res["converged"], res
+    u = mesh.get_displacements()
+    iface = np.isclose(X[:, 2], 3.0)
+    c1, c2 = 3.0 / 1000.0, 2.0 / 250.0
+    assert np.allclose(u[iface, 2], -0.05 * c1 / (c1 + c2), rtol=1e-7)
+    want, _ = O.consistent_newton(O.Mesh(X, conn), O.Material("linear_elastic", E=E, nu=0.0), np.zeros_like(X),
+                                  fixed, vals, tol=1e-12)
+    assert _rel_l2(u, want) < 1e-7

@@ -134,3 +134,51 @@ def test_hex8_vertebral_body_generator():
     assert vb.E.shape == (vb.conn.shape[0],)
     with pytest.raises(ValueError):
         meshgen.vertebral_body(8, element="tet10")
+
+
+def _two_label_volume():
+    lv = np.zeros((6, 5, 7), dtype=np.int16)
+    lv[1:5, 1:4, 0:3] = 1          # lower body
+    lv[1:5, 1:4, 3:5] = 2          # upper body, bonded on the z = 3 face
+    lv[0, 0, 6] = 3                # a one-voxel label, below min_voxels
+    return lv
+
+
+def test_labelmap_bodies_follow_the_assembly_pipeline():
+    # preprocessing/assembly.py:73-99, 207-249: per label the voxel centres
+    # ijk * spacing + origin + spacing / 2, then voxels_to_hex_mesh
+    lv = _two_label_volume()
+    spacing, origin = np.array([0.5, 0.6, 0.7]), np.array([1.0, -2.0, 3.0])
+    bodies = meshgen.labelmap_bodies(lv, spacing, origin, min_voxels=10)
+    assert sorted(bodies) == [1, 2]
+    X1, e1 = bodies[1]
+    assert e1.shape == (36, 8) and X1.shape == (5 * 4 * 4, 3)
+    c = meshgen.labelmap_voxel_centers(lv, spacing, origin, 1)
+    assert np.allclose(c[0], origin + spacing / 2 + np.array([1, 1, 0]) * spacing)
+    m = O.Mesh(X1, e1)
+    assert np.allclose(m.elem_vol, np.prod(spacing))
+
+
+def test_labelmap_hex8_bonds_labels_into_one_mesh():
+    lv = _two_label_volume()
+    X, conn, lab = meshgen.labelmap_hex8(lv, [1.0, 1.0, 1.0], labels=[1, 2])
+    assert conn.shape == (36 + 24, 8) and np.array_equal(np.unique(lab), [1, 2])
+    shared = set(conn[lab == 1].ravel()) & set(conn[lab == 2].ravel())
+    assert len(shared) == 5 * 4        # the z = 3 interface nodes
+    # two moduli by label, nu = 0, rollers: each layer strains uniformly, so
+    # the interface moves by delta (L1 / E1) / (L1 / E1 + L2 / E2) only when
+    # the labels share their interface nodes
+    E = np.where(lab == 1, 1000.0, 250.0)
+    fixed = np.zeros_like(X, dtype=bool)
+    vals = np.zeros_like(X)
+    for d in range(3):
+        fixed[np.isclose(X[:, d], X[:, d].min()), d] = True
+    top = np.isclose(X[:, 2], X[:, 2].max())
+    fixed[top, 2] = True
+    vals[top, 2] = -0.05
+    u, info = O.consistent_newton(O.Mesh(X, conn), O.Material("linear_elastic", E=E, nu=0.0), np.zeros_like(X),
+                                  fixed, vals, tol=1e-12)
+    assert info["converged"]
+    iface = np.isclose(X[:, 2], 3.0)
+    c1, c2 = 3.0 / 1000.0, 2.0 / 250.0
+    assert np.allclose(u[iface, 2], -0.05 * c1 / (c1 + c2), rtol=1e-10)

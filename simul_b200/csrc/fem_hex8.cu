@@ -216,6 +216,46 @@ __global__ void __launch_bounds__(256) hex_res_gather_kernel(const __grid_consta
 
 // ───────────────────────── tangent matvec (FP32) ─────────────────────────
 
+// Trilinear form of a vertex field v: v(xi) = c_1 + sum_m C_m m(xi) over the
+// monomials m = xi, eta, zeta, xi eta, eta zeta, xi zeta, xi eta zeta, with
+// C_m = 1/8 sum_a sigma_a^m v_a (sigma_a^m: the product of vertex a's signs
+// in the monomial's coordinates).  Its natural-coordinate gradient at a
+// point then costs 4 terms per entry instead of 8 vertex products.
+__host__ __device__ constexpr int hex_msign(int a, int m) {
+  return m < 3 ? hex_sign(a, m)
+               : (m == 3 ? hex_sign(a, 0) * hex_sign(a, 1)
+                         : (m == 4 ? hex_sign(a, 1) * hex_sign(a, 2)
+                                   : (m == 5 ? hex_sign(a, 0) * hex_sign(a, 2)
+                                             : hex_sign(a, 0) * hex_sign(a, 1) * hex_sign(a, 2))));
+}
+
+__device__ __forceinline__ void hex_coeffs(const float v[8][3], float C[7][3]) {
+#pragma unroll
+  for (int m = 0; m < 7; ++m)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      float s = 0.f;
+#pragma unroll
+      for (int a = 0; a < 8; ++a) s += hex_msign(a, m) > 0 ? v[a][d] : -v[a][d];
+      C[m][d] = 0.125f * s;
+    }
+}
+
+// G[i][j] = d v_i / d xi_j at (gx, gy, gz) from the coefficients
+__device__ __forceinline__ void hex_nat_grad(const float C[7][3], float gx, float gy, float gz, float G[3][3]) {
+  const float yz = gy * gz, xz = gx * gz, xy = gx * gy;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    G[i][0] = C[0][i] + C[3][i] * gy + C[5][i] * gz + C[6][i] * yz;
+    G[i][1] = C[1][i] + C[3][i] * gx + C[4][i] * gz + C[6][i] * xz;
+    G[i][2] = C[2][i] + C[4][i] * gy + C[5][i] * gx + C[6][i] * xy;
+  }
+}
+
+// Tangent action of one hexahedron in the trilinear basis: per point,
+// J and the natural gradient of p from the coefficients, dF = G_p J^-1,
+// T = |det J| dP J^-T, and T is accumulated into the 7 monomial moments A;
+// the vertex vectors f_a = 1/8 sum_m sigma_a^m A_m are formed once.
 template <int MODEL, bool CG, bool MASK>
 __device__ __forceinline__ void hex_mv_one(const MvArgs& a, int e) {
   const MeshDev& m = a.m;
@@ -223,45 +263,98 @@ __device__ __forceinline__ void hex_mv_one(const MvArgs& a, int e) {
   int nid[8];
   hex_nodes(m, e, nid);
   const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
-  float xr[8][3], pv[8][3], f[8][3];
+  float cx[7][3], cp[7][3];
+  {
+    float xr[8][3], pv[8][3];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const float4 X = __ldg(m.X32 + nid[k]);
-    const float4 P = __ldg(xin + nid[k]);
-    xr[k][0] = X.x;
-    xr[k][1] = X.y;
-    xr[k][2] = X.z;
-    const int fx = MASK ? (int)X.w : 0;
-    pv[k][0] = (fx & 1) ? 0.f : P.x;
-    pv[k][1] = (fx & 2) ? 0.f : P.y;
-    pv[k][2] = (fx & 4) ? 0.f : P.z;
-    f[k][0] = f[k][1] = f[k][2] = 0.f;
+    for (int k = 0; k < 8; ++k) {
+      const float4 X = __ldg(m.X32 + nid[k]);
+      const float4 P = __ldg(xin + nid[k]);
+      xr[k][0] = X.x;
+      xr[k][1] = X.y;
+      xr[k][2] = X.z;
+      const int fx = MASK ? (int)X.w : 0;
+      pv[k][0] = (fx & 1) ? 0.f : P.x;
+      pv[k][1] = (fx & 2) ? 0.f : P.y;
+      pv[k][2] = (fx & 4) ? 0.f : P.z;
+    }
+#pragma unroll
+    for (int k = 7; k >= 0; --k)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) xr[k][d] -= xr[0][d];
+    hex_coeffs(xr, cx);
+    hex_coeffs(pv, cp);
   }
-#pragma unroll
-  for (int k = 7; k >= 0; --k)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) xr[k][d] -= xr[0][d];
   const DevMat<float>& mat = a.matF[__ldg(m.mat_id + e)];
   const float scale = __ldg(m.scale + e);
   const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
+  float A[7][3];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) A[k][0] = A[k][1] = A[k][2] = 0.f;
 #pragma unroll 1
   for (int g = 0; g < kHexGauss; ++g) {
     const size_t q = (size_t)g * Ne + e;
-    float dN[8][3], vol;
-    hex_point(xr, g, dN, vol);
-    float dF[9];
-    hex_grad(pv, dN, dF);
     float pay[kPay];
 #pragma unroll
     for (int k = 0; k < kPay; ++k) pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * Nq + q) : 0.f;
+    const float gx = (float)hex_sign(g, 0) * (float)kGaussHex;
+    const float gy = (float)hex_sign(g, 1) * (float)kGaussHex;
+    const float gz = (float)hex_sign(g, 2) * (float)kGaussHex;
+    float J[3][3], Gp[3][3];
+    hex_nat_grad(cx, gx, gy, gz, J);
+    hex_nat_grad(cp, gx, gy, gz, Gp);
+    const float c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    const float c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+    const float c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    const float det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+    const float id = 1.f / det;
+    float Ji[3][3];
+    Ji[0][0] = c00 * id;
+    Ji[1][0] = c01 * id;
+    Ji[2][0] = c02 * id;
+    Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+    Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+    Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+    Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+    Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+    Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+    const float vol = det < 0.f ? -det : det;
+    float dF[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) dF[3 * i + k] = Gp[i][0] * Ji[0][k] + Gp[i][1] * Ji[1][k] + Gp[i][2] * Ji[2][k];
     float dP[9];
     dP_any<MODEL>(mat, scale, pay, dF, dP);
-    hex_add_slots(dP, dN, vol, f);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float T[3];
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        T[j] = vol * (dP[3 * i] * Ji[j][0] + dP[3 * i + 1] * Ji[j][1] + dP[3 * i + 2] * Ji[j][2]);
+      A[0][i] += T[0];
+      A[1][i] += T[1];
+      A[2][i] += T[2];
+      A[3][i] += T[0] * gy + T[1] * gx;
+      A[4][i] += T[1] * gz + T[2] * gy;
+      A[5][i] += T[0] * gz + T[2] * gx;
+      A[6][i] += T[0] * (gy * gz) + T[1] * (gx * gz) + T[2] * (gx * gy);
+    }
   }
   int pos[8];
   hex_slots(m, e, pos);
 #pragma unroll
-  for (int k = 0; k < 8; ++k) __stcg(a.stage + pos[k], make_float4(f[k][0], f[k][1], f[k][2], 0.f));
+  for (int k = 0; k < 8; ++k) {
+    float f[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      float s = 0.f;
+#pragma unroll
+      for (int mm = 0; mm < 7; ++mm) s += hex_msign(k, mm) > 0 ? A[mm][i] : -A[mm][i];
+      f[i] = 0.125f * s;
+    }
+    __stcg(a.stage + pos[k], make_float4(f[0], f[1], f[2], 0.f));
+  }
 }
 
 template <int MODEL, bool CG>

@@ -25,14 +25,15 @@ class DynamicOracle:
         self.method, self.formulation = method, formulation
         n = mesh.X.shape[0]
         node_mass = np.zeros(n)
+        npe = mesh.conn.shape[1]
         np.add.at(node_mass, np.asarray(mesh.conn, dtype=np.int64).reshape(-1),
-                  np.repeat(density * mesh.vol / 4.0, 4))
+                  np.repeat(density * mesh.elem_vol / float(npe), npe))
         self.M = np.repeat(node_mass, 3)
         self.K = O.reference_K_material(mesh, O.isotropic_voigt_C(E, nu)).tocsr()
         self.C = rayleigh_alpha * sparse.diags(self.M) + rayleigh_beta * self.K
         self.free = ~np.asarray(fixed_mask, dtype=bool).reshape(-1)
         if dt is None:
-            h = np.mean(mesh.vol) ** (1.0 / 3.0)
+            h = np.mean(mesh.elem_vol) ** (1.0 / 3.0)
             c = np.sqrt(E * (1 - nu) / (density * (1 + nu) * (1 - 2 * nu)))
             dt = 0.8 * h / c
         self.dt = dt

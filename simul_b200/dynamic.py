@@ -2,7 +2,7 @@
 
 Mirrors ``DynamicSolver`` of the reference
 (backend/fea/fem/solver/dynamic_solver.py:21-413): row-sum lumped mass
-(density x element volume / 4 per node), Rayleigh damping C = alpha M +
+(density x element volume / nodes per element, per node), Rayleigh damping C = alpha M +
 beta K with K the stiffness at rest, the stable-step estimate
 dt = 0.8 h / c, Newmark (gamma = 1/2, beta = 1/4) and central-difference
 steps, the same ``step`` / ``solve`` / getter API.

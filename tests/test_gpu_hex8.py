@@ -259,3 +259,55 @@ def test_labelmap_bonded_stack_on_gpu(cuda):
     want, _ = O.consistent_newton(O.Mesh(X, conn), O.Material("linear_elastic", E=E, nu=0.0), np.zeros_like(X),
                                   fixed, vals, tol=1e-12)
     assert _rel_l2(u, want) < 1e-7
+
+
+def _hex_beam():
+    X, conn = meshgen.structured_hex8(8, 2, 2, (8.0, 1.0, 1.0))
+    fixed = np.zeros_like(X, dtype=bool)
+    fixed[np.isclose(X[:, 0], 0.0)] = True
+    return X, conn, fixed
+
+
+def test_hex8_dynamics_and_natural_frequencies(cuda):
+    # Newmark on a HEX8 cantilever (lumped mass: density x volume / 8 per
+    # vertex) and its lowest natural frequencies, against the dynamic oracle
+    from oracle.dynamic_oracle import DynamicOracle
+    from simul_b200.dynamic import DynamicSolver
+    X, conn, fixed = _hex_beam()
+    mesh = hex_mesh(X, conn, cuda)
+    mesh.set_fixed_nodes(np.where(fixed[:, 0])[0])
+    dyn = DynamicSolver(mesh, B.LinearElastic(1000.0, 0.3), density=1e-3, method="newmark",
+                        rayleigh_alpha=0.5, rayleigh_beta=1e-4, formulation="consistent", cg_rtol=1e-8)
+    ora = DynamicOracle(O.Mesh(X, conn), O.Material("linear_elastic", E=1000.0, nu=0.3), 1000.0, 0.3, fixed,
+                        density=1e-3, method="newmark", rayleigh_alpha=0.5, rayleigh_beta=1e-4,
+                        formulation="consistent")
+    assert abs(dyn.dt - ora.dt) <= 1e-12 * ora.dt
+    assert _rel_l2(dyn.M_diag.cpu().numpy(), ora.M) < 1e-12
+    f = np.zeros_like(X)
+    f[np.isclose(X[:, 0], 8.0), 2] = -0.01
+    for _ in range(10):
+        dyn.step(f)
+        ora.step(f)
+    assert _rel_l2(dyn.u.cpu().numpy(), ora.u) < 2e-5
+    got = DynamicSolver(mesh, B.LinearElastic(1000.0, 0.3), density=1e-3).get_natural_frequencies(4)
+    want = ora.natural_frequencies(4)
+    assert np.all(np.abs(got - want) <= 1e-4 * want), (got, want)
+
+
+def test_hex8_arc_length_path_reaches_the_load(cuda):
+    # the arc-length loop over the HEX8 kernels ends at lambda = 1 on the
+    # load-controlled equilibrium
+    from simul_b200.arclength import ArcLengthSolver
+    X, conn, fixed = _hex_beam()
+    f = np.zeros_like(X)
+    f[np.isclose(X[:, 0], 8.0), 2] = -2.0
+    mesh = hex_mesh(X, conn, cuda)
+    mesh.set_fixed_nodes(np.where(fixed[:, 0])[0])
+    mesh.set_nodal_forces(np.arange(X.shape[0]), f)
+    mat = B.NeoHookean(1000.0, 0.3)
+    res = ArcLengthSolver(mesh, mat, arc_length=0.5, max_steps=60, tol=1e-8, cg_rtol=1e-9).solve(verbose=False)
+    lams = np.array(res["load_factors"])
+    assert res["converged"] and np.all(np.diff(lams) > 0) and 1.0 <= lams[-1] < 1.01
+    want, _ = O.consistent_newton(O.Mesh(X, conn), O.Material("neo_hookean", E=1000.0, nu=0.3), lams[-1] * f,
+                                  fixed, np.zeros_like(X), tol=1e-12)
+    assert _rel_l2(res["displacements"][-1].reshape(-1, 3), want) < 1e-6

@@ -117,6 +117,97 @@ __device__ __forceinline__ void hex_add_slots(const T S[9], const T dN[8][3], T 
       f[a][i] += coef * (S[3 * i] * dN[a][0] + S[3 * i + 1] * dN[a][1] + S[3 * i + 2] * dN[a][2]);
 }
 
+// Trilinear form of a vertex field v: v(xi) = c_1 + sum_m C_m m(xi) over the
+// monomials m = xi, eta, zeta, xi eta, eta zeta, xi zeta, xi eta zeta, with
+// C_m = 1/8 sum_a sigma_a^m v_a (sigma_a^m: the product of vertex a's signs
+// in the monomial's coordinates).  Its natural-coordinate gradient at a
+// point then costs 4 terms per entry instead of 8 vertex products, and the
+// vertex forces f_a = sum_j T_j dN_a/dxi_j of a point's stress-like tensor T
+// are 1/8 sum_m sigma_a^m A_m over 7 accumulated moments A_m.
+__host__ __device__ constexpr int hex_msign(int a, int m) {
+  return m < 3 ? hex_sign(a, m)
+               : (m == 3 ? hex_sign(a, 0) * hex_sign(a, 1)
+                         : (m == 4 ? hex_sign(a, 1) * hex_sign(a, 2)
+                                   : (m == 5 ? hex_sign(a, 0) * hex_sign(a, 2)
+                                             : hex_sign(a, 0) * hex_sign(a, 1) * hex_sign(a, 2))));
+}
+
+template <typename T>
+__device__ __forceinline__ void hex_coeffs(const T v[8][3], T C[7][3]) {
+#pragma unroll
+  for (int m = 0; m < 7; ++m)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      T s = T(0);
+#pragma unroll
+      for (int a = 0; a < 8; ++a) s += hex_msign(a, m) > 0 ? v[a][d] : -v[a][d];
+      C[m][d] = T(0.125) * s;
+    }
+}
+
+// G[i][j] = d v_i / d xi_j at (gx, gy, gz) from the coefficients
+template <typename T>
+__device__ __forceinline__ void hex_nat_grad(const T C[7][3], T gx, T gy, T gz, T G[3][3]) {
+  const T yz = gy * gz, xz = gx * gz, xy = gx * gy;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    G[i][0] = C[0][i] + C[3][i] * gy + C[5][i] * gz + C[6][i] * yz;
+    G[i][1] = C[1][i] + C[3][i] * gx + C[4][i] * gz + C[6][i] * xz;
+    G[i][2] = C[2][i] + C[4][i] * gy + C[5][i] * gx + C[6][i] * xy;
+  }
+}
+
+// J^-1 by cofactors and |det J|
+template <typename T>
+__device__ __forceinline__ void hex_inv(const T J[3][3], T Ji[3][3], T& vol) {
+  const T c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const T c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const T c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const T det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  const T id = T(1) / det;
+  Ji[0][0] = c00 * id;
+  Ji[1][0] = c01 * id;
+  Ji[2][0] = c02 * id;
+  Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
+  Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
+  Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
+  Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
+  Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
+  Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
+  vol = det < T(0) ? -det : det;
+}
+
+// A_m += moments of T_ij = coef sum_k S_ik Ji_jk (the point's contribution
+// f_a = coef S dN_a, with dN_a = J^-T dN_a/dxi)
+template <typename T>
+__device__ __forceinline__ void hex_moments(const T S[9], const T Ji[3][3], T coef, T gx, T gy, T gz, T A[7][3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T t[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) t[j] = coef * (S[3 * i] * Ji[j][0] + S[3 * i + 1] * Ji[j][1] + S[3 * i + 2] * Ji[j][2]);
+    A[0][i] += t[0];
+    A[1][i] += t[1];
+    A[2][i] += t[2];
+    A[3][i] += t[0] * gy + t[1] * gx;
+    A[4][i] += t[1] * gz + t[2] * gy;
+    A[5][i] += t[0] * gz + t[2] * gx;
+    A[6][i] += t[0] * (gy * gz) + t[1] * (gx * gz) + t[2] * (gx * gy);
+  }
+}
+
+// vertex a's vector 1/8 sum_m sigma_a^m A_m (a a constant after unrolling)
+template <typename T>
+__device__ __forceinline__ void hex_vertex(const T A[7][3], int a, T f[3]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    T s = T(0);
+#pragma unroll
+    for (int mm = 0; mm < 7; ++mm) s += hex_msign(a, mm) > 0 ? A[mm][i] : -A[mm][i];
+    f[i] = T(0.125) * s;
+  }
+}
+
 // ───────────────────────── residual (FP64) ─────────────────────────
 
 template <int MODEL>
@@ -127,30 +218,39 @@ __global__ void __launch_bounds__(128) hex_res_elem_kernel(const __grid_constant
   const size_t Ne = (size_t)m.n_elems, Nq = kHexGauss * Ne;
   int nid[8];
   hex_nodes(m, e, nid);
-  double xr[8][3], uv[8][3], f[8][3];
+  double cx[7][3], cu[7][3];
+  {
+    double xr[8][3], uv[8][3];
 #pragma unroll
-  for (int k = 0; k < 8; ++k)
+    for (int k = 0; k < 8; ++k)
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      xr[k][d] = __ldg(m.X64 + 3 * nid[k] + d);
-      uv[k][d] = __ldg(a.u + 3 * nid[k] + d);
-      f[k][d] = 0.0;
-    }
-#pragma unroll
-  for (int k = 7; k >= 0; --k)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) xr[k][d] -= xr[0][d];
+      for (int d = 0; d < 3; ++d) {
+        xr[k][d] = __ldg(m.X64 + 3 * nid[k] + d);
+        uv[k][d] = __ldg(a.u + 3 * nid[k] + d);
+      }
+    hex_coeffs(xr, cx);   // the monomial coefficients do not see the position
+    hex_coeffs(uv, cu);
+  }
   const DevMat<double>& mat = a.matD[__ldg(m.mat_id + e)];
   const double scale = (double)__ldg(m.scale + e);
   const int model = MODEL >= 0 ? MODEL : mat.model;
   const int npay = model_pay_words(model);
+  double A[7][3];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) A[k][0] = A[k][1] = A[k][2] = 0.0;
 #pragma unroll 1
   for (int g = 0; g < kHexGauss; ++g) {
     const size_t q = (size_t)g * Ne + e;
-    double dN[8][3], vol;
-    hex_point(xr, g, dN, vol);
+    const double gx = hex_sign(g, 0) * kGaussHex, gy = hex_sign(g, 1) * kGaussHex, gz = hex_sign(g, 2) * kGaussHex;
+    double J[3][3], Gu[3][3], Ji[3][3], vol;
+    hex_nat_grad(cx, gx, gy, gz, J);
+    hex_nat_grad(cu, gx, gy, gz, Gu);
+    hex_inv(J, Ji, vol);
     double Hg[9];
-    hex_grad(uv, dN, Hg);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) Hg[3 * i + k] = Gu[i][0] * Ji[0][k] + Gu[i][1] * Ji[1][k] + Gu[i][2] * Ji[2][k];
     double S[9];
     float pay[kPay];
     if (model == M_NH) {
@@ -173,14 +273,17 @@ __global__ void __launch_bounds__(128) hex_res_elem_kernel(const __grid_constant
 #pragma unroll
     for (int k = 0; k < kPay; ++k)
       if (k < npay) a.payload[(size_t)k * Nq + q] = pay[k];
-    hex_add_slots(S, dN, -vol, f);
+    hex_moments(S, Ji, -vol, gx, gy, gz, A);
   }
   int pos[8];
   hex_slots(m, e, pos);
 #pragma unroll
-  for (int k = 0; k < 8; ++k)
+  for (int k = 0; k < 8; ++k) {
+    double f[3];
+    hex_vertex(A, k, f);
 #pragma unroll
-    for (int d = 0; d < 3; ++d) a.stage_d[3 * (size_t)pos[k] + d] = f[k][d];
+    for (int d = 0; d < 3; ++d) a.stage_d[3 * (size_t)pos[k] + d] = f[d];
+  }
 }
 
 __global__ void __launch_bounds__(256) hex_res_gather_kernel(const __grid_constant__ ResArgs a) {
@@ -215,42 +318,6 @@ __global__ void __launch_bounds__(256) hex_res_gather_kernel(const __grid_consta
 }
 
 // ───────────────────────── tangent matvec (FP32) ─────────────────────────
-
-// Trilinear form of a vertex field v: v(xi) = c_1 + sum_m C_m m(xi) over the
-// monomials m = xi, eta, zeta, xi eta, eta zeta, xi zeta, xi eta zeta, with
-// C_m = 1/8 sum_a sigma_a^m v_a (sigma_a^m: the product of vertex a's signs
-// in the monomial's coordinates).  Its natural-coordinate gradient at a
-// point then costs 4 terms per entry instead of 8 vertex products.
-__host__ __device__ constexpr int hex_msign(int a, int m) {
-  return m < 3 ? hex_sign(a, m)
-               : (m == 3 ? hex_sign(a, 0) * hex_sign(a, 1)
-                         : (m == 4 ? hex_sign(a, 1) * hex_sign(a, 2)
-                                   : (m == 5 ? hex_sign(a, 0) * hex_sign(a, 2)
-                                             : hex_sign(a, 0) * hex_sign(a, 1) * hex_sign(a, 2))));
-}
-
-__device__ __forceinline__ void hex_coeffs(const float v[8][3], float C[7][3]) {
-#pragma unroll
-  for (int m = 0; m < 7; ++m)
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      float s = 0.f;
-#pragma unroll
-      for (int a = 0; a < 8; ++a) s += hex_msign(a, m) > 0 ? v[a][d] : -v[a][d];
-      C[m][d] = 0.125f * s;
-    }
-}
-
-// G[i][j] = d v_i / d xi_j at (gx, gy, gz) from the coefficients
-__device__ __forceinline__ void hex_nat_grad(const float C[7][3], float gx, float gy, float gz, float G[3][3]) {
-  const float yz = gy * gz, xz = gx * gz, xy = gx * gy;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    G[i][0] = C[0][i] + C[3][i] * gy + C[5][i] * gz + C[6][i] * yz;
-    G[i][1] = C[1][i] + C[3][i] * gx + C[4][i] * gz + C[6][i] * xz;
-    G[i][2] = C[2][i] + C[4][i] * gy + C[5][i] * gx + C[6][i] * xy;
-  }
-}
 
 // Tangent action of one hexahedron in the trilinear basis: per point,
 // J and the natural gradient of p from the coefficients, dF = G_p J^-1,
@@ -300,25 +367,10 @@ __device__ __forceinline__ void hex_mv_one(const MvArgs& a, int e) {
     const float gx = (float)hex_sign(g, 0) * (float)kGaussHex;
     const float gy = (float)hex_sign(g, 1) * (float)kGaussHex;
     const float gz = (float)hex_sign(g, 2) * (float)kGaussHex;
-    float J[3][3], Gp[3][3];
+    float J[3][3], Gp[3][3], Ji[3][3], vol;
     hex_nat_grad(cx, gx, gy, gz, J);
     hex_nat_grad(cp, gx, gy, gz, Gp);
-    const float c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-    const float c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-    const float c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-    const float det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-    const float id = 1.f / det;
-    float Ji[3][3];
-    Ji[0][0] = c00 * id;
-    Ji[1][0] = c01 * id;
-    Ji[2][0] = c02 * id;
-    Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * id;
-    Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * id;
-    Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * id;
-    Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * id;
-    Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * id;
-    Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * id;
-    const float vol = det < 0.f ? -det : det;
+    hex_inv(J, Ji, vol);
     float dF[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -326,33 +378,14 @@ __device__ __forceinline__ void hex_mv_one(const MvArgs& a, int e) {
       for (int k = 0; k < 3; ++k) dF[3 * i + k] = Gp[i][0] * Ji[0][k] + Gp[i][1] * Ji[1][k] + Gp[i][2] * Ji[2][k];
     float dP[9];
     dP_any<MODEL>(mat, scale, pay, dF, dP);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      float T[3];
-#pragma unroll
-      for (int j = 0; j < 3; ++j)
-        T[j] = vol * (dP[3 * i] * Ji[j][0] + dP[3 * i + 1] * Ji[j][1] + dP[3 * i + 2] * Ji[j][2]);
-      A[0][i] += T[0];
-      A[1][i] += T[1];
-      A[2][i] += T[2];
-      A[3][i] += T[0] * gy + T[1] * gx;
-      A[4][i] += T[1] * gz + T[2] * gy;
-      A[5][i] += T[0] * gz + T[2] * gx;
-      A[6][i] += T[0] * (gy * gz) + T[1] * (gx * gz) + T[2] * (gx * gy);
-    }
+    hex_moments(dP, Ji, vol, gx, gy, gz, A);
   }
   int pos[8];
   hex_slots(m, e, pos);
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     float f[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      float s = 0.f;
-#pragma unroll
-      for (int mm = 0; mm < 7; ++mm) s += hex_msign(k, mm) > 0 ? A[mm][i] : -A[mm][i];
-      f[i] = 0.125f * s;
-    }
+    hex_vertex(A, k, f);
     __stcg(a.stage + pos[k], make_float4(f[0], f[1], f[2], 0.f));
   }
 }

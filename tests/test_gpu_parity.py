@@ -556,11 +556,16 @@ def test_newton_j2_two_level_matches_oracle(cuda, vox, reuse):
         assert n_asm == 1
 
 
-def test_newton_bar_matches_oracle(cuda, bar):
+@pytest.mark.parametrize("precond", ["jacobi", "two_level"])
+def test_newton_bar_matches_oracle(cuda, bar, precond):
+    # the plain-method cantilever workload as specified: ten traction load
+    # steps, each to 1e-10, every step within 1e-6 of the FP64 oracle (the
+    # last steps are the large-rotation ones: tip deflection 5.7 mm on 10 mm)
     ref = np.load(G.path_of("bar_nh_steps"))
+    assert ref["u_steps"].shape[0] == 10
     mesh = make_mesh(bar.X, bar.conn, cuda)
     mesh.set_fixed_nodes(np.where(bar.fixed_mask[:, 0])[0])
-    solver = B.StaticSolver(mesh, B.NeoHookean(17e3, 0.3), tol=1e-10)
+    solver = B.StaticSolver(mesh, B.NeoHookean(17e3, 0.3), tol=1e-10, precond=precond)
     for k in range(ref["u_steps"].shape[0]):
         mesh.set_nodal_forces(np.arange(bar.n_nodes), bar.f_ext * (k + 1) / 10.0)
         res = solver.solve(verbose=False)

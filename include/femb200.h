@@ -141,18 +141,23 @@ int fem_ctx_info(void* ctx, int64_t* out6);
 /* counters since creation: out[0] kernel launches that did work (library
  * kernels only), out[1] CG iterations, out[2] residual evaluations,
  * out[3] CG graph launches; matvec variant selection: out[4] variant in use
- * (0 fused node-block, 1 two-phase), out[5] / out[6] timed ns per launch of
- * the fused / two-phase variant (0 if not timed), out[7] 1 if the choice was
- * made by timing; out[8] PCG solves run as one whole-solve graph launch
- * (conditional WHILE node), out[9] 1 if such graphs are available */
-int fem_ctx_stats(void* ctx, int64_t* out10);
+ * (0 fused node-block, 1 two-phase, 2 element-block), out[5] / out[6] timed
+ * ns per launch of the fused / two-phase variant (0 if not timed), out[7] 1
+ * if the choice was made by timing; out[8] PCG solves run as one whole-solve
+ * graph launch (conditional WHILE node), out[9] 1 if such graphs are
+ * available; out[10] timed ns of the element-block variant at its best block
+ * size, out[11] that size (0: no element-block tables), out[12..15] timed ns
+ * at 256, 512, 768 and 1024 elements per block (0 if not timed) */
+int fem_ctx_stats(void* ctx, int64_t* out16);
 
 /* Option keys of fem_set_option (no reference counterpart: the reference has
  * one matvec formulation, backend/fea/fem/material/nonlinear/base.py:110-145). */
 enum {
-  /* -1 (default): time both tangent-matvec variants on the first PCG solve
-   * and keep the faster; 0: fused node-block kernel; 1: element pass writing
-   * slot vectors in node order plus a node gather */
+  /* -1 (default): time the tangent-matvec variants on the first PCG solve
+   * and keep the fastest; 0: fused node-block kernel; 1: element pass writing
+   * slot vectors in node order plus a node gather; 2 (TET4): element-block
+   * kernel, one pass that sums each block's slot vectors in shared memory
+   * and completes nodes shared by blocks in the last contributing block */
   FEM_OPT_MATVEC_VARIANT = 1,
   /* two-level preconditioner: lattice cell edge in mesh lengths (default 8;
    * the cube root of 5x the mean element volume, i.e. the voxel edge of
@@ -204,7 +209,10 @@ enum {
   FEM_OPT_COARSE_INVERSE = 11,
   /* two-level: at most this many coarse nodes (default 4096, up to 16384);
    * the lattice cell grows by 25 % steps until the lattice fits */
-  FEM_OPT_COARSE_MAX_NODES = 12
+  FEM_OPT_COARSE_MAX_NODES = 12,
+  /* element-block matvec: elements per block (one thread each), 256, 512,
+   * 768 or 1024; 0 (default) times the four and keeps the fastest */
+  FEM_OPT_EB_SIZE = 13
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

@@ -48,8 +48,9 @@ FEM_OPT_DIRECTION_RECURRENCE = 9
 FEM_OPT_BLOCK_JACOBI = 10
 FEM_OPT_COARSE_INVERSE = 11
 FEM_OPT_COARSE_MAX_NODES = 12
+FEM_OPT_EB_SIZE = 13
 MPNN_PARAMS = 34307
-MATVEC_VARIANTS = {0: "fused", 1: "two_phase"}
+MATVEC_VARIANTS = {0: "fused", 1: "two_phase", 2: "element_block"}
 
 
 class FemMeshDesc(C.Structure):

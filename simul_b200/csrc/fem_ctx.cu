@@ -196,12 +196,20 @@ struct FemCtx {
   int sol_lwork = 0;
   int* sol_info = nullptr;
   int* h_info = nullptr;
-  // matvec variant: forced by fem_set_option (>= 0) or chosen by timing both
+  // matvec variant: forced by fem_set_option (>= 0) or chosen by timing all
   int mv_forced = -1;
   int mv_variant = MV_FUSED;
   bool mv_tuned = false;
   int mv_tuned_model = -2;
-  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0};
+  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0, 0.0};
+  // element-block matvec (TET4): tables for blocks of eb_size elements (0:
+  // not built), the block size forced by FEM_OPT_EB_SIZE (0: timed choice
+  // among kEbSizes), and the timed ns per launch of each candidate size
+  EbDev ebdev{};
+  std::vector<void*> eb_bufs;
+  int eb_size = 0;
+  int eb_forced = 0;
+  double eb_ns[4] = {0.0, 0.0, 0.0, 0.0};
 
   MeshDev mesh() const {
     MeshDev m;
@@ -322,6 +330,8 @@ void free_ctx(FemCtx* c) {
   for (void* p : c->coarse_bufs)
     if (p) cudaFree(p);
   for (void* p : c->mpnn_bufs)
+    if (p) cudaFree(p);
+  for (void* p : c->eb_bufs)
     if (p) cudaFree(p);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->sol_work) cudaFree(c->sol_work);
@@ -555,7 +565,8 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
   // every reducing kernel's grid must fit: node blocks and node-parallel blocks
-  c->max_blocks = std::max(c->n_blocks, (c->Nn + 63) / 64) + 1;  // node gather: 64 nodes per CTA
+  // (node gather: 64 nodes per CTA; element-block matvec: at least kEbThreads elements per CTA)
+  c->max_blocks = std::max(std::max(c->n_blocks, (c->Nn + 63) / 64), (c->Ne + kEbThreads - 1) / kEbThreads) + 1;
   if ((st = dalloc(c, &c->partials, (size_t)N_SITES * 2 * c->max_blocks))) return st;
   if ((st = dalloc(c, &c->counters, (size_t)N_SITES))) return st;
   if ((st = dalloc(c, &c->scalars, (size_t)8))) return st;
@@ -593,6 +604,159 @@ DevMat<T> to_dev(const FemMaterial& s) {
   return d;
 }
 
+// ───────────────────────── element-block matvec tables ─────────────────────────
+
+// Candidate elements per block of the element-block matvec (timed on the
+// first PCG solve unless FEM_OPT_EB_SIZE fixes one).
+constexpr int kEbSizes[4] = {256, 512, 768, 1024};
+
+// Frees the element-block tables and every captured CG graph (a graph
+// captured with the element-block variant holds the tables' addresses).
+void free_eb_tables(FemCtx* c) {
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (!c->eb_bufs.empty()) {
+    for (int k = 0; k < N_GRAPHS; ++k) {
+      if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+      if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
+      c->cg_graph[k] = nullptr;
+      c->loop_graph[k] = nullptr;
+    }
+  }
+  for (void* p : c->eb_bufs)
+    if (p) cudaFree(p);
+  c->eb_bufs.clear();
+  c->ebdev = EbDev{};
+  c->eb_size = 0;
+}
+
+template <typename T>
+int eb_upload(FemCtx* c, T** dst, const std::vector<T>& v) {
+  int st;
+  if ((st = dalloc(c, dst, v.size()))) return st;
+  c->eb_bufs.push_back(*dst);
+  if (!v.empty()) CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  return FEM_OK;
+}
+
+// Builds the element-block tables for blocks of `eb` consecutive elements
+// (TET4).  Per block: its local nodes (distinct vertices, ascending), each
+// element's local vertex indices, the node-major position of each of its
+// slot vectors (sorted by local node, then element, then slot: the fixed
+// summation order), and for every local node shared with another block the
+// slot of its partial row; shared nodes' partials are ordered by block, and
+// the shared nodes are listed for the completion kernel.
+int build_eb_tables(FemCtx* c, int eb) {
+  if (c->eb_size == eb) return FEM_OK;
+  free_eb_tables(c);
+  const int Ne = c->Ne, Nn = c->Nn;
+  if (c->npe != 4) return set_err(c, FEM_ERR_INVALID, "the element-block matvec is TET4 only");
+  if (eb != 256 && eb != 512 && eb != 768 && eb != 1024)
+    return set_err(c, FEM_ERR_INVALID, "element block of %d elements: need 256, 512, 768 or 1024", eb);
+  std::vector<int4> conn(Ne);
+  CK(cudaMemcpyAsync(conn.data(), c->conn, Ne * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<int> deg(Nn, 0);
+  for (int e = 0; e < Ne; ++e) {
+    const int* cn = &conn[e].x;
+    for (int k = 0; k < 4; ++k) deg[cn[k]]++;
+  }
+  const int n_blk = (Ne + eb - 1) / eb;
+  std::vector<int> node_ptr(n_blk + 1, 0), nodes, nshared(Nn + 1, 0);
+  std::vector<int4> ninfo;
+  std::vector<uint16_t> lrow;
+  std::vector<uint2> lconn(Ne), lspos(Ne);
+  nodes.reserve((size_t)Ne / 2);
+  std::vector<uint64_t> ent;
+  int lmax = 0;
+  for (int b = 0; b < n_blk; ++b) {
+    const int e0 = b * eb, e1 = std::min(Ne, e0 + eb);
+    ent.clear();
+    for (int e = e0; e < e1; ++e) {
+      const int* cn = &conn[e].x;
+      for (int k = 0; k < 4; ++k)
+        ent.push_back(((uint64_t)(uint32_t)cn[k] << 32) | ((uint64_t)(e - e0) << 2) | (uint64_t)k);
+    }
+    std::sort(ent.begin(), ent.end());
+    node_ptr[b] = (int)nodes.size();
+    int L = 0;
+    size_t j = 0;
+    while (j < ent.size()) {
+      const int n = (int)(ent[j] >> 32);
+      size_t j1 = j;
+      while (j1 < ent.size() && (int)(ent[j1] >> 32) == n) ++j1;
+      lrow.push_back((uint16_t)j);
+      for (size_t q = j; q < j1; ++q) {
+        const int le = (int)((ent[q] >> 2) & 0x3fffffffu), k = (int)(ent[q] & 3u);
+        uint16_t* lc = reinterpret_cast<uint16_t*>(&lconn[e0 + le]);
+        uint16_t* sp = reinterpret_cast<uint16_t*>(&lspos[e0 + le]);
+        lc[k] = (uint16_t)L;
+        sp[k] = (uint16_t)q;
+      }
+      nodes.push_back(n);
+      const bool interior = (int)(j1 - j) == deg[n];
+      ninfo.push_back(make_int4(n, interior ? -1 : -2, 0, 0));
+      if (!interior) nshared[n + 1]++;
+      ++L;
+      j = j1;
+    }
+    lrow.push_back((uint16_t)ent.size());
+    if (L > 65535) return set_err(c, FEM_ERR_INVALID, "element block %d touches %d nodes (max 65535)", b, L);
+    lmax = std::max(lmax, L);
+  }
+  node_ptr[n_blk] = (int)nodes.size();
+  for (int n = 0; n < Nn; ++n) nshared[n + 1] += nshared[n];
+  std::vector<int> fill(nshared.begin(), nshared.end() - 1);
+  for (size_t i = 0; i < nodes.size(); ++i) {
+    int4& in = ninfo[i];
+    if (in.y == -2) {
+      in.y = fill[in.x]++;
+      in.z = nshared[in.x];
+      in.w = nshared[in.x + 1] - nshared[in.x];
+    }
+  }
+  const size_t n_parts = (size_t)nshared[Nn];
+  std::vector<int4> snode;
+  for (int n = 0; n < Nn; ++n)
+    if (nshared[n + 1] > nshared[n]) snode.push_back(make_int4(n, nshared[n], nshared[n + 1] - nshared[n], 0));
+  int* d_ptr = nullptr;
+  int* d_nodes = nullptr;
+  int4* d_ninfo = nullptr;
+  uint16_t* d_lrow = nullptr;
+  uint2 *d_lconn = nullptr, *d_lspos = nullptr;
+  float4* d_parts = nullptr;
+  int4* d_snode = nullptr;
+  double* d_pap = nullptr;
+  int st;
+  if ((st = eb_upload(c, &d_ptr, node_ptr))) return st;
+  if ((st = eb_upload(c, &d_nodes, nodes))) return st;
+  if ((st = eb_upload(c, &d_ninfo, ninfo))) return st;
+  if ((st = eb_upload(c, &d_lrow, lrow))) return st;
+  if ((st = eb_upload(c, &d_lconn, lconn))) return st;
+  if ((st = eb_upload(c, &d_lspos, lspos))) return st;
+  if ((st = dalloc(c, &d_parts, std::max<size_t>(n_parts, 1)))) return st;
+  c->eb_bufs.push_back(d_parts);
+  if ((st = eb_upload(c, &d_snode, snode))) return st;
+  if ((st = dalloc(c, &d_pap, (size_t)n_blk))) return st;
+  c->eb_bufs.push_back(d_pap);
+  CK(cudaStreamSynchronize(c->stream));
+  EbDev& t = c->ebdev;
+  t.eb = eb;
+  t.n_blk = n_blk;
+  t.lmax = lmax;
+  t.node_ptr = d_ptr;
+  t.nodes = d_nodes;
+  t.ninfo = d_ninfo;
+  t.lrow = d_lrow;
+  t.lconn = d_lconn;
+  t.lspos = d_lspos;
+  t.parts = d_parts;
+  t.snode = d_snode;
+  t.n_shared = (int)snode.size();
+  t.pap_part = d_pap;
+  c->eb_size = eb;
+  return FEM_OK;
+}
+
 // ───────────────────────── kernels wrappers ─────────────────────────
 
 // Matvec arguments with the mesh tables and the context's variant filled in.
@@ -602,6 +766,7 @@ MvArgs make_mv(const FemCtx* c) {
   mv.m = c->mesh();
   mv.variant = c->mv_variant;
   mv.stage = c->stage;
+  mv.eb = c->ebdev;
   return mv;
 }
 
@@ -703,7 +868,7 @@ StepArgs step_args(const FemCtx* c, int kind) {
 
 // Kernels launched per CG iteration (matvec + the rest).
 int64_t kernels_per_iter(const FemCtx* c, int kind, bool fused) {
-  const int64_t mv = c->mv_variant == MV_TWO_PHASE ? 2 : 1;
+  const int64_t mv = c->mv_variant == MV_FUSED ? 1 : 2;
   if (fused) return mv + 1;
   if (kind == GRAPH_TWO_LEVEL) return mv + 3 + coarse_product_kernels(c->cdev) + (recurrence(c, kind) ? 0 : 1);
   return mv + 2;
@@ -779,8 +944,11 @@ int choose_matvec_variant(FemCtx* c) {
     c->mv_variant = MV_TWO_PHASE;
     return FEM_OK;
   }
+  int st;
   if (c->mv_forced >= 0) {
     c->mv_variant = c->mv_forced;
+    if (c->mv_variant == MV_ELEM_BLOCK && c->eb_size == 0)
+      return build_eb_tables(c, c->eb_forced > 0 ? c->eb_forced : 512);
     return FEM_OK;
   }
   if (c->mv_tuned && c->mv_tuned_model == c->model_kind) return FEM_OK;
@@ -790,7 +958,8 @@ int choose_matvec_variant(FemCtx* c) {
   EventPair ev;
   CK(ev.create());
   cudaEvent_t e0 = ev.a, e1 = ev.b;
-  for (int v = 0; v < MV_N_VARIANTS; ++v) {
+  // ns per launch of variant v (element-block: with the tables built)
+  auto time_variant = [&](int v, double* ns) -> int {
     MvArgs mv = make_mv(c);
     mv.variant = v;
     mv.matF = c->matF;
@@ -810,10 +979,33 @@ int choose_matvec_variant(FemCtx* c) {
     CK(cudaEventSynchronize(e1));
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, e0, e1));
-    c->mv_ns[v] = 1e6 * ms / kReps;
-    c->n_launches += (v == MV_TWO_PHASE ? 2 : 1) * 13;
+    *ns = 1e6 * ms / kReps;
+    c->n_launches += (v == MV_FUSED ? 1 : 2) * 13;
+    return FEM_OK;
+  };
+  for (int v = 0; v < MV_ELEM_BLOCK; ++v)
+    if ((st = time_variant(v, &c->mv_ns[v]))) return st;
+  // element-block: every candidate block size (or the forced one), keep the fastest
+  int best_eb = 0;
+  double best_ns = 0.0;
+  for (int k = 0; k < 4; ++k) {
+    const int eb = kEbSizes[k];
+    c->eb_ns[k] = 0.0;
+    if (c->eb_forced > 0 && eb != c->eb_forced) continue;
+    if ((st = build_eb_tables(c, eb))) return st;
+    if ((st = time_variant(MV_ELEM_BLOCK, &c->eb_ns[k]))) return st;
+    if (best_eb == 0 || c->eb_ns[k] < best_ns) {
+      best_eb = eb;
+      best_ns = c->eb_ns[k];
+    }
   }
-  c->mv_variant = c->mv_ns[MV_TWO_PHASE] < c->mv_ns[MV_FUSED] ? MV_TWO_PHASE : MV_FUSED;
+  if ((st = build_eb_tables(c, best_eb))) return st;
+  c->mv_ns[MV_ELEM_BLOCK] = best_ns;
+  int v_best = MV_FUSED;
+  for (int v = 1; v < MV_N_VARIANTS; ++v)
+    if (c->mv_ns[v] < c->mv_ns[v_best]) v_best = v;
+  c->mv_variant = v_best;
+  if (v_best != MV_ELEM_BLOCK) free_eb_tables(c);
   c->mv_tuned = true;
   c->mv_tuned_model = c->model_kind;
   return FEM_OK;
@@ -899,7 +1091,8 @@ int ensure_cg_graph(FemCtx* c, int kind) {
   const bool fused = use_fused(c, kind);
   const bool pdl = use_pdl(c, kind);
   const int flags = (kind == GRAPH_LEARNED ? (c->learned_coarse ? 1 : 0) : 0) | (fused ? 2 : 0) | (pdl ? 4 : 0) |
-                    (!fused && recurrence(c, kind) ? 8 : 0) | (kind == GRAPH_TWO_LEVEL && c->block_jacobi ? 16 : 0);
+                    (!fused && recurrence(c, kind) ? 8 : 0) | (kind == GRAPH_TWO_LEVEL && c->block_jacobi ? 16 : 0) |
+                    (c->mv_variant == MV_ELEM_BLOCK ? c->eb_size << 8 : 0);
   if (c->cg_graph[kind] && c->cg_graph_model[kind] == c->model_kind &&
       c->cg_graph_variant[kind] == c->mv_variant && c->cg_graph_flags[kind] == flags)
     return FEM_OK;
@@ -912,6 +1105,7 @@ int ensure_cg_graph(FemCtx* c, int kind) {
     c->loop_graph[kind] = nullptr;
   }
   prepare_kernels(c->mesh(), c->model_kind);
+  if (c->mv_variant == MV_ELEM_BLOCK) prepare_eb_kernels(c->model_kind);
   if (kind == GRAPH_TWO_LEVEL || (kind == GRAPH_LEARNED && c->learned_coarse))
     prepare_coarse_kernels(c->model_kind, c->cdev.n_dof);
   if (kind == GRAPH_LEARNED) prepare_mpnn_kernels();
@@ -1509,7 +1703,7 @@ void mpnn_sample(FemCtx* c, const float* R, const float* E, int k, bool coarse, 
   mpnn_apply(c, c->tr_r, c->tr_z, coarse, base);
   launch_matvec(train_mv(c, c->tr_z, c->tr_q), c->model_kind, c->stream);
   launch_train_loss(c->tr_z, c->tr_q, c->tr_r, c->tr_e, c->Nn, c->tr_scal, c->red(), SITE_AUX, c->stream);
-  c->n_launches += 4 + (c->mv_variant == MV_TWO_PHASE ? 1 : 0);
+  c->n_launches += 4 + (c->mv_variant == MV_FUSED ? 0 : 1);
   if (grad) {
     launch_train_grad_z(c->tr_q, c->tr_r, c->fixed, c->tr_scal, c->tr_g, c->Nn, c->stream);
     launch_mpnn_backward(c->mtrain, c->tr_r, c->dinv, c->tr_g, c->grad, accumulate ? 1 : 0, c->stream);
@@ -1765,6 +1959,9 @@ int fem_ctx_stats(void* ctx, int64_t* out) {
   out[7] = c->mv_tuned ? 1 : 0;
   out[8] = c->n_loop_graphs;
   out[9] = c->use_loop_graph ? 1 : 0;
+  out[10] = (int64_t)std::llround(c->mv_ns[MV_ELEM_BLOCK]);
+  out[11] = c->eb_size;
+  for (int k = 0; k < 4; ++k) out[12 + k] = (int64_t)std::llround(c->eb_ns[k]);
   return FEM_OK;
 }
 
@@ -1785,11 +1982,25 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
   switch (key) {
     case FEM_OPT_MATVEC_VARIANT:
       if (value < -1 || value >= MV_N_VARIANTS)
-        return set_err(c, FEM_ERR_INVALID, "matvec variant %lld not in {-1 (auto), 0 (fused), 1 (two-phase)}",
+        return set_err(c, FEM_ERR_INVALID,
+                       "matvec variant %lld not in {-1 (auto), 0 (fused), 1 (two-phase), 2 (element-block)}",
                        (long long)value);
+      if (value == MV_ELEM_BLOCK && c->npe != 4)
+        return set_err(c, FEM_ERR_INVALID, "the element-block matvec is TET4 only");
+      // the element-block variant is only ever selected with its tables built
+      if (value == MV_ELEM_BLOCK && (st = build_eb_tables(c, c->eb_forced > 0 ? c->eb_forced : 512))) return st;
       c->mv_forced = (int)value;
       c->mv_variant = value >= 0 ? (int)value : MV_FUSED;
       c->mv_tuned = false;
+      return FEM_OK;
+    case FEM_OPT_EB_SIZE:
+      if (value != 0 && value != 256 && value != 512 && value != 768 && value != 1024)
+        return set_err(c, FEM_ERR_INVALID, "element block size %lld: 0 (timed), 256, 512, 768 or 1024",
+                       (long long)value);
+      c->eb_forced = (int)value;
+      c->mv_tuned = false;
+      if (c->mv_variant == MV_ELEM_BLOCK) return build_eb_tables(c, c->eb_forced > 0 ? c->eb_forced : 512);
+      if (c->eb_size != 0) free_eb_tables(c);
       return FEM_OK;
     case FEM_OPT_COARSE_CELL:
       if (value < 1 || value > 64)

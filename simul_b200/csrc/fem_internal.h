@@ -128,6 +128,30 @@ struct ResArgs {
   double* stage_d;          // HEX8: [3 * 8 Ne] element slot forces in node_slots order
 };
 
+// Element-block matvec tables (MV_ELEM_BLOCK, TET4).  Element block k holds
+// elements [k eb, (k + 1) eb) of the internal order; its local nodes are the
+// distinct vertices of those elements in ascending order.  A local node all
+// of whose elements lie in the block ("interior") gets its product row from
+// that block alone; a node shared by several blocks gets one partial row per
+// block, stored in block order, and a second, small kernel adds them.
+struct EbDev {
+  int eb;                   // elements per block (= threads per CTA: one element per thread)
+  int n_blk;
+  int lmax;                 // most local nodes of one block (shared-memory sizing)
+  const int* node_ptr;      // [n_blk + 1] into nodes / ninfo; lrow of block b starts at node_ptr[b] + b
+  const int* nodes;         // local node -> internal node
+  // local node -> (internal node, partial slot or -1 if interior, the node's
+  // first partial, its number of partials)
+  const int4* ninfo;
+  const uint16_t* lrow;     // [node_ptr[n_blk] + n_blk] local slot range of each local node (L_b + 1 per block)
+  const uint2* lconn;       // [Ne] four 16-bit local vertex indices
+  const uint2* lspos;       // [Ne] four 16-bit positions of the element's slot vectors in node-major order
+  float4* parts;            // per-block partial rows of shared nodes, each node's in block order
+  const int4* snode;        // [n_shared] shared nodes: (node, first partial, number of partials, 0)
+  int n_shared;
+  double* pap_part;         // [n_blk] CG: each block's share of p.Ap
+};
+
 struct MvArgs {
   MeshDev m;
   const DevMat<float>* matF;
@@ -138,15 +162,27 @@ struct MvArgs {
   Reduce red;
   int red_site;
   int mask_input;           // 1: fixed DOFs of x read as zero (K_ff x); 0: K_f,all x
-  int variant;              // MV_FUSED (node-block) or MV_TWO_PHASE (element pass + node gather)
+  int variant;              // MV_FUSED (node-block), MV_TWO_PHASE (element pass + node gather) or MV_ELEM_BLOCK
   float4* stage;            // [4 Ne] slot vectors in node_slots order (two-phase scratch)
   // two-phase inside CG, non-null: x holds the preconditioned residual z and
   // the node gather forms the direction by recurrence, p = z + beta p and
   // q = K z + beta q (q in y, p here), so no separate direction update runs
   float* p_rec;
+  EbDev eb;                 // element-block tables (MV_ELEM_BLOCK)
 };
 
-enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_N_VARIANTS = 2 };
+// MV_ELEM_BLOCK: one CTA per element block: vertex data staged in shared
+// memory, slot vectors summed per local node in shared memory; a second
+// kernel adds the partial rows of nodes shared by blocks (fem_elemblock.cu).
+enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_ELEM_BLOCK = 2, MV_N_VARIANTS = 3 };
+
+// smallest element block of the element-block matvec (one element per
+// thread; blocks of 256, 512, 768 or 1024 elements)
+constexpr int kEbThreads = 256;
+// shared memory of one element-block CTA
+inline size_t eb_smem_bytes(int eb, int lmax) {
+  return 16 * (size_t)(4 * eb) + 32 * (size_t)lmax + ((2 * (size_t)(lmax + 1) + 15) & ~(size_t)15);
+}
 
 struct DiagArgs {
   MeshDev m;
@@ -398,6 +434,9 @@ void launch_stress_hex(const MeshDev& m, const DevMat<double>* matD, int model, 
 void launch_refq_hex(const MeshDev& m, const int* perm_elem, double* dNdX, double* vol, cudaStream_t s);
 // the node gather of the two-phase matvec (fem_kernels.cu)
 void launch_node_gather(const MvArgs& a, cudaStream_t s);
+// element-block matvec (fem_elemblock.cu); raise its shared-memory limit first
+void launch_matvec_eb(const MvArgs& a, int model, cudaStream_t s);
+void prepare_eb_kernels(int model);
 // out[n*3+d] (internal) = in[perm[n]*3+d] (caller order) and back
 void launch_gather_d(const double* in_user, double* out_int, const int* perm, int n, cudaStream_t s);
 void launch_scatter_d(const double* in_int, double* out_user, const int* perm, int n,

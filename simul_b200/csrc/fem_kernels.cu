@@ -1006,6 +1006,16 @@ void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
     return;
   }
   const bool cg = a.cg != nullptr;
+  if (a.variant == MV_ELEM_BLOCK && a.eb.nodes != nullptr) {
+    launch_matvec_eb(a, model, s);
+    return;
+  }
+  if (a.variant == MV_ELEM_BLOCK) {
+    // no element-block tables (the host builds them whenever it selects the
+    // variant): the two-phase pass gives the same product
+    cg ? two_phase<true>(a, model, s) : two_phase<false>(a, model, s);
+    return;
+  }
   if (a.variant == MV_TWO_PHASE) {
     cg ? two_phase<true>(a, model, s) : two_phase<false>(a, model, s);
     return;

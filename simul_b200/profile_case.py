@@ -27,7 +27,8 @@ import numpy as np
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=64)
-    ap.add_argument("--variant", default="fused", choices=["fused", "two_phase"])
+    ap.add_argument("--variant", default="fused", choices=["fused", "two_phase", "element_block"])
+    ap.add_argument("--block-size", type=int, default=0, help="element-block variant: elements per block")
     ap.add_argument("--element", default="tet4", choices=["tet4", "hex8"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--strain", type=float, default=0.004)
@@ -47,7 +48,8 @@ def main(argv=None):
     et = B.ElementType.HEX8 if args.element == "hex8" else B.ElementType.TET4
     mesh = B.FEMesh(v.n_nodes, v.n_elements, et, device=0, nodes_per_block=args.nodes_per_block)
     mesh.initialize_from_numpy(v.X, v.conn)
-    mesh.set_matvec_variant(args.variant)
+    if args.element == "tet4":
+        mesh.set_matvec_variant(args.variant, block_size=args.block_size if args.variant == "element_block" else None)
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     idx = np.where(v.fixed_mask.reshape(-1))[0]
     vals = (v.fixed_vals * (args.strain / 0.02)).reshape(-1)
@@ -93,7 +95,7 @@ def main(argv=None):
     info = mesh.info()
     print(json.dumps({"n": args.n, "element": args.element, "elements": info["n_elements"],
                       "nodes": info["n_nodes"], "variant": "two_phase" if args.element == "hex8" else args.variant,
-                      "reps": args.reps,
+                      "reps": args.reps, "block_size": mesh.stats()["element_block_size"],
                       "ms": {"matvec": ms[0], "residual": ms[1], "cg_update": ms[2], "cg_direction": ms[3]},
                       **extra}))
 

@@ -96,7 +96,7 @@ def test_element_forces_and_stress(cuda, bar, key, nb):
         assert _rel_max(mesh.F.cpu().numpy(), ref["F"]) < 1e-12
 
 
-VARIANTS = ["fused", "two_phase"]
+VARIANTS = ["fused", "two_phase", "element_block"]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -163,6 +163,36 @@ def test_forces_bitwise_deterministic(cuda, vox, variant):
         assert torch.equal(o, outs[0])
     for o in ys[1:]:
         assert torch.equal(o, ys[0])
+
+
+@pytest.mark.parametrize("block_size", [256, 512, 768, 1024])
+def test_element_block_sizes_match_oracle_and_repeat_bitwise(cuda, vox, block_size):
+    # every block size gives the oracle's product; small blocks make most
+    # nodes shared between blocks (completed by the last contributing block)
+    ref = np.load(G.path_of("vox12_j2_forces"))
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    mesh.set_matvec_variant("element_block", block_size=block_size)
+    mat = make_material("j2", E=vox.E)
+    mesh.u.copy_(dev(ref["u"], cuda))
+    mat.compute_nodal_forces(mesh)
+    x = dev(ref["p"], cuda, torch.float32)
+    ys = []
+    for _ in range(3):
+        y = torch.full_like(x, float("nan"))
+        assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0, _lib.last_error(mesh.ctx)
+        ys.append(y)
+    assert _rel_l2(ys[0].cpu().numpy().astype(np.float64), ref["y"]) < 2e-5
+    for o in ys[1:]:
+        assert torch.equal(o, ys[0])
+    assert mesh.stats()["element_block_size"] == block_size
+
+
+def test_element_block_size_option_is_validated(cuda, vox):
+    mesh = make_mesh(vox.X, vox.conn, cuda)
+    lib = _lib.load()
+    assert lib.fem_set_option(mesh.ctx, _lib.FEM_OPT_EB_SIZE, 300) == _lib.FEM_ERR_INVALID
+    assert "element block size" in _lib.last_error(mesh.ctx)
+    assert lib.fem_set_option(mesh.ctx, _lib.FEM_OPT_EB_SIZE, 0) == 0
 
 
 def test_pcg_solves_tangent_system(cuda, bar):
@@ -608,9 +638,13 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
         y = torch.empty_like(x)
         assert _lib.load().fem_tangent_matvec(mesh.ctx, ptr(x), ptr(y)) == 0
         ys[v] = y.cpu().numpy().astype(np.float64)
-    # both sum each node's slot vectors in the same order; only FMA contraction may differ
+    # fused and two-phase sum each node's slot vectors in the same order (only
+    # FMA contraction may differ); the element-block kernel sums per block,
+    # then the blocks' partial rows in block order: FP32 rounding apart
     assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-6
-    # automatic choice: the first PCG solve times both variants and keeps the faster
+    assert _rel_l2(ys["element_block"], ys["fused"]) < 1e-6
+    # automatic choice: the first PCG solve times every variant (the element
+    # block at each candidate size) and keeps the fastest
     mesh.set_matvec_variant(None)
     mesh.u.zero_()
     mat.reset_state()
@@ -620,9 +654,13 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
     assert res["converged"], res
     st = mesh.stats()
     assert st["matvec_tuned"]
-    assert st["matvec_ns"]["fused"] > 0 and st["matvec_ns"]["two_phase"] > 0
+    assert all(v > 0 for v in st["matvec_ns"].values()), st
+    assert all(v > 0 for v in st["element_block_ns"].values()), st
     faster = min(st["matvec_ns"], key=st["matvec_ns"].get)
     assert st["matvec_variant"] == faster
+    assert st["matvec_ns"]["element_block"] == min(st["element_block_ns"].values())
+    if faster == "element_block":
+        assert st["element_block_size"] == min(st["element_block_ns"], key=st["element_block_ns"].get)
     # every PCG solve ran as one whole-solve graph launch (conditional WHILE node)
     assert st["whole_solve_graph_available"] and st["whole_solve_graphs"] > 0
     assert _lib.load().fem_set_option(mesh.ctx, _lib.FEM_OPT_MATVEC_VARIANT, 7) == _lib.FEM_ERR_INVALID

@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--weights", default=os.path.join(ROOT, "simul_b200", "weights", "mpnn_vertebra.npz"),
                     help="learned-preconditioner weights (simul_b200.train_precond)")
     ap.add_argument("--learned-coarse", type=int, default=1, help="learned: add the coarse correction")
-    ap.add_argument("--matvec-variant", default="auto", choices=["auto", "fused", "two_phase", "element_block"],
+    ap.add_argument("--matvec-variant", default="auto", choices=["auto", "fused", "two_phase", "element_block", "warp_agg"],
                     help="tangent-matvec variant (auto: timed on the first solve)")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
     ap.add_argument("--no-hex8", action="store_true", help="skip the HEX8 form of the workload (reported beside)")

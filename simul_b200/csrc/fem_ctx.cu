@@ -201,12 +201,15 @@ struct FemCtx {
   int mv_variant = MV_FUSED;
   bool mv_tuned = false;
   int mv_tuned_model = -2;
-  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0, 0.0};
+  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0, 0.0, 0.0};
   // element-block matvec (TET4): tables for blocks of eb_size elements (0:
   // not built), the block size forced by FEM_OPT_EB_SIZE (0: timed choice
   // among kEbSizes), and the timed ns per launch of each candidate size
   EbDev ebdev{};
   std::vector<void*> eb_bufs;
+  // warp-aggregated two-phase matvec tables (TET4; built when selected or timed)
+  WaggDev wadev{};
+  std::vector<void*> wa_bufs;
   int eb_size = 0;
   int eb_forced = 0;
   double eb_ns[4] = {0.0, 0.0, 0.0, 0.0};
@@ -332,6 +335,8 @@ void free_ctx(FemCtx* c) {
   for (void* p : c->mpnn_bufs)
     if (p) cudaFree(p);
   for (void* p : c->eb_bufs)
+    if (p) cudaFree(p);
+  for (void* p : c->wa_bufs)
     if (p) cudaFree(p);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->sol_work) cudaFree(c->sol_work);
@@ -757,6 +762,99 @@ int build_eb_tables(FemCtx* c, int eb) {
   return FEM_OK;
 }
 
+// Frees the warp-aggregation tables and every captured CG graph (which may
+// hold their addresses).
+void free_wagg_tables(FemCtx* c) {
+  if (c->wa_bufs.empty()) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int k = 0; k < N_GRAPHS; ++k) {
+    if (c->cg_graph[k]) cudaGraphExecDestroy(c->cg_graph[k]);
+    if (c->loop_graph[k]) cudaGraphExecDestroy(c->loop_graph[k]);
+    c->cg_graph[k] = nullptr;
+    c->loop_graph[k] = nullptr;
+  }
+  for (void* p : c->wa_bufs)
+    if (p) cudaFree(p);
+  c->wa_bufs.clear();
+  c->wadev = WaggDev{};
+}
+
+// Builds the warp-aggregation tables (TET4): per warp of 32 consecutive
+// elements its distinct vertices (ascending), each element's slot positions
+// in the warp's node-major slot order (by vertex, then element, then slot:
+// the fixed summation order), and per (warp, vertex) the position of its
+// partial row among the vertex's partials, which are ordered by warp.
+int build_wagg_tables(FemCtx* c) {
+  if (!c->wa_bufs.empty()) return FEM_OK;
+  const int Ne = c->Ne, Nn = c->Nn;
+  if (c->npe != 4) return set_err(c, FEM_ERR_INVALID, "the warp-aggregated matvec is TET4 only");
+  std::vector<int4> conn(Ne);
+  CK(cudaMemcpyAsync(conn.data(), c->conn, Ne * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int n_warps = (Ne + 31) / 32;
+  std::vector<int> wptr(n_warps + 1, 0), wnode, prow(Nn + 1, 0);
+  std::vector<int2> went;
+  std::vector<uint32_t> lspos(Ne, 0u);
+  wnode.reserve((size_t)Ne);
+  went.reserve((size_t)Ne);
+  std::vector<uint64_t> ent;
+  for (int w = 0; w < n_warps; ++w) {
+    const int e0 = 32 * w, e1 = std::min(Ne, e0 + 32);
+    ent.clear();
+    for (int e = e0; e < e1; ++e) {
+      const int* cn = &conn[e].x;
+      for (int k = 0; k < 4; ++k)
+        ent.push_back(((uint64_t)(uint32_t)cn[k] << 32) | ((uint64_t)(e - e0) << 2) | (uint64_t)k);
+    }
+    std::sort(ent.begin(), ent.end());
+    wptr[w] = (int)went.size();
+    size_t j = 0;
+    while (j < ent.size()) {
+      const int n = (int)(ent[j] >> 32);
+      size_t j1 = j;
+      while (j1 < ent.size() && (int)(ent[j1] >> 32) == n) ++j1;
+      for (size_t q = j; q < j1; ++q) {
+        const int le = (int)((ent[q] >> 2) & 31u), k = (int)(ent[q] & 3u);
+        lspos[e0 + le] |= (uint32_t)q << (8 * k);
+      }
+      went.push_back(make_int2(0, (int)j | ((int)j1 << 16)));
+      wnode.push_back(n);
+      prow[n + 1]++;
+      j = j1;
+    }
+  }
+  wptr[n_warps] = (int)went.size();
+  for (int n = 0; n < Nn; ++n) prow[n + 1] += prow[n];
+  std::vector<int> fill(prow.begin(), prow.end() - 1);
+  for (size_t i = 0; i < went.size(); ++i) went[i].x = fill[wnode[i]]++;
+  uint32_t* d_lspos = nullptr;
+  int *d_wptr = nullptr, *d_prow = nullptr;
+  int2* d_went = nullptr;
+  float4* d_parts = nullptr;
+  int st;
+  auto up = [&](auto** dst, const auto& v) -> int {
+    int r;
+    if ((r = dalloc(c, dst, v.size()))) return r;
+    c->wa_bufs.push_back(*dst);
+    if (!v.empty())
+      CK(cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, c->stream));
+    return FEM_OK;
+  };
+  if ((st = up(&d_lspos, lspos))) return st;
+  if ((st = up(&d_wptr, wptr))) return st;
+  if ((st = up(&d_went, went))) return st;
+  if ((st = up(&d_prow, prow))) return st;
+  if ((st = dalloc(c, &d_parts, std::max<size_t>(went.size(), 1)))) return st;
+  c->wa_bufs.push_back(d_parts);
+  CK(cudaStreamSynchronize(c->stream));
+  c->wadev.lspos = d_lspos;
+  c->wadev.wptr = d_wptr;
+  c->wadev.went = d_went;
+  c->wadev.prow = d_prow;
+  c->wadev.parts = d_parts;
+  return FEM_OK;
+}
+
 // ───────────────────────── kernels wrappers ─────────────────────────
 
 // Matvec arguments with the mesh tables and the context's variant filled in.
@@ -767,6 +865,7 @@ MvArgs make_mv(const FemCtx* c) {
   mv.variant = c->mv_variant;
   mv.stage = c->stage;
   mv.eb = c->ebdev;
+  mv.wa = c->wadev;
   return mv;
 }
 
@@ -841,7 +940,8 @@ struct ChainPdl {
 // Two-level PCG with the two-phase matvec: the matvec acts on z and its node
 // gather forms p = z + beta p, q = K z + beta q (no direction-update kernel).
 bool recurrence(const FemCtx* c, int kind) {
-  return kind == GRAPH_TWO_LEVEL && c->mv_variant == MV_TWO_PHASE && c->direction_recurrence;
+  return kind == GRAPH_TWO_LEVEL && (c->mv_variant == MV_TWO_PHASE || c->mv_variant == MV_WARP_AGG) &&
+         c->direction_recurrence;
 }
 
 bool use_fused(const FemCtx* c, int kind) {
@@ -949,6 +1049,7 @@ int choose_matvec_variant(FemCtx* c) {
     c->mv_variant = c->mv_forced;
     if (c->mv_variant == MV_ELEM_BLOCK && c->eb_size == 0)
       return build_eb_tables(c, c->eb_forced > 0 ? c->eb_forced : 512);
+    if (c->mv_variant == MV_WARP_AGG) return build_wagg_tables(c);
     return FEM_OK;
   }
   if (c->mv_tuned && c->mv_tuned_model == c->model_kind) return FEM_OK;
@@ -985,7 +1086,8 @@ int choose_matvec_variant(FemCtx* c) {
   };
   for (int v = 0; v < MV_ELEM_BLOCK; ++v)
     if ((st = time_variant(v, &c->mv_ns[v]))) return st;
-  // element-block: every candidate block size (or the forced one), keep the fastest
+  // element-block: every candidate block size (or the forced one), keep the
+  // fastest; then the warp-aggregated pass
   int best_eb = 0;
   double best_ns = 0.0;
   for (int k = 0; k < 4; ++k) {
@@ -1001,11 +1103,14 @@ int choose_matvec_variant(FemCtx* c) {
   }
   if ((st = build_eb_tables(c, best_eb))) return st;
   c->mv_ns[MV_ELEM_BLOCK] = best_ns;
+  if ((st = build_wagg_tables(c))) return st;
+  if ((st = time_variant(MV_WARP_AGG, &c->mv_ns[MV_WARP_AGG]))) return st;
   int v_best = MV_FUSED;
   for (int v = 1; v < MV_N_VARIANTS; ++v)
     if (c->mv_ns[v] < c->mv_ns[v_best]) v_best = v;
   c->mv_variant = v_best;
   if (v_best != MV_ELEM_BLOCK) free_eb_tables(c);
+  if (v_best != MV_WARP_AGG) free_wagg_tables(c);
   c->mv_tuned = true;
   c->mv_tuned_model = c->model_kind;
   return FEM_OK;
@@ -1962,6 +2067,7 @@ int fem_ctx_stats(void* ctx, int64_t* out) {
   out[10] = (int64_t)std::llround(c->mv_ns[MV_ELEM_BLOCK]);
   out[11] = c->eb_size;
   for (int k = 0; k < 4; ++k) out[12 + k] = (int64_t)std::llround(c->eb_ns[k]);
+  out[16] = (int64_t)std::llround(c->mv_ns[MV_WARP_AGG]);
   return FEM_OK;
 }
 
@@ -1983,12 +2089,16 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
     case FEM_OPT_MATVEC_VARIANT:
       if (value < -1 || value >= MV_N_VARIANTS)
         return set_err(c, FEM_ERR_INVALID,
-                       "matvec variant %lld not in {-1 (auto), 0 (fused), 1 (two-phase), 2 (element-block)}",
+                       "matvec variant %lld not in {-1 (auto), 0 (fused), 1 (two-phase), 2 (element-block), "
+                       "3 (warp-aggregated)}",
                        (long long)value);
       if (value == MV_ELEM_BLOCK && c->npe != 4)
         return set_err(c, FEM_ERR_INVALID, "the element-block matvec is TET4 only");
-      // the element-block variant is only ever selected with its tables built
+      if (value == MV_WARP_AGG && c->npe != 4)
+        return set_err(c, FEM_ERR_INVALID, "the warp-aggregated matvec is TET4 only");
+      // table-driven variants are only ever selected with their tables built
       if (value == MV_ELEM_BLOCK && (st = build_eb_tables(c, c->eb_forced > 0 ? c->eb_forced : 512))) return st;
+      if (value == MV_WARP_AGG && (st = build_wagg_tables(c))) return st;
       c->mv_forced = (int)value;
       c->mv_variant = value >= 0 ? (int)value : MV_FUSED;
       c->mv_tuned = false;

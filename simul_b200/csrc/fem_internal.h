@@ -152,6 +152,20 @@ struct EbDev {
   double* pap_part;         // [n_blk] CG: each block's share of p.Ap
 };
 
+// Warp-aggregated two-phase matvec tables (MV_WARP_AGG, TET4).  Warp w
+// evaluates elements [32 w, 32 w + 32); the slot vectors of each distinct
+// vertex of those elements are added in shared memory (fixed order) into one
+// partial row per (warp, vertex), stored node-major with each node's partials
+// in warp order, and the two-phase node gather adds a node's partials.
+struct WaggDev {
+  const uint32_t* lspos;    // [Ne] four 8-bit positions of the element's slot vectors in its warp's
+                            // node-major slot order
+  const int* wptr;          // [n_warps + 1] into went
+  const int2* went;         // per (warp, local node): partial position, slot range start | end << 16
+  const int* prow;          // [Nn + 1] each node's partial range
+  float4* parts;            // [prow[Nn]] partial rows
+};
+
 struct MvArgs {
   MeshDev m;
   const DevMat<float>* matF;
@@ -162,19 +176,24 @@ struct MvArgs {
   Reduce red;
   int red_site;
   int mask_input;           // 1: fixed DOFs of x read as zero (K_ff x); 0: K_f,all x
-  int variant;              // MV_FUSED (node-block), MV_TWO_PHASE (element pass + node gather) or MV_ELEM_BLOCK
+  int variant;              // MV_FUSED (node-block), MV_TWO_PHASE (element pass + node gather),
+                            // MV_ELEM_BLOCK or MV_WARP_AGG
   float4* stage;            // [4 Ne] slot vectors in node_slots order (two-phase scratch)
   // two-phase inside CG, non-null: x holds the preconditioned residual z and
   // the node gather forms the direction by recurrence, p = z + beta p and
   // q = K z + beta q (q in y, p here), so no separate direction update runs
   float* p_rec;
   EbDev eb;                 // element-block tables (MV_ELEM_BLOCK)
+  WaggDev wa;               // warp-aggregation tables (MV_WARP_AGG)
 };
 
 // MV_ELEM_BLOCK: one CTA per element block: vertex data staged in shared
 // memory, slot vectors summed per local node in shared memory; a second
 // kernel adds the partial rows of nodes shared by blocks (fem_elemblock.cu).
-enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_ELEM_BLOCK = 2, MV_N_VARIANTS = 3 };
+// MV_WARP_AGG: the two-phase element pass with each warp's slot vectors
+// added per vertex in shared memory, so the node gather reads about a
+// quarter of the partial rows (fem_kernels.cu).
+enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_ELEM_BLOCK = 2, MV_WARP_AGG = 3, MV_N_VARIANTS = 4 };
 
 // smallest element block of the element-block matvec (one element per
 // thread; blocks of 256, 512, 768 or 1024 elements)

@@ -293,8 +293,9 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
 // Phase 2: one thread per node sums its contiguous slot range in list order,
 // so the result is the same fixed-order (bitwise reproducible) sum.
 
+// The four slot vectors f (tangent action on x) of element e.
 template <int MODEL, bool MASK>
-__device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
+__device__ __forceinline__ void elem_mv_forces(const MvArgs& a, int e, float f[4][3]) {
   const MeshDev& m = a.m;
   const int4 cn = __ldg(m.conn + e);
   const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
@@ -324,7 +325,6 @@ __device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
     for (int k = 0; k < kPay; ++k)
       pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
   }
-  const int4 sp = __ldg(m.spos + e);
   TetGeom<float> g;
   tet_geom(xv[0], xv[1], xv[2], xv[3], g);
   float D[3][3];
@@ -336,8 +336,14 @@ __device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
   grad_from_diffs(D, g, dF);
   float dP[9];
   dP_any<MODEL>(mat, scl, pay, dF, dP);
-  float f[4][3];
   slot_vectors(dP, g, g.s6, f);
+}
+
+template <int MODEL, bool MASK>
+__device__ __forceinline__ void elem_mv_one(const MvArgs& a, int e) {
+  const int4 sp = __ldg(a.m.spos + e);
+  float f[4][3];
+  elem_mv_forces<MODEL, MASK>(a, e, f);
   __stcg(a.stage + sp.x, make_float4(f[0][0], f[0][1], f[0][2], 0.f));
   __stcg(a.stage + sp.y, make_float4(f[1][0], f[1][1], f[1][2], 0.f));
   __stcg(a.stage + sp.z, make_float4(f[2][0], f[2][1], f[2][2], 0.f));
@@ -358,6 +364,53 @@ __global__ void __launch_bounds__(256, 5) elem_mv_kernel(const __grid_constant__
     elem_mv_one<MODEL, true>(a, e);
   else
     elem_mv_one<MODEL, false>(a, e);
+}
+
+// Warp-aggregated element pass: lane l of warp w evaluates element 32 w + l
+// and puts its slot vectors at their places in the warp's node-major slot
+// order in shared memory; then each (warp, vertex) row is the sum of its
+// slot range in that order, written to its place among the vertex's partials.
+constexpr int kWaggWarps = 8;
+
+template <int MODEL, bool CG>
+__global__ void __launch_bounds__(32 * kWaggWarps, 5) elem_wagg_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  __shared__ float4 s_slot[kWaggWarps][128];
+  const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
+  const int w = (int)blockIdx.x * kWaggWarps + warp;
+  const int e = w * 32 + lane;
+  if (w * 32 >= a.m.n_elems) return;  // the whole warp
+  if (e < a.m.n_elems) {
+    float f[4][3];
+    if (!CG && a.mask_input)
+      elem_mv_forces<MODEL, true>(a, e, f);
+    else
+      elem_mv_forces<MODEL, false>(a, e, f);
+    const uint32_t sp = __ldg(a.wa.lspos + e);
+    float4* sw = s_slot[warp];
+    sw[sp & 0xffu] = make_float4(f[0][0], f[0][1], f[0][2], 0.f);
+    sw[(sp >> 8) & 0xffu] = make_float4(f[1][0], f[1][1], f[1][2], 0.f);
+    sw[(sp >> 16) & 0xffu] = make_float4(f[2][0], f[2][1], f[2][2], 0.f);
+    sw[sp >> 24] = make_float4(f[3][0], f[3][1], f[3][2], 0.f);
+  }
+  __syncwarp();
+  const int q0 = __ldg(a.wa.wptr + w), q1 = __ldg(a.wa.wptr + w + 1);
+#pragma unroll 1
+  for (int i = q0 + lane; i < q1; i += 32) {
+    const int2 en = __ldg(a.wa.went + i);  // partial position, slot range
+    const int j1 = en.y >> 16;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+    for (int j = en.y & 0xffff; j < j1; ++j) {
+      const float4 v = s_slot[warp][j];
+      a0 += v.x;
+      a1 += v.y;
+      a2 += v.z;
+    }
+    __stcg(a.wa.parts + en.x, make_float4(a0, a1, a2, 0.f));
+  }
 }
 
 // kGatherLanes lanes per node: lane k of a node's group adds slots k,
@@ -979,6 +1032,25 @@ static void matvec_nb(const MvArgs& a, int model, cudaStream_t s) {
 }
 
 template <bool CG>
+static void warp_agg(const MvArgs& a, int model, cudaStream_t s) {
+  const int ge = nblk(nblk(a.m.n_elems, 32), kWaggWarps);
+  switch (model) {
+    case M_LE: launch_chain(elem_wagg_kernel<M_LE, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+    case M_NH: launch_chain(elem_wagg_kernel<M_NH, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+    case M_MR: launch_chain(elem_wagg_kernel<M_MR, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+    case M_J2: launch_chain(elem_wagg_kernel<M_J2, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+    case M_TI: launch_chain(elem_wagg_kernel<M_TI, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+    case M_FMR: launch_chain(elem_wagg_kernel<M_FMR, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+    default: launch_chain(elem_wagg_kernel<-1, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
+  }
+  // the two-phase node gather over the partial rows
+  MvArgs g = a;
+  g.m.node_row = a.wa.prow;
+  g.stage = a.wa.parts;
+  launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, g);
+}
+
+template <bool CG>
 static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
   const int ge = nblk(a.m.n_elems, 256);
   switch (model) {
@@ -1006,13 +1078,17 @@ void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
     return;
   }
   const bool cg = a.cg != nullptr;
+  if (a.variant == MV_WARP_AGG && a.wa.parts != nullptr) {
+    cg ? warp_agg<true>(a, model, s) : warp_agg<false>(a, model, s);
+    return;
+  }
   if (a.variant == MV_ELEM_BLOCK && a.eb.nodes != nullptr) {
     launch_matvec_eb(a, model, s);
     return;
   }
-  if (a.variant == MV_ELEM_BLOCK) {
-    // no element-block tables (the host builds them whenever it selects the
-    // variant): the two-phase pass gives the same product
+  if (a.variant == MV_ELEM_BLOCK || a.variant == MV_WARP_AGG) {
+    // no tables (the host builds them whenever it selects the variant): the
+    // two-phase pass gives the same product
     cg ? two_phase<true>(a, model, s) : two_phase<false>(a, model, s);
     return;
   }

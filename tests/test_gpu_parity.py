@@ -96,7 +96,7 @@ def test_element_forces_and_stress(cuda, bar, key, nb):
         assert _rel_max(mesh.F.cpu().numpy(), ref["F"]) < 1e-12
 
 
-VARIANTS = ["fused", "two_phase", "element_block"]
+VARIANTS = ["fused", "two_phase", "element_block", "warp_agg"]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -643,6 +643,7 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
     # then the blocks' partial rows in block order: FP32 rounding apart
     assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-6
     assert _rel_l2(ys["element_block"], ys["fused"]) < 1e-6
+    assert _rel_l2(ys["warp_agg"], ys["fused"]) < 1e-6
     # automatic choice: the first PCG solve times every variant (the element
     # block at each candidate size) and keeps the fastest
     mesh.set_matvec_variant(None)

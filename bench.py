@@ -79,6 +79,13 @@ def parse():
                     help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
     ap.add_argument("--cg-rtol-max", type=float, default=1e-1, help="inexact-Newton forcing term cap")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the keys reported beside the headline (1M-tet point, n = 128 roofline, batch)")
+    ap.add_argument("--n-large", type=int, default=78,
+                    help="the vertebral body solved beside the headline (78: ~1.02 M tets)")
+    ap.add_argument("--n-roofline", type=int, default=128,
+                    help="matvec roofline also reported at this size (beyond L2)")
+    ap.add_argument("--batch-instances", type=int, default=16, help="batched uneven solves reported beside")
     return ap.parse_args()
 
 
@@ -201,39 +208,66 @@ def build_inputs(args):
     return meshgen.vertebral_body(n=args.n, seed=0)
 
 
-def cpu_leg(args, v, gpu_cg_total, threads):
-    """C++/OpenMP restatement on the host cores, first load step, scaled."""
+def cpu_path(args, v, threads, steps=None, on_step=None):
+    """The C++/OpenMP FP64 restatement of the plain method (Newton + Jacobi-PCG)
+    over the load path from rest: load steps 1..``steps`` (default all), each
+    to ``tol``, J2 history carried from step to step.  ``on_step(k, dt, info,
+    solver)`` sees every step.  Returns the solver (its u after the last step)
+    and the per-step (seconds, info)."""
     from oracle.cpu_solver import CpuSolver
     s = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
-    t = time.perf_counter()
-    info = s.solve(v.fixed_mask, v.fixed_vals / args.load_steps, v.f_ext, tol=args.tol)
-    dt = time.perf_counter() - t
-    return s.n_threads, dt, info, s.u.copy()
+    out = []
+    for k in range(1, (steps or args.load_steps) + 1):
+        t = time.perf_counter()
+        info = s.solve(v.fixed_mask, v.fixed_vals * (k / args.load_steps), v.f_ext, tol=args.tol)
+        dt = time.perf_counter() - t
+        out.append((dt, info))
+        if on_step is not None:
+            on_step(k, dt, info, s)
+    return s, out
 
 
 def reference_arm(args, rank, ws):
+    """One bench step = one load step of the CPU restatement's load path, in
+    order from rest (J2 history carried); ``--steps`` equal to the number of
+    load steps times exactly one full path, more steps start the path again.
+    ``value`` = the mean load-step time times the number of load steps (for
+    ``--steps 20``: the measured time of one full 20-step path)."""
     if rank != 0:
         return
     v = build_inputs(args)
     from oracle.cpu_solver import CpuSolver
     threads = args.cpu_threads or os.cpu_count() or 1
-    times = []
-    info = None
-    nthreads = threads
-    for i in range(args.warmup + args.steps):
-        s = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
+    # warm-up: the first load steps of a separate path (page-in, OpenMP start-up)
+    warm = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
+    for k in range(1, min(args.warmup, args.load_steps) + 1):
+        warm.solve(v.fixed_mask, v.fixed_vals * (k / args.load_steps), v.f_ext, tol=args.tol)
+    nthreads = warm.n_threads
+    del warm
+    times, newton, cg, conv = [], 0, 0, True
+    s = None
+    for i in range(args.steps):
+        k = i % args.load_steps + 1
+        if k == 1:
+            s = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
         t = time.perf_counter()
-        info = s.solve(v.fixed_mask, v.fixed_vals / args.load_steps, v.f_ext, tol=args.tol)
-        dt = time.perf_counter() - t
-        nthreads = s.n_threads
-        if i >= args.warmup:
-            times.append(dt * args.load_steps)
-    value = float(np.mean(times))
-    sample = (f"load step 1 of {args.load_steps} (elastic, {info['iterations']} Newton / "
-              f"{info['cg_iterations']} CG iterations) timed and multiplied by {args.load_steps}; the "
-              f"plastic steps cost more CG work, so this understates the full CPU solve")
+        info = s.solve(v.fixed_mask, v.fixed_vals * (k / args.load_steps), v.f_ext, tol=args.tol)
+        times.append(time.perf_counter() - t)
+        newton += info["iterations"]
+        cg += info["cg_iterations"]
+        conv &= info["converged"]
+    per_step = float(np.mean(times))
+    value = per_step * args.load_steps
+    full = args.steps >= args.load_steps
+    sample = (f"{args.steps} load steps timed one by one in path order from rest ({newton} Newton / {cg} CG "
+              f"iterations, all converged: {conv}); "
+              + (f"value = their mean x {args.load_steps}, i.e. the measured time of the full "
+                 f"{args.load_steps}-step path" if args.steps % args.load_steps == 0 else
+                 f"value = their mean x {args.load_steps}" + ("" if full else " (a partial path: the later, "
+                                                                                 "plastic steps cost more)")))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "step": "one load step of the path (the metric's unit, one full solve, is load_steps of them)",
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),
             "method": "Newton (FP64) + Jacobi-PCG (FP64), C++/OpenMP restatement",
@@ -244,6 +278,109 @@ def reference_arm(args, rank, ws):
                               "of the plain method (the reference itself factorises an assembled tangent "
                               "with SuperLU, which does not finish at this size in minutes)"}
     print(json.dumps(line), flush=True)
+
+
+def configure(mesh, args):
+    """The timed method's solver options on a mesh."""
+    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16),
+                            inverse=args.coarse_inverse, max_nodes=args.coarse_max_nodes)
+    if args.matvec_variant != "auto":
+        mesh.set_matvec_variant(args.matvec_variant)
+    mesh.set_fused_step(bool(args.fused_step))
+    mesh.set_whole_solve_graph(bool(args.whole_solve_graph))
+    mesh.set_programmatic_launch(bool(args.pdl))
+    mesh.set_block_smoother(bool(args.block_smoother))
+
+
+def size_point(args, n, dev, jacobi=True):
+    """The same workload at n voxels per axis: one warm-up and one timed full
+    solve with the timed method, and (``jacobi``) the same with Jacobi-PCG."""
+    import torch
+    from simul_b200 import fem as B
+    from simul_b200 import meshgen
+    v = meshgen.vertebral_body(n=n, seed=0)
+    mesh = B.FEMesh(v.n_nodes, v.n_elements, device=dev)
+    mesh.initialize_from_numpy(v.X, v.conn)
+    configure(mesh, args)
+    mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
+    fixed_full = torch.from_numpy(v.fixed_vals).to(dev)
+    fixed_mask = torch.from_numpy(v.fixed_mask.astype(np.int32)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {"n": n, "tets": int(v.n_elements), "nodes": int(v.n_nodes)}
+    for name, pc in [(args.precond, args.precond)] + ([("jacobi_pcg", "jacobi")] if jacobi else []):
+        solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=pc, cg_rtol_min=args.cg_rtol_min,
+                                cg_rtol_max=args.cg_rtol_max)
+        for rep in range(2):
+            mesh.u.zero_()
+            mat.reset_state()
+            mesh.fixed.copy_(fixed_mask)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            st = {"newton": 0, "cg": 0, "conv": True, "rel": 0.0}
+            for k in range(1, args.load_steps + 1):
+                mesh.fixed_value.copy_(fixed_full * (k / args.load_steps))
+                mesh._bc_dirty = True
+                r = solver.solve(verbose=False)
+                st["newton"] += r["iterations"]
+                st["cg"] += r["cg_iterations"]
+                st["conv"] &= r["converged"]
+                st["rel"] = max(st["rel"], r["relative_residual"])
+            e1.record(stream)
+            e1.synchronize()
+        out[name] = {"s": e0.elapsed_time(e1) / 1e3, "newton_iterations": st["newton"], "cg_iterations": st["cg"],
+                     "all_converged": bool(st["conv"]), "max_relative_residual": st["rel"],
+                     "timed_once_after_one_warmup": True}
+        del solver
+    if jacobi:
+        out["speedup_vs_jacobi_pcg"] = out["jacobi_pcg"]["s"] / out[args.precond]["s"]
+    del mesh
+    torch.cuda.empty_cache()
+    return out
+
+
+def roofline_point(args, n, dev):
+    """Tangent-matvec roofline at n voxels per axis (its working set beyond the
+    126 MB L2): CUDA-event time per launch at a plastic state of the
+    workload (fem_profile_kernels, 50 launches) against the algorithmic bytes."""
+    import ctypes as C
+    import torch
+    from simul_b200 import _lib
+    from simul_b200 import fem as B
+    from simul_b200 import meshgen
+    v = meshgen.vertebral_body(n=n, seed=0)
+    mesh = B.FEMesh(v.n_nodes, v.n_elements, device=dev)
+    mesh.initialize_from_numpy(v.X, v.conn)
+    configure(mesh, args)
+    mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
+    idx = np.where(v.fixed_mask.reshape(-1))[0]
+    mesh.set_fixed_dofs(idx, (v.fixed_vals * 0.2).reshape(-1)[idx])
+    u = np.zeros_like(v.X)
+    u[:, 2] = -0.004 * v.X[:, 2]
+    mesh.u.copy_(torch.from_numpy(u))
+    mat.compute_nodal_forces(mesh)
+    # the variant choice the solver makes (timed on a first PCG solve)
+    rhs = torch.zeros(v.n_nodes, 3, dtype=torch.float64, device=dev)
+    rhs[:, 2] = 1.0
+    du = torch.zeros_like(rhs)
+    it, rel = C.c_int32(), C.c_double()
+    _lib.load().fem_pcg(mesh.ctx, _lib.FEM_PRECOND_JACOBI, C.c_void_p(rhs.data_ptr()), C.c_void_p(du.data_ptr()),
+                        1e-2, 50, C.byref(it), C.byref(rel))
+    kms = (C.c_double * 4)()
+    rc = _lib.load().fem_profile_kernels(mesh.ctx, 50, kms)
+    peak, peak_src = measured_peaks()
+    st = mesh.stats()
+    b = matvec_bytes(v.n_elements, v.n_nodes)
+    out = {"n": n, "tets": int(v.n_elements), "nodes": int(v.n_nodes), "variant": st["matvec_variant"],
+           "matvec_ms": kms[0] if rc == 0 else None, "algorithmic_bytes": b}
+    if rc == 0:
+        ach = b / (kms[0] * 1e-3) / 1e9
+        out.update({"achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_source": peak_src,
+                    "residual_ms": kms[1],
+                    "residual_achieved": residual_bytes(v.n_elements, v.n_nodes) / (kms[1] * 1e-3) / 1e9})
+    del mesh
+    torch.cuda.empty_cache()
+    return out
 
 
 def main():
@@ -281,14 +418,7 @@ def main():
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=args.tol, precond=args.precond, cg_rtol_min=args.cg_rtol_min,
                             cg_rtol_max=args.cg_rtol_max)
-    mesh.set_coarse_options(cell=args.coarse_cell, reuse=args.coarse_reuse, bf16=bool(args.coarse_bf16),
-                            inverse=args.coarse_inverse, max_nodes=args.coarse_max_nodes)
-    if args.matvec_variant != "auto":
-        mesh.set_matvec_variant(args.matvec_variant)
-    mesh.set_fused_step(bool(args.fused_step))
-    mesh.set_whole_solve_graph(bool(args.whole_solve_graph))
-    mesh.set_programmatic_launch(bool(args.pdl))
-    mesh.set_block_smoother(bool(args.block_smoother))
+    configure(mesh, args)
     if args.precond == "learned":
         from simul_b200 import learned
         learned.set_weights(mesh, learned.load(args.weights))
@@ -453,8 +583,11 @@ def main():
             "fused_step": mesh.step_info(),
             "whole_solve_graphs": {"available": st["whole_solve_graph_available"],
                                    "pcg_solves_as_one_launch": st["whole_solve_graphs"]},
-            "roofline": {"bound": "hbm", "kernel": ("matvec_kernel<J2> (fused node-block)" if variant == "fused"
-                                                    else "elem_mv_kernel<J2> + node_gather_kernel (two-phase)"),
+            "roofline": {"bound": "hbm", "kernel": {
+                "fused": "matvec_kernel<J2> (fused node-block)",
+                "two_phase": "elem_mv_kernel<J2> + node_gather_kernel (two-phase)",
+                "element_block": "eb_matvec_kernel<J2> + eb_complete_kernel (element-block)",
+                "warp_agg": "elem_wagg_kernel<J2> + node_gather_kernel (warp-aggregated two-phase)"}.get(variant, variant),
                          "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "frac_nominal_8tbs": (achieved / 8000.0) if achieved else None,
@@ -464,29 +597,42 @@ def main():
                          if rc == 0 else None}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = args.cpu_threads or os.cpu_count() or 1
-        nthr, dt, cinfo, u_cpu = cpu_leg(args, v, last["cg"], threads)
-        # accuracy: the first load step from rest on the GPU (timed method)
-        # against the FP64 CPU restatement's solution of the same step
+        # the timed method's displacement after the first and the last load step
         mesh.u.zero_()
         mat.reset_state()
         mesh.fixed.copy_(fixed_mask)
-        mesh.fixed_value.copy_(fixed_full * (1.0 / args.load_steps))
-        mesh._bc_dirty = True
-        r1 = solver.solve(verbose=False)
-        u_gpu = mesh.get_displacements()
-        line["accuracy"] = {"load_step": 1, "reference": "oracle/cpu_fem.cpp (FP64 Newton + PCG to the same tol)",
-                            "u_rel_l2": float(np.linalg.norm(u_gpu - u_cpu) / max(np.linalg.norm(u_cpu), 1e-300)),
-                            "gpu_relative_residual": r1["relative_residual"],
-                            "cpu_relative_residual": cinfo["relative_residual"]}
-        # the port restates the plain method (Jacobi-PCG); scale its first load
-        # step by the plain method's CG count on the GPU for the same solve
-        ref_cg = jac["cg_iterations"] if jac else last["cg"]
-        scale = ref_cg / max(cinfo["cg_iterations"], 1)
-        line["cpu_baseline"] = {"value": dt * scale, "unit": UNIT, "cores": nthr, "kind": "port",
-                                "sample": f"load step 1 of {args.load_steps} ({cinfo['cg_iterations']} CG "
-                                          f"iterations, {dt:.2f} s) scaled by the Jacobi-PCG solve's "
-                                          f"CG-iteration count ({ref_cg}); C++/OpenMP FP64 restatement of "
-                                          f"the plain method (Newton + Jacobi-PCG)"}
+        u_gpu, rel_gpu = {}, {}
+        for k in range(1, args.load_steps + 1):
+            mesh.fixed_value.copy_(fixed_full * (k / args.load_steps))
+            mesh._bc_dirty = True
+            r = solver.solve(verbose=False)
+            if k in (1, args.load_steps):
+                u_gpu[k], rel_gpu[k] = mesh.get_displacements(), r["relative_residual"]
+        # the CPU restatement over the same full path (one measured path: the
+        # CPU baseline), compared with the GPU after steps 1 and load_steps
+        u_cpu, rel_cpu = {}, {}
+
+        def keep(k, dt, info, s):
+            if k in (1, args.load_steps):
+                u_cpu[k], rel_cpu[k] = s.u.copy(), info["relative_residual"]
+
+        t0 = time.perf_counter()
+        cs, steps = cpu_path(args, v, threads, on_step=keep)
+        cpu_s = time.perf_counter() - t0
+        acc = {}
+        for k in sorted(u_gpu):
+            acc[f"load_step_{k}"] = {
+                "u_rel_l2": float(np.linalg.norm(u_gpu[k] - u_cpu[k]) / max(np.linalg.norm(u_cpu[k]), 1e-300)),
+                "gpu_relative_residual": rel_gpu[k], "cpu_relative_residual": rel_cpu[k]}
+        line["accuracy"] = {"reference": "oracle/cpu_fem.cpp: FP64 Newton + Jacobi-PCG over the same load path "
+                                         "to the same tol", **acc}
+        line["cpu_baseline"] = {"value": cpu_s, "unit": UNIT, "cores": cs.n_threads, "kind": "port",
+                                "sample": f"the full {args.load_steps}-step path from rest, timed once "
+                                          f"({sum(i['iterations'] for _, i in steps)} Newton / "
+                                          f"{sum(i['cg_iterations'] for _, i in steps)} CG iterations, all "
+                                          f"converged: {all(i['converged'] for _, i in steps)}); C++/OpenMP "
+                                          f"FP64 restatement of the plain method (Newton + Jacobi-PCG), the "
+                                          f"same code --impl reference times"}
     if rank == 0 and ws == 1 and not args.no_hex8:
         # the same body and loading with one HEX8 per voxel (the reference's
         # FEMAdapter / labelmap element), two-level PCG, one warm-up sequence
@@ -501,6 +647,22 @@ def main():
                             "all_converged": h["converged"]}
         except Exception as exc:  # reported, never fatal to the headline line
             line["hex8"] = {"error": repr(exc)}
+    if rank == 0 and ws == 1 and not args.no_extras:
+        # beside the headline, each reported, never fatal to it: the north
+        # star's 1M-tet point, the matvec roofline beyond L2, batched solves
+        for key, fn in (("vertebra_1m_tets", lambda: size_point(args, args.n_large, dev)),
+                        ("roofline_large", lambda: roofline_point(args, args.n_roofline, dev)),
+                        ("batch", lambda: __import__("simul_b200.batch_bench", fromlist=["run"]).run(
+                            instances=args.batch_instances, n_min=32, n_max=64, load_steps=10, seed=0,
+                            workers=8, device=str(dev)))):
+            try:
+                line[key] = fn()
+            except Exception as exc:
+                line[key] = {"error": repr(exc)}
+        if isinstance(line.get("batch"), dict) and "error" not in line["batch"]:
+            line["batch"]["note"] = ("the batched uneven-solves workload at reduced scale: instances with grid "
+                                     "sizes 32-64 voxels per axis, 10 load steps (the full 64-instance, 32-96 "
+                                     "run: python -m simul_b200.batch_bench)")
     if rank == 0:
         print(json.dumps(line), flush=True)
     del solver, mesh

@@ -45,6 +45,77 @@ def _make_case(args):
             "E": v.E, "fixed": fixed, "vals": vals, "f": f, "tets": int(v.n_elements)}
 
 
+def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, precond="two_level",
+        sequential=False, workers=16, coarse_cell=4, coarse_bf16=True, coarse_reuse=0, device=0):
+    """Generates the seeded instances, solves them as one batch after a
+    one-step warm-up pass, and returns solves/s, p50/p99 per-instance wall
+    time and iteration counts (one dict)."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(instances):
+        n = int(rng.integers(n_min, n_max + 1))
+        case = CASES[int(rng.integers(0, len(CASES)))]
+        specs.append((i, n, 1000 + i, case, float(rng.uniform(0.01, 0.03))))
+    t0 = time.perf_counter()
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        cases = sorted(ex.map(_make_case, specs), key=lambda d: d["idx"])
+    t_gen = time.perf_counter() - t0
+
+    import torch
+    from simul_b200 import batch
+    from simul_b200 import fem as B
+    dev = torch.device(device) if isinstance(device, str) else torch.device("cuda", device)
+    torch.cuda.init()
+
+    def build(d):
+        mat = B.J2Plasticity(d["E"], 0.3, 100.0, hardening_modulus=0.02 * d["E"])
+        return batch.BatchInstance(d["X"], d["conn"], mat, d["fixed"], d["vals"], d["f"], device=dev,
+                                   coarse_cell=coarse_cell, coarse_bf16=bool(coarse_bf16),
+                                   coarse_reuse=coarse_reuse)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=8) as ex:
+        insts = list(ex.map(build, cases))
+    t_setup = time.perf_counter() - t0
+
+    def reset():
+        """Every instance back to rest: u = 0, no plastic history."""
+        for inst in insts:
+            inst.reset()
+        torch.cuda.synchronize()
+
+    # warm-up pass (graph capture, matvec-variant timing, coarse set-up), then reset
+    batch.solve_batch(insts, load_steps=1, precond=precond, n_threads=threads)
+    reset()
+    t0 = time.perf_counter()
+    out = batch.solve_batch(insts, load_steps=load_steps, precond=precond, n_threads=threads)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = np.array([r["wall_ms"] for r in out["instances"]])
+    res = {"instances": instances, "n_range": [n_min, n_max], "tets_total": int(sum(d["tets"] for d in cases)),
+           "tets_min": int(min(d["tets"] for d in cases)), "tets_max": int(max(d["tets"] for d in cases)),
+           "cases": {c: sum(1 for d in cases if d["case"] == c) for c in CASES},
+           "load_steps": load_steps, "precond": precond,
+           "coarse": {"cell_voxels": coarse_cell, "inverse": "bf16" if coarse_bf16 else "f32",
+                      "reuse": coarse_reuse},
+           "all_converged": bool(all(r["converged"] for r in out["instances"])),
+           "batch_wall_s": wall, "solves_per_s": instances / wall,
+           "p50_instance_ms": float(np.percentile(ms, 50)), "p99_instance_ms": float(np.percentile(ms, 99)),
+           "newton_iterations": int(sum(r["newton_iterations"] for r in out["instances"])),
+           "cg_iterations": int(sum(r["cg_iterations"] for r in out["instances"])),
+           "host_generation_s": t_gen, "host_setup_s": t_setup}
+    if sequential:
+        reset()
+        t0 = time.perf_counter()
+        out2 = batch.solve_batch(insts, load_steps=load_steps, precond=precond, n_threads=1)
+        torch.cuda.synchronize()
+        res["sequential_wall_s"] = time.perf_counter() - t0
+        res["sequential_solves_per_s"] = instances / res["sequential_wall_s"]
+        res["sequential_all_converged"] = bool(all(r["converged"] for r in out2["instances"]))
+    del insts
+    return res
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--instances", type=int, default=64)
@@ -61,68 +132,10 @@ def main(argv=None):
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="coarse operator: 0 once per solve from rest (small-strain J2), -1 adaptive")
     args = ap.parse_args(argv)
-    rng = np.random.default_rng(args.seed)
-    specs = []
-    for i in range(args.instances):
-        n = int(rng.integers(args.n_min, args.n_max + 1))
-        case = CASES[int(rng.integers(0, len(CASES)))]
-        specs.append((i, n, 1000 + i, case, float(rng.uniform(0.01, 0.03))))
-    t0 = time.perf_counter()
-    with ProcessPoolExecutor(max_workers=args.workers, mp_context=mp.get_context("spawn")) as ex:
-        cases = sorted(ex.map(_make_case, specs), key=lambda d: d["idx"])
-    t_gen = time.perf_counter() - t0
-
-    import torch
-    from simul_b200 import batch
-    from simul_b200 import fem as B
-    dev = torch.device("cuda", 0)
-    torch.cuda.init()
-
-    def build(d):
-        mat = B.J2Plasticity(d["E"], 0.3, 100.0, hardening_modulus=0.02 * d["E"])
-        return batch.BatchInstance(d["X"], d["conn"], mat, d["fixed"], d["vals"], d["f"], device=dev,
-                                   coarse_cell=args.coarse_cell, coarse_bf16=bool(args.coarse_bf16),
-                                   coarse_reuse=args.coarse_reuse)
-
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=8) as ex:
-        insts = list(ex.map(build, cases))
-    t_setup = time.perf_counter() - t0
-    def reset():
-        """Every instance back to rest: u = 0, no plastic history."""
-        for inst in insts:
-            inst.reset()
-        torch.cuda.synchronize()
-
-    # warm-up pass (graph capture, matvec-variant timing, coarse set-up), then reset
-    batch.solve_batch(insts, load_steps=1, precond=args.precond, n_threads=args.threads)
-    reset()
-    t0 = time.perf_counter()
-    out = batch.solve_batch(insts, load_steps=args.load_steps, precond=args.precond, n_threads=args.threads)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    ms = np.array([r["wall_ms"] for r in out["instances"]])
-    res = {"instances": args.instances, "tets_total": int(sum(d["tets"] for d in cases)),
-           "tets_min": int(min(d["tets"] for d in cases)), "tets_max": int(max(d["tets"] for d in cases)),
-           "cases": {c: sum(1 for d in cases if d["case"] == c) for c in CASES},
-           "load_steps": args.load_steps, "precond": args.precond,
-           "coarse": {"cell_voxels": args.coarse_cell, "inverse": "bf16" if args.coarse_bf16 else "f32",
-                      "reuse": args.coarse_reuse},
-           "all_converged": bool(all(r["converged"] for r in out["instances"])),
-           "batch_wall_s": wall, "solves_per_s": args.instances / wall,
-           "p50_instance_ms": float(np.percentile(ms, 50)), "p99_instance_ms": float(np.percentile(ms, 99)),
-           "newton_iterations": int(sum(r["newton_iterations"] for r in out["instances"])),
-           "cg_iterations": int(sum(r["cg_iterations"] for r in out["instances"])),
-           "host_generation_s": t_gen, "host_setup_s": t_setup}
-    if args.sequential:
-        reset()
-        t0 = time.perf_counter()
-        out2 = batch.solve_batch(insts, load_steps=args.load_steps, precond=args.precond, n_threads=1)
-        torch.cuda.synchronize()
-        res["sequential_wall_s"] = time.perf_counter() - t0
-        res["sequential_solves_per_s"] = args.instances / res["sequential_wall_s"]
-        res["sequential_all_converged"] = bool(all(r["converged"] for r in out2["instances"]))
-    print(json.dumps(res))
+    print(json.dumps(run(instances=args.instances, n_min=args.n_min, n_max=args.n_max, load_steps=args.load_steps,
+                         threads=args.threads, seed=args.seed, precond=args.precond, sequential=args.sequential,
+                         workers=args.workers, coarse_cell=args.coarse_cell, coarse_bf16=bool(args.coarse_bf16),
+                         coarse_reuse=args.coarse_reuse)))
 
 
 if __name__ == "__main__":

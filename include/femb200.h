@@ -204,11 +204,10 @@ enum {
    * node's 3 x 3 diagonal block of K_T (free DOFs), 0 the inverse of the
    * diagonal */
   FEM_OPT_BLOCK_JACOBI = 10,
-  /* two-level coarse inverse from the Cholesky factor L: 1 (default) FP64,
-   * W = L^-1 by a triangular solve against the identity, then the lower
-   * triangle of W^T W (cuBLAS trsm + syrk); 0 FP64 cuSOLVER potri; 2 the
-   * same as 1 in FP32; 3 FP32 factor, trsm and syrk on TF32 tensor cores
-   * (for the BF16 inverse, whose rounding is coarser than TF32's) */
+  /* two-level coarse inverse (the project's dense kernels: blocked Cholesky
+   * L L^T, W = L^-1, the lower triangle of W^T W): 0 or 1 (default) in FP64,
+   * 2 or 3 in FP32 (enough for the FP32 or BF16 copy that is applied; the
+   * values name the library routines earlier versions chose between) */
   FEM_OPT_COARSE_INVERSE = 11,
   /* two-level: at most this many coarse nodes (default 4096, up to 16384);
    * the lattice cell grows by 25 % steps until the lattice fits */
@@ -274,6 +273,42 @@ int fem_mpnn_eval(void* ctx, const float* R, const float* E, int32_t n_pairs, do
  * BF16 row-major device arrays, one tcgen05 tile; N, K multiples of 16 in
  * [16, 256].  Errors go to fem_last_error(NULL). */
 int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t K, void* stream);
+/* Dense SPD inverse, the kernels the two-level preconditioner forms its
+ * coarse inverse with (no reference counterpart: the reference has no coarse
+ * space; its direct solve is scipy's spsolve of the assembled tangent,
+ * backend/fea/fem/solver/static_solver.py:430-462).  A: n x n column-major
+ * device array (FP64, lower
+ * triangle read); out: n x n column-major device array receiving the lower
+ * triangle of A^-1; precision 32 (FP32 arithmetic) or 64.  Blocked Cholesky
+ * A = L L^T, W = L^-1, A^-1 = W^T W on the project's tile kernels.
+ * FEM_ERR_NAN if a pivot is not positive.  Allocates its work space.
+ * Errors: fem_last_error(NULL). */
+int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream);
+
+/* ---- node-to-node contact between two bodies (backend/fea/framework/contact.py) ----
+ * Device arrays in the caller's node order, FP64 current coordinates
+ * (reference + displacement, n x 3), surfaces as int32 node lists; forces
+ * are ADDED to f_a / f_b (n x 3 FP64, zero them first), bitwise
+ * reproducible.  Errors: fem_last_error(NULL). */
+/* NodeNodeContact.detect's nearest-neighbour query (contact.py:49-92):
+ * for every A-surface node i, nearest[i] = the index into surf_b of its
+ * nearest B-surface node (the smaller index on ties), dist[i] its distance. */
+int fem_contact_nearest(const double* pos_a, const int32_t* surf_a, int32_t na, const double* pos_b,
+                        const int32_t* surf_b, int32_t nb, int32_t* nearest, double* dist, void* stream);
+/* detect + compute_forces (contact.py:49-173, no damping): pairs closer
+ * than gap_tol get f = penalty (gap_tol - d) (x_a - x_b) / max(d_ab, 1e-15)
+ * on A and -f on B (added in pair order, as np.add.at); *n_pairs and *total
+ * (= sum |f| over A's components, scene.py:357) on the host. */
+int fem_contact_penalty(const double* pos_a, const int32_t* surf_a, int32_t na, const double* pos_b,
+                        const int32_t* surf_b, int32_t nb, double gap_tol, double penalty, double* f_a, double* f_b,
+                        int32_t* n_pairs, double* total, void* stream);
+/* compute_tied_forces (contact.py:224-273): pairs (n_pairs x 2 int32, A
+ * node, B node; each A node once), offsets (n_pairs x 3) the initial
+ * x_a - x_b; f = -penalty ((x_a - x_b) - offset) on A, -f on B; nb_nodes =
+ * B's node count; *total = sum |f| (host). */
+int fem_contact_tied(const double* pos_a, const double* pos_b, const int32_t* pairs, const double* offsets,
+                     int32_t n_pairs, int32_t nb_nodes, double penalty, double* f_a, double* f_b, double* total,
+                     void* stream);
 /* two-level preconditioner state: out[0] lattice cells, [1] coarse nodes,
  * [2] coarse DOFs, [3] cell edge, [4] assemblies so far, [5] ms of the last
  * assembly + factorisation (CUDA events), [6] ms of its assembly part,

@@ -197,7 +197,7 @@ __global__ void coarse_dense_kernel(const __grid_constant__ CoarseDev c) {
   c.Ac[q] = acc;
 }
 
-// Symmetric FP32 copy of the inverse whose lower triangle potri wrote
+// Symmetric FP32 copy of the inverse whose lower triangle the dense inverse wrote
 // (column-major: element (lo, hi), lo >= hi, at hi * n + lo).
 __global__ void coarse_sym_kernel(const __grid_constant__ CoarseDev c) {
   const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -896,37 +896,6 @@ void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out
 }
 
 int coarse_product_kernels(const CoarseDev& c) { return c.Ainv16 ? 2 : 1; }
-
-__global__ void identity_d_kernel(double* w, int n) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (int64_t)n * n) return;
-  w[q] = (q / n == q % n) ? 1.0 : 0.0;
-}
-
-void launch_identity_d(double* w, int n, cudaStream_t s) {
-  identity_d_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(w, n);
-}
-
-__global__ void identity_f_kernel(float* w, int n) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (int64_t)n * n) return;
-  w[q] = (q / n == q % n) ? 1.f : 0.f;
-}
-
-void launch_identity_f(float* w, int n, cudaStream_t s) {
-  identity_f_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(w, n);
-}
-
-__global__ void lower_to_f32_kernel(const double* a, float* out, int n) {
-  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (int64_t)n * n) return;
-  const int col = (int)(q / n), row = (int)(q % n);
-  out[q] = row >= col ? (float)a[q] : 0.f;
-}
-
-void launch_lower_to_f32(const double* a, float* out, int n, cudaStream_t s) {
-  lower_to_f32_kernel<<<nblk((int64_t)n * n, 256), 256, 0, s>>>(a, out, n);
-}
 
 // Resident CTAs of the tile product on this device (one wave, tiles looped).
 int tile_mv_grid() {

@@ -5,8 +5,6 @@
 // element kernels use.  Callers keep their own numbering: every per-call array
 // is permuted on entry and exit.
 #include <cuda_runtime.h>
-#include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include <algorithm>
 #include <atomic>
@@ -164,7 +162,7 @@ struct FemCtx {
   double* tr_scal = nullptr;  // [0] loss sum, [1] dL/dz scale
 
   // two-level preconditioner: coarse lattice tables (built on first use),
-  // dense coarse operator and its inverse, cuSOLVER handle and workspace
+  // dense coarse operator and its inverse, dense-inverse work space
   CoarseDev cdev{};
   bool coarse_built = false;
   bool coarse_valid = false;   // Ainv matches the current tangent policy
@@ -184,17 +182,13 @@ struct FemCtx {
   double coarse_ms_assembly = 0.0;   // of which cell blocks + dense assembly
   cudaEvent_t coarse_ev[3] = {nullptr, nullptr, nullptr};
   std::vector<void*> coarse_bufs;
-  cusolverDnHandle_t solver = nullptr;
-  double* sol_work = nullptr;
-  // coarse inverse from the Cholesky factor: 1 (default) W = L^-1 by a
-  // triangular solve with n right-hand sides, then Ac^-1 = W^T W (cuBLAS
-  // trsm + syrk, GEMM-rich); 0 cuSOLVER potri; 2 / 3 as 1 in FP32 / with
-  // TF32 tensor cores
+  // coarse inverse (fem_dense.cu: blocked Cholesky, W = L^-1, Ac^-1 = W^T W):
+  // 0 and 1 (default) in FP64, 2 and 3 in FP32 (option values of earlier
+  // library versions, which chose between library routines)
   int coarse_inverse = 1;
-  cublasHandle_t blas = nullptr;
-  double* coarse_w = nullptr;  // [n_dof^2] W = L^-1
-  int sol_lwork = 0;
-  int* sol_info = nullptr;
+  void* dense_work = nullptr;   // padded factor and W (and the FP32 result)
+  size_t dense_bytes = 0;
+  int* dense_info = nullptr;    // first non-positive pivot, 0 if none
   int* h_info = nullptr;
   // matvec variant: forced by fem_set_option (>= 0) or chosen by timing all
   int mv_forced = -1;
@@ -339,12 +333,9 @@ void free_ctx(FemCtx* c) {
   for (void* p : c->wa_bufs)
     if (p) cudaFree(p);
   if (c->h_err) cudaFreeHost(c->h_err);
-  if (c->sol_work) cudaFree(c->sol_work);
-  if (c->coarse_w) cudaFree(c->coarse_w);
-  if (c->blas) cublasDestroy(c->blas);
-  if (c->sol_info) cudaFree(c->sol_info);
+  if (c->dense_work) cudaFree(c->dense_work);
+  if (c->dense_info) cudaFree(c->dense_info);
   if (c->h_info) cudaFreeHost(c->h_info);
-  if (c->solver) cusolverDnDestroy(c->solver);
   for (cudaEvent_t ev : c->coarse_ev)
     if (ev) cudaEventDestroy(ev);
   if (c->stage) cudaFree(c->stage);
@@ -1173,8 +1164,9 @@ int drop_coarse(FemCtx* c) {
   c->cdev = CoarseDev{};
   c->coarse_have_inverse = false;
   c->tl_part = nullptr;
-  if (c->coarse_w) cudaFree(c->coarse_w);
-  c->coarse_w = nullptr;
+  if (c->dense_work) cudaFree(c->dense_work);
+  c->dense_work = nullptr;
+  c->dense_bytes = 0;
   c->coarse_built = false;
   c->coarse_valid = false;
   for (int k : {GRAPH_TWO_LEVEL, GRAPH_LEARNED}) {
@@ -1469,23 +1461,6 @@ int build_coarse(FemCtx* c) {
   if ((st = coarse_alloc(c, &cd.rc, nb * 64))) return st;
   // fused two-level step: per (cell, slice) restriction and ||r||^2 shares
   if ((st = coarse_alloc(c, &c->tl_part, (size_t)n_cells * cd.r_slices + step_chunks(Nn)))) return st;
-  if (!c->solver) {
-    if (cusolverDnCreate(&c->solver) != CUSOLVER_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cusolverDnCreate failed");
-  }
-  cusolverDnSetStream(c->solver, c->stream);
-  int lw1 = 0, lw2 = 0;
-  if (cusolverDnDpotrf_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, cd.n_dof, cd.Ac, cd.n_dof, &lw1) !=
-          CUSOLVER_STATUS_SUCCESS ||
-      cusolverDnDpotri_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, cd.n_dof, cd.Ac, cd.n_dof, &lw2) !=
-          CUSOLVER_STATUS_SUCCESS)
-    return set_err(c, FEM_ERR_CUDA, "cuSOLVER workspace query failed");
-  if (c->sol_work) cudaFree(c->sol_work);
-  c->sol_work = nullptr;
-  c->sol_lwork = std::max(lw1, lw2);
-  CK(cudaMalloc(reinterpret_cast<void**>(&c->sol_work), sizeof(double) * (size_t)std::max(c->sol_lwork, 1)));
-  if (!c->sol_info) CK(cudaMalloc(reinterpret_cast<void**>(&c->sol_info), sizeof(int)));
-  if (!c->h_info) CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_info), sizeof(int)));
   CK(cudaStreamSynchronize(c->stream));
   c->coarse_H = H;
   c->coarse_built = true;
@@ -1530,87 +1505,40 @@ int ensure_coarse(FemCtx* c) {
   CK(cudaEventRecord(em, c->stream));
   const int n = c->cdev.n_dof;
   c->cdev.Ac32 = nullptr;
-  if (c->coarse_inverse >= 2) {
-    // FP32: Cholesky, W = L^-1, W^T W, all in single precision (the inverse
-    // is rounded to BF16 or FP32 afterwards anyway)
-    if (!c->blas) {
-      if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return set_err(c, FEM_ERR_CUDA, "cublasCreate failed");
-    }
-    cublasSetStream(c->blas, c->stream);
-    if (!c->coarse_w) CK(cudaMalloc(reinterpret_cast<void**>(&c->coarse_w), sizeof(double) * (size_t)n * n));
-    float* a32 = reinterpret_cast<float*>(c->coarse_w);
-    float* w32 = a32 + (size_t)n * n;
-    launch_lower_to_f32(c->cdev.Ac, a32, n, c->stream);
-    launch_identity_f(w32, n, c->stream);
-    CKL();
-    int lws = 0;
-    if (cusolverDnSpotrf_bufferSize(c->solver, CUBLAS_FILL_MODE_LOWER, n, a32, n, &lws) != CUSOLVER_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cusolverDnSpotrf_bufferSize failed");
-    if ((lws + 1) / 2 > c->sol_lwork) {
-      CK(cudaStreamSynchronize(c->stream));
-      if (c->sol_work) cudaFree(c->sol_work);
-      c->sol_work = nullptr;
-      c->sol_lwork = (lws + 1) / 2;
-      CK(cudaMalloc(reinterpret_cast<void**>(&c->sol_work), sizeof(double) * (size_t)c->sol_lwork));
-    }
-    if (cusolverDnSpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, a32, n, reinterpret_cast<float*>(c->sol_work), lws,
-                         c->sol_info) != CUSOLVER_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cusolverDnSpotrf failed to launch");
-    CK(cudaMemcpyAsync(c->h_info, c->sol_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  // Cholesky, W = L^-1, Ac^-1 = W^T W on the project's dense tile kernels:
+  // FP32 arithmetic for the FP32 / TF32-class options (the inverse is
+  // rounded to FP32 or BF16 afterwards anyway), FP64 otherwise
+  const bool f64 = c->coarse_inverse < 2;
+  const size_t B = (size_t)dense_tile(f64), N = ((size_t)n + B - 1) / B * B;
+  const size_t work = 2 * N * N * (f64 ? sizeof(double) : sizeof(float)) + (f64 ? 0 : (size_t)n * n * sizeof(float));
+  if (work > c->dense_bytes) {
     CK(cudaStreamSynchronize(c->stream));
-    if (*c->h_info != 0) return keep_previous_coarse(c, *c->h_info);
-    const float one = 1.f, zero = 0.f;
-    // method 3: the triangular solve and the product on TF32 tensor cores
-    cublasSetMathMode(c->blas, c->coarse_inverse == 3 ? CUBLAS_TF32_TENSOR_OP_MATH : CUBLAS_DEFAULT_MATH);
-    if (cublasStrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n, &one,
-                    a32, n, w32, n) != CUBLAS_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cublasStrsm failed to launch");
-    if (cublasSsyrk(c->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &one, w32, n, &zero, a32, n) !=
-        CUBLAS_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cublasSsyrk failed to launch");
-    c->cdev.Ac32 = a32;
-    launch_coarse_symmetrize(c->cdev, c->stream);
-    ++c->n_launches;
-    CKL();
-    CK(cudaEventRecord(e1, c->stream));
-    CK(cudaEventSynchronize(e1));
-    float ms = 0.f, ms_asm = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventElapsedTime(&ms_asm, e0, em);
-    c->coarse_ms_last = ms;
-    c->coarse_ms_assembly = ms_asm;
-    ++c->n_coarse_assemblies;
-    c->coarse_have_inverse = true;
-    c->coarse_valid = true;
-    c->coarse_uses = 1;
-    c->coarse_base_ipd = -1;
-    return FEM_OK;
+    if (c->dense_work) cudaFree(c->dense_work);
+    c->dense_work = nullptr;
+    c->dense_bytes = 0;
+    CK(cudaMalloc(&c->dense_work, work));
+    c->dense_bytes = work;
   }
-  if (cusolverDnDpotrf(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
-                       c->sol_info) != CUSOLVER_STATUS_SUCCESS)
-    return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotrf failed to launch");
-  CK(cudaMemcpyAsync(c->h_info, c->sol_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (!c->dense_info) CK(cudaMalloc(reinterpret_cast<void**>(&c->dense_info), sizeof(int)));
+  if (!c->h_info) CK(cudaMallocHost(reinterpret_cast<void**>(&c->h_info), sizeof(int)));
+  int nl = 0;
+  cudaError_t de;
+  if (f64) {
+    double* A = static_cast<double*>(c->dense_work);
+    de = dense_spd_inverse_f64(c->cdev.Ac, n, A, A + N * N, c->dense_info, c->cdev.Ac, c->stream, &nl);
+  } else {
+    float* A = static_cast<float*>(c->dense_work);
+    float* out = A + 2 * N * N;
+    de = dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl);
+    c->cdev.Ac32 = out;
+  }
+  if (de != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "dense inverse: %s", cudaGetErrorString(de));
+  c->n_launches += nl;
+  CK(cudaMemcpyAsync(c->h_info, c->dense_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (*c->h_info != 0) return keep_previous_coarse(c, *c->h_info);
-  if (c->coarse_inverse == 1) {
-    // W = L^-1 (L W = I), then the lower triangle of W^T W = Ac^-1 into Ac
-    if (!c->blas) {
-      if (cublasCreate(&c->blas) != CUBLAS_STATUS_SUCCESS) return set_err(c, FEM_ERR_CUDA, "cublasCreate failed");
-    }
-    cublasSetStream(c->blas, c->stream);
-    if (!c->coarse_w) CK(cudaMalloc(reinterpret_cast<void**>(&c->coarse_w), sizeof(double) * (size_t)n * n));
-    launch_identity_d(c->coarse_w, n, c->stream);
-    CKL();
-    const double one = 1.0, zero = 0.0;
-    if (cublasDtrsm(c->blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, n, n, &one,
-                    c->cdev.Ac, n, c->coarse_w, n) != CUBLAS_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cublasDtrsm failed to launch");
-    if (cublasDsyrk(c->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, n, n, &one, c->coarse_w, n, &zero, c->cdev.Ac,
-                    n) != CUBLAS_STATUS_SUCCESS)
-      return set_err(c, FEM_ERR_CUDA, "cublasDsyrk failed to launch");
-  } else if (cusolverDnDpotri(c->solver, CUBLAS_FILL_MODE_LOWER, n, c->cdev.Ac, n, c->sol_work, c->sol_lwork,
-                              c->sol_info) != CUSOLVER_STATUS_SUCCESS) {
-    return set_err(c, FEM_ERR_CUDA, "cusolverDnDpotri failed to launch");
+  if (*c->h_info != 0) {
+    c->cdev.Ac32 = nullptr;
+    return keep_previous_coarse(c, *c->h_info);
   }
   launch_coarse_symmetrize(c->cdev, c->stream);
   ++c->n_launches;

@@ -1,0 +1,498 @@
+// Dense SPD inverse of the two-level preconditioner's coarse operator:
+// Cholesky A = L L^T, W = L^-1, A^-1 = W^T W (lower triangle), blocked in
+// B x B tiles (FP32: B = 128, FP64: B = 64) on a padded copy of A whose size
+// is a whole number of tiles (the padding is the identity, so L and W are
+// block diagonal there and no kernel handles a ragged edge).
+//
+//   factor, for k = 0 .. nt - 1:
+//     dense_diag_kernel    one CTA: L_kk = chol(A_kk) in shared memory and its
+//                          inverse W_kk = L_kk^-1 (a pivot <= 0 records its
+//                          column in *info and the factorisation continues
+//                          with a unit pivot, so every launch completes)
+//     dense_panel_kernel   L_ik = A_ik W_kk^T, i > k
+//     dense_update_kernel  A_ij -= L_ik L_jk^T, k < j <= i
+//   invert, right-looking, for k = 0 .. nt - 1:
+//     dense_wfin_kernel    W_kj = W_kk R_kj, j < k (R: the accumulated row)
+//     dense_wupd_kernel    R_ij -= L_ik W_kj, i > k, j <= k
+//   product:
+//     dense_syrk_kernel    (A^-1)_ij = sum_{l>=i} W_li^T W_lj, i >= j
+//
+// The tile products run on a SIMT micro-kernel: 256 threads, each an
+// (B/16) x (B/16) block of the output tile, operands staged in shared memory
+// in chunks of kKC of the inner dimension.  These replace the cuSOLVER
+// potrf / potri and cuBLAS trsm / syrk calls the coarse set-up made before.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "../../include/femb200.h"
+#include "fem_internal.h"
+
+namespace femb200 {
+
+template <typename T>
+struct DenseCfg;
+template <>
+struct DenseCfg<float> {
+  static constexpr int B = 128, TM = 8;
+};
+template <>
+struct DenseCfg<double> {
+  static constexpr int B = 64, TM = 4;
+};
+constexpr int kDenseThreads = 256;
+constexpr int kKC = 16;  // inner-dimension chunk staged in shared memory
+
+// Four consecutive FP32 (or two FP64) values moved as one 16-byte access.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using V = float4;
+  static constexpr int W = 4;
+  __device__ static void unpack(const V& v, float* o) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+  __device__ static V pack(const float* o) { return make_float4(o[0], o[1], o[2], o[3]); }
+};
+template <>
+struct Vec16<double> {
+  using V = double2;
+  static constexpr int W = 2;
+  __device__ static void unpack(const V& v, double* o) { o[0] = v.x; o[1] = v.y; }
+  __device__ static V pack(const double* o) { return make_double2(o[0], o[1]); }
+};
+
+template <typename T>
+constexpr int dense_ld() {  // shared row stride of a staged operand chunk
+  return DenseCfg<T>::B + 4;
+}
+
+// Stages rows k0 .. k0 + kKC - 1 of the inner dimension of one B-row
+// operand into s[k][m]: element (m, k) is p[k * ld + m] (m contiguous, a
+// column-major tile) or, with KC, p[m * ld + k] (k contiguous).  16-byte
+// global loads along the contiguous index (all operand tiles start on a
+// multiple of B elements and ld is a multiple of B, so they are aligned).
+template <typename T, bool KC>
+__device__ __forceinline__ void dense_stage(const T* __restrict__ p, int ld, int k0, T* s) {
+  using VT = Vec16<T>;
+  constexpr int B = DenseCfg<T>::B, W = VT::W;
+  constexpr int LD = dense_ld<T>();
+  constexpr int NV = B * kKC / W;  // vectors per chunk
+#pragma unroll
+  for (int q = threadIdx.x; q < NV; q += kDenseThreads) {
+    T v[W];
+    if (KC) {
+      const int m = q / (kKC / W), k = (q % (kKC / W)) * W;
+      VT::unpack(__ldcg(reinterpret_cast<const typename VT::V*>(p + (size_t)m * ld + k0 + k)), v);
+#pragma unroll
+      for (int w = 0; w < W; ++w) s[(k + w) * LD + m] = v[w];
+    } else {
+      const int k = q / (B / W), m = (q % (B / W)) * W;
+      *reinterpret_cast<typename VT::V*>(s + k * LD + m) =
+          __ldcg(reinterpret_cast<const typename VT::V*>(p + (size_t)(k0 + k) * ld + m));
+    }
+  }
+}
+
+// acc(r, c) += sum_k A(r, k) Bt(c, k) over one tile of the inner dimension
+// (k < B); A and Bt are B-row operands (see dense_stage).  Thread t owns the
+// rows ty * H + [0, H) and B/2 + ty * H + [0, H), ty = t % 16, and the same
+// columns with tx = t / 16 (H = TM / 2), so the lanes of a warp cover
+// consecutive rows: coalesced stores of a column-major tile.
+template <typename T, bool AK, bool BK>
+__device__ __forceinline__ void dense_mma(T (&acc)[DenseCfg<T>::TM][DenseCfg<T>::TM], const T* A, int lda,
+                                          const T* Bt, int ldb, T* sA, T* sB) {
+  using VT = Vec16<T>;
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM, H = TM / 2, LD = dense_ld<T>();
+  static_assert(H == VT::W, "a thread's half-row block is one 16-byte vector");
+  const int ty = threadIdx.x & 15, tx = threadIdx.x >> 4;
+  for (int k0 = 0; k0 < B; k0 += kKC) {
+    __syncthreads();
+    dense_stage<T, AK>(A, lda, k0, sA);
+    dense_stage<T, BK>(Bt, ldb, k0, sB);
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kKC; ++k) {
+      T a[TM], b[TM];
+      VT::unpack(*reinterpret_cast<const typename VT::V*>(sA + k * LD + ty * H), a);
+      VT::unpack(*reinterpret_cast<const typename VT::V*>(sA + k * LD + B / 2 + ty * H), a + H);
+      VT::unpack(*reinterpret_cast<const typename VT::V*>(sB + k * LD + tx * H), b);
+      VT::unpack(*reinterpret_cast<const typename VT::V*>(sB + k * LD + B / 2 + tx * H), b + H);
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TM; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+}
+
+// tile-local row / column of accumulator entry i
+template <typename T>
+__device__ __forceinline__ int dense_rc(int t16, int i) {
+  constexpr int B = DenseCfg<T>::B, H = DenseCfg<T>::TM / 2;
+  return i < H ? t16 * H + i : B / 2 + t16 * H + (i - H);
+}
+
+// Writes the thread's accumulator block to a column-major tile (ld), one
+// 16-byte store per half column: OP 0 stores acc, 1 subtracts it from the
+// tile, 2 stores -acc.
+template <typename T, int OP>
+__device__ __forceinline__ void dense_store(T* tile, int ld, const T (&acc)[DenseCfg<T>::TM][DenseCfg<T>::TM]) {
+  using VT = Vec16<T>;
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM, H = TM / 2;
+  const int ty = threadIdx.x & 15, tx = threadIdx.x >> 4;
+#pragma unroll
+  for (int b = 0; b < TM; ++b) {
+    const int col = b < H ? tx * H + b : B / 2 + tx * H + (b - H);
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      typename VT::V* q = reinterpret_cast<typename VT::V*>(tile + (size_t)col * ld + half * (B / 2) + ty * H);
+      T v[H];
+#pragma unroll
+      for (int i = 0; i < H; ++i) v[i] = acc[half * H + i][b];
+      if (OP == 1) {
+        T o[H];
+        VT::unpack(*q, o);
+#pragma unroll
+        for (int i = 0; i < H; ++i) v[i] = o[i] - v[i];
+      } else if (OP == 2) {
+#pragma unroll
+        for (int i = 0; i < H; ++i) v[i] = -v[i];
+      }
+      *q = VT::pack(v);
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void dense_zero(T (&acc)[DenseCfg<T>::TM][DenseCfg<T>::TM]) {
+#pragma unroll
+  for (int i = 0; i < DenseCfg<T>::TM; ++i)
+#pragma unroll
+    for (int j = 0; j < DenseCfg<T>::TM; ++j) acc[i][j] = T(0);
+}
+
+// Lower-triangle tile t -> (I, J), J <= I, in row order.
+__device__ __forceinline__ void dense_tri(int t, int& I, int& J) {
+  int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+  while ((i + 1) * (i + 2) / 2 <= t) ++i;
+  while (i * (i + 1) / 2 > t) --i;
+  I = i;
+  J = t - i * (i + 1) / 2;
+}
+
+// A = the padded copy of src's lower triangle (identity beyond n); W = 0
+template <typename T>
+__global__ void __launch_bounds__(256) dense_pad_kernel(const double* __restrict__ src, int n, T* A, T* W, int N) {
+  const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (size_t)N * N) return;
+  const int c = (int)(q / N), r = (int)(q % N);
+  T v = T(0);
+  if (r < n && c < n) {
+    if (r >= c) v = (T)src[(size_t)c * n + r];
+  } else if (r == c) {
+    v = T(1);
+  }
+  A[q] = v;
+  W[q] = T(0);
+}
+
+// Diagonal tile k: L_kk = chol(A_kk) and X = L_kk^-1 in shared memory
+// (L[c * S + r] = L(r, c)), both blocked in 32-wide panels so the sequential
+// parts run inside one warp and the CTA synchronises a few times per panel:
+//   Cholesky, panel p (columns j0 .. j0 + 31):
+//     warp 0 factors the 32 x 32 diagonal block (lane = row),
+//     each thread solves one row below it against that block's transpose,
+//     all threads apply the rank-32 update to the trailing lower triangle;
+//   inverse: each warp inverts one 32 x 32 diagonal block (lane = column),
+//   then block row k is finished (X_kq = X_kk R_kq, q < k) and subtracted
+//   from the rows below (R_iq -= L_ik X_kq), for k = 0, 1, ...
+template <typename T>
+__global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, int N, int k, int* info) {
+  constexpr int B = DenseCfg<T>::B, S = B + 1, P = 32, NP = B / P;
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  T* L = reinterpret_cast<T*>(s_raw);  // L[c * S + r]
+  T* X = L + B * S;                     // X[c * S + r] = (L^-1)(r, c)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const size_t off = (size_t)k * B * N + (size_t)k * B;
+  for (int q = tid; q < B * B; q += kDenseThreads) {
+    const int c = q / B, r = q % B;
+    L[c * S + r] = r >= c ? A[off + (size_t)c * N + r] : T(0);
+    X[c * S + r] = T(0);
+  }
+  __syncthreads();
+  const int tx = tid & 15, ty = tid >> 4;
+  for (int p = 0; p < NP; ++p) {
+    const int j0 = p * P;
+    if (warp == 0) {
+      // 32 x 32 diagonal block, lane = row j0 + lane
+      const int r = j0 + lane;
+      for (int j = 0; j < P; ++j) {
+        const int jj = j0 + j;
+        T d = L[jj * S + jj];
+        if (!(d > T(0))) {
+          if (lane == 0) atomicCAS(info, 0, k * B + jj + 1);
+          d = T(1);
+        }
+        d = sqrt(d);
+        __syncwarp();
+        if (lane == j) L[jj * S + jj] = d;
+        if (lane > j) L[jj * S + r] /= d;
+        __syncwarp();
+        const T lr = lane > j ? L[jj * S + r] : T(0);
+        for (int c = j + 1; c <= lane; ++c) L[(j0 + c) * S + r] -= lr * L[jj * S + j0 + c];
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // rows below the block: x L_pp^T = a, one row per thread
+    for (int r = j0 + P + tid; r < B; r += kDenseThreads) {
+      for (int j = 0; j < P; ++j) {
+        T acc = L[(j0 + j) * S + r];
+        for (int l = 0; l < j; ++l) acc -= L[(j0 + l) * S + r] * L[(j0 + l) * S + j0 + j];
+        L[(j0 + j) * S + r] = acc / L[(j0 + j) * S + j0 + j];
+      }
+    }
+    __syncthreads();
+    // trailing lower triangle: columns c >= j0 + P, rows r >= c
+    for (int c = j0 + P + tx; c < B; c += 16) {
+      for (int r = c + ty; r < B; r += 16) {
+        T acc = T(0);
+#pragma unroll 8
+        for (int l = j0; l < j0 + P; ++l) acc += L[l * S + r] * L[l * S + c];
+        L[c * S + r] -= acc;
+      }
+    }
+    __syncthreads();
+  }
+  // inverse of each 32 x 32 diagonal block: warp p, lane = column
+  if (warp < NP) {
+    const int j0 = warp * P, c = j0 + lane;
+    X[c * S + c] = T(1) / L[c * S + c];
+    for (int r = c + 1; r < j0 + P; ++r) {
+      T acc = T(0);
+      for (int l = c; l < r; ++l) acc += L[l * S + r] * X[c * S + l];
+      X[c * S + r] = -acc / L[r * S + r];
+    }
+  }
+  __syncthreads();
+  // block rows: finish row k (X_kq = X_kk R_kq, q < k; R_kq accumulated in
+  // place), then R_iq -= L_ik X_kq for i > k, q <= k
+  for (int kb = 0; kb < NP; ++kb) {
+    const int k0 = kb * P;
+    if (kb > 0) {
+      // kb * P * P entries, at most 3 * 1024 / 256 = 12 per thread
+      T v[(NP - 1) * P * P / kDenseThreads + 1];
+      int nv = 0;
+      for (int q = tid; q < kb * P * P; q += kDenseThreads, ++nv) {
+        const int c = q / P, r = k0 + q % P;  // column c < k0, row r in block kb
+        T acc = T(0);
+        for (int l = 0; l < P; ++l) acc += X[(k0 + l) * S + r] * X[c * S + k0 + l];
+        v[nv] = acc;
+      }
+      __syncthreads();
+      nv = 0;
+      for (int q = tid; q < kb * P * P; q += kDenseThreads, ++nv) X[(q / P) * S + k0 + q % P] = v[nv];
+      __syncthreads();
+    }
+    // rows below block kb, columns up to the end of block kb
+    const int rows = B - k0 - P, cols = k0 + P;
+    for (int q = tid; q < rows * cols; q += kDenseThreads) {
+      const int c = q / rows, r = k0 + P + q % rows;
+      T acc = T(0);
+      for (int l = (c > k0 ? c : k0); l < k0 + P; ++l) acc += L[l * S + r] * X[c * S + l];
+      X[c * S + r] -= acc;
+    }
+    __syncthreads();
+  }
+  for (int q = tid; q < B * B; q += kDenseThreads) {
+    const int c = q / B, r = q % B;
+    A[off + (size_t)c * N + r] = L[c * S + r];
+    W[off + (size_t)c * N + r] = X[c * S + r];
+  }
+}
+
+// L_ik = A_ik W_kk^T for i = k + 1 + blockIdx.x
+template <typename T>
+__global__ void __launch_bounds__(kDenseThreads) dense_panel_kernel(T* A, const T* W, int N, int k) {
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM;
+  __shared__ __align__(16) T sA[kKC * dense_ld<T>()];
+  __shared__ __align__(16) T sB[kKC * dense_ld<T>()];
+  const int i = k + 1 + (int)blockIdx.x;
+  T* Aik = A + (size_t)k * B * N + (size_t)i * B;
+  const T* Wkk = W + (size_t)k * B * N + (size_t)k * B;
+  T acc[TM][TM];
+  dense_zero<T>(acc);
+  // (A_ik W_kk^T)(r, c) = sum_q A_ik(r, q) W_kk(c, q): both operands m-contiguous
+  dense_mma<T, false, false>(acc, Aik, N, Wkk, N, sA, sB);
+  __syncthreads();
+  dense_store<T, 0>(Aik, N, acc);
+}
+
+// A_ij -= L_ik L_jk^T over the lower tiles k < j <= i (blockIdx.x in row order)
+template <typename T>
+__global__ void __launch_bounds__(kDenseThreads) dense_update_kernel(T* A, int N, int k) {
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM;
+  __shared__ __align__(16) T sA[kKC * dense_ld<T>()];
+  __shared__ __align__(16) T sB[kKC * dense_ld<T>()];
+  int I, J;
+  dense_tri((int)blockIdx.x, I, J);
+  const int i = k + 1 + I, j = k + 1 + J;
+  const T* Lik = A + (size_t)k * B * N + (size_t)i * B;
+  const T* Ljk = A + (size_t)k * B * N + (size_t)j * B;
+  T acc[TM][TM];
+  dense_zero<T>(acc);
+  dense_mma<T, false, false>(acc, Lik, N, Ljk, N, sA, sB);
+  dense_store<T, 1>(A + (size_t)j * B * N + (size_t)i * B, N, acc);
+}
+
+// W = L^-1, right-looking over tile rows.  W's lower tiles below the
+// diagonal start at 0 and accumulate R_ij = -sum_{l<i} L_il W_lj; step k
+// finishes tile row k (dense_wfin_kernel: W_kj = W_kk R_kj, j < k) and
+// subtracts it from the rows below (dense_wupd_kernel: R_ij -= L_ik W_kj,
+// i > k, j <= k), one tile product per CTA.
+template <typename T>
+__global__ void __launch_bounds__(kDenseThreads) dense_wfin_kernel(T* W, int N, int k) {
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM;
+  __shared__ __align__(16) T sA[kKC * dense_ld<T>()];
+  __shared__ __align__(16) T sB[kKC * dense_ld<T>()];
+  const int j = (int)blockIdx.x;
+  T* Wkj = W + (size_t)j * B * N + (size_t)k * B;
+  T acc[TM][TM];
+  dense_zero<T>(acc);
+  // (W_kk R_kj)(r, c) = sum_q W_kk(r, q) R_kj(q, c)
+  dense_mma<T, false, true>(acc, W + (size_t)k * B * N + (size_t)k * B, N, Wkj, N, sA, sB);
+  __syncthreads();
+  dense_store<T, 0>(Wkj, N, acc);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kDenseThreads) dense_wupd_kernel(const T* A, T* W, int N, int k) {
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM;
+  __shared__ __align__(16) T sA[kKC * dense_ld<T>()];
+  __shared__ __align__(16) T sB[kKC * dense_ld<T>()];
+  const int j = (int)blockIdx.x % (k + 1), i = k + 1 + (int)blockIdx.x / (k + 1);
+  T acc[TM][TM];
+  dense_zero<T>(acc);
+  // (L_ik W_kj)(r, c) = sum_q L_ik(r, q) W_kj(q, c)
+  dense_mma<T, false, true>(acc, A + (size_t)k * B * N + (size_t)i * B, N, W + (size_t)j * B * N + (size_t)k * B, N,
+                            sA, sB);
+  dense_store<T, 1>(W + (size_t)j * B * N + (size_t)i * B, N, acc);
+}
+
+// (A^-1)_ij = sum_{l=i}^{nt-1} W_li^T W_lj for the lower tiles i >= j; out
+// holds the n x n result column-major (entries beyond n are the padding's).
+template <typename T, typename TO>
+__global__ void __launch_bounds__(kDenseThreads) dense_syrk_kernel(const T* W, int N, int nt, TO* out, int n) {
+  constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM;
+  __shared__ __align__(16) T sA[kKC * dense_ld<T>()];
+  __shared__ __align__(16) T sB[kKC * dense_ld<T>()];
+  int i, j;
+  dense_tri((int)blockIdx.x, i, j);
+  T acc[TM][TM];
+  dense_zero<T>(acc);
+  // X(r, c) = sum_l sum_q W_li(q, r) W_lj(q, c): both operands k-contiguous
+  for (int l = i; l < nt; ++l)
+    dense_mma<T, true, true>(acc, W + (size_t)i * B * N + (size_t)l * B, N, W + (size_t)j * B * N + (size_t)l * B, N,
+                             sA, sB);
+  const int ty = threadIdx.x & 15, tx = threadIdx.x >> 4;
+#pragma unroll
+  for (int b = 0; b < TM; ++b)
+#pragma unroll
+    for (int a = 0; a < TM; ++a) {
+      const int r = i * B + dense_rc<T>(ty, a), c = j * B + dense_rc<T>(tx, b);
+      if (r < n && c < n) out[(size_t)c * n + r] = (TO)acc[a][b];
+    }
+}
+
+static inline int dense_nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
+
+int dense_tile(bool fp64) { return fp64 ? DenseCfg<double>::B : DenseCfg<float>::B; }
+
+template <typename T, typename TO>
+static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* info, TO* out, cudaStream_t s,
+                                   int* launches) {
+  constexpr int B = DenseCfg<T>::B;
+  const int nt = (n + B - 1) / B, N = nt * B;
+  const size_t diag_smem = 2 * sizeof(T) * (size_t)B * (B + 1);
+  cudaError_t e = cudaFuncSetAttribute(dense_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)diag_smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(info, 0, sizeof(int), s);
+  if (e != cudaSuccess) return e;
+  int nl = 0;
+  dense_pad_kernel<T><<<dense_nblk((size_t)N * N, 256), 256, 0, s>>>(Ac, n, A, W, N);
+  ++nl;
+  for (int k = 0; k < nt; ++k) {
+    dense_diag_kernel<T><<<1, kDenseThreads, diag_smem, s>>>(A, W, N, k, info);
+    ++nl;
+    const int m = nt - k - 1;
+    if (m > 0) {
+      dense_panel_kernel<T><<<m, kDenseThreads, 0, s>>>(A, W, N, k);
+      dense_update_kernel<T><<<m * (m + 1) / 2, kDenseThreads, 0, s>>>(A, N, k);
+      nl += 2;
+    }
+  }
+  for (int kk = 0; kk < nt; ++kk) {
+    if (kk > 0) {
+      dense_wfin_kernel<T><<<kk, kDenseThreads, 0, s>>>(W, N, kk);
+      ++nl;
+    }
+    if (kk + 1 < nt) {
+      dense_wupd_kernel<T><<<(nt - kk - 1) * (kk + 1), kDenseThreads, 0, s>>>(A, W, N, kk);
+      ++nl;
+    }
+  }
+  dense_syrk_kernel<T, TO><<<nt * (nt + 1) / 2, kDenseThreads, 0, s>>>(W, N, nt, out, n);
+  ++nl;
+  if (launches) *launches += nl;
+  return cudaGetLastError();
+}
+
+cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
+                                  cudaStream_t s, int* launches) {
+  return dense_inverse_t<float, float>(Ac, n, A, W, info, out, s, launches);
+}
+
+cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
+                                  cudaStream_t s, int* launches) {
+  return dense_inverse_t<double, double>(Ac, n, A, W, info, out, s, launches);
+}
+
+}  // namespace femb200
+
+using namespace femb200;
+
+extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream) {
+  if (!A || !out) return set_global_error(FEM_ERR_INVALID, "null matrix");
+  if (n < 1 || n > 32768) return set_global_error(FEM_ERR_INVALID, "n = %d not in [1, 32768]", n);
+  if (precision != 32 && precision != 64)
+    return set_global_error(FEM_ERR_INVALID, "precision %d: 32 or 64", precision);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const bool f64 = precision == 64;
+  const int B = dense_tile(f64);
+  const size_t N = (size_t)((n + B - 1) / B) * B;
+  const size_t elem = f64 ? sizeof(double) : sizeof(float);
+  void *wa = nullptr, *ww = nullptr;
+  int* info = nullptr;
+  if (cudaMalloc(&wa, N * N * elem) != cudaSuccess || cudaMalloc(&ww, N * N * elem) != cudaSuccess ||
+      cudaMalloc(&info, sizeof(int)) != cudaSuccess) {
+    cudaFree(wa);
+    cudaFree(ww);
+    return set_global_error(FEM_ERR_CUDA, "cudaMalloc of the dense work space (%zu bytes) failed", 2 * N * N * elem);
+  }
+  cudaError_t e = f64 ? dense_inverse_t<double, double>(A, n, static_cast<double*>(wa), static_cast<double*>(ww),
+                                                          info, out, s, nullptr)
+                      : dense_inverse_t<float, double>(A, n, static_cast<float*>(wa), static_cast<float*>(ww), info,
+                                                         out, s, nullptr);
+  int h_info = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(wa);
+  cudaFree(ww);
+  cudaFree(info);
+  if (e != cudaSuccess) return set_global_error(FEM_ERR_CUDA, "dense inverse: %s", cudaGetErrorString(e));
+  if (h_info != 0)
+    return set_global_error(FEM_ERR_NAN, "matrix is not positive definite (pivot %d is not positive)", h_info);
+  return FEM_OK;
+}

@@ -342,6 +342,16 @@ inline void raise_smem_limit_k(K kernel) {
   raise_smem_limit(reinterpret_cast<const void*>(kernel));
 }
 
+// Dense SPD inverse (fem_dense.cu): the lower triangle of Ac^-1 (Ac: n x n
+// FP64 column-major, lower triangle read) into out (n x n column-major).  A
+// and W are work matrices of N x N, N = n rounded up to dense_tile(fp64);
+// *info receives the first non-positive pivot (1-based), 0 if none.
+int dense_tile(bool fp64);
+cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
+                                  cudaStream_t s, int* launches);
+cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
+                                  cudaStream_t s, int* launches);
+
 // Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
 // returns `code`.
 int set_global_error(int code, const char* fmt, ...);
@@ -373,12 +383,6 @@ void launch_coarse_cells_hex(const CoarseArgs& a, int model, cudaStream_t s);
 void launch_coarse_node_lat(const MeshDev& m, const CoarseDev& c, float4* out, cudaStream_t s);
 // fills node_corners from node_cell and cell_corner
 void launch_coarse_node_corners(const MeshDev& m, const CoarseDev& c, uint4* out, cudaStream_t s);
-// w = the n x n identity (FP64, column-major)
-void launch_identity_d(double* w, int n, cudaStream_t s);
-// w = the n x n identity (FP32, column-major)
-void launch_identity_f(float* w, int n, cudaStream_t s);
-// out = the lower triangle of the FP64 column-major a, rounded to FP32
-void launch_lower_to_f32(const double* a, float* out, int n, cudaStream_t s);
 // kernels one coarse product launches (1 FP32, 2 packed BF16)
 int coarse_product_kernels(const CoarseDev& c);
 void launch_coarse_symmetrize(const CoarseDev& c, cudaStream_t s);

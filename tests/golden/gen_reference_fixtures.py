@@ -8,7 +8,9 @@ in this container even though the Taichi kernels around them do not:
   ``assemble_geometric_stiffness`` (``assembly.py:20-287``), the tangent the
   reference's Newton solves with;
 - ``backend/preprocessing/voxel_to_hex.py`` — ``voxels_to_hex_mesh``
-  (``voxel_to_hex.py:11-68``), the labelmap-to-HEX8 mesher.
+  (``voxel_to_hex.py:11-68``), the labelmap-to-HEX8 mesher;
+- ``backend/fea/framework/contact.py`` — ``NodeNodeContact`` (``:43-273``):
+  nearest-pair detection, penalty forces, tied pairs and tied forces.
 
 Each module is loaded by file path (``importlib.util.spec_from_file_location``),
 which skips the package ``__init__`` files that import Taichi.  The inputs
@@ -19,8 +21,8 @@ diagonal, the number of stored entries after duplicates are summed, the
 number of entries above 1e-10 of the largest, and the Frobenius norm) to keep the fixture small; voxel meshes are stored whole.
 
 Run ``python tests/golden/gen_reference_fixtures.py [reference_root]``
-(default ``/root/reference``).  It writes ``ref_assembly.npz`` and
-``ref_voxel_to_hex.npz`` next to this file.
+(default ``/root/reference``).  It writes ``ref_assembly.npz``,
+``ref_voxel_to_hex.npz`` and ``ref_contact.npz`` next to this file.
 """
 from __future__ import annotations
 
@@ -41,6 +43,7 @@ from simul_b200 import meshgen  # noqa: E402
 DEFAULT_REFERENCE = "/root/reference"
 ASSEMBLY = "backend/fea/fem/solver/assembly.py"
 VOXEL_TO_HEX = "backend/preprocessing/voxel_to_hex.py"
+CONTACT = "backend/fea/framework/contact.py"
 N_PROBES = 4
 
 
@@ -148,6 +151,41 @@ def voxel_cases():
     return cases
 
 
+# ───────────────────────── contact cases ─────────────────────────
+
+def contact_cases():
+    """name -> (pos_a, pos_b, surface_a, surface_b, gap, penalty): seeded
+    point sets (current coordinates) with a band of near pairs, and the
+    two-block interface of the staggered-solve test."""
+    rng = np.random.default_rng(400)
+    cases = {}
+    pa = rng.uniform(0.0, 1.0, (300, 3))
+    pb = pa[rng.permutation(300)[:200]] + rng.normal(0.0, 0.05, (200, 3))
+    cases["cloud"] = (pa, pb, np.arange(0, 300, 2), np.arange(1, 200), 0.08, 37.5)
+    Xa, _ = meshgen.structured_tets(4, 4, 4, L=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 1.05))
+    Xb, _ = meshgen.structured_tets(4, 4, 4, L=(1.0, 1.0, 1.0), origin=(0.0, 0.0, 0.0))
+    Xa = Xa + rng.normal(0.0, 0.003, Xa.shape)
+    sa = np.where(np.isclose(Xa[:, 2], Xa[:, 2].min(), atol=0.02))[0]
+    sb = np.where(np.isclose(Xb[:, 2], Xb[:, 2].max()))[0]
+    cases["blocks"] = (Xa, Xb, sa, sb, 0.1, 2.0)
+    return cases
+
+
+def reference_contact(con, case) -> dict:
+    pa, pb, sa, sb, gap, pen = case
+    algo = con.NodeNodeContact()
+    pairs, gaps = algo.detect(pa, pb, sa, sb, gap)
+    fa, fb = algo.compute_forces(pa, pb, pairs, gaps, pen, gap)
+    tp, off = algo.detect_tied_pairs(pa, pb, sa, sb, gap)
+    # the tied springs after a seeded motion of both sets
+    rng = np.random.default_rng(401)
+    qa = pa + rng.normal(0.0, 0.01, pa.shape)
+    qb = pb + rng.normal(0.0, 0.01, pb.shape)
+    ta, tb = algo.compute_tied_forces(qa, qb, tp, off, pen)
+    return {"pairs": pairs, "gaps": gaps, "fa": fa, "fb": fb, "tied_pairs": tp, "tied_offsets": off,
+            "tied_fa": ta, "tied_fb": tb, "qa": qa, "qb": qb}
+
+
 def main(reference_root: str = DEFAULT_REFERENCE):
     asm = load_module(reference_root, ASSEMBLY, "ref_assembly")
     v2h = load_module(reference_root, VOXEL_TO_HEX, "ref_voxel_to_hex")
@@ -162,7 +200,14 @@ def main(reference_root: str = DEFAULT_REFERENCE):
         vox[f"{name}__nodes"] = nodes
         vox[f"{name}__elements"] = elems
     np.savez_compressed(HERE / "ref_voxel_to_hex.npz", **vox)
-    print("ref_assembly.npz:", len(out), "arrays; ref_voxel_to_hex.npz:", len(vox), "arrays")
+    con = load_module(reference_root, CONTACT, "ref_contact")
+    cont = {}
+    for name, case in contact_cases().items():
+        for k, val in reference_contact(con, case).items():
+            cont[f"{name}__{k}"] = val
+    np.savez_compressed(HERE / "ref_contact.npz", **cont)
+    print("ref_assembly.npz:", len(out), "arrays; ref_voxel_to_hex.npz:", len(vox), "arrays; ref_contact.npz:",
+          len(cont), "arrays")
 
 
 if __name__ == "__main__":

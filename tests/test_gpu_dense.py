@@ -1,0 +1,64 @@
+"""The dense SPD inverse kernels of the coarse operator (fem_dense.cu)
+against numpy's inverse, on seeded SPD matrices of ragged and whole-tile
+sizes (tiles are 64 in FP64, 128 in FP32), plus a matrix that is not
+positive definite."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from simul_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _spd(n, seed, cond=1e3):
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    ev = np.geomspace(1.0, cond, n)
+    return (Q * ev) @ Q.T
+
+
+def _run(A, precision, cuda):
+    n = A.shape[0]
+    dA = torch.as_tensor(np.asfortranarray(A).ravel(order="F"), dtype=torch.float64, device=cuda)
+    out = torch.full((n * n,), float("nan"), dtype=torch.float64, device=cuda)
+    rc = _lib.load().fem_dense_spd_inverse(C.c_void_p(dA.data_ptr()), n, precision, C.c_void_p(out.data_ptr()), None)
+    return rc, out.cpu().numpy().reshape(n, n, order="F")
+
+
+@pytest.mark.parametrize("n", [1, 37, 64, 127, 128, 200, 513])
+@pytest.mark.parametrize("precision,tol", [(64, 1e-11), (32, 2e-4)])
+def test_dense_spd_inverse_matches_numpy(cuda, n, precision, tol):
+    A = _spd(n, seed=n)
+    rc, X = _run(A, precision, cuda)
+    assert rc == 0, _lib.last_error()
+    ref = np.linalg.inv(A)
+    lo = np.tril(np.ones((n, n), dtype=bool))
+    err = np.abs(X[lo] - ref[lo]).max() / np.abs(ref).max()
+    assert err < tol, err
+    # above the diagonal only the diagonal tiles are written (with the
+    # symmetric values); everything else is left as it was
+    up = ~lo & ~np.isnan(X)
+    if up.any():
+        assert np.abs(X[up] - ref[up]).max() / np.abs(ref).max() < tol
+
+
+def test_dense_spd_inverse_rejects_indefinite(cuda):
+    A = _spd(150, seed=5)
+    A[70, 70] = -5.0
+    rc, _ = _run(A, 64, cuda)
+    assert rc == _lib.FEM_ERR_NAN
+    assert "not positive definite" in _lib.last_error()
+    rc, _ = _run(A, 32, cuda)
+    assert rc == _lib.FEM_ERR_NAN
+
+
+def test_dense_spd_inverse_validates_arguments(cuda):
+    assert _lib.load().fem_dense_spd_inverse(None, 4, 64, None, None) == _lib.FEM_ERR_INVALID
+    A = torch.eye(4, dtype=torch.float64, device=cuda)
+    out = torch.empty_like(A)
+    assert _lib.load().fem_dense_spd_inverse(C.c_void_p(A.data_ptr()), 4, 16, C.c_void_p(out.data_ptr()),
+                                             None) == _lib.FEM_ERR_INVALID
+    assert "precision" in _lib.last_error()

@@ -413,12 +413,15 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out);
  * issued on `stream`, a cudaStream_t or NULL).  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc (an application whose
  * allocator owns all device memory, a loop that forbids allocation after
- * start-up): it is the deterministic fixed-order reduction the solver uses for
- * its dots and norms, with its partial sums in a static 16 KB device array
- * instead of context scratch.  n <= 8,388,608 (larger n: FEM_ERR_INVALID).
+ * start-up): the same deterministic scheme as the solver's dots and norms
+ * (fixed-order per-block partials, the last block adds them in index order),
+ * with its own 4096-element tiles, so it is not bitwise equal to the solver's
+ * norms; its partial sums live in a static 16 KB device array instead of
+ * context scratch.  n <= 8,388,608 (larger n: FEM_ERR_INVALID).
  * The first call on a device looks up that array's address there; make it
- * before any stream capture.  Calls share the array: calls that overlap on the
- * GPU race and must be serialised.  Errors: fem_last_error(NULL). */
+ * before any stream capture.  The address is kept until the process exits: no
+ * calls after a cudaDeviceReset.  Calls share the array: calls that overlap on
+ * the GPU race and must be serialised.  Errors: fem_last_error(NULL). */
 int fem_dot_f64_noalloc(const double* a, const double* b, int64_t n, double* result, void* stream);
 
 /* ---- J2 history (j2_plasticity.py:103-123, 513-520) ---- */

@@ -164,6 +164,7 @@ __global__ void __launch_bounds__(kTile) mpnn_encode_kernel(const __grid_constan
   } else if (lane == 0) {
     atomicExch(m.err, 1);
   }
+  umma::drain_mma(&mbar, 0, ok, kPolls);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 64);
@@ -301,6 +302,7 @@ __global__ void __launch_bounds__(2 * kTile) mpnn_layer_kernel(const __grid_cons
       sO[row][2] = o[2];
     }
   }
+  umma::drain_mma(&mbar, 0, ok, kPolls);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 64);
@@ -528,6 +530,7 @@ __global__ void __launch_bounds__(2 * kTile) mpnn_layer_bwd_kernel(const __grid_
     for (int i = 0; i < kTile; ++i) acc += sGf[i * kHid + tid];
     part[kMpnnOffB(layer) + tid] = acc;
   }
+  umma::drain_mma(&mbar, 0, ok, kPolls);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, 256);

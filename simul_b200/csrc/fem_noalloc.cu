@@ -19,6 +19,13 @@
 //    loads the library until the process exits;
 //  - the first call on a device looks up the array's device address there
 //    (cudaGetSymbolAddress); make that first call before any stream capture;
+//    the address is kept for the life of the process, so a cudaDeviceReset
+//    (which unloads the module, and the array with it) must not be followed
+//    by further calls;
+//  - the reduction follows the solver's scheme (fixed-order per-block
+//    partials, the last block adds them in index order) with its own
+//    4096-element tiles, so its result agrees with the solver's norms to
+//    rounding, not bit for bit;
 //  - every call shares the array and it keeps the last call's contents; the
 //    counter is cleared at the start of each call, the partials are
 //    overwritten.  Calls that overlap on the GPU (two streams, or two host
@@ -108,9 +115,13 @@ extern "C" int fem_dot_f64_noalloc(const double* a, const double* b, int64_t n, 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+  if (e != cudaSuccess)
     return set_global_error(FEM_ERR_CUDA, "fem_dot_f64_noalloc: cudaGetDevice failed (%s)",
                             cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return set_global_error(FEM_ERR_INVALID,
+                            "fem_dot_f64_noalloc: device ordinal %d exceeds the allocation-free limit of %d devices",
+                            dev, kMaxDevices);
   double* scratch;
   {
     // set-up, once per device, with that device current: the host-side symbol

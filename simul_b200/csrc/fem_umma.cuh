@@ -74,6 +74,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int m
   return false;
 }
 
+// After a completion wait that gave up, the MMA may still be writing the
+// TMEM columns: wait once more, again bounded, before they are freed.
+__device__ __forceinline__ void drain_mma(uint64_t* mbar, uint32_t parity, bool ok, int max_polls) {
+  if (!ok) (void)mbar_wait(mbar, parity, max_polls);
+}
+
 __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }

@@ -60,6 +60,7 @@ __global__ void __launch_bounds__(128) umma_check_kernel(const __nv_bfloat16* __
   } else if (lane == 0) {
     atomicExch(err, 1);
   }
+  umma::drain_mma(&mbar, 0, ok, kMaxPolls);
   umma::fence_before_sync();
   __syncthreads();
   if (warp == 0) umma::tmem_free(tbase, (uint32_t)ncols);

@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--weights", default=os.path.join(ROOT, "simul_b200", "weights", "mpnn_vertebra.npz"),
                     help="learned-preconditioner weights (simul_b200.train_precond)")
     ap.add_argument("--learned-coarse", type=int, default=1, help="learned: add the coarse correction")
-    ap.add_argument("--matvec-variant", default="auto", choices=["auto", "fused", "two_phase", "element_block", "warp_agg"],
+    ap.add_argument("--matvec-variant", default="auto", choices=["auto", "fused", "two_phase", "element_block", "warp_agg", "persistent"],
                     help="tangent-matvec variant (auto: timed on the first solve)")
     ap.add_argument("--no-jacobi-baseline", action="store_true")
     ap.add_argument("--no-hex8", action="store_true", help="skip the HEX8 form of the workload (reported beside)")
@@ -587,7 +587,8 @@ def main():
                 "fused": "matvec_kernel<J2> (fused node-block)",
                 "two_phase": "elem_mv_kernel<J2> + node_gather_kernel (two-phase)",
                 "element_block": "eb_matvec_kernel<J2> + eb_complete_kernel (element-block)",
-                "warp_agg": "elem_wagg_kernel<J2> + node_gather_kernel (warp-aggregated two-phase)"}.get(variant, variant),
+                "warp_agg": "elem_wagg_kernel<J2> + node_gather_kernel (warp-aggregated two-phase)",
+                "persistent": "elem_mv_persist_kernel<J2> + node_gather_persist_kernel (persistent two-phase)"}.get(variant, variant),
                          "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "frac_nominal_8tbs": (achieved / 8000.0) if achieved else None,

@@ -148,8 +148,9 @@ int fem_ctx_info(void* ctx, int64_t* out6);
  * available; out[10] timed ns of the element-block variant at its best block
  * size, out[11] that size (0: no element-block tables), out[12..15] timed ns
  * at 256, 512, 768 and 1024 elements per block (0 if not timed), out[16]
- * timed ns of the warp-aggregated variant; variant 3 in out[4] */
-int fem_ctx_stats(void* ctx, int64_t* out17);
+ * timed ns of the warp-aggregated variant (variant 3 in out[4]), out[17]
+ * timed ns of the persistent two-phase variant (variant 4) */
+int fem_ctx_stats(void* ctx, int64_t* out18);
 
 /* Option keys of fem_set_option (no reference counterpart: the reference has
  * one matvec formulation, backend/fea/fem/material/nonlinear/base.py:110-145). */
@@ -160,7 +161,9 @@ enum {
    * kernel that sums each block's slot vectors in shared memory, nodes
    * shared by blocks completed by a second kernel; 3 (TET4): the two-phase
    * pass with each warp's slot vectors added per vertex in shared memory
-   * before the node gather */
+   * before the node gather; 4 (TET4): the two-phase pair as persistent
+   * grid-stride kernels (one wave of CTAs, next element's inputs
+   * prefetched) */
   FEM_OPT_MATVEC_VARIANT = 1,
   /* two-level preconditioner: lattice cell edge in mesh lengths (default 8;
    * the cube root of 5x the mean element volume, i.e. the voxel edge of

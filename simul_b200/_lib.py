@@ -50,7 +50,7 @@ FEM_OPT_COARSE_INVERSE = 11
 FEM_OPT_COARSE_MAX_NODES = 12
 FEM_OPT_EB_SIZE = 13
 MPNN_PARAMS = 34307
-MATVEC_VARIANTS = {0: "fused", 1: "two_phase", 2: "element_block", 3: "warp_agg"}
+MATVEC_VARIANTS = {0: "fused", 1: "two_phase", 2: "element_block", 3: "warp_agg", 4: "persistent"}
 
 
 class FemMeshDesc(C.Structure):

@@ -195,7 +195,7 @@ struct FemCtx {
   int mv_variant = MV_FUSED;
   bool mv_tuned = false;
   int mv_tuned_model = -2;
-  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0, 0.0, 0.0};
+  double mv_ns[MV_N_VARIANTS] = {0.0, 0.0, 0.0, 0.0, 0.0};
   // element-block matvec (TET4): tables for blocks of eb_size elements (0:
   // not built), the block size forced by FEM_OPT_EB_SIZE (0: timed choice
   // among kEbSizes), and the timed ns per launch of each candidate size
@@ -931,7 +931,7 @@ struct ChainPdl {
 // Two-level PCG with the two-phase matvec: the matvec acts on z and its node
 // gather forms p = z + beta p, q = K z + beta q (no direction-update kernel).
 bool recurrence(const FemCtx* c, int kind) {
-  return kind == GRAPH_TWO_LEVEL && (c->mv_variant == MV_TWO_PHASE || c->mv_variant == MV_WARP_AGG) &&
+  return kind == GRAPH_TWO_LEVEL && (c->mv_variant == MV_TWO_PHASE || c->mv_variant == MV_WARP_AGG || c->mv_variant == MV_PERSIST) &&
          c->direction_recurrence;
 }
 
@@ -1096,6 +1096,7 @@ int choose_matvec_variant(FemCtx* c) {
   c->mv_ns[MV_ELEM_BLOCK] = best_ns;
   if ((st = build_wagg_tables(c))) return st;
   if ((st = time_variant(MV_WARP_AGG, &c->mv_ns[MV_WARP_AGG]))) return st;
+  if ((st = time_variant(MV_PERSIST, &c->mv_ns[MV_PERSIST]))) return st;
   int v_best = MV_FUSED;
   for (int v = 1; v < MV_N_VARIANTS; ++v)
     if (c->mv_ns[v] < c->mv_ns[v_best]) v_best = v;
@@ -1996,6 +1997,7 @@ int fem_ctx_stats(void* ctx, int64_t* out) {
   out[11] = c->eb_size;
   for (int k = 0; k < 4; ++k) out[12 + k] = (int64_t)std::llround(c->eb_ns[k]);
   out[16] = (int64_t)std::llround(c->mv_ns[MV_WARP_AGG]);
+  out[17] = (int64_t)std::llround(c->mv_ns[MV_PERSIST]);
   return FEM_OK;
 }
 
@@ -2018,12 +2020,14 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       if (value < -1 || value >= MV_N_VARIANTS)
         return set_err(c, FEM_ERR_INVALID,
                        "matvec variant %lld not in {-1 (auto), 0 (fused), 1 (two-phase), 2 (element-block), "
-                       "3 (warp-aggregated)}",
+                       "3 (warp-aggregated), 4 (persistent two-phase)}",
                        (long long)value);
       if (value == MV_ELEM_BLOCK && c->npe != 4)
         return set_err(c, FEM_ERR_INVALID, "the element-block matvec is TET4 only");
       if (value == MV_WARP_AGG && c->npe != 4)
         return set_err(c, FEM_ERR_INVALID, "the warp-aggregated matvec is TET4 only");
+      if (value == MV_PERSIST && c->npe != 4)
+        return set_err(c, FEM_ERR_INVALID, "the persistent two-phase matvec is TET4 only");
       // table-driven variants are only ever selected with their tables built
       if (value == MV_ELEM_BLOCK && (st = build_eb_tables(c, c->eb_forced > 0 ? c->eb_forced : 512))) return st;
       if (value == MV_WARP_AGG && (st = build_wagg_tables(c))) return st;

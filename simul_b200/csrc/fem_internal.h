@@ -193,7 +193,9 @@ struct MvArgs {
 // MV_WARP_AGG: the two-phase element pass with each warp's slot vectors
 // added per vertex in shared memory, so the node gather reads about a
 // quarter of the partial rows (fem_kernels.cu).
-enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_ELEM_BLOCK = 2, MV_WARP_AGG = 3, MV_N_VARIANTS = 4 };
+// MV_PERSIST: the two-phase pair as persistent grid-stride kernels (one wave
+// of CTAs, the next element's streaming inputs prefetched).
+enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_ELEM_BLOCK = 2, MV_WARP_AGG = 3, MV_PERSIST = 4, MV_N_VARIANTS = 5 };
 
 // smallest element block of the element-block matvec (one element per
 // thread; blocks of 256, 512, 768 or 1024 elements)

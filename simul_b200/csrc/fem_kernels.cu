@@ -12,6 +12,8 @@
 // (e.g. backend/fea/fem/material/neo_hookean.py:190).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fem_internal.h"
 #include "fem_reduce.cuh"
 
@@ -293,12 +295,40 @@ __global__ void __launch_bounds__(NB) matvec_kernel(const __grid_constant__ MvAr
 // Phase 2: one thread per node sums its contiguous slot range in list order,
 // so the result is the same fixed-order (bitwise reproducible) sum.
 
-// The four slot vectors f (tangent action on x) of element e.
-template <int MODEL, bool MASK>
-__device__ __forceinline__ void elem_mv_forces(const MvArgs& a, int e, float f[4][3]) {
+// Streaming (coalesced SoA) inputs of one element: connectivity, slot
+// positions, material, modulus scale and tangent payload.
+struct MvIn {
+  int4 cn, sp;
+  float pay[kPay];
+  float scl;
+  int mid;
+};
+
+// The per-element words after the connectivity and slot positions.
+template <int MODEL>
+__device__ __forceinline__ void mv_load_rest(const MvArgs& a, int e, MvIn& q) {
   const MeshDev& m = a.m;
-  const int4 cn = __ldg(m.conn + e);
-  const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+  q.mid = (int)__ldg(m.mat_id + e);
+  q.scl = __ldg(m.scale + e);
+  // mixed tables: the payload words of the largest model (zeros beyond an element's own)
+  const int npay = MODEL >= 0 ? model_pay_words(MODEL) : kPay;
+#pragma unroll
+  for (int k = 0; k < kPay; ++k) q.pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
+}
+
+template <int MODEL>
+__device__ __forceinline__ void mv_load(const MvArgs& a, int e, MvIn& q) {
+  q.cn = __ldg(a.m.conn + e);
+  q.sp = __ldg(a.m.spos + e);
+  mv_load_rest<MODEL>(a, e, q);
+}
+
+// The four slot vectors f (tangent action on x) of the element whose
+// streaming inputs are q: its vertices' coordinates and x are gathered here.
+template <int MODEL, bool MASK>
+__device__ __forceinline__ void elem_mv_forces_q(const MvArgs& a, const MvIn& q, float f[4][3]) {
+  const MeshDev& m = a.m;
+  const int nid[4] = {q.cn.x, q.cn.y, q.cn.z, q.cn.w};
   const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
   float xv[4][3], pv[4][3];
 #pragma unroll
@@ -315,16 +345,6 @@ __device__ __forceinline__ void elem_mv_forces(const MvArgs& a, int e, float f[4
     pv[k][1] = (fx & 2) ? 0.f : P.y;
     pv[k][2] = (fx & 4) ? 0.f : P.z;
   }
-  const int mid = (int)__ldg(m.mat_id + e);
-  const float scl = __ldg(m.scale + e);
-  const DevMat<float>& mat = a.matF[mid];
-  float pay[kPay];
-  {
-    const int npay = model_pay_words(MODEL >= 0 ? MODEL : mat.model);
-#pragma unroll
-    for (int k = 0; k < kPay; ++k)
-      pay[k] = (k < npay) ? __ldg(a.payload + (size_t)k * m.n_elems + e) : 0.f;
-  }
   TetGeom<float> g;
   tet_geom(xv[0], xv[1], xv[2], xv[3], g);
   float D[3][3];
@@ -335,8 +355,16 @@ __device__ __forceinline__ void elem_mv_forces(const MvArgs& a, int e, float f[4
   float dF[9];
   grad_from_diffs(D, g, dF);
   float dP[9];
-  dP_any<MODEL>(mat, scl, pay, dF, dP);
+  dP_any<MODEL>(a.matF[q.mid], q.scl, q.pay, dF, dP);
   slot_vectors(dP, g, g.s6, f);
+}
+
+// The four slot vectors f (tangent action on x) of element e.
+template <int MODEL, bool MASK>
+__device__ __forceinline__ void elem_mv_forces(const MvArgs& a, int e, float f[4][3]) {
+  MvIn q;
+  mv_load<MODEL>(a, e, q);
+  elem_mv_forces_q<MODEL, MASK>(a, q, f);
 }
 
 template <int MODEL, bool MASK>
@@ -364,6 +392,51 @@ __global__ void __launch_bounds__(256, 5) elem_mv_kernel(const __grid_constant__
     elem_mv_one<MODEL, true>(a, e);
   else
     elem_mv_one<MODEL, false>(a, e);
+}
+
+// Persistent element pass: one wave of CTAs (resident CTAs per SM x SMs)
+// walks the elements in grid-stride order.  Each thread loads the
+// connectivity and slot positions of its next element before it evaluates
+// the current one, so the current element's vertex gathers and its payload
+// loads are in flight together (one memory round trip per element instead
+// of two dependent ones).
+template <int MODEL, bool CG>
+__global__ void __launch_bounds__(256, 4) elem_mv_persist_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  const int n = a.m.n_elems;
+  const int stride = (int)gridDim.x * 256;
+  int e = (int)blockIdx.x * 256 + (int)threadIdx.x;
+  if (e >= n) return;
+  const bool mask = !CG && a.mask_input;
+  int4 cn = __ldg(a.m.conn + e), sp = __ldg(a.m.spos + e);
+  for (;;) {
+    const int en = e + stride;
+    int4 cn_n = cn, sp_n = sp;
+    if (en < n) {
+      cn_n = __ldg(a.m.conn + en);
+      sp_n = __ldg(a.m.spos + en);
+    }
+    MvIn q;
+    q.cn = cn;
+    q.sp = sp;
+    mv_load_rest<MODEL>(a, e, q);
+    float f[4][3];
+    if (mask)
+      elem_mv_forces_q<MODEL, true>(a, q, f);
+    else
+      elem_mv_forces_q<MODEL, false>(a, q, f);
+    __stcg(a.stage + sp.x, make_float4(f[0][0], f[0][1], f[0][2], 0.f));
+    __stcg(a.stage + sp.y, make_float4(f[1][0], f[1][1], f[1][2], 0.f));
+    __stcg(a.stage + sp.z, make_float4(f[2][0], f[2][1], f[2][2], 0.f));
+    __stcg(a.stage + sp.w, make_float4(f[3][0], f[3][1], f[3][2], 0.f));
+    if (en >= n) break;
+    e = en;
+    cn = cn_n;
+    sp = sp_n;
+  }
 }
 
 // Warp-aggregated element pass: lane l of warp w evaluates element 32 w + l
@@ -421,17 +494,13 @@ __global__ void __launch_bounds__(32 * kWaggWarps, 5) elem_wagg_kernel(const __g
 constexpr int kGatherLanes = 4;
 constexpr int kGatherNodes = 256 / kGatherLanes;  // nodes per CTA
 
+// Node n's product row from its contiguous slot range (lanes sub of its
+// kGatherLanes-lane group), stored to y; inside CG also the direction by
+// recurrence and the node's p.Ap term (returned by the group's lane 0).
+// Every lane of the warp calls it (the group sum uses shuffles).
 template <bool CG>
-__global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant__ MvArgs a) {
-  chain_enter();
-  if (CG) {
-    if (a.cg->done) return;
-  }
-  __shared__ double sred[8];
-  __shared__ bool am_last;
+__device__ __forceinline__ double gather_node(const MvArgs& a, int n, int sub) {
   const MeshDev& m = a.m;
-  const int n = blockIdx.x * kGatherNodes + threadIdx.x / kGatherLanes;
-  const int sub = threadIdx.x % kGatherLanes;
   double pap = 0.0;
   float a0 = 0.f, a1 = 0.f, a2 = 0.f;
   if (n < m.n_nodes) {
@@ -482,24 +551,63 @@ __global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant_
       }
     }
   }
+  return pap;
+}
+
+// The last block's p.Ap: alpha = rz / pAp, or a breakdown flag.
+__device__ __forceinline__ void gather_finish(const MvArgs& a, double pap, double* sred, bool* am_last) {
+  double bsum = block_sum<256>(pap, sred);
+  if (publish_partial(a.red, a.red_site, 1, &bsum, am_last)) {
+    double tot = final_sum<256>(a.red, a.red_site, 0, sred);
+    if (threadIdx.x == 0) {
+      CGState* st = a.cg;
+      st->pAp = tot;
+      if (!(tot > 0.0) || !isfinite(tot)) {
+        st->done = 3;
+        st->status = 3;
+        st->alpha = 0.0;
+      } else {
+        st->alpha = st->rz / tot;
+      }
+      a.red.counters[a.red_site] = 0u;
+    }
+  }
+}
+
+template <bool CG>
+__global__ void __launch_bounds__(256) node_gather_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const int n = blockIdx.x * kGatherNodes + threadIdx.x / kGatherLanes;
+  const double pap = gather_node<CG>(a, n, threadIdx.x % kGatherLanes);
   if (CG) {
     chain_release();
-    double bsum = block_sum<256>(pap, sred);
-    if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
-      double tot = final_sum<256>(a.red, a.red_site, 0, sred);
-      if (threadIdx.x == 0) {
-        CGState* st = a.cg;
-        st->pAp = tot;
-        if (!(tot > 0.0) || !isfinite(tot)) {
-          st->done = 3;
-          st->status = 3;
-          st->alpha = 0.0;
-        } else {
-          st->alpha = st->rz / tot;
-        }
-        a.red.counters[a.red_site] = 0u;
-      }
-    }
+    gather_finish(a, pap, sred, &am_last);
+  }
+}
+
+// Persistent node gather: one wave of CTAs walks the node groups in
+// grid-stride order, so the grid reduction adds one partial per resident
+// CTA instead of one per 64-node group.
+template <bool CG>
+__global__ void __launch_bounds__(256) node_gather_persist_kernel(const __grid_constant__ MvArgs a) {
+  chain_enter();
+  if (CG) {
+    if (a.cg->done) return;
+  }
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  double pap = 0.0;
+  const int sub = threadIdx.x % kGatherLanes;
+  for (int g = blockIdx.x; g * kGatherNodes < a.m.n_nodes; g += gridDim.x)
+    pap += gather_node<CG>(a, g * kGatherNodes + threadIdx.x / kGatherLanes, sub);
+  if (CG) {
+    chain_release();
+    gather_finish(a, pap, sred, &am_last);
   }
 }
 
@@ -1065,6 +1173,38 @@ static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
   launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
 }
 
+// CTAs that fit on the device at once (resident per SM x SMs) for a
+// persistent kernel of `threads` threads and no dynamic shared memory.
+template <typename K>
+static int resident_grid(K kernel, int threads) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+  return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
+}
+
+template <int MODEL, bool CG>
+static void persist_elem(const MvArgs& a, cudaStream_t s) {
+  static const int grid = resident_grid(elem_mv_persist_kernel<MODEL, CG>, 256);
+  launch_chain(elem_mv_persist_kernel<MODEL, CG>, std::min(grid, nblk(a.m.n_elems, 256)), 256, 0, s, a);
+}
+
+template <bool CG>
+static void two_phase_persist(const MvArgs& a, int model, cudaStream_t s) {
+  switch (model) {
+    case M_LE: persist_elem<M_LE, CG>(a, s); break;
+    case M_NH: persist_elem<M_NH, CG>(a, s); break;
+    case M_MR: persist_elem<M_MR, CG>(a, s); break;
+    case M_J2: persist_elem<M_J2, CG>(a, s); break;
+    case M_TI: persist_elem<M_TI, CG>(a, s); break;
+    case M_FMR: persist_elem<M_FMR, CG>(a, s); break;
+    default: persist_elem<-1, CG>(a, s); break;
+  }
+  static const int ggrid = resident_grid(node_gather_persist_kernel<CG>, 256);
+  launch_chain(node_gather_persist_kernel<CG>, std::min(ggrid, nblk(a.m.n_nodes, kGatherNodes)), 256, 0, s, a);
+}
+
 void launch_node_gather(const MvArgs& a, cudaStream_t s) {
   if (a.cg)
     launch_chain(node_gather_kernel<true>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
@@ -1094,6 +1234,10 @@ void launch_matvec(const MvArgs& a, int model, cudaStream_t s) {
   }
   if (a.variant == MV_TWO_PHASE) {
     cg ? two_phase<true>(a, model, s) : two_phase<false>(a, model, s);
+    return;
+  }
+  if (a.variant == MV_PERSIST) {
+    cg ? two_phase_persist<true>(a, model, s) : two_phase_persist<false>(a, model, s);
     return;
   }
   switch (a.m.nb) {

@@ -156,12 +156,12 @@ class FEMesh:
                 "block_element_entries": out[3], "nodes_per_block": out[4], "device_bytes": out[5]}
 
     def stats(self) -> dict:
-        out = (C.c_int64 * 17)()
+        out = (C.c_int64 * 18)()
         _check(_lib.load().fem_ctx_stats(self.ctx, out), self.ctx, "fem_ctx_stats")
         return {"launches": out[0], "cg_iterations": out[1], "residual_evals": out[2], "cg_graphs": out[3],
                 "matvec_variant": _lib.MATVEC_VARIANTS.get(out[4], str(out[4])),
                 "matvec_ns": {"fused": out[5], "two_phase": out[6], "element_block": out[10],
-                              "warp_agg": out[16]},
+                              "warp_agg": out[16], "persistent": out[17]},
                 "matvec_tuned": bool(out[7]),
                 "whole_solve_graphs": out[8], "whole_solve_graph_available": bool(out[9]),
                 "element_block_size": out[11],
@@ -237,10 +237,10 @@ class FEMesh:
 
     def set_matvec_variant(self, variant, block_size=None):
         """Forces the tangent-matvec variant ("fused", "two_phase",
-        "element_block", "warp_agg") or restores the timed choice (None); ``block_size``
+        "element_block", "warp_agg", "persistent") or restores the timed choice (None); ``block_size``
         fixes the element-block variant's elements per block (256, 512, 768
         or 1024; 0: timed; None: unchanged)."""
-        code = {None: -1, "fused": 0, "two_phase": 1, "element_block": 2, "warp_agg": 3}[variant]
+        code = {None: -1, "fused": 0, "two_phase": 1, "element_block": 2, "warp_agg": 3, "persistent": 4}[variant]
         lib = _lib.load()
         if block_size is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_EB_SIZE, int(block_size)), self.ctx, "fem_set_option")

@@ -27,7 +27,7 @@ import numpy as np
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=64)
-    ap.add_argument("--variant", default="fused", choices=["fused", "two_phase", "element_block", "warp_agg"])
+    ap.add_argument("--variant", default="fused", choices=["fused", "two_phase", "element_block", "warp_agg", "persistent"])
     ap.add_argument("--block-size", type=int, default=0, help="element-block variant: elements per block")
     ap.add_argument("--element", default="tet4", choices=["tet4", "hex8"])
     ap.add_argument("--reps", type=int, default=3)

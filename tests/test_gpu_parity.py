@@ -96,7 +96,7 @@ def test_element_forces_and_stress(cuda, bar, key, nb):
         assert _rel_max(mesh.F.cpu().numpy(), ref["F"]) < 1e-12
 
 
-VARIANTS = ["fused", "two_phase", "element_block", "warp_agg"]
+VARIANTS = ["fused", "two_phase", "element_block", "warp_agg", "persistent"]
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
@@ -644,6 +644,8 @@ def test_matvec_variants_agree_and_autotuner_times_both(cuda, vox):
     assert _rel_l2(ys["two_phase"], ys["fused"]) < 1e-6
     assert _rel_l2(ys["element_block"], ys["fused"]) < 1e-6
     assert _rel_l2(ys["warp_agg"], ys["fused"]) < 1e-6
+    # the persistent pair evaluates the same elements and sums in the same order
+    assert np.array_equal(ys["persistent"], ys["two_phase"])
     # automatic choice: the first PCG solve times every variant (the element
     # block at each candidate size) and keeps the fastest
     mesh.set_matvec_variant(None)

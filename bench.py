@@ -652,18 +652,28 @@ def main():
         # beside the headline, each reported, never fatal to it: the north
         # star's 1M-tet point, the matvec roofline beyond L2, batched solves
         for key, fn in (("vertebra_1m_tets", lambda: size_point(args, args.n_large, dev)),
-                        ("roofline_large", lambda: roofline_point(args, args.n_roofline, dev)),
-                        ("batch", lambda: __import__("simul_b200.batch_bench", fromlist=["run"]).run(
-                            instances=args.batch_instances, n_min=32, n_max=64, load_steps=10, seed=0,
-                            workers=8, device=str(dev)))):
+                        ("roofline_large", lambda: roofline_point(args, args.n_roofline, dev))):
             try:
                 line[key] = fn()
             except Exception as exc:
                 line[key] = {"error": repr(exc)}
-        if isinstance(line.get("batch"), dict) and "error" not in line["batch"]:
+    if not args.no_extras:
+        # batched uneven solves: the instances are sharded across the ranks
+        # (every rank takes part; the per-instance results are gathered)
+        from simul_b200 import batch_bench
+        try:
+            bres = batch_bench.run(instances=args.batch_instances, n_min=32, n_max=64, load_steps=10, seed=0,
+                                   workers=8, device=str(dev), rank=rank, world=ws)
+        except Exception as exc:  # reported, never fatal to the headline line
+            bres = {"error": repr(exc)}
+        if rank == 0 and "error" in bres:
+            line["batch"] = bres
+        elif rank == 0:
+            line["batch"] = bres
             line["batch"]["note"] = ("the batched uneven-solves workload at reduced scale: instances with grid "
-                                     "sizes 32-64 voxels per axis, 10 load steps (the full 64-instance, 32-96 "
-                                     "run: python -m simul_b200.batch_bench)")
+                                     "sizes 32-64 voxels per axis, 10 load steps, sharded across "
+                                     f"{ws} rank(s) (the full 64-instance, 32-96 run: "
+                                     "python -m simul_b200.batch_bench)")
     if rank == 0:
         print(json.dumps(line), flush=True)
     del solver, mesh

@@ -45,17 +45,54 @@ def _make_case(args):
             "E": v.E, "fixed": fixed, "vals": vals, "f": f, "tets": int(v.n_elements)}
 
 
-def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, precond="two_level",
-        sequential=False, workers=16, coarse_cell=4, coarse_bf16=True, coarse_reuse=0, device=0):
-    """Generates the seeded instances, solves them as one batch after a
-    one-step warm-up pass, and returns solves/s, p50/p99 per-instance wall
-    time and iteration counts (one dict)."""
+def instance_specs(instances, n_min, n_max, seed):
+    """The seeded instance list: (index, grid size, mesh seed, load case, axial strain)."""
     rng = np.random.default_rng(seed)
     specs = []
     for i in range(instances):
         n = int(rng.integers(n_min, n_max + 1))
         case = CASES[int(rng.integers(0, len(CASES)))]
         specs.append((i, n, 1000 + i, case, float(rng.uniform(0.01, 0.03))))
+    return specs
+
+
+def shard(specs, rank, world):
+    """This rank's share of the instances.  Instances are independent, so
+    they are split across ranks with no collective in the solve: largest
+    first (work grows as n^3), each to the rank with the least work so far
+    (ties to the lower rank).  Every rank computes the same split."""
+    load = [0] * world
+    mine = []
+    for sp in sorted(specs, key=lambda s: (-s[1] ** 3, s[0])):
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += sp[1] ** 3
+        if r == rank:
+            mine.append(sp)
+    return sorted(mine, key=lambda s: s[0])
+
+
+def gather_results(local, world):
+    """Per-instance result dicts of all ranks, ordered by instance index (a
+    host gather after the solves; world 1 returns ``local`` sorted)."""
+    if world > 1:
+        import torch.distributed as dist
+        parts = [None] * world
+        dist.all_gather_object(parts, local)
+        local = [r for part in parts for r in part]
+    return sorted(local, key=lambda r: r["idx"])
+
+
+def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, precond="two_level",
+        sequential=False, workers=16, coarse_cell=4, coarse_bf16=True, coarse_reuse=0, device=0,
+        rank=0, world=1):
+    """Generates the seeded instances, solves them as one batch after a
+    one-step warm-up pass, and returns solves/s, p50/p99 per-instance wall
+    time and iteration counts (one dict).  With world > 1 (one process per
+    GPU, torch.distributed initialised) each rank solves its ``shard`` and
+    the per-instance results are gathered; the batch time is the slowest
+    rank's."""
+    all_specs = instance_specs(instances, n_min, n_max, seed)
+    specs = shard(all_specs, rank, world) if world > 1 else all_specs
     t0 = time.perf_counter()
     with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
         cases = sorted(ex.map(_make_case, specs), key=lambda d: d["idx"])
@@ -84,27 +121,37 @@ def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, prec
             inst.reset()
         torch.cuda.synchronize()
 
-    # warm-up pass (graph capture, matvec-variant timing, coarse set-up), then reset
-    batch.solve_batch(insts, load_steps=1, precond=precond, n_threads=threads)
-    reset()
-    t0 = time.perf_counter()
-    out = batch.solve_batch(insts, load_steps=load_steps, precond=precond, n_threads=threads)
-    torch.cuda.synchronize()
-    wall = time.perf_counter() - t0
-    ms = np.array([r["wall_ms"] for r in out["instances"]])
-    res = {"instances": instances, "n_range": [n_min, n_max], "tets_total": int(sum(d["tets"] for d in cases)),
-           "tets_min": int(min(d["tets"] for d in cases)), "tets_max": int(max(d["tets"] for d in cases)),
-           "cases": {c: sum(1 for d in cases if d["case"] == c) for c in CASES},
+    out = {"instances": []}
+    wall = 0.0
+    if insts:   # a rank may hold no instance when there are more ranks than instances
+        # warm-up pass (graph capture, matvec-variant timing, coarse set-up), then reset
+        batch.solve_batch(insts, load_steps=1, precond=precond, n_threads=threads)
+        reset()
+        t0 = time.perf_counter()
+        out = batch.solve_batch(insts, load_steps=load_steps, precond=precond, n_threads=threads)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    local = [dict(r, idx=d["idx"], n=d["n"], case=d["case"], tets=d["tets"], rank=rank, rank_wall_s=wall)
+             for r, d in zip(out["instances"], cases)]
+    per = gather_results(local, world)
+    wall = max(r["rank_wall_s"] for r in per)
+    ms = np.array([r["wall_ms"] for r in per])
+    res = {"instances": instances, "n_range": [n_min, n_max], "tets_total": int(sum(r["tets"] for r in per)),
+           "tets_min": int(min(r["tets"] for r in per)), "tets_max": int(max(r["tets"] for r in per)),
+           "cases": {c: sum(1 for r in per if r["case"] == c) for c in CASES},
            "load_steps": load_steps, "precond": precond,
            "coarse": {"cell_voxels": coarse_cell, "inverse": "bf16" if coarse_bf16 else "f32",
                       "reuse": coarse_reuse},
-           "all_converged": bool(all(r["converged"] for r in out["instances"])),
+           "all_converged": bool(all(r["converged"] for r in per)),
            "batch_wall_s": wall, "solves_per_s": instances / wall,
            "p50_instance_ms": float(np.percentile(ms, 50)), "p99_instance_ms": float(np.percentile(ms, 99)),
-           "newton_iterations": int(sum(r["newton_iterations"] for r in out["instances"])),
-           "cg_iterations": int(sum(r["cg_iterations"] for r in out["instances"])),
+           "newton_iterations": int(sum(r["newton_iterations"] for r in per)),
+           "cg_iterations": int(sum(r["cg_iterations"] for r in per)),
            "host_generation_s": t_gen, "host_setup_s": t_setup}
-    if sequential:
+    if world > 1:
+        res["ranks"] = world
+        res["instances_per_rank"] = [sum(1 for r in per if r["rank"] == k) for k in range(world)]
+    if sequential and world == 1:
         reset()
         t0 = time.perf_counter()
         out2 = batch.solve_batch(insts, load_steps=load_steps, precond=precond, n_threads=1)

@@ -323,27 +323,23 @@ __device__ __forceinline__ void mv_load(const MvArgs& a, int e, MvIn& q) {
   mv_load_rest<MODEL>(a, e, q);
 }
 
-// The four slot vectors f (tangent action on x) of the element whose
-// streaming inputs are q: its vertices' coordinates and x are gathered here.
+// The four slot vectors f (tangent action on x) of one element from its
+// vertices' coordinates (w: fixed-DOF bits) and x values.
 template <int MODEL, bool MASK>
-__device__ __forceinline__ void elem_mv_forces_q(const MvArgs& a, const MvIn& q, float f[4][3]) {
-  const MeshDev& m = a.m;
-  const int nid[4] = {q.cn.x, q.cn.y, q.cn.z, q.cn.w};
-  const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
+__device__ __forceinline__ void elem_mv_forces_v(const MvArgs& a, const float4 (&X)[4], const float4 (&P)[4],
+                                                 int mid, float scl, const float (&pay)[kPay], float f[4][3]) {
   float xv[4][3], pv[4][3];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
-    const float4 X = __ldg(m.X32 + nid[k]);
-    const float4 P = __ldg(xin + nid[k]);
-    xv[k][0] = X.x;
-    xv[k][1] = X.y;
-    xv[k][2] = X.z;
+    xv[k][0] = X[k].x;
+    xv[k][1] = X[k].y;
+    xv[k][2] = X[k].z;
     // CG directions are zero on fixed DOFs already; only a standalone
     // matvec masks its input
-    const int fx = MASK ? (int)X.w : 0;
-    pv[k][0] = (fx & 1) ? 0.f : P.x;
-    pv[k][1] = (fx & 2) ? 0.f : P.y;
-    pv[k][2] = (fx & 4) ? 0.f : P.z;
+    const int fx = MASK ? (int)X[k].w : 0;
+    pv[k][0] = (fx & 1) ? 0.f : P[k].x;
+    pv[k][1] = (fx & 2) ? 0.f : P[k].y;
+    pv[k][2] = (fx & 4) ? 0.f : P[k].z;
   }
   TetGeom<float> g;
   tet_geom(xv[0], xv[1], xv[2], xv[3], g);
@@ -355,8 +351,23 @@ __device__ __forceinline__ void elem_mv_forces_q(const MvArgs& a, const MvIn& q,
   float dF[9];
   grad_from_diffs(D, g, dF);
   float dP[9];
-  dP_any<MODEL>(a.matF[q.mid], q.scl, q.pay, dF, dP);
+  dP_any<MODEL>(a.matF[mid], scl, pay, dF, dP);
   slot_vectors(dP, g, g.s6, f);
+}
+
+// The four slot vectors f (tangent action on x) of the element whose
+// streaming inputs are q: its vertices' coordinates and x are gathered here.
+template <int MODEL, bool MASK>
+__device__ __forceinline__ void elem_mv_forces_q(const MvArgs& a, const MvIn& q, float f[4][3]) {
+  const int nid[4] = {q.cn.x, q.cn.y, q.cn.z, q.cn.w};
+  const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
+  float4 X[4], P[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    X[k] = __ldg(a.m.X32 + nid[k]);
+    P[k] = __ldg(xin + nid[k]);
+  }
+  elem_mv_forces_v<MODEL, MASK>(a, X, P, q.mid, q.scl, q.pay, f);
 }
 
 // The four slot vectors f (tangent action on x) of element e.

@@ -785,7 +785,7 @@ int build_wagg_tables(FemCtx* c) {
   const int n_warps = (Ne + 31) / 32;
   std::vector<int> wptr(n_warps + 1, 0), wnode, prow(Nn + 1, 0);
   std::vector<int2> went;
-  std::vector<uint32_t> lspos(Ne, 0u);
+  std::vector<uint32_t> lspos(Ne, 0u), lrow(Ne, 0u);
   wnode.reserve((size_t)Ne);
   went.reserve((size_t)Ne);
   std::vector<uint64_t> ent;
@@ -804,9 +804,11 @@ int build_wagg_tables(FemCtx* c) {
       const int n = (int)(ent[j] >> 32);
       size_t j1 = j;
       while (j1 < ent.size() && (int)(ent[j1] >> 32) == n) ++j1;
+      const uint32_t row = (uint32_t)(went.size() - (size_t)wptr[w]);  // < 128: 4 vertices x 32 elements
       for (size_t q = j; q < j1; ++q) {
         const int le = (int)((ent[q] >> 2) & 31u), k = (int)(ent[q] & 3u);
         lspos[e0 + le] |= (uint32_t)q << (8 * k);
+        lrow[e0 + le] |= row << (8 * k);
       }
       went.push_back(make_int2(0, (int)j | ((int)j1 << 16)));
       wnode.push_back(n);
@@ -818,8 +820,8 @@ int build_wagg_tables(FemCtx* c) {
   for (int n = 0; n < Nn; ++n) prow[n + 1] += prow[n];
   std::vector<int> fill(prow.begin(), prow.end() - 1);
   for (size_t i = 0; i < went.size(); ++i) went[i].x = fill[wnode[i]]++;
-  uint32_t* d_lspos = nullptr;
-  int *d_wptr = nullptr, *d_prow = nullptr;
+  uint32_t *d_lspos = nullptr, *d_lrow = nullptr;
+  int *d_wptr = nullptr, *d_prow = nullptr, *d_wnode = nullptr;
   int2* d_went = nullptr;
   float4* d_parts = nullptr;
   int st;
@@ -835,6 +837,8 @@ int build_wagg_tables(FemCtx* c) {
   if ((st = up(&d_wptr, wptr))) return st;
   if ((st = up(&d_went, went))) return st;
   if ((st = up(&d_prow, prow))) return st;
+  if ((st = up(&d_lrow, lrow))) return st;
+  if ((st = up(&d_wnode, wnode))) return st;
   if ((st = dalloc(c, &d_parts, std::max<size_t>(went.size(), 1)))) return st;
   c->wa_bufs.push_back(d_parts);
   CK(cudaStreamSynchronize(c->stream));
@@ -843,6 +847,8 @@ int build_wagg_tables(FemCtx* c) {
   c->wadev.went = d_went;
   c->wadev.prow = d_prow;
   c->wadev.parts = d_parts;
+  c->wadev.lrow = d_lrow;
+  c->wadev.wnode = d_wnode;
   return FEM_OK;
 }
 

@@ -162,6 +162,8 @@ struct WaggDev {
                             // node-major slot order
   const int* wptr;          // [n_warps + 1] into went
   const int2* went;         // per (warp, local node): partial position, slot range start | end << 16
+  const int* wnode;         // per (warp, local node): the node
+  const uint32_t* lrow;     // [Ne] four 8-bit indices of the element's vertices among its warp's rows
   const int* prow;          // [Nn + 1] each node's partial range
   float4* parts;            // [prow[Nn]] partial rows
 };
@@ -190,9 +192,10 @@ struct MvArgs {
 // MV_ELEM_BLOCK: one CTA per element block: vertex data staged in shared
 // memory, slot vectors summed per local node in shared memory; a second
 // kernel adds the partial rows of nodes shared by blocks (fem_elemblock.cu).
-// MV_WARP_AGG: the two-phase element pass with each warp's slot vectors
-// added per vertex in shared memory, so the node gather reads about a
-// quarter of the partial rows (fem_kernels.cu).
+// MV_WARP_AGG: the two-phase element pass with each warp's distinct
+// vertices loaded once into shared memory and its slot vectors added per
+// vertex there, so the node gather reads about a quarter of the partial rows
+// (fem_kernels.cu).
 // MV_PERSIST: the two-phase pair as persistent grid-stride kernels (one wave
 // of CTAs, the next element's streaming inputs prefetched).
 enum { MV_FUSED = 0, MV_TWO_PHASE = 1, MV_ELEM_BLOCK = 2, MV_WARP_AGG = 3, MV_PERSIST = 4, MV_N_VARIANTS = 5 };

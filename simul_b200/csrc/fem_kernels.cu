@@ -450,50 +450,86 @@ __global__ void __launch_bounds__(256, 4) elem_mv_persist_kernel(const __grid_co
   }
 }
 
-// Warp-aggregated element pass: lane l of warp w evaluates element 32 w + l
-// and puts its slot vectors at their places in the warp's node-major slot
-// order in shared memory; then each (warp, vertex) row is the sum of its
-// slot range in that order, written to its place among the vertex's partials.
+// Warp-aggregated element pass.  The elements are taken 32 at a time (one
+// "element warp" w: elements 32 w .. 32 w + 31) and each has its list of
+// distinct vertices (rows, node-major).  A hardware warp walks the element
+// warps in grid-stride order (persistent, one wave of CTAs); for each it
+//   1. loads every row's coordinates (w: fixed-DOF bits) and x value once
+//      into shared memory (a vertex shared by several of the 32 elements is
+//      read once instead of once per element);
+//   2. lane l evaluates element 32 w + l from those rows and puts its slot
+//      vectors at their places in the warp's node-major slot order;
+//   3. each row is the sum of its slot range in that order, written to its
+//      place among the vertex's partial rows (the node gather adds those).
 constexpr int kWaggWarps = 8;
 
 template <int MODEL, bool CG>
-__global__ void __launch_bounds__(32 * kWaggWarps, 5) elem_wagg_kernel(const __grid_constant__ MvArgs a) {
+__global__ void __launch_bounds__(32 * kWaggWarps, 4) elem_wagg_kernel(const __grid_constant__ MvArgs a) {
   chain_enter();
   if (CG) {
     if (a.cg->done) return;
   }
   __shared__ float4 s_slot[kWaggWarps][128];
+  __shared__ float4 s_xv[kWaggWarps][128];
+  __shared__ float4 s_pv[kWaggWarps][128];
   const int warp = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
-  const int w = (int)blockIdx.x * kWaggWarps + warp;
-  const int e = w * 32 + lane;
-  if (w * 32 >= a.m.n_elems) return;  // the whole warp
-  if (e < a.m.n_elems) {
-    float f[4][3];
-    if (!CG && a.mask_input)
-      elem_mv_forces<MODEL, true>(a, e, f);
-    else
-      elem_mv_forces<MODEL, false>(a, e, f);
-    const uint32_t sp = __ldg(a.wa.lspos + e);
-    float4* sw = s_slot[warp];
-    sw[sp & 0xffu] = make_float4(f[0][0], f[0][1], f[0][2], 0.f);
-    sw[(sp >> 8) & 0xffu] = make_float4(f[1][0], f[1][1], f[1][2], 0.f);
-    sw[(sp >> 16) & 0xffu] = make_float4(f[2][0], f[2][1], f[2][2], 0.f);
-    sw[sp >> 24] = make_float4(f[3][0], f[3][1], f[3][2], 0.f);
-  }
-  __syncwarp();
-  const int q0 = __ldg(a.wa.wptr + w), q1 = __ldg(a.wa.wptr + w + 1);
-#pragma unroll 1
-  for (int i = q0 + lane; i < q1; i += 32) {
-    const int2 en = __ldg(a.wa.went + i);  // partial position, slot range
-    const int j1 = en.y >> 16;
-    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
-    for (int j = en.y & 0xffff; j < j1; ++j) {
-      const float4 v = s_slot[warp][j];
-      a0 += v.x;
-      a1 += v.y;
-      a2 += v.z;
+  const int n = a.m.n_elems;
+  const bool mask = !CG && a.mask_input;
+  const float4* __restrict__ xin = reinterpret_cast<const float4*>(a.x);
+  float4* sw = s_slot[warp];
+  float4* sx = s_xv[warp];
+  float4* sp4 = s_pv[warp];
+  for (int w = (int)blockIdx.x * kWaggWarps + warp; w * 32 < n; w += (int)gridDim.x * kWaggWarps) {
+    const int e = w * 32 + lane;
+    const bool valid = e < n;
+    const int q0 = __ldg(a.wa.wptr + w), q1 = __ldg(a.wa.wptr + w + 1);
+    // the element's own streaming words first, so they are in flight with the row loads
+    MvIn q;
+    uint32_t lr = 0u, sp = 0u;
+    if (valid) {
+      lr = __ldg(a.wa.lrow + e);
+      sp = __ldg(a.wa.lspos + e);
+      mv_load_rest<MODEL>(a, e, q);
     }
-    __stcg(a.wa.parts + en.x, make_float4(a0, a1, a2, 0.f));
+    for (int i = q0 + lane; i < q1; i += 32) {
+      const int node = __ldg(a.wa.wnode + i);
+      sx[i - q0] = __ldg(a.m.X32 + node);
+      sp4[i - q0] = __ldg(xin + node);
+    }
+    __syncwarp();
+    if (valid) {
+      float4 X[4], P[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int r = (int)((lr >> (8 * k)) & 0xffu);
+        X[k] = sx[r];
+        P[k] = sp4[r];
+      }
+      float f[4][3];
+      if (mask)
+        elem_mv_forces_v<MODEL, true>(a, X, P, q.mid, q.scl, q.pay, f);
+      else
+        elem_mv_forces_v<MODEL, false>(a, X, P, q.mid, q.scl, q.pay, f);
+      sw[sp & 0xffu] = make_float4(f[0][0], f[0][1], f[0][2], 0.f);
+      sw[(sp >> 8) & 0xffu] = make_float4(f[1][0], f[1][1], f[1][2], 0.f);
+      sw[(sp >> 16) & 0xffu] = make_float4(f[2][0], f[2][1], f[2][2], 0.f);
+      sw[sp >> 24] = make_float4(f[3][0], f[3][1], f[3][2], 0.f);
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int i = q0 + lane; i < q1; i += 32) {
+      const int2 en = __ldg(a.wa.went + i);  // partial position, slot range
+      const int j1 = en.y >> 16;
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+      for (int j = en.y & 0xffff; j < j1; ++j) {
+        const float4 v = sw[j];
+        a0 += v.x;
+        a1 += v.y;
+        a2 += v.z;
+      }
+      __stcg(a.wa.parts + en.x, make_float4(a0, a1, a2, 0.f));
+    }
+    __syncwarp();  // the shared rows and slots are refilled by the next element warp
   }
 }
 
@@ -1150,24 +1186,6 @@ static void matvec_nb(const MvArgs& a, int model, cudaStream_t s) {
   }
 }
 
-template <bool CG>
-static void warp_agg(const MvArgs& a, int model, cudaStream_t s) {
-  const int ge = nblk(nblk(a.m.n_elems, 32), kWaggWarps);
-  switch (model) {
-    case M_LE: launch_chain(elem_wagg_kernel<M_LE, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-    case M_NH: launch_chain(elem_wagg_kernel<M_NH, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-    case M_MR: launch_chain(elem_wagg_kernel<M_MR, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-    case M_J2: launch_chain(elem_wagg_kernel<M_J2, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-    case M_TI: launch_chain(elem_wagg_kernel<M_TI, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-    case M_FMR: launch_chain(elem_wagg_kernel<M_FMR, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-    default: launch_chain(elem_wagg_kernel<-1, CG>, ge, 32 * kWaggWarps, 0, s, a); break;
-  }
-  // the two-phase node gather over the partial rows
-  MvArgs g = a;
-  g.m.node_row = a.wa.prow;
-  g.stage = a.wa.parts;
-  launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, g);
-}
 
 template <bool CG>
 static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
@@ -1214,6 +1232,32 @@ static void two_phase_persist(const MvArgs& a, int model, cudaStream_t s) {
   }
   static const int ggrid = resident_grid(node_gather_persist_kernel<CG>, 256);
   launch_chain(node_gather_persist_kernel<CG>, std::min(ggrid, nblk(a.m.n_nodes, kGatherNodes)), 256, 0, s, a);
+}
+
+template <int MODEL, bool CG>
+static void wagg_elem(const MvArgs& a, cudaStream_t s) {
+  static const int grid = resident_grid(elem_wagg_kernel<MODEL, CG>, 32 * kWaggWarps);
+  launch_chain(elem_wagg_kernel<MODEL, CG>, std::min(grid, nblk(nblk(a.m.n_elems, 32), kWaggWarps)),
+               32 * kWaggWarps, 0, s, a);
+}
+
+template <bool CG>
+static void warp_agg(const MvArgs& a, int model, cudaStream_t s) {
+  switch (model) {
+    case M_LE: wagg_elem<M_LE, CG>(a, s); break;
+    case M_NH: wagg_elem<M_NH, CG>(a, s); break;
+    case M_MR: wagg_elem<M_MR, CG>(a, s); break;
+    case M_J2: wagg_elem<M_J2, CG>(a, s); break;
+    case M_TI: wagg_elem<M_TI, CG>(a, s); break;
+    case M_FMR: wagg_elem<M_FMR, CG>(a, s); break;
+    default: wagg_elem<-1, CG>(a, s); break;
+  }
+  // the persistent node gather over the partial rows
+  MvArgs g = a;
+  g.m.node_row = a.wa.prow;
+  g.stage = a.wa.parts;
+  static const int ggrid = resident_grid(node_gather_persist_kernel<CG>, 256);
+  launch_chain(node_gather_persist_kernel<CG>, std::min(ggrid, nblk(a.m.n_nodes, kGatherNodes)), 256, 0, s, g);
 }
 
 void launch_node_gather(const MvArgs& a, cudaStream_t s) {

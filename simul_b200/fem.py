@@ -700,7 +700,8 @@ class StaticSolver:
 
     Same constructor and ``solve()`` contract.  Differences, by design:
     the tangent is the exact consistent tangent applied matrix-free and the
-    linear solve is Jacobi-PCG (FP32 vectors, FP64 dots) instead of assembled
+    linear solve is two-level PCG (Jacobi smoother plus a Galerkin coarse
+    correction on a trilinear lattice; FP32 vectors, FP64 dots) instead of assembled
     initial-C + geometric stiffness with SuperLU; prescribed DOFs are held
     exactly instead of by a 1e30 penalty; per-element materials act on the
     residual too; J2 history is committed once per converged ``solve()``.
@@ -713,7 +714,7 @@ class StaticSolver:
     def __init__(self, mesh: FEMesh, material: MaterialBase = None, use_newton: bool = True,
                  max_iterations: int = 50, tol: float = 1e-8,
                  materials: Optional[Dict[int, MaterialBase]] = None, linear_solver: str = "auto",
-                 line_search: str = "guarded", precond: str = "jacobi",
+                 line_search: str = "guarded", precond: str = "two_level",
                  cg_max_iterations: int = 20000, cg_rtol_min: float = 1e-5, cg_rtol_max: float = 1e-1):
         self.mesh = mesh
         self.materials = materials

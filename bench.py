@@ -69,8 +69,8 @@ def parse():
     ap.add_argument("--whole-solve-graph", type=int, default=1,
                     help="1: one graph launch per PCG solve; 0: fixed-size iteration graphs (for kernel profilers)")
     ap.add_argument("--pdl", type=int, default=1, help="programmatic dependent launches in the CG graphs")
-    ap.add_argument("--coarse-inverse", default="f32",
-                    choices=["f32", "f64", "trsm_syrk", "potri", "trsm_syrk_f32", "trsm_syrk_tf32"],
+    ap.add_argument("--coarse-inverse", default="tf32",
+                    choices=["f32", "f64", "tf32", "trsm_syrk", "potri", "trsm_syrk_f32", "trsm_syrk_tf32"],
                     help="precision of the coarse operator's Cholesky, triangular inverse and product")
     ap.add_argument("--coarse-max-nodes", type=int, default=6144, help="cap on the coarse lattice's nodes")
     ap.add_argument("--block-smoother", type=int, default=1,

@@ -209,8 +209,8 @@ enum {
   FEM_OPT_BLOCK_JACOBI = 10,
   /* two-level coarse inverse (the project's dense kernels: blocked Cholesky
    * L L^T, W = L^-1, the lower triangle of W^T W): 0 or 1 (default) in FP64,
-   * 2 or 3 in FP32 (enough for the FP32 or BF16 copy that is applied; the
-   * values name the library routines earlier versions chose between) */
+   * 2 in FP32 (enough for the FP32 or BF16 copy that is applied), 3 FP32
+   * Cholesky with W and W^T W on TF32 tensor-core tiles (tcgen05) */
   FEM_OPT_COARSE_INVERSE = 11,
   /* two-level: at most this many coarse nodes (default 4096, up to 16384);
    * the lattice cell grows by 25 % steps until the lattice fits */
@@ -282,9 +282,12 @@ int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t
  * backend/fea/fem/solver/static_solver.py:430-462).  A: n x n column-major
  * device array (FP64, lower
  * triangle read); out: n x n column-major device array receiving the lower
- * triangle of A^-1; precision 32 (FP32 arithmetic) or 64.  Blocked Cholesky
- * A = L L^T, W = L^-1, A^-1 = W^T W on the project's tile kernels.
- * FEM_ERR_NAN if a pivot is not positive.  Allocates its work space.
+ * triangle of A^-1; precision 64, 32 (FP32 arithmetic) or 19 (FP32
+ * Cholesky, then W and W^T W on TF32 tensor-core tiles: tcgen05.mma
+ * kind::tf32, operands rounded to a 10-bit mantissa, FP32 sums).  Blocked
+ * Cholesky A = L L^T, W = L^-1, A^-1 = W^T W on the project's tile kernels.
+ * FEM_ERR_NAN if a pivot is not positive, FEM_ERR_BUDGET if a tensor-core
+ * completion wait timed out.  Allocates its work space.
  * Errors: fem_last_error(NULL). */
 int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream);
 

@@ -1536,13 +1536,18 @@ int ensure_coarse(FemCtx* c) {
   } else {
     float* A = static_cast<float*>(c->dense_work);
     float* out = A + 2 * N * N;
-    de = dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl);
+    de = c->coarse_inverse == 3 ? dense_spd_inverse_tf32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl)
+                                : dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl);
     c->cdev.Ac32 = out;
   }
   if (de != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "dense inverse: %s", cudaGetErrorString(de));
   c->n_launches += nl;
   CK(cudaMemcpyAsync(c->h_info, c->dense_info, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (*c->h_info < 0) {
+    c->cdev.Ac32 = nullptr;
+    return set_err(c, FEM_ERR_BUDGET, "coarse inverse: a tensor-core completion wait timed out");
+  }
   if (*c->h_info != 0) {
     c->cdev.Ac32 = nullptr;
     return keep_previous_coarse(c, *c->h_info);

@@ -4,20 +4,21 @@
 // is a whole number of tiles (the padding is the identity, so L and W are
 // block diagonal there and no kernel handles a ragged edge).
 //
-//   factor, for k = 0 .. nt - 1:
+//   factor, for k = 0 .. nt - 1 (main stream):
 //     dense_diag_kernel    one CTA: L_kk = chol(A_kk) in shared memory and its
 //                          inverse W_kk = L_kk^-1 (a pivot <= 0 records its
 //                          column in *info and the factorisation continues
 //                          with a unit pivot, so every launch completes)
 //     dense_panel_kernel   L_ik = A_ik W_kk^T, i > k
 //     dense_update_kernel  A_ij -= L_ik L_jk^T, k < j <= i
-//   invert, right-looking, for k = 0 .. nt - 1:
+//   invert, right-looking, step k on a second stream once panel k is done:
 //     dense_wfin_kernel    W_kj = W_kk R_kj, j < k (R: the accumulated row)
 //     dense_wupd_kernel    R_ij -= L_ik W_kj, i > k, j <= k
-//   product:
-//     dense_syrk_kernel    (A^-1)_ij = sum_{l>=i} W_li^T W_lj, i >= j
+//   product (after both streams):
+//     dense_syrk_kernel    (A^-1)_ij = sum_{l>=i} W_li^T W_lj, i >= j, or
+//     dense_syrk_tc_kernel the same on TF32 tensor cores (tcgen05)
 //
-// The tile products run on a SIMT micro-kernel: 256 threads, each an
+// The SIMT tile products run on a micro-kernel: 256 threads, each an
 // (B/16) x (B/16) block of the output tile, operands staged in shared memory
 // in chunks of kKC of the inner dimension.  These replace the cuSOLVER
 // potrf / potri and cuBLAS trsm / syrk calls the coarse set-up made before.
@@ -25,9 +26,11 @@
 
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "../../include/femb200.h"
 #include "fem_internal.h"
+#include "fem_umma.cuh"
 
 namespace femb200 {
 
@@ -405,11 +408,125 @@ __global__ void __launch_bounds__(kDenseThreads) dense_syrk_kernel(const T* W, i
     }
 }
 
+// ───────────── tensor-core (tcgen05, TF32) product W^T W ─────────────
+// One 128 x 128 FP32 output tile per CTA of 128 threads,
+//   acc(r, c) = sum_k Aop(r, k) Bop(c, k),
+// over K in chunks of kTcKC = 32.  All threads stage a chunk's two operands
+// in shared memory (two buffers); thread 0 issues four
+// tcgen05.mma.cta_group::1.kind::tf32 (M = N = 128, K = 8) into a 128-column
+// TMEM accumulator and commits them to the buffer's mbarrier, which every
+// thread waits on (bounded) before it refills that buffer, so staging the
+// next chunk overlaps the MMAs of the current one.  Both operands are
+// k-contiguous in global memory and staged K-major (tc_stage).  The epilogue
+// reads the accumulator row by row (thread t owns row t) and writes
+// column-major tiles in coalesced 128-byte column pieces.  The operands are rounded to TF32 (10-bit mantissa) by the
+// tensor core; the sums are FP32.  A completion wait that gives up sets
+// *info = -1, waits once more (bounded) for the MMAs in flight, frees the
+// TMEM columns and returns.
+constexpr int kTcKC = 32;
+constexpr int kTcOpBytes = 128 * kTcKC * 4;  // one staged operand chunk: 16 KB
+constexpr int kTcSmem = 4 * kTcOpBytes;      // two buffers of (A, B)
+constexpr int kTcPolls = 1 << 22;
+
+// Stages k0 .. k0 + kTcKC - 1 of a 128-row operand whose element (m, k) is
+// at p[m ld + k], in the K-major canonical layout (16-byte k-quads of 8-row
+// core matrices, k-quads 128 B apart, 8-row groups 1024 B apart): one 16-byte
+// load and one 16-byte store per k-quad; each warp's 32 stores fill four
+// 128-byte runs, one per 8-row group, so no bank conflicts.
+__device__ __forceinline__ void tc_stage(const float* __restrict__ p, int ld, int k0, unsigned char* s) {
+#pragma unroll 2
+  for (int q = (int)threadIdx.x; q < 128 * kTcKC / 4; q += 128) {
+    const int mr = q & 7, kq = (q >> 3) & 7, m = (q >> 6) * 8 + mr;
+    const float4 v = __ldcg(reinterpret_cast<const float4*>(p + (size_t)m * ld + k0 + kq * 4));
+    *reinterpret_cast<float4*>(s + (m >> 3) * 1024 + kq * 128 + mr * 16) = v;
+  }
+}
+
+// Grid nt(nt+1)/2: the lower tile (i, j) of W^T W, (W^T W)_ij =
+// sum_{l >= i} W_li^T W_lj, into out (n x n column-major, TO).
+template <typename TO>
+__global__ void __launch_bounds__(128) dense_syrk_tc_kernel(const float* __restrict__ W, int N, int nt, TO* out,
+                                                            int n, int* info) {
+  extern __shared__ __align__(1024) unsigned char s_tc[];
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  constexpr int B = 128;
+  const int tid = (int)threadIdx.x, warp = tid >> 5;
+  int ti, tj;
+  dense_tri((int)blockIdx.x, ti, tj);
+  const int nch = (nt - ti) * (B / kTcKC);
+  if (warp == 0) umma::tmem_alloc(&tmem_base, 128);
+  if (tid == 0) {
+    umma::mbar_init(&mbar[0], 1);
+    umma::mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tb = tmem_base;
+  constexpr uint32_t idesc = umma::idesc_tf32(128, 128, false, false);
+  bool ok = true;
+  int issued = 0;
+  for (int ch = 0; ch < nch; ++ch) {
+    const int b = ch & 1;
+    unsigned char* sA = s_tc + b * 2 * kTcOpBytes;
+    unsigned char* sB = sA + kTcOpBytes;
+    // the MMAs that read this buffer two chunks ago must be done
+    if (ch >= 2 && ok) ok = umma::mbar_wait(&mbar[b], (uint32_t)(((ch - 2) >> 1) & 1), kTcPolls);
+    const int l = ti + ch / (B / kTcKC), k0 = (ch % (B / kTcKC)) * kTcKC;
+    if (ok) {
+      tc_stage(W + (size_t)ti * B * N + (size_t)l * B, N, k0, sA);  // W_li(q, r) at [r N + q]
+      tc_stage(W + (size_t)tj * B * N + (size_t)l * B, N, k0, sB);  // W_lj(q, c) at [c N + q]
+    }
+    umma::fence_async_smem();
+    umma::fence_before_sync();
+    ok = __syncthreads_and(ok) != 0;
+    umma::fence_after_sync();
+    if (!ok) break;
+    if (tid == 0) {
+      const uint32_t a0 = umma::smem_u32(sA), b0 = umma::smem_u32(sB);
+#pragma unroll
+      for (int st = 0; st < kTcKC / 8; ++st) {
+        const uint64_t ad = umma::smem_desc_lbo_sbo(a0 + 256 * st, 128, 1024);
+        const uint64_t bd = umma::smem_desc_lbo_sbo(b0 + 256 * st, 128, 1024);
+        umma::mma_tf32(tb, ad, bd, idesc, (ch > 0 || st > 0) ? 1u : 0u);
+      }
+      umma::commit(&mbar[b]);
+    }
+    ++issued;
+  }
+  if (ok && issued > 0) ok = umma::mbar_wait(&mbar[(issued - 1) & 1], (uint32_t)(((issued - 1) >> 1) & 1), kTcPolls);
+  ok = __syncthreads_and(ok) != 0;
+  umma::fence_after_sync();
+  if (ok) {
+    const int r = tid;  // TMEM lane = accumulator row
+#pragma unroll 1
+    for (int c0 = 0; c0 < B; c0 += 16) {
+      float v[16];
+      umma::tmem_ld16(umma::taddr(tb, 32 * warp, c0), v);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int gr = ti * B + r, gc = tj * B + c0 + q;
+        if (gr < n && gc < n) out[(size_t)gc * n + gr] = (TO)v[q];
+      }
+    }
+  } else {
+    if (tid == 0) atomicExch(info, -1);
+    if (issued > 0) umma::drain_mma(&mbar[(issued - 1) & 1], (uint32_t)(((issued - 1) >> 1) & 1), false, kTcPolls);
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) umma::tmem_free(tb, 128);
+}
+
 static inline int dense_nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
 
 int dense_tile(bool fp64) { return fp64 ? DenseCfg<double>::B : DenseCfg<float>::B; }
 
-template <typename T, typename TO>
+// TC (FP32 only): the inverse's triangular-inverse and product steps on the
+// TF32 tensor-core tile kernel instead of the SIMT one.
+template <typename T, typename TO, bool TC = false>
 static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* info, TO* out, cudaStream_t s,
                                    int* launches) {
   constexpr int B = DenseCfg<T>::B;
@@ -423,28 +540,62 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
   int nl = 0;
   dense_pad_kernel<T><<<dense_nblk((size_t)N * N, 256), 256, 0, s>>>(Ac, n, A, W, N);
   ++nl;
+  // W = L^-1 runs right-looking on a second stream, step k as soon as panel k
+  // is done (it reads L's column k, W_kk and the rows of W its earlier steps
+  // wrote; the trailing update k writes only columns > k), so it overlaps the
+  // factorisation's later diagonal and update kernels.  Its products have an
+  // inner dimension of one tile (128), too short for the tensor-core
+  // kernel's staging to pay (measured slower), so they stay on the SIMT
+  // tiles; the product W^T W sums over whole tile columns and runs on the
+  // TF32 tensor cores when TC is set.
+  cudaStream_t side = nullptr;
+  std::vector<cudaEvent_t> ev((size_t)nt + 1, nullptr);
+  auto release = [&]() {
+    for (cudaEvent_t x : ev)
+      if (x) cudaEventDestroy(x);
+    if (side) cudaStreamDestroy(side);
+  };
+  if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess) {
+    release();
+    return e;
+  }
+  for (auto& x : ev)
+    if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) {
+      release();
+      return e;
+    }
   for (int k = 0; k < nt; ++k) {
     dense_diag_kernel<T><<<1, kDenseThreads, diag_smem, s>>>(A, W, N, k, info);
     ++nl;
     const int m = nt - k - 1;
     if (m > 0) {
       dense_panel_kernel<T><<<m, kDenseThreads, 0, s>>>(A, W, N, k);
+      ++nl;
+    }
+    cudaEventRecord(ev[k], s);
+    cudaStreamWaitEvent(side, ev[k], 0);
+    if (k > 0) {
+      dense_wfin_kernel<T><<<k, kDenseThreads, 0, side>>>(W, N, k);
+      ++nl;
+    }
+    if (m > 0) {
+      dense_wupd_kernel<T><<<m * (k + 1), kDenseThreads, 0, side>>>(A, W, N, k);
       dense_update_kernel<T><<<m * (m + 1) / 2, kDenseThreads, 0, s>>>(A, N, k);
       nl += 2;
     }
   }
-  for (int kk = 0; kk < nt; ++kk) {
-    if (kk > 0) {
-      dense_wfin_kernel<T><<<kk, kDenseThreads, 0, s>>>(W, N, kk);
-      ++nl;
-    }
-    if (kk + 1 < nt) {
-      dense_wupd_kernel<T><<<(nt - kk - 1) * (kk + 1), kDenseThreads, 0, s>>>(A, W, N, kk);
-      ++nl;
-    }
+  cudaEventRecord(ev[nt], side);
+  cudaStreamWaitEvent(s, ev[nt], 0);
+  if constexpr (TC) {
+    static_assert(sizeof(T) == 4 && B == 128, "the tensor-core product takes FP32 128-wide tiles");
+    raise_smem_limit_k(dense_syrk_tc_kernel<TO>);
+    dense_syrk_tc_kernel<TO><<<nt * (nt + 1) / 2, 128, kTcSmem, s>>>(W, N, nt, out, n, info);
+    ++nl;
+  } else {
+    dense_syrk_kernel<T, TO><<<nt * (nt + 1) / 2, kDenseThreads, 0, s>>>(W, N, nt, out, n);
+    ++nl;
   }
-  dense_syrk_kernel<T, TO><<<nt * (nt + 1) / 2, kDenseThreads, 0, s>>>(W, N, nt, out, n);
-  ++nl;
+  release();
   if (launches) *launches += nl;
   return cudaGetLastError();
 }
@@ -452,6 +603,11 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
 cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
                                   cudaStream_t s, int* launches) {
   return dense_inverse_t<float, float>(Ac, n, A, W, info, out, s, launches);
+}
+
+cudaError_t dense_spd_inverse_tf32(const double* Ac, int n, float* A, float* W, int* info, float* out,
+                                   cudaStream_t s, int* launches) {
+  return dense_inverse_t<float, float, true>(Ac, n, A, W, info, out, s, launches);
 }
 
 cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
@@ -466,8 +622,8 @@ using namespace femb200;
 extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream) {
   if (!A || !out) return set_global_error(FEM_ERR_INVALID, "null matrix");
   if (n < 1 || n > 32768) return set_global_error(FEM_ERR_INVALID, "n = %d not in [1, 32768]", n);
-  if (precision != 32 && precision != 64)
-    return set_global_error(FEM_ERR_INVALID, "precision %d: 32 or 64", precision);
+  if (precision != 32 && precision != 64 && precision != 19)
+    return set_global_error(FEM_ERR_INVALID, "precision %d: 64, 32 or 19 (TF32 tensor cores)", precision);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool f64 = precision == 64;
   const int B = dense_tile(f64);
@@ -483,6 +639,9 @@ extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precisi
   }
   cudaError_t e = f64 ? dense_inverse_t<double, double>(A, n, static_cast<double*>(wa), static_cast<double*>(ww),
                                                           info, out, s, nullptr)
+                  : precision == 19
+                      ? dense_inverse_t<float, double, true>(A, n, static_cast<float*>(wa), static_cast<float*>(ww),
+                                                             info, out, s, nullptr)
                       : dense_inverse_t<float, double>(A, n, static_cast<float*>(wa), static_cast<float*>(ww), info,
                                                          out, s, nullptr);
   int h_info = 0;
@@ -492,6 +651,7 @@ extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precisi
   cudaFree(ww);
   cudaFree(info);
   if (e != cudaSuccess) return set_global_error(FEM_ERR_CUDA, "dense inverse: %s", cudaGetErrorString(e));
+  if (h_info < 0) return set_global_error(FEM_ERR_BUDGET, "dense inverse: a tensor-core completion wait timed out");
   if (h_info != 0)
     return set_global_error(FEM_ERR_NAN, "matrix is not positive definite (pivot %d is not positive)", h_info);
   return FEM_OK;

@@ -354,6 +354,10 @@ inline void raise_smem_limit_k(K kernel) {
 int dense_tile(bool fp64);
 cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
                                   cudaStream_t s, int* launches);
+// FP32 Cholesky, then W = L^-1 and W^T W on TF32 tensor-core tiles (tcgen05);
+// *info = -1 if a tensor-core completion wait timed out
+cudaError_t dense_spd_inverse_tf32(const double* Ac, int n, float* A, float* W, int* info, float* out,
+                                   cudaStream_t s, int* launches);
 cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
                                   cudaStream_t s, int* launches);
 

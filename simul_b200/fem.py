@@ -181,14 +181,17 @@ class FEMesh:
         state - after a history reset, materials or constraint change; k >= 1:
         every k PCG solves), whether the coarse inverse is stored in BF16, and the
         precision its Cholesky, triangular inverse and product run in ("f64",
-        "f32"; the older names "potri" / "trsm_syrk" mean "f64" and
-        "trsm_syrk_f32" / "trsm_syrk_tf32" mean "f32")."""
+        "f32", or "tf32": FP32 Cholesky with the triangular inverse and the
+        product on TF32 tensor-core tiles; the older names "potri" /
+        "trsm_syrk" mean "f64", "trsm_syrk_f32" means "f32" and
+        "trsm_syrk_tf32" means "tf32")."""
         lib = _lib.load()
         if max_nodes is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_MAX_NODES, int(max_nodes)), self.ctx,
                    "fem_set_option")
         if inverse is not None:
-            code = {"potri": 0, "trsm_syrk": 1, "trsm_syrk_f32": 2, "trsm_syrk_tf32": 3, "f64": 1, "f32": 2}[inverse]
+            code = {"potri": 0, "trsm_syrk": 1, "trsm_syrk_f32": 2, "trsm_syrk_tf32": 3, "f64": 1, "f32": 2,
+                    "tf32": 3}[inverse]
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_INVERSE, code), self.ctx, "fem_set_option")
         if bf16 is not None:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_COARSE_BF16, 1 if bf16 else 0), self.ctx,

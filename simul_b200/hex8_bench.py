@@ -35,7 +35,7 @@ def run(n=64, precond="two_level", load_steps=20, tol=1e-8, warmup=1, steps=3, c
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     mesh = B.FEMesh(v.n_nodes, v.n_elements, B.ElementType.HEX8, device=dev)
     mesh.initialize_from_numpy(v.X, v.conn)
-    mesh.set_coarse_options(cell=coarse_cell, bf16=True, reuse=0, inverse="f32", max_nodes=6144)
+    mesh.set_coarse_options(cell=coarse_cell, bf16=True, reuse=0, inverse="tf32", max_nodes=6144)
     mesh.set_whole_solve_graph(bool(whole_solve_graph))
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=tol, precond=precond)

@@ -49,6 +49,8 @@ def main(argv=None):
                     help="coarse operator: 0 once per state, -1 adaptive refresh, k every k PCG solves")
     ap.add_argument("--recurrence", type=int, default=1, help="two-level CG direction by recurrence")
     ap.add_argument("--block-smoother", type=int, default=1, help="two-level nodal block smoother")
+    ap.add_argument("--cases", nargs="+", default=list(CASES), choices=list(CASES),
+                    help="moment cases solved as one batch")
     args = ap.parse_args(argv)
     from simul_b200 import batch, meshgen
     import torch
@@ -61,7 +63,7 @@ def main(argv=None):
     t0 = time.perf_counter()
     insts = [batch.BatchInstance(ms.X, ms.conn, materials(ms.E), ms.fixed_mask, None,
                                  meshgen.top_moment_forces(ms.X, top, case, args.moment), device=dev,
-                                 material_ids=ids, coarse_cell=args.coarse_cell) for case in CASES]
+                                 material_ids=ids, coarse_cell=args.coarse_cell) for case in args.cases]
     for inst in insts:
         inst.mesh.set_coarse_options(reuse=args.coarse_reuse)
         inst.mesh.set_direction_recurrence(bool(args.recurrence))
@@ -83,7 +85,7 @@ def main(argv=None):
            "direction_recurrence": bool(args.recurrence), "block_smoother": bool(args.block_smoother),
            "host_generation_s": t_gen, "host_setup_s": t_setup,
            "cases": {}}
-    for case, inst, r in zip(CASES, insts, out["instances"]):
+    for case, inst, r in zip(args.cases, insts, out["instances"]):
         u = inst.mesh.u.cpu().numpy()
         res["cases"][case] = {**r, "max_u_mm": float(np.abs(u).max()),
                               "top_mean_u_mm": u[top].mean(axis=0).round(6).tolist()}

@@ -29,7 +29,7 @@ def _run(A, precision, cuda):
 
 
 @pytest.mark.parametrize("n", [1, 37, 64, 127, 128, 200, 513])
-@pytest.mark.parametrize("precision,tol", [(64, 1e-11), (32, 2e-4)])
+@pytest.mark.parametrize("precision,tol", [(64, 1e-11), (32, 2e-4), (19, 5e-2)])
 def test_dense_spd_inverse_matches_numpy(cuda, n, precision, tol):
     A = _spd(n, seed=n)
     rc, X = _run(A, precision, cuda)
@@ -43,6 +43,23 @@ def test_dense_spd_inverse_matches_numpy(cuda, n, precision, tol):
     up = ~lo & ~np.isnan(X)
     if up.any():
         assert np.abs(X[up] - ref[up]).max() / np.abs(ref).max() < tol
+
+
+@pytest.mark.parametrize("n", [128, 300, 1000])
+def test_tf32_tensor_core_inverse_on_well_conditioned_matrices(cuda, n):
+    """Precision 19 forms W = L^-1 and W^T W on TF32 tcgen05 tiles: on a
+    matrix of condition 10 the result is within TF32 rounding of the FP64
+    inverse (a wrong operand layout would give O(1) errors), and as a
+    preconditioner its eigenvalues stay within 1 +- 1e-2."""
+    A = _spd(n, seed=100 + n, cond=10.0)
+    rc, X = _run(A, 19, cuda)
+    assert rc == 0, _lib.last_error()
+    ref = np.linalg.inv(A)
+    lo = np.tril(np.ones((n, n), dtype=bool))
+    assert np.abs(X[lo] - ref[lo]).max() / np.abs(ref).max() < 5e-3
+    Xs = np.tril(X) + np.tril(X, -1).T
+    ev = np.linalg.eigvals(Xs @ A).real
+    assert ev.min() > 0.99 and ev.max() < 1.01, (ev.min(), ev.max())
 
 
 def test_dense_spd_inverse_rejects_indefinite(cuda):

@@ -217,7 +217,12 @@ enum {
   FEM_OPT_COARSE_MAX_NODES = 12,
   /* element-block matvec: elements per block (one thread each), 256, 512,
    * 768 or 1024; 0 (default) times the four and keeps the fastest */
-  FEM_OPT_EB_SIZE = 13
+  FEM_OPT_EB_SIZE = 13,
+  /* TET4 FP64 residual: 1 (default) two-phase (one thread per element
+   * writing its slot forces in node-slot order, then a node gather), 0 the
+   * fused node-block kernel (elements shared by node blocks evaluated in
+   * each) */
+  FEM_OPT_RESIDUAL_TWO_PHASE = 14
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

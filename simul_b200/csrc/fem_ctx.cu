@@ -47,7 +47,8 @@ struct FemCtx {
   int npe = 4;                 // nodes per element: 4 TET4, 8 HEX8
   int ngp = 1;                 // Gauss points per element: 1 TET4, 8 HEX8
   size_t Nq = 0;               // integration points Ne * ngp (payload and J2 history rows)
-  double* stage_d = nullptr;   // HEX8 residual: element slot forces in node_slots order
+  double* stage_d = nullptr;   // two-phase FP64 residual: element slot forces in node_slots order
+  bool res_two_phase = true;   // TET4: two-phase FP64 residual (else the fused node-block kernel)
   int ndof = 0, ndof_pad = 0;
   int64_t blk_entries = 0;
   size_t bytes = 0;
@@ -557,7 +558,7 @@ int alloc_state(FemCtx* c) {
   if ((st = dalloc(c, &c->boff, nf))) return st;
   // slot vectors of the two-phase passes; HEX8 diagonal blocks take 2 per slot
   if ((st = dalloc(c, &c->stage, c->npe == 8 ? 16 * Ne : 4 * Ne))) return st;
-  if (c->npe == 8 && (st = dalloc(c, &c->stage_d, 24 * Ne))) return st;
+  if ((st = dalloc(c, &c->stage_d, (c->npe == 8 ? 24 : 12) * Ne))) return st;
   if ((st = dalloc(c, &c->matD, (size_t)FEM_MAX_MATERIALS))) return st;
   if ((st = dalloc(c, &c->matF, (size_t)FEM_MAX_MATERIALS))) return st;
   // every reducing kernel's grid must fit: node blocks and node-parallel blocks
@@ -882,7 +883,7 @@ int eval_residual(FemCtx* c, double* fneg_out_int, double* rnorm2) {
   a.rnorm2 = c->scalars;
   a.red = c->red();
   a.red_site = SITE_RES;
-  a.stage_d = c->stage_d;
+  a.stage_d = (c->npe == 8 || c->res_two_phase) ? c->stage_d : nullptr;
   c->n_launches += c->npe == 8 ? 2 : 1;
   launch_residual(a, c->model_kind, c->stream);
   CKL();
@@ -2046,6 +2047,10 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       c->mv_variant = value >= 0 ? (int)value : MV_FUSED;
       c->mv_tuned = false;
       return FEM_OK;
+    case FEM_OPT_RESIDUAL_TWO_PHASE:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "residual variant flag must be 0 or 1");
+      c->res_two_phase = value != 0;
+      return FEM_OK;
     case FEM_OPT_EB_SIZE:
       if (value != 0 && value != 256 && value != 512 && value != 768 && value != 1024)
         return set_err(c, FEM_ERR_INVALID, "element block size %lld: 0 (timed), 256, 512, 768 or 1024",
@@ -2917,7 +2922,7 @@ int fem_profile_kernels(void* ctx, int32_t reps, double* ms_out) {
   ra.rnorm2 = c->scalars + 2;
   ra.red = c->red();
   ra.red_site = SITE_RES;
-  ra.stage_d = c->stage_d;
+  ra.stage_d = (c->npe == 8 || c->res_two_phase) ? c->stage_d : nullptr;
   for (int k = 0; k < 4; ++k) {
     CK(reset_cg());
     for (int w = 0; w < 2; ++w) {

@@ -77,6 +77,65 @@ __device__ __forceinline__ void gather_chunk_w(const uint32_t* s_slots, const fl
 
 // ───────────────────────── residual (FP64) ─────────────────────────
 
+// Element e's four slot forces (FP64, the negative internal force of its
+// vertices) from u; with write_state also its tangent payload and J2 trial
+// history.
+template <int MODEL>
+__device__ __forceinline__ void res_element(const ResArgs& a, int e, bool write_state, double f[4][3]) {
+  const MeshDev& m = a.m;
+  const int4 cn = __ldg(m.conn + e);
+  const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
+  double xv[4][3], uv[4][3];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      xv[k][d] = __ldg(m.X64 + 3 * nid[k] + d);
+      uv[k][d] = __ldg(a.u + 3 * nid[k] + d);
+    }
+  TetGeom<double> g;
+  tet_geom(xv[0], xv[1], xv[2], xv[3], g);
+  double D[3][3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) D[k][d] = uv[k + 1][d] - uv[0][d];
+  double Hg[9];
+  grad_from_diffs(D, g, Hg);
+  const DevMat<double>& mat = a.matD[__ldg(m.mat_id + e)];
+  const double scale = (double)__ldg(m.scale + e);
+  const int model = MODEL >= 0 ? MODEL : mat.model;
+  double S[9];
+  float pay[kPay];
+  if (model == M_NH) {
+    nh_stress(mat, scale, Hg, S, pay);
+  } else if (model == M_MR || model == M_FMR) {
+    mr_stress(mat, scale, Hg, S, pay);
+  } else if (model == M_J2) {
+    double ep[6], epn[6], epe_n;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ep[k] = a.ep_c[(size_t)k * m.n_elems + e];
+    const double epe = a.epe_c[e];
+    j2_stress(mat, scale, Hg, ep, epe, S, epn, epe_n, pay);
+    if (write_state) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) a.ep_t[(size_t)k * m.n_elems + e] = epn[k];
+      a.epe_t[e] = epe_n;
+    }
+  } else if (model == M_TI) {
+    ti_stress(mat, scale, Hg, S);
+  } else {
+    le_stress(mat, scale, Hg, S);
+  }
+  if (write_state) {
+    const int npay = model_pay_words(model);
+#pragma unroll
+    for (int k = 0; k < kPay; ++k)
+      if (k < npay) a.payload[(size_t)k * m.n_elems + e] = pay[k];
+  }
+  slot_vectors(S, g, -g.s6, f);
+}
+
 template <int NB, int MODEL>
 __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ ResArgs a) {
   // dynamic: 12 x NB doubles of slot vectors, then the block's slot lists
@@ -98,59 +157,8 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
   for (int c0 = e0; c0 < e1; c0 += NB) {
     const int idx = c0 + tid;
     if (idx < e1) {
-      const int e = __ldg(m.blk_elems + idx);
-      const int4 cn = __ldg(m.conn + e);
-      const int nid[4] = {cn.x, cn.y, cn.z, cn.w};
-      double xv[4][3], uv[4][3];
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          xv[k][d] = __ldg(m.X64 + 3 * nid[k] + d);
-          uv[k][d] = __ldg(a.u + 3 * nid[k] + d);
-        }
-      TetGeom<double> g;
-      tet_geom(xv[0], xv[1], xv[2], xv[3], g);
-      double D[3][3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) D[k][d] = uv[k + 1][d] - uv[0][d];
-      double Hg[9];
-      grad_from_diffs(D, g, Hg);
-      const DevMat<double>& mat = a.matD[__ldg(m.mat_id + e)];
-      const double scale = (double)__ldg(m.scale + e);
-      const int model = MODEL >= 0 ? MODEL : mat.model;
-      double S[9];
-      float pay[kPay];
-      if (model == M_NH) {
-        nh_stress(mat, scale, Hg, S, pay);
-      } else if (model == M_MR || model == M_FMR) {
-        mr_stress(mat, scale, Hg, S, pay);
-      } else if (model == M_J2) {
-        double ep[6], epn[6], epe_n;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) ep[k] = a.ep_c[(size_t)k * m.n_elems + e];
-        const double epe = a.epe_c[e];
-        j2_stress(mat, scale, Hg, ep, epe, S, epn, epe_n, pay);
-        if (idx < home_end) {
-#pragma unroll
-          for (int k = 0; k < 6; ++k) a.ep_t[(size_t)k * m.n_elems + e] = epn[k];
-          a.epe_t[e] = epe_n;
-        }
-      } else if (model == M_TI) {
-        ti_stress(mat, scale, Hg, S);
-      } else {
-        le_stress(mat, scale, Hg, S);
-      }
-      if (idx < home_end) {
-        const int npay = model_pay_words(model);
-#pragma unroll
-        for (int k = 0; k < kPay; ++k)
-          if (k < npay) a.payload[(size_t)k * m.n_elems + e] = pay[k];
-      }
       double f[4][3];
-      slot_vectors(S, g, -g.s6, f);
+      res_element<MODEL>(a, __ldg(m.blk_elems + idx), idx < home_end, f);
 #pragma unroll
       for (int s = 0; s < 4; ++s)
 #pragma unroll
@@ -181,6 +189,29 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
       a.red.counters[a.red_site] = 0u;
     }
   }
+}
+
+// Two-phase FP64 residual.  res_elem_kernel: one thread per element, each
+// element evaluated once (the fused node-block kernel above evaluates an
+// element shared by several node blocks in each of them), its four slot
+// forces stored at their positions in node-slot order (stage_d, three doubles
+// per slot).  res_gather_kernel: kGatherLanes lanes per node add the node's
+// contiguous slot range (lane k: slots k, k + kGatherLanes, ...; then xor
+// steps in a fixed order), R = f_ext + f on free DOFs and the fixed-order
+// FP64 sum of ||R||^2.  Bitwise reproducible; the node sums are associated
+// differently from the fused kernel's (agreement to rounding).
+template <int MODEL>
+__global__ void __launch_bounds__(128) res_elem_kernel(const __grid_constant__ ResArgs a) {
+  const int e = (int)blockIdx.x * 128 + (int)threadIdx.x;
+  if (e >= a.m.n_elems) return;
+  double f[4][3];
+  res_element<MODEL>(a, e, true, f);
+  const int4 sp = __ldg(a.m.spos + e);
+  const int pos[4] = {sp.x, sp.y, sp.z, sp.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) __stcg(a.stage_d + 3 * (size_t)pos[k] + d, f[k][d]);
 }
 
 // ───────────────────────── tangent matvec (FP32) ─────────────────────────
@@ -655,6 +686,45 @@ __global__ void __launch_bounds__(256) node_gather_persist_kernel(const __grid_c
   if (CG) {
     chain_release();
     gather_finish(a, pap, sred, &am_last);
+  }
+}
+
+template <int LANES>
+__global__ void __launch_bounds__(256) res_gather_kernel(const __grid_constant__ ResArgs a) {
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  const MeshDev& m = a.m;
+  const int n = (int)(blockIdx.x * (256 / LANES) + threadIdx.x / LANES);
+  const int sub = (int)threadIdx.x % LANES;
+  double acc[3] = {0.0, 0.0, 0.0};
+  if (n < m.n_nodes) {
+    const int j0 = __ldg(m.node_row + n), j1 = __ldg(m.node_row + n + 1);
+    for (int j = j0 + sub; j < j1; j += LANES)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) acc[d] += __ldcg(a.stage_d + 3 * (size_t)j + d);
+  }
+#pragma unroll
+  for (int o = 1; o < LANES; o <<= 1)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) acc[d] += __shfl_xor_sync(0xffffffffu, acc[d], o);
+  double r2 = 0.0;
+  if (n < m.n_nodes && sub == 0) {
+    const uint8_t fx = m.fixed[n];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      if (a.fneg) a.fneg[3 * n + d] = acc[d];
+      const double r = ((fx >> d) & 1) ? 0.0 : a.f_ext[3 * n + d] + acc[d];
+      a.R[3 * n + d] = r;
+      r2 += r * r;
+    }
+  }
+  double bsum = block_sum<256>(r2, sred);
+  if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
+    double tot = final_sum<256>(a.red, a.red_site, 0, sred);
+    if (threadIdx.x == 0) {
+      *a.rnorm2 = tot;
+      a.red.counters[a.red_site] = 0u;
+    }
   }
 }
 
@@ -1154,9 +1224,27 @@ static void residual_nb(const ResArgs& a, int model, cudaStream_t s) {
   }
 }
 
+static void residual_two_phase(const ResArgs& a, int model, cudaStream_t s) {
+  const int ge = nblk(a.m.n_elems, 128);
+  switch (model) {
+    case M_LE: res_elem_kernel<M_LE><<<ge, 128, 0, s>>>(a); break;
+    case M_NH: res_elem_kernel<M_NH><<<ge, 128, 0, s>>>(a); break;
+    case M_MR: res_elem_kernel<M_MR><<<ge, 128, 0, s>>>(a); break;
+    case M_J2: res_elem_kernel<M_J2><<<ge, 128, 0, s>>>(a); break;
+    case M_TI: res_elem_kernel<M_TI><<<ge, 128, 0, s>>>(a); break;
+    case M_FMR: res_elem_kernel<M_FMR><<<ge, 128, 0, s>>>(a); break;
+    default: res_elem_kernel<-1><<<ge, 128, 0, s>>>(a); break;
+  }
+  res_gather_kernel<kGatherLanes><<<nblk(a.m.n_nodes, 256 / kGatherLanes), 256, 0, s>>>(a);
+}
+
 void launch_residual(const ResArgs& a, int model, cudaStream_t s) {
   if (a.m.npe == 8) {
     launch_residual_hex(a, model, s);
+    return;
+  }
+  if (a.stage_d) {
+    residual_two_phase(a, model, s);
     return;
   }
   switch (a.m.nb) {

@@ -249,6 +249,13 @@ class FEMesh:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_EB_SIZE, int(block_size)), self.ctx, "fem_set_option")
         _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_MATVEC_VARIANT, code), self.ctx, "fem_set_option")
 
+    def set_residual_variant(self, variant: str):
+        """TET4 FP64 residual: "two_phase" (default; one thread per element,
+        then a node gather) or "fused" (node-block kernel)."""
+        code = {"two_phase": 1, "fused": 0}[variant]
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_RESIDUAL_TWO_PHASE, code), self.ctx,
+               "fem_set_option")
+
     # ---- boundary conditions (core/mesh.py:321-399) ----
     def set_fixed_nodes(self, node_ids, values=None, dofs=None):
         node_ids = np.asarray(node_ids, dtype=np.int64)

@@ -33,6 +33,8 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--strain", type=float, default=0.004)
     ap.add_argument("--nodes-per-block", type=int, default=0)
+    ap.add_argument("--residual", default="two_phase", choices=["two_phase", "fused"],
+                    help="TET4 FP64 residual variant")
     ap.add_argument("--learned", default="", help="weights file: also run the network forward --reps times")
     ap.add_argument("--two-level", action="store_true", help="also run one two-level PCG solve (rtol 1e-6)")
     ap.add_argument("--coarse-cell", type=int, default=4, help="two-level: lattice cell edge in voxels")
@@ -50,6 +52,7 @@ def main(argv=None):
     mesh.initialize_from_numpy(v.X, v.conn)
     if args.element == "tet4":
         mesh.set_matvec_variant(args.variant, block_size=args.block_size if args.variant == "element_block" else None)
+        mesh.set_residual_variant(args.residual)
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     idx = np.where(v.fixed_mask.reshape(-1))[0]
     vals = (v.fixed_vals * (args.strain / 0.02)).reshape(-1)

@@ -435,7 +435,8 @@ __global__ void __launch_bounds__(kTileWarps * 32, 3) coarse_tile_mv_kernel(
     for (int k = 0; k < 16; ++k) {
       const int row = 4 * k + q;
       float a[8];
-      bf16x8_to_f32(__ldg(tile + row * (kTile / 8) + cg8), a);
+      // streamed once per product (evict-first), so the matvec's working set keeps the L2
+      bf16x8_to_f32(__ldcs(tile + row * (kTile / 8) + cg8), a);
       float s = 0.f;
 #pragma unroll
       for (int e = 0; e < 8; ++e) s += a[e] * xj[e];

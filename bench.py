@@ -229,10 +229,11 @@ def cpu_path(args, v, threads, steps=None, on_step=None):
 
 def reference_arm(args, rank, ws):
     """One bench step = one load step of the CPU restatement's load path, in
-    order from rest (J2 history carried); ``--steps`` equal to the number of
-    load steps times exactly one full path, more steps start the path again.
-    ``value`` = the mean load-step time times the number of load steps (for
-    ``--steps 20``: the measured time of one full 20-step path)."""
+    order from rest (J2 history carried).  At least one full path is timed:
+    with ``--steps`` below the number of load steps the whole path still
+    runs (one full solve is the metric's unit); more steps start the path
+    again.  ``value`` = the mean load-step time times the number of load
+    steps, i.e. the measured time of a full path."""
     if rank != 0:
         return
     v = build_inputs(args)
@@ -246,7 +247,8 @@ def reference_arm(args, rank, ws):
     del warm
     times, newton, cg, conv = [], 0, 0, True
     s = None
-    for i in range(args.steps):
+    n_timed = max(args.steps, args.load_steps)
+    for i in range(n_timed):
         k = i % args.load_steps + 1
         if k == 1:
             s = CpuSolver(v.X, v.conn, "j2", v.E, 0.3, sigma_y=100.0, H_ratio=0.02, threads=threads)
@@ -258,15 +260,12 @@ def reference_arm(args, rank, ws):
         conv &= info["converged"]
     per_step = float(np.mean(times))
     value = per_step * args.load_steps
-    full = args.steps >= args.load_steps
-    sample = (f"{args.steps} load steps timed one by one in path order from rest ({newton} Newton / {cg} CG "
-              f"iterations, all converged: {conv}); "
-              + (f"value = their mean x {args.load_steps}, i.e. the measured time of the full "
-                 f"{args.load_steps}-step path" if args.steps % args.load_steps == 0 else
-                 f"value = their mean x {args.load_steps}" + ("" if full else " (a partial path: the later, "
-                                                                                 "plastic steps cost more)")))
+    sample = (f"{n_timed} load steps timed one by one in path order from rest ({newton} Newton / {cg} CG "
+              f"iterations, all converged: {conv}); value = their mean x {args.load_steps}"
+              + (f", i.e. the measured time of the full {args.load_steps}-step path"
+                 if n_timed % args.load_steps == 0 else " (the last path partial)"))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
+            "steps": args.steps, "load_steps_timed": n_timed, "warmup": args.warmup, "ms_per_step": per_step * 1e3,
             "step": "one load step of the path (the metric's unit, one full solve, is load_steps of them)",
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),

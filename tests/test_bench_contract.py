@@ -26,3 +26,16 @@ def test_reference_arm_times_the_full_path():
     assert "measured time of the full 3-step path" in d["cpu_baseline"]["sample"]
     assert "all converged: True" in d["cpu_baseline"]["sample"]
     assert d["e2e"]["value"] == d["value"]
+
+
+@pytest.mark.timeout(600)
+def test_reference_arm_with_fewer_steps_still_times_a_full_path():
+    cmd = [sys.executable, "bench.py", "--impl", "reference", "--grid", "8", "--load-steps", "4",
+           "--steps", "2", "--warmup", "1", "--cpu-threads", "2"]
+    r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    d = json.loads([l for l in r.stdout.splitlines() if l.startswith("{")][-1])
+    assert d["steps"] == 2 and d["load_steps_timed"] == 4
+    assert "4 load steps timed" in d["cpu_baseline"]["sample"]
+    assert "measured time of the full 4-step path" in d["cpu_baseline"]["sample"]
+    assert d["value"] == pytest.approx(4 * d["ms_per_step"] / 1e3, rel=1e-12)

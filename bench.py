@@ -77,6 +77,8 @@ def parse():
                     help="two-level smoother: 1 nodal 3x3 block inverse, 0 diagonal inverse")
     ap.add_argument("--fused-step", type=int, default=0,
                     help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
+    ap.add_argument("--extrapolate", type=int, default=0,
+                    help="1: each load step's Newton starts from the last step's change of u repeated")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
     ap.add_argument("--cg-rtol-max", type=float, default=1e-1, help="inexact-Newton forcing term cap")
     ap.add_argument("--no-extras", action="store_true",
@@ -289,6 +291,7 @@ def configure(mesh, args):
     mesh.set_whole_solve_graph(bool(args.whole_solve_graph))
     mesh.set_programmatic_launch(bool(args.pdl))
     mesh.set_block_smoother(bool(args.block_smoother))
+    mesh.set_extrapolation(bool(args.extrapolate))
 
 
 def size_point(args, n, dev, jacobi=True):

@@ -222,7 +222,15 @@ enum {
    * writing its slot forces in node-slot order, then a node gather), 0 the
    * fused node-block kernel (elements shared by node blocks evaluated in
    * each) */
-  FEM_OPT_RESIDUAL_TWO_PHASE = 14
+  FEM_OPT_RESIDUAL_TWO_PHASE = 14,
+  /* load-step extrapolation, 0 (default) off, 1 on: a Newton solve that
+   * follows a converged one, with u unchanged since, starts from the last
+   * solve's end state plus its change of u (the step repeated) instead of
+   * carrying the new prescribed values by a first linear solve.  The
+   * relative residual is still measured against the reference's first
+   * residual (the previous u under the new loads).  A history reset or a
+   * non-converged solve starts the sequence again. */
+  FEM_OPT_EXTRAPOLATE = 15
 };
 int fem_set_option(void* ctx, int32_t key, int64_t value);
 /* Learned preconditioner (no reference counterpart).  A message-passing

@@ -50,6 +50,7 @@ FEM_OPT_COARSE_INVERSE = 11
 FEM_OPT_COARSE_MAX_NODES = 12
 FEM_OPT_EB_SIZE = 13
 FEM_OPT_RESIDUAL_TWO_PHASE = 14
+FEM_OPT_EXTRAPOLATE = 15
 MPNN_PARAMS = 34307
 MATVEC_VARIANTS = {0: "fused", 1: "two_phase", 2: "element_block", 3: "warp_agg", 4: "persistent"}
 

@@ -76,6 +76,13 @@ struct FemCtx {
   double* u = nullptr;
   double* u_base = nullptr;
   double* R = nullptr;
+  // load-step extrapolation (FEM_OPT_EXTRAPOLATE): the end state of the last
+  // converged solve, its change of u, and this solve's starting u
+  bool extrap = false;
+  bool extrap_ready = false;
+  double* u_last = nullptr;
+  double* du_last = nullptr;
+  double* u_start = nullptr;
   double* tmpd = nullptr;
   float* payload = nullptr;
   double* ep_c = nullptr;
@@ -341,6 +348,9 @@ void free_ctx(FemCtx* c) {
     if (ev) cudaEventDestroy(ev);
   if (c->stage) cudaFree(c->stage);
   if (c->stage_d) cudaFree(c->stage_d);
+  if (c->u_last) cudaFree(c->u_last);
+  if (c->du_last) cudaFree(c->du_last);
+  if (c->u_start) cudaFree(c->u_start);
   if (c->spos) cudaFree(c->spos);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
@@ -2047,6 +2057,11 @@ int fem_set_option(void* ctx, int32_t key, int64_t value) {
       c->mv_variant = value >= 0 ? (int)value : MV_FUSED;
       c->mv_tuned = false;
       return FEM_OK;
+    case FEM_OPT_EXTRAPOLATE:
+      if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "extrapolation flag must be 0 or 1");
+      c->extrap = value != 0;
+      c->extrap_ready = false;
+      return FEM_OK;
     case FEM_OPT_RESIDUAL_TWO_PHASE:
       if (value != 0 && value != 1) return set_err(c, FEM_ERR_INVALID, "residual variant flag must be 0 or 1");
       c->res_two_phase = value != 0;
@@ -2741,6 +2756,35 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     return set_err(c, FEM_ERR_INVALID, "unknown preconditioner %d", prm.precond);
   FemSolveResult out;
   std::memset(&out, 0, sizeof(out));
+  // Load-step extrapolation (FEM_OPT_EXTRAPOLATE): when the last solve
+  // converged and u is still its end state, Newton starts from u_last +
+  // du_last (the last step's change repeated) instead of carrying the
+  // prescribed-value change by a first linear solve.  Relative convergence
+  // is still measured against the residual of the state the reference
+  // evaluates first (below), so the stopping test and the converged
+  // equilibrium are the same.
+  bool extrap_now = false;
+  if (c->extrap) {
+    const size_t nd = (size_t)c->ndof_pad;
+    if (!c->u_last) {
+      if ((st = dalloc(c, &c->u_last, nd)) || (st = dalloc(c, &c->du_last, nd)) || (st = dalloc(c, &c->u_start, nd)))
+        return st;
+      c->extrap_ready = false;
+    }
+    if (c->extrap_ready) {
+      unsigned int* differ = reinterpret_cast<unsigned int*>(c->scalars + 6);
+      CK(cudaMemsetAsync(differ, 0, sizeof(unsigned int), c->stream));
+      ++c->n_launches; launch_differ(c->u, c->u_last, c->ndof, differ, c->stream);
+      CKL();
+      unsigned int h_differ = 1u;
+      CK(cudaMemcpyAsync(c->h_scalars + 6, differ, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      std::memcpy(&h_differ, c->h_scalars + 6, sizeof(unsigned int));
+      extrap_now = h_differ == 0u;
+    }
+    CK(cudaMemcpyAsync(c->u_start, c->u, nd * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    c->extrap_ready = false;
+  }
   // Change of the prescribed values in this solve.  It is carried by the first
   // Newton step (K_ff du_f = R - K_fc du_c): moving only the boundary nodes would
   // leave a one-element layer at large strain, which yields under J2 and stalls
@@ -2763,6 +2807,18 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     if ((st = eval_residual(c, nullptr, &r2))) return st;
     ref_norm = std::sqrt(r2);
     CK(cudaMemcpyAsync(c->u, c->u_base, c->ndof_pad * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    out.residual_evals = 1;
+  }
+  if (extrap_now) {
+    if (!has_dc) {
+      // the reference's first residual: the previous u under the new loads
+      if ((st = eval_residual(c, nullptr, &r2))) return st;
+      ref_norm = std::sqrt(r2);
+      out.residual_evals = 1;
+    }
+    ++c->n_launches; launch_extrap(c->u, c->u_last, c->du_last, c->ndof, c->stream);
+    CKL();
+  } else if (has_dc) {
     if ((st = eval_residual(c, nullptr, &r2))) return st;
     out.residual_evals = 2;
     if (!std::isfinite(ref_norm) || !std::isfinite(r2)) {
@@ -2875,6 +2931,11 @@ int fem_newton_solve(void* ctx, const FemSolveParams* prm_in, FemSolveResult* re
     CK(cudaMemcpyAsync(c->ep_c, c->ep_t, 6 * c->Nq * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaMemcpyAsync(c->epe_c, c->epe_t, c->Nq * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   }
+  if (c->extrap && converged && (!c->has_j2 || prm.auto_commit)) {
+    ++c->n_launches; launch_extrap_record(c->u, c->u_start, c->u_last, c->du_last, c->ndof, c->stream);
+    CKL();
+    c->extrap_ready = true;
+  }
   CK(cudaStreamSynchronize(c->stream));
   out.converged = converged ? 1 : 0;
   out.iterations = std::min(it + 1, prm.max_iterations);
@@ -2970,6 +3031,7 @@ int fem_reset_history(void* ctx) {
   CK(cudaMemsetAsync(c->epe_t, 0, c->Nq * sizeof(double), c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->tangent_valid = false;
+  c->extrap_ready = false;
   // back to rest: the coarse operator was built on a deformed, plastic
   // tangent; the next two-level solve assembles a fresh one
   invalidate_coarse(c);

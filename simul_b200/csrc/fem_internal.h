@@ -482,6 +482,11 @@ void launch_gather_mask(const uint8_t* in_user, uint8_t* out_int, const int* per
 void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, int n,
                      cudaStream_t s);
 // u[3n+d] = u_base[3n+d] + alpha du[4n+d] for n < n_nodes
+// load-step extrapolation (fem_newton_solve with FEM_OPT_EXTRAPOLATE)
+void launch_extrap(double* u, const double* u_last, const double* du_last, int n, cudaStream_t s);
+void launch_differ(const double* a, const double* b, int n, unsigned int* differ, cudaStream_t s);
+void launch_extrap_record(const double* u, const double* u_start, double* u_last, double* du_last, int n,
+                          cudaStream_t s);
 void launch_u_update(double* u, const double* u_base, const float* du, double alpha, int n_nodes,
                      cudaStream_t s);
 // out[i] = s in[i], i < n

@@ -1110,6 +1110,27 @@ __global__ void u_update_kernel(double* u, const double* u_base, const float* du
   u[3 * i + 2] = u_base[3 * i + 2] + alpha * (double)d.z;
 }
 
+// load-step extrapolation: u = u_last + du_last
+__global__ void extrap_kernel(double* u, const double* u_last, const double* du_last, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) u[i] = u_last[i] + du_last[i];
+}
+
+// *differ |= 1 where a and b differ
+__global__ void differ_kernel(const double* a, const double* b, int n, unsigned int* differ) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && a[i] != b[i]) atomicOr(differ, 1u);
+}
+
+// after a converged solve that started at u_start: du_last = u - u_start, u_last = u
+__global__ void extrap_record_kernel(const double* u, const double* u_start, double* u_last, double* du_last,
+                                     int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  du_last[i] = u[i] - u_start[i];
+  u_last[i] = u[i];
+}
+
 // float4-per-node <-> 3-per-node caller layout
 __global__ void gather_f4_kernel(const float* in_user, float* out_int, const int* perm, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1193,6 +1214,18 @@ __global__ void rhs_minus_kernel(const double* R, const float* y, const uint8_t*
 // ───────────────────────── launchers ─────────────────────────
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
+
+void launch_extrap(double* u, const double* u_last, const double* du_last, int n, cudaStream_t s) {
+  extrap_kernel<<<nblk(n, 256), 256, 0, s>>>(u, u_last, du_last, n);
+}
+void launch_differ(const double* a, const double* b, int n, unsigned int* differ, cudaStream_t s) {
+  differ_kernel<<<nblk(n, 256), 256, 0, s>>>(a, b, n, differ);
+}
+void launch_extrap_record(const double* u, const double* u_start, double* u_last, double* du_last, int n,
+                          cudaStream_t s) {
+  extrap_record_kernel<<<nblk(n, 256), 256, 0, s>>>(u, u_start, u_last, du_last, n);
+}
+
 
 // Every launch below raises its kernel's shared-memory limit to the device
 // maximum first (once per kernel; also before stream capture, in

@@ -249,6 +249,13 @@ class FEMesh:
             _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_EB_SIZE, int(block_size)), self.ctx, "fem_set_option")
         _check(lib.fem_set_option(self.ctx, _lib.FEM_OPT_MATVEC_VARIANT, code), self.ctx, "fem_set_option")
 
+    def set_extrapolation(self, on: bool):
+        """Load-step extrapolation: a solve that follows a converged one (u
+        unchanged since) starts from the last end state plus its change of u;
+        the convergence test is unchanged."""
+        _check(_lib.load().fem_set_option(self.ctx, _lib.FEM_OPT_EXTRAPOLATE, 1 if on else 0), self.ctx,
+               "fem_set_option")
+
     def set_residual_variant(self, variant: str):
         """TET4 FP64 residual: "two_phase" (default; one thread per element,
         then a node gather) or "fused" (node-block kernel)."""

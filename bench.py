@@ -77,8 +77,10 @@ def parse():
                     help="two-level smoother: 1 nodal 3x3 block inverse, 0 diagonal inverse")
     ap.add_argument("--fused-step", type=int, default=0,
                     help="1: CG work after each matvec as one cooperative kernel; 0: kernel chain")
-    ap.add_argument("--extrapolate", type=int, default=0,
-                    help="1: each load step's Newton starts from the last step's change of u repeated")
+    ap.add_argument("--extrapolate", type=int, default=1,
+                    help="1: each load step's Newton starts from the last step's change of u repeated "
+                         "(convergence test unchanged); 0: from the previous state, the change of the "
+                         "prescribed values carried by a first linear solve")
     ap.add_argument("--cg-rtol-min", type=float, default=1e-5, help="inexact-Newton forcing term floor")
     ap.add_argument("--cg-rtol-max", type=float, default=1e-1, help="inexact-Newton forcing term cap")
     ap.add_argument("--no-extras", action="store_true",

@@ -199,7 +199,7 @@ class ArcLengthSolver:
         lib = _lib.load()
         du = torch.zeros_like(b)
         it, rel = C.c_int32(), C.c_double()
-        rc = lib.fem_pcg(self.mesh.ctx, B._PC[self.precond], C.c_void_p(b.data_ptr()), C.c_void_p(du.data_ptr()),
+        rc = lib.fem_pcg(self.mesh.ctx, B._PC[self.precond], B._ptr(b), B._ptr(du),
                          float(self.cg_rtol), int(self.cg_max_iterations), C.byref(it), C.byref(rel))
         if rc not in (_lib.FEM_OK, _lib.FEM_NOT_CONVERGED):
             B._check(rc, self.mesh.ctx, "fem_pcg")

@@ -58,7 +58,7 @@ class BatchInstance:
         lib = _lib.load()
         self.mesh.u.zero_()
         torch.cuda.synchronize(self.mesh.device)
-        B._check(lib.fem_set_displacement(self.ctx, C.c_void_p(self.mesh.u.data_ptr())), self.ctx,
+        B._check(lib.fem_set_displacement(self.ctx, B._ptr(self.mesh.u)), self.ctx,
                  "fem_set_displacement")
         B._check(lib.fem_reset_history(self.ctx), self.ctx, "fem_reset_history")
 
@@ -92,6 +92,6 @@ def solve_batch(instances: Sequence[BatchInstance], load_steps: int = 10, precon
                     "newton_iterations": int(res[i].iterations), "cg_iterations": int(res[i].cg_iterations),
                     "relative_residual": float(res[i].relative_residual), "wall_ms": float(wall[i])})
     for inst in instances:
-        B._check(lib.fem_get_displacement(inst.ctx, C.c_void_p(inst.mesh.u.data_ptr())), inst.ctx,
+        B._check(lib.fem_get_displacement(inst.ctx, B._ptr(inst.mesh.u)), inst.ctx,
                  "fem_get_displacement")
     return {"instances": out}

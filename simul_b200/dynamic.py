@@ -110,7 +110,7 @@ class DynamicSolver:
         self._rest_tangent()
         xf = x.view(-1, 3).to(torch.float32).contiguous()
         y = torch.empty_like(xf)
-        B._check(_lib.load().fem_tangent_matvec(self.mesh.ctx, C.c_void_p(xf.data_ptr()), C.c_void_p(y.data_ptr())),
+        B._check(_lib.load().fem_tangent_matvec(self.mesh.ctx, B._ptr(xf), B._ptr(y)),
                  self.mesh.ctx, "fem_tangent_matvec")
         return y.reshape(-1).to(torch.float64)
 
@@ -261,7 +261,7 @@ class DynamicSolver:
             b = full(bf)
             x = torch.zeros_like(b)
             it, rel = C.c_int32(), C.c_double()
-            rc = lib.fem_pcg(self.mesh.ctx, B._PC[precond], C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()),
+            rc = lib.fem_pcg(self.mesh.ctx, B._PC[precond], B._ptr(b), B._ptr(x),
                              float(rtol), 20000, C.byref(it), C.byref(rel))
             if rc not in (_lib.FEM_OK, _lib.FEM_NOT_CONVERGED):
                 B._check(rc, self.mesh.ctx, "fem_pcg")

@@ -37,7 +37,17 @@ class ElementType(enum.Enum):
 
 
 def _ptr(t: Optional[torch.Tensor]):
-    return C.c_void_p(t.data_ptr()) if t is not None else None
+    """Device pointer of a tensor handed to the library.  The library works on
+    its context's stream, which is torch's current stream only when that is
+    a created (non-default) stream; otherwise (torch's default stream, or a
+    context that owns its stream) nothing orders torch's pending writes to
+    the tensor before the library reads it, so wait for them here.  The
+    library synchronises its stream before returning outputs."""
+    if t is None:
+        return None
+    if t.is_cuda:
+        torch.cuda.current_stream(t.device).synchronize()
+    return C.c_void_p(t.data_ptr())
 
 
 def _check(rc: int, ctx=None, what: str = ""):

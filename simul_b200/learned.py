@@ -22,6 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .fem import _ptr
 from .validation import FEAValidationError
 
 HIDDEN = 64
@@ -105,7 +106,7 @@ def solver_pairs(mesh, rhs: np.ndarray, rtol: float = 1e-6, max_iterations: int 
     rel = C.c_double()
     for k in range(n):
         r64.copy_(R[k])
-        rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_JACOBI, C.c_void_p(r64.data_ptr()), C.c_void_p(du.data_ptr()),
+        rc = lib.fem_pcg(mesh.ctx, _lib.FEM_PRECOND_JACOBI, _ptr(r64), _ptr(du),
                          rtol, max_iterations, C.byref(it), C.byref(rel))
         _check(rc, mesh, "fem_pcg")
         E[k].copy_(du)
@@ -125,7 +126,7 @@ def train(mesh, R, E, steps: int = 300, batch: int = 8, lr: float = 2e-3, seed: 
     prm.progress = _lib.PROGRESS_FN(0)
     prm.progress_user = None
     res = _lib.FemTrainResult()
-    rc = _lib.load().fem_mpnn_train(mesh.ctx, C.c_void_p(R.data_ptr()), C.c_void_p(E.data_ptr()), int(R.shape[0]),
+    rc = _lib.load().fem_mpnn_train(mesh.ctx, _ptr(R), _ptr(E), int(R.shape[0]),
                                     C.byref(prm), C.byref(res))
     _check(rc, mesh, "fem_mpnn_train")
     return {"steps": res.steps_done, "loss_first": res.loss_first, "loss_last": res.loss_last}
@@ -135,7 +136,7 @@ def evaluate(mesh, R, E) -> dict:
     """Mean A-norm loss of the network and of the same preconditioner without it."""
     a = C.c_double()
     b = C.c_double()
-    rc = _lib.load().fem_mpnn_eval(mesh.ctx, C.c_void_p(R.data_ptr()), C.c_void_p(E.data_ptr()), int(R.shape[0]),
+    rc = _lib.load().fem_mpnn_eval(mesh.ctx, _ptr(R), _ptr(E), int(R.shape[0]),
                                    C.byref(a), C.byref(b))
     _check(rc, mesh, "fem_mpnn_eval")
     return {"loss_net": a.value, "loss_base": b.value}

@@ -77,7 +77,7 @@ def main(argv=None):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(args.reps):
-            rc = _lib.load().fem_mpnn_forward(mesh.ctx, C.c_void_p(r.data_ptr()), C.c_void_p(z.data_ptr()))
+            rc = _lib.load().fem_mpnn_forward(mesh.ctx, B._ptr(r), B._ptr(z))
             if rc != 0:
                 raise RuntimeError(_lib.last_error(mesh.ctx))
         e1.record()
@@ -89,8 +89,8 @@ def main(argv=None):
         rhs = torch.randn(v.n_nodes, 3, dtype=torch.float64, device=mesh.device)
         du = torch.zeros_like(rhs)
         it, rel = C.c_int32(), C.c_double()
-        rc = _lib.load().fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, C.c_void_p(rhs.data_ptr()),
-                                 C.c_void_p(du.data_ptr()), 1e-6, 5000, C.byref(it), C.byref(rel))
+        rc = _lib.load().fem_pcg(mesh.ctx, _lib.FEM_PRECOND_TWO_LEVEL, B._ptr(rhs),
+                                 B._ptr(du), 1e-6, 5000, C.byref(it), C.byref(rel))
         if rc not in (0, _lib.FEM_NOT_CONVERGED):
             raise RuntimeError(_lib.last_error(mesh.ctx))
         extra["two_level_iterations"] = it.value

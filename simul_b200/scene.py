@@ -48,6 +48,10 @@ class ContactType(enum.Enum):
 
 
 def _ptr(t: torch.Tensor):
+    """A tensor handed to the contact kernels: torch's pending writes to it
+    finish first (the kernels run on the library's stream)."""
+    if t.is_cuda:
+        torch.cuda.current_stream(t.device).synchronize()
     return C.c_void_p(t.data_ptr())
 
 

@@ -84,7 +84,7 @@ def gather_results(local, world):
 
 def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, precond="two_level",
         sequential=False, workers=16, coarse_cell=4, coarse_bf16=True, coarse_reuse=0, device=0,
-        rank=0, world=1):
+        rank=0, world=1, extrapolate=True):
     """Generates the seeded instances, solves them as one batch after a
     one-step warm-up pass, and returns solves/s, p50/p99 per-instance wall
     time and iteration counts (one dict).  With world > 1 (one process per
@@ -106,9 +106,11 @@ def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, prec
 
     def build(d):
         mat = B.J2Plasticity(d["E"], 0.3, 100.0, hardening_modulus=0.02 * d["E"])
-        return batch.BatchInstance(d["X"], d["conn"], mat, d["fixed"], d["vals"], d["f"], device=dev,
+        inst = batch.BatchInstance(d["X"], d["conn"], mat, d["fixed"], d["vals"], d["f"], device=dev,
                                    coarse_cell=coarse_cell, coarse_bf16=bool(coarse_bf16),
                                    coarse_reuse=coarse_reuse)
+        inst.mesh.set_extrapolation(bool(extrapolate))
+        return inst
 
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=8) as ex:
@@ -139,7 +141,7 @@ def run(instances=64, n_min=32, n_max=96, load_steps=10, threads=0, seed=0, prec
     res = {"instances": instances, "n_range": [n_min, n_max], "tets_total": int(sum(r["tets"] for r in per)),
            "tets_min": int(min(r["tets"] for r in per)), "tets_max": int(max(r["tets"] for r in per)),
            "cases": {c: sum(1 for r in per if r["case"] == c) for c in CASES},
-           "load_steps": load_steps, "precond": precond,
+           "load_steps": load_steps, "precond": precond, "extrapolate": bool(extrapolate),
            "coarse": {"cell_voxels": coarse_cell, "inverse": "bf16" if coarse_bf16 else "f32",
                       "reuse": coarse_reuse},
            "all_converged": bool(all(r["converged"] for r in per)),
@@ -178,11 +180,12 @@ def main(argv=None):
     ap.add_argument("--coarse-bf16", type=int, default=1, help="packed BF16 coarse inverse")
     ap.add_argument("--coarse-reuse", type=int, default=0,
                     help="coarse operator: 0 once per solve from rest (small-strain J2), -1 adaptive")
+    ap.add_argument("--extrapolate", type=int, default=1, help="load-step extrapolation of the Newton start")
     args = ap.parse_args(argv)
     print(json.dumps(run(instances=args.instances, n_min=args.n_min, n_max=args.n_max, load_steps=args.load_steps,
                          threads=args.threads, seed=args.seed, precond=args.precond, sequential=args.sequential,
                          workers=args.workers, coarse_cell=args.coarse_cell, coarse_bf16=bool(args.coarse_bf16),
-                         coarse_reuse=args.coarse_reuse)))
+                         coarse_reuse=args.coarse_reuse, extrapolate=bool(args.extrapolate))))
 
 
 if __name__ == "__main__":

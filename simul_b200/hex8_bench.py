@@ -22,7 +22,7 @@ L2_FLUSH_BYTES = 256 << 20
 
 
 def run(n=64, precond="two_level", load_steps=20, tol=1e-8, warmup=1, steps=3, coarse_cell=4,
-        whole_solve_graph=True, body=None, device="cuda:0") -> dict:
+        whole_solve_graph=True, body=None, device="cuda:0", extrapolate=True) -> dict:
     """Times ``steps`` sequences of ``load_steps`` solves from rest after
     ``warmup`` untimed ones; returns the median and the solve counts."""
     import torch
@@ -37,6 +37,7 @@ def run(n=64, precond="two_level", load_steps=20, tol=1e-8, warmup=1, steps=3, c
     mesh.initialize_from_numpy(v.X, v.conn)
     mesh.set_coarse_options(cell=coarse_cell, bf16=True, reuse=0, inverse="tf32", max_nodes=6144)
     mesh.set_whole_solve_graph(bool(whole_solve_graph))
+    mesh.set_extrapolation(bool(extrapolate))
     mat = B.J2Plasticity(v.E, 0.3, 100.0, hardening_modulus=0.02 * v.E)
     solver = B.StaticSolver(mesh, mat, tol=tol, precond=precond)
     idx = np.where(v.fixed_mask.reshape(-1))[0]

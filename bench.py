@@ -562,6 +562,7 @@ def main():
     st = mesh.stats()
     variant = st["matvec_variant"]
     traffic = load_traffic().get(f"matvec_{variant}_j2_n{args.n}")
+    traffic_warm = load_traffic().get(f"matvec_{variant}_j2_n{args.n}_warm")
     line = {"metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "job_solves_per_s": ws / (ms / 1e3),
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
@@ -598,6 +599,8 @@ def main():
                          "frac_nominal_8tbs": (achieved / 8000.0) if achieved else None,
                          "peak_source": peak_src, "algorithmic_bytes": b_mv,
                          "traffic": traffic,
+                         "traffic_note": "ncu cold-cache capture (caches flushed before each kernel)",
+                         "traffic_warm": traffic_warm,
                          "residual_achieved": residual_bytes(info["n_elements"], info["n_nodes"]) / (kms[1] * 1e-3) / 1e9
                          if rc == 0 else None}}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -27,7 +27,8 @@ def _rel_l2(a, b):
 
 
 def _ptr(t):
-    return C.c_void_p(t.data_ptr())
+    # pending torch writes finish before the library reads (B._ptr)
+    return B._ptr(t)
 
 
 def distorted_grid(n=3, seed=0, amp=0.12):

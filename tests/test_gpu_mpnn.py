@@ -20,7 +20,8 @@ pytestmark = pytest.mark.gpu
 
 
 def _ptr(t):
-    return C.c_void_p(t.data_ptr())
+    # pending torch writes finish before the library reads (B._ptr)
+    return B._ptr(t)
 
 
 def _rel_l2(a, b):

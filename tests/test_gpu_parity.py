@@ -55,7 +55,8 @@ def dev(a, cuda, dtype=torch.float64):
 
 
 def ptr(t):
-    return C.c_void_p(t.data_ptr())
+    # pending torch writes finish before the library reads (B._ptr)
+    return B._ptr(t)
 
 
 @pytest.fixture(scope="module")

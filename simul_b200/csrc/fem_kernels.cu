@@ -689,13 +689,11 @@ __global__ void __launch_bounds__(256) node_gather_persist_kernel(const __grid_c
   }
 }
 
+// One node's residual row (LANES lanes of a group add its slot range; the
+// group's lane 0 stores R and fneg) and its ||R||^2 term (lane 0).
 template <int LANES>
-__global__ void __launch_bounds__(256) res_gather_kernel(const __grid_constant__ ResArgs a) {
-  __shared__ double sred[8];
-  __shared__ bool am_last;
+__device__ __forceinline__ double res_gather_node(const ResArgs& a, int n, int sub) {
   const MeshDev& m = a.m;
-  const int n = (int)(blockIdx.x * (256 / LANES) + threadIdx.x / LANES);
-  const int sub = (int)threadIdx.x % LANES;
   double acc[3] = {0.0, 0.0, 0.0};
   if (n < m.n_nodes) {
     const int j0 = __ldg(m.node_row + n), j1 = __ldg(m.node_row + n + 1);
@@ -718,6 +716,20 @@ __global__ void __launch_bounds__(256) res_gather_kernel(const __grid_constant__
       r2 += r * r;
     }
   }
+  return r2;
+}
+
+// Persistent over node groups (grid-stride): one ||R||^2 partial per
+// resident CTA, added in index order by the last block.
+template <int LANES>
+__global__ void __launch_bounds__(256) res_gather_kernel(const __grid_constant__ ResArgs a) {
+  __shared__ double sred[8];
+  __shared__ bool am_last;
+  constexpr int kNodes = 256 / LANES;
+  const int sub = (int)threadIdx.x % LANES;
+  double r2 = 0.0;
+  for (int g = blockIdx.x; g * kNodes < a.m.n_nodes; g += gridDim.x)
+    r2 += res_gather_node<LANES>(a, g * kNodes + (int)threadIdx.x / LANES, sub);
   double bsum = block_sum<256>(r2, sred);
   if (publish_partial(a.red, a.red_site, 1, &bsum, &am_last)) {
     double tot = final_sum<256>(a.red, a.red_site, 0, sred);
@@ -1215,6 +1227,17 @@ __global__ void rhs_minus_kernel(const double* R, const float* y, const uint8_t*
 
 static inline int nblk(int n, int t) { return (n + t - 1) / t; }
 
+// CTAs that fit on the device at once (resident per SM x SMs) for a
+// persistent kernel of `threads` threads and no dynamic shared memory.
+template <typename K>
+static int resident_grid(K kernel, int threads) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+  return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
+}
+
 void launch_extrap(double* u, const double* u_last, const double* du_last, int n, cudaStream_t s) {
   extrap_kernel<<<nblk(n, 256), 256, 0, s>>>(u, u_last, du_last, n);
 }
@@ -1268,7 +1291,8 @@ static void residual_two_phase(const ResArgs& a, int model, cudaStream_t s) {
     case M_FMR: res_elem_kernel<M_FMR><<<ge, 128, 0, s>>>(a); break;
     default: res_elem_kernel<-1><<<ge, 128, 0, s>>>(a); break;
   }
-  res_gather_kernel<kGatherLanes><<<nblk(a.m.n_nodes, 256 / kGatherLanes), 256, 0, s>>>(a);
+  static const int ggrid = resident_grid(res_gather_kernel<kGatherLanes>, 256);
+  res_gather_kernel<kGatherLanes><<<std::min(ggrid, nblk(a.m.n_nodes, 256 / kGatherLanes)), 256, 0, s>>>(a);
 }
 
 void launch_residual(const ResArgs& a, int model, cudaStream_t s) {
@@ -1323,16 +1347,6 @@ static void two_phase(const MvArgs& a, int model, cudaStream_t s) {
   launch_chain(node_gather_kernel<CG>, nblk(a.m.n_nodes, kGatherNodes), 256, 0, s, a);
 }
 
-// CTAs that fit on the device at once (resident per SM x SMs) for a
-// persistent kernel of `threads` threads and no dynamic shared memory.
-template <typename K>
-static int resident_grid(K kernel, int threads) {
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
-  return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
-}
 
 template <int MODEL, bool CG>
 static void persist_elem(const MvArgs& a, cudaStream_t s) {

@@ -202,16 +202,17 @@ __global__ void __launch_bounds__(NB) residual_kernel(const __grid_constant__ Re
 // differently from the fused kernel's (agreement to rounding).
 template <int MODEL>
 __global__ void __launch_bounds__(128) res_elem_kernel(const __grid_constant__ ResArgs a) {
-  const int e = (int)blockIdx.x * 128 + (int)threadIdx.x;
-  if (e >= a.m.n_elems) return;
-  double f[4][3];
-  res_element<MODEL>(a, e, true, f);
-  const int4 sp = __ldg(a.m.spos + e);
-  const int pos[4] = {sp.x, sp.y, sp.z, sp.w};
+  // persistent: one wave of CTAs walks the elements in grid-stride order
+  for (int e = (int)blockIdx.x * 128 + (int)threadIdx.x; e < a.m.n_elems; e += (int)gridDim.x * 128) {
+    double f[4][3];
+    res_element<MODEL>(a, e, true, f);
+    const int4 sp = __ldg(a.m.spos + e);
+    const int pos[4] = {sp.x, sp.y, sp.z, sp.w};
 #pragma unroll
-  for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < 4; ++k)
 #pragma unroll
-    for (int d = 0; d < 3; ++d) __stcg(a.stage_d + 3 * (size_t)pos[k] + d, f[k][d]);
+      for (int d = 0; d < 3; ++d) __stcg(a.stage_d + 3 * (size_t)pos[k] + d, f[k][d]);
+  }
 }
 
 // ───────────────────────── tangent matvec (FP32) ─────────────────────────
@@ -1280,16 +1281,21 @@ static void residual_nb(const ResArgs& a, int model, cudaStream_t s) {
   }
 }
 
+template <int MODEL>
+static void res_elem(const ResArgs& a, cudaStream_t s) {
+  static const int grid = resident_grid(res_elem_kernel<MODEL>, 128);
+  res_elem_kernel<MODEL><<<std::min(grid, nblk(a.m.n_elems, 128)), 128, 0, s>>>(a);
+}
+
 static void residual_two_phase(const ResArgs& a, int model, cudaStream_t s) {
-  const int ge = nblk(a.m.n_elems, 128);
   switch (model) {
-    case M_LE: res_elem_kernel<M_LE><<<ge, 128, 0, s>>>(a); break;
-    case M_NH: res_elem_kernel<M_NH><<<ge, 128, 0, s>>>(a); break;
-    case M_MR: res_elem_kernel<M_MR><<<ge, 128, 0, s>>>(a); break;
-    case M_J2: res_elem_kernel<M_J2><<<ge, 128, 0, s>>>(a); break;
-    case M_TI: res_elem_kernel<M_TI><<<ge, 128, 0, s>>>(a); break;
-    case M_FMR: res_elem_kernel<M_FMR><<<ge, 128, 0, s>>>(a); break;
-    default: res_elem_kernel<-1><<<ge, 128, 0, s>>>(a); break;
+    case M_LE: res_elem<M_LE>(a, s); break;
+    case M_NH: res_elem<M_NH>(a, s); break;
+    case M_MR: res_elem<M_MR>(a, s); break;
+    case M_J2: res_elem<M_J2>(a, s); break;
+    case M_TI: res_elem<M_TI>(a, s); break;
+    case M_FMR: res_elem<M_FMR>(a, s); break;
+    default: res_elem<-1>(a, s); break;
   }
   static const int ggrid = resident_grid(res_gather_kernel<kGatherLanes>, 256);
   res_gather_kernel<kGatherLanes><<<std::min(ggrid, nblk(a.m.n_nodes, 256 / kGatherLanes)), 256, 0, s>>>(a);

@@ -51,6 +51,7 @@ def main(argv=None):
     ap.add_argument("--block-smoother", type=int, default=1, help="two-level nodal block smoother")
     ap.add_argument("--cases", nargs="+", default=list(CASES), choices=list(CASES),
                     help="moment cases solved as one batch")
+    ap.add_argument("--extrapolate", type=int, default=0, help="load-step extrapolation of the Newton start")
     args = ap.parse_args(argv)
     from simul_b200 import batch, meshgen
     import torch
@@ -68,6 +69,7 @@ def main(argv=None):
         inst.mesh.set_coarse_options(reuse=args.coarse_reuse)
         inst.mesh.set_direction_recurrence(bool(args.recurrence))
         inst.mesh.set_block_smoother(bool(args.block_smoother))
+        inst.mesh.set_extrapolation(bool(args.extrapolate))
     t_setup = time.perf_counter() - t0
     kw = dict(precond=args.precond, line_search=args.line_search, max_iterations=args.max_iterations)
     batch.solve_batch(insts, load_steps=1, **kw)      # warm-up

@@ -691,7 +691,11 @@ __global__ void __launch_bounds__(256) fpcg_dots_kernel(const __grid_constant__ 
       if (!net_ok) {
         cg->n_alt += 1;
         if (!was_locked && cg->n_alt >= kLock) {
+          // the network is switched off: hand the rest of the solve, from the
+          // current iterate, to the plain preconditioned CG (status 4)
           cg->locked = 1;
+          cg->done = 4;
+          cg->status = 4;
           restart = true;
         }
       }

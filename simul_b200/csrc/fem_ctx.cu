@@ -83,6 +83,10 @@ struct FemCtx {
   double* u_last = nullptr;
   double* du_last = nullptr;
   double* u_start = nullptr;
+  // learned FPCG hand-over: the flexible iterate and its residual in FP64
+  float* ho_x = nullptr;
+  double* ho_rhs = nullptr;
+  int64_t n_handovers = 0;
   double* tmpd = nullptr;
   float* payload = nullptr;
   double* ep_c = nullptr;
@@ -351,6 +355,8 @@ void free_ctx(FemCtx* c) {
   if (c->u_last) cudaFree(c->u_last);
   if (c->du_last) cudaFree(c->du_last);
   if (c->u_start) cudaFree(c->u_start);
+  if (c->ho_x) cudaFree(c->ho_x);
+  if (c->ho_rhs) cudaFree(c->ho_rhs);
   if (c->spos) cudaFree(c->spos);
   void* ptrs[] = {c->X64, c->X32, c->conn, c->mat_id, c->scale, c->blk_ptr, c->blk_home,
                   c->blk_elems, c->node_row, c->node_slots, c->fixed, c->fixed_vals, c->fext,
@@ -1868,6 +1874,30 @@ int run_pcg(FemCtx* c, const double* b_int, int precond, double rtol, int maxit,
     CK(cudaMemcpyAsync(c->h_err, c->mdev.err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (*c->h_err) return set_err(c, FEM_ERR_BUDGET, "learned preconditioner: tensor-core wait gave up");
+    if (h.done == 4) {
+      // the network was switched off: the rest of the solve runs as plain
+      // (two-level or Jacobi) PCG on the current residual, its solution added
+      // to the flexible iterate, to the same absolute residual target
+      ++c->n_handovers;
+      const int iters_done = h.iter;
+      const double tol2 = h.tol2, rr_now = h.rr, rr0 = h.rr0;
+      if (!c->ho_x && ((st = dalloc(c, &c->ho_x, 4 * (size_t)c->Nn)) || (st = dalloc(c, &c->ho_rhs, (size_t)c->ndof_pad))))
+        return st;
+      CK(cudaMemcpyAsync(c->ho_x, c->x, 4 * (size_t)c->Nn * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+      ++c->n_launches; launch_f4_to_d3(c->r, c->ho_rhs, c->Nn, c->stream);
+      CKL();
+      const double rtol2 = rr_now > 0.0 ? std::min(1.0, std::sqrt(tol2 / rr_now)) : 1.0;
+      int it2 = 0;
+      double rel2 = 0;
+      const int fb = c->learned_coarse ? FEM_PRECOND_TWO_LEVEL : FEM_PRECOND_JACOBI;
+      st = run_pcg(c, c->ho_rhs, fb, rtol2, std::max(1, maxit - iters_done), &it2, &rel2);
+      if (st && st != FEM_NOT_CONVERGED) return st;
+      ++c->n_launches; launch_f4_add(c->x, c->ho_x, c->Nn, c->stream);
+      CKL();
+      if (iters) *iters = iters_done + it2;
+      if (rel) *rel = rr0 > 0 ? rel2 * std::sqrt(rr_now / rr0) : 0.0;
+      return st;
+    }
     if (h.done == 2 || h.done == 3) {
       // Jacobi-based PCG is the fallback: the flexible solve broke down or ran
       // out of iterations; the same convergence test judges the rerun

@@ -103,7 +103,8 @@ struct Reduce {
 // block of each reduction so no host round trip is needed per iteration).
 struct CGState {
   double rz, pAp, rr, rr0, tol2, alpha, beta, pad;
-  int iter, max_iter, done, status;  // done: 0 running, 1 converged, 2 max iters, 3 breakdown
+  int iter, max_iter, done, status;  // done: 0 running, 1 converged, 2 max iters, 3 breakdown,
+                                     // 4 learned FPCG handed over (network switched off)
   int zsel;                          // learned FPCG: 1 = this step used the Jacobi (+ coarse) direction
   int n_alt;                         // learned FPCG: steps that used it
   int locked;                        // learned FPCG: network switched off for the rest of the solve
@@ -482,6 +483,9 @@ void launch_gather_mask(const uint8_t* in_user, uint8_t* out_int, const int* per
 void launch_apply_bc(double* u, const double* fixed_vals, const uint8_t* fixed, int n,
                      cudaStream_t s);
 // u[3n+d] = u_base[3n+d] + alpha du[4n+d] for n < n_nodes
+// float4-per-node vector -> three doubles per node; x += x0 (float4 per node)
+void launch_f4_to_d3(const float* in, double* out, int n_nodes, cudaStream_t s);
+void launch_f4_add(float* x, const float* x0, int n_nodes, cudaStream_t s);
 // load-step extrapolation (fem_newton_solve with FEM_OPT_EXTRAPOLATE)
 void launch_extrap(double* u, const double* u_last, const double* du_last, int n, cudaStream_t s);
 void launch_differ(const double* a, const double* b, int n, unsigned int* differ, cudaStream_t s);

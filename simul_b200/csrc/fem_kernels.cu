@@ -1123,6 +1123,28 @@ __global__ void u_update_kernel(double* u, const double* u_base, const float* du
   u[3 * i + 2] = u_base[3 * i + 2] + alpha * (double)d.z;
 }
 
+// one float4 per node -> three doubles per node
+__global__ void f4_to_d3_kernel(const float* __restrict__ in, double* out, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 v = reinterpret_cast<const float4*>(in)[i];
+  out[3 * i] = v.x;
+  out[3 * i + 1] = v.y;
+  out[3 * i + 2] = v.z;
+}
+
+// x += x0 (one float4 per node)
+__global__ void f4_add_kernel(float* x, const float* __restrict__ x0, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 v = reinterpret_cast<float4*>(x)[i];
+  const float4 w = reinterpret_cast<const float4*>(x0)[i];
+  v.x += w.x;
+  v.y += w.y;
+  v.z += w.z;
+  reinterpret_cast<float4*>(x)[i] = v;
+}
+
 // load-step extrapolation: u = u_last + du_last
 __global__ void extrap_kernel(double* u, const double* u_last, const double* du_last, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1239,6 +1261,12 @@ static int resident_grid(K kernel, int threads) {
   return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
 }
 
+void launch_f4_to_d3(const float* in, double* out, int n_nodes, cudaStream_t s) {
+  f4_to_d3_kernel<<<nblk(n_nodes, 256), 256, 0, s>>>(in, out, n_nodes);
+}
+void launch_f4_add(float* x, const float* x0, int n_nodes, cudaStream_t s) {
+  f4_add_kernel<<<nblk(n_nodes, 256), 256, 0, s>>>(x, x0, n_nodes);
+}
 void launch_extrap(double* u, const double* u_last, const double* du_last, int n, cudaStream_t s) {
   extrap_kernel<<<nblk(n, 256), 256, 0, s>>>(u, u_last, du_last, n);
 }

@@ -185,8 +185,8 @@ def test_mpnn_backward_matches_oracle(cuda, bar_setup):
 
 def test_training_gains_over_jacobi(cuda):
     """Train on pairs the plain solver generates; on held-out pairs the trained
-    network's one-step A-norm error beats Jacobi's by more than 10 %.  Flexible
-    PCG with the trained network still converges on its own."""
+    network's one-step A-norm error beats Jacobi's by more than 10 % (the
+    gain), while the CG iteration count is not reduced (the measured loss)."""
     from simul_b200 import learned
     from tests.golden import gen_golden as G
     vox = G.vox_mesh()
@@ -218,9 +218,14 @@ def test_training_gains_over_jacobi(cuda):
         its[name] = it.value
     st = (C.c_int64 * 4)()
     lib.fem_learned_stats(mesh.ctx, st)
-    # The flexible solve converges on its own (no rerun with Jacobi-PCG).  The
-    # network's one-step gain above does not carry over to Krylov iterations
-    # on this mesh: flexible PCG with it needs more iterations than Jacobi-PCG
-    # (measured about 3.3x).  The bound only guards against a regression.
+    # The flexible solve converges without a rerun: once the network is
+    # switched off it hands over to plain Jacobi-PCG from its iterate.  The
+    # one-step gain above does not carry over to Krylov iterations: the
+    # learned solve needs about as many CG iterations as Jacobi-PCG or more
+    # (the network's directions are descent directions but poor conjugate
+    # ones; tests/test_learned_headroom.py bounds what a linear learned form
+    # of the two-level method could gain).  Both bounds record that.
+    print("CG iterations", its)
     assert st[0] == 0, its
-    assert its["learned"] <= 5 * its["jacobi"], its
+    assert its["learned"] >= 0.8 * its["jacobi"], its
+    assert its["learned"] <= 3 * its["jacobi"], its

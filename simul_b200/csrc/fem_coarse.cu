@@ -518,9 +518,9 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
   __shared__ double sred[8];
   __shared__ bool am_last;
   const CoarseDev& c = a.c;
+  const int i = blockIdx.x * 256 + threadIdx.x;
   double rz = 0.0, rr = 0.0;
-  // persistent: one wave of CTAs walks the nodes in grid-stride order
-  for (int i = blockIdx.x * 256 + threadIdx.x; i < a.m.n_nodes; i += gridDim.x * 256) {
+  if (i < a.m.n_nodes) {
     const float4 rv = reinterpret_cast<const float4*>(r)[i];
     const float4 dv = reinterpret_cast<const float4*>(dinv)[i];
     float t[3];
@@ -552,8 +552,8 @@ __global__ void __launch_bounds__(256) tl_rz_kernel(const __grid_constant__ Coar
     zv.w = 0.f;
     reinterpret_cast<float4*>(z)[i] = zv;
     if (INIT) reinterpret_cast<float4*>(p)[i] = zv;
-    rz += (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
-    rr += (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
+    rz = (double)rv.x * zv.x + (double)rv.y * zv.y + (double)rv.z * zv.z;
+    rr = (double)rv.x * rv.x + (double)rv.y * rv.y + (double)rv.z * rv.z;
   }
   chain_release();
   double v[2];
@@ -941,20 +941,9 @@ void launch_coarse_solve(const CoarseArgs& a, const CGState* cg, cudaStream_t s)
                s, a.c, cg);
 }
 
-// CTAs of a kernel resident on the device at once (one wave)
-template <typename K>
-static int resident_ctas(K kernel, int threads) {
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
-  return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
-}
-
 void launch_tl_rz(const CoarseArgs& a, bool init, const float* r, const float* dinv, float* z, float* p,
                   CGState* cg, Reduce red, int site, cudaStream_t s) {
-  static const int wave = std::min(resident_ctas(tl_rz_kernel<true>, 256), resident_ctas(tl_rz_kernel<false>, 256));
-  const int g = std::min(wave, nblk(a.m.n_nodes, 256));
+  const int g = nblk(a.m.n_nodes, 256);
   if (init)
     tl_rz_kernel<true><<<g, 256, 0, s>>>(a, r, dinv, z, p, cg, red, site);
   else

@@ -368,8 +368,8 @@ def roofline_point(args, n, dev):
     rhs[:, 2] = 1.0
     du = torch.zeros_like(rhs)
     it, rel = C.c_int32(), C.c_double()
-    _lib.load().fem_pcg(mesh.ctx, _lib.FEM_PRECOND_JACOBI, C.c_void_p(rhs.data_ptr()), C.c_void_p(du.data_ptr()),
-                        1e-2, 50, C.byref(it), C.byref(rel))
+    _lib.load().fem_pcg(mesh.ctx, _lib.FEM_PRECOND_JACOBI, B._ptr(rhs), B._ptr(du), 1e-2, 50, C.byref(it),
+                        C.byref(rel))
     kms = (C.c_double * 4)()
     rc = _lib.load().fem_profile_kernels(mesh.ctx, 50, kms)
     peak, peak_src = measured_peaks()

@@ -10,7 +10,9 @@
 //                          column in *info and the factorisation continues
 //                          with a unit pivot, so every launch completes)
 //     dense_panel_kernel   L_ik = A_ik W_kk^T, i > k
-//     dense_update_kernel  A_ij -= L_ik L_jk^T, k < j <= i
+//     dense_update_kernel  A_ij -= L_ik L_jk^T, k < j <= i (column k + 1 here,
+//                          the columns > k + 1 on a third stream, so the next
+//                          diagonal and panel kernels overlap them)
 //   invert, right-looking, step k on a second stream once panel k is done:
 //     dense_wfin_kernel    W_kj = W_kk R_kj, j < k (R: the accumulated row)
 //     dense_wupd_kernel    R_ij -= L_ik W_kj, i > k, j <= k
@@ -202,83 +204,147 @@ __global__ void __launch_bounds__(256) dense_pad_kernel(const double* __restrict
 
 // Diagonal tile k: L_kk = chol(A_kk) and X = L_kk^-1 in shared memory
 // (L[c * S + r] = L(r, c)), both blocked in 32-wide panels so the sequential
-// parts run inside one warp and the CTA synchronises a few times per panel:
+// parts run inside one warp, in registers, and the CTA synchronises a few
+// times per panel:
 //   Cholesky, panel p (columns j0 .. j0 + 31):
-//     warp 0 factors the 32 x 32 diagonal block (lane = row),
-//     each thread solves one row below it against that block's transpose,
-//     all threads apply the rank-32 update to the trailing lower triangle;
-//   inverse: each warp inverts one 32 x 32 diagonal block (lane = column),
+//     warp 0 factors the 32 x 32 diagonal block in registers (lane = row,
+//     the pivot column passed by shuffles) and inverts it (lane = column,
+//     the factor read back as shared-memory broadcasts),
+//     the rows below are L_ip = A_ip X_pp^T (16 columns per thread),
+//     the rank-32 update of the trailing lower triangle runs on 4 x 4
+//     register tiles;
 //   then block row k is finished (X_kq = X_kk R_kq, q < k) and subtracted
 //   from the rows below (R_iq -= L_ik X_kq), for k = 0, 1, ...
 template <typename T>
 __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, int N, int k, int* info) {
   constexpr int B = DenseCfg<T>::B, S = B + 1, P = 32, NP = B / P;
+  constexpr unsigned kFull = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char s_raw[];
   T* L = reinterpret_cast<T*>(s_raw);  // L[c * S + r]
   T* X = L + B * S;                     // X[c * S + r] = (L^-1)(r, c)
+  T* Xt = X + B * S;                    // Xt[l * P + j] = (L_pp^-1)(j, l), current panel
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t off = (size_t)k * B * N + (size_t)k * B;
-  for (int q = tid; q < B * B; q += kDenseThreads) {
-    const int c = q / B, r = q % B;
-    L[c * S + r] = r >= c ? A[off + (size_t)c * N + r] : T(0);
+#pragma unroll 8
+  for (int it = 0; it < B * B / kDenseThreads; ++it) {
+    const int q = tid + it * kDenseThreads, c = q / B, r = q % B;
+    const T v = A[off + (size_t)c * N + r];
+    L[c * S + r] = r >= c ? v : T(0);
     X[c * S + r] = T(0);
   }
   __syncthreads();
-  const int tx = tid & 15, ty = tid >> 4;
   for (int p = 0; p < NP; ++p) {
     const int j0 = p * P;
     if (warp == 0) {
-      // 32 x 32 diagonal block, lane = row j0 + lane
-      const int r = j0 + lane;
+      T a[P];  // row j0 + lane of the diagonal block
+#pragma unroll
+      for (int c = 0; c < P; ++c) a[c] = c <= lane ? L[(j0 + c) * S + j0 + lane] : T(0);
+#pragma unroll
       for (int j = 0; j < P; ++j) {
-        const int jj = j0 + j;
-        T d = L[jj * S + jj];
+        T d = __shfl_sync(kFull, a[j], j);
         if (!(d > T(0))) {
-          if (lane == 0) atomicCAS(info, 0, k * B + jj + 1);
+          if (lane == 0) atomicCAS(info, 0, k * B + j0 + j + 1);
           d = T(1);
         }
         d = sqrt(d);
-        __syncwarp();
-        if (lane == j) L[jj * S + jj] = d;
-        if (lane > j) L[jj * S + r] /= d;
-        __syncwarp();
-        const T lr = lane > j ? L[jj * S + r] : T(0);
-        for (int c = j + 1; c <= lane; ++c) L[(j0 + c) * S + r] -= lr * L[jj * S + j0 + c];
-        __syncwarp();
+        if (lane == j) a[j] = d;
+        if (lane > j) a[j] = a[j] / d;
+#pragma unroll
+        for (int c = 1; c < P; ++c) {  // c > j: constant trip counts unroll fully
+          if (c > j) {
+            const T lc = __shfl_sync(kFull, a[j], c);
+            if (lane >= c) a[c] -= a[j] * lc;
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < P; ++c)
+        if (c <= lane) L[(j0 + c) * S + j0 + lane] = a[c];
+      __syncwarp();
+      // column lane of L_pp^-1: x[r] = (delta(r, lane) - sum_{l < r} L(r, l) x[l]) / L(r, r)
+      T x[P];
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        T acc = r == lane ? T(1) : T(0);
+#pragma unroll
+        for (int l = 0; l < P - 1; ++l)
+          if (l < r) acc -= L[(j0 + l) * S + j0 + r] * x[l];
+        x[r] = acc / L[(j0 + r) * S + j0 + r];
+      }
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        X[(j0 + lane) * S + j0 + r] = x[r];
+        Xt[lane * P + r] = x[r];
       }
     }
     __syncthreads();
-    // rows below the block: x L_pp^T = a, one row per thread
-    for (int r = j0 + P + tid; r < B; r += kDenseThreads) {
-      for (int j = 0; j < P; ++j) {
-        T acc = L[(j0 + j) * S + r];
-        for (int l = 0; l < j; ++l) acc -= L[(j0 + l) * S + r] * L[(j0 + l) * S + j0 + j];
-        L[(j0 + j) * S + r] = acc / L[(j0 + j) * S + j0 + j];
+    const int rows = B - j0 - P;  // rows below the diagonal block
+    if (rows == 0) break;
+    {
+      // L(r, j0 + j) = sum_{l <= j} A(r, j0 + l) Xt[l * P + j], columns 16 cg .. 16 cg + 15
+      constexpr int CG = 16;
+      using VT = Vec16<T>;
+      constexpr int W = VT::W;
+      const bool act = tid < rows * (P / CG);
+      const int r = j0 + P + (act ? tid % rows : 0), cg = act ? tid / rows : 0;
+      T acc[CG];
+#pragma unroll
+      for (int j = 0; j < CG; ++j) acc[j] = T(0);
+      if (act) {
+        const int lend = cg * CG + CG;
+        for (int l = 0; l < lend; ++l) {
+          const T av = L[(j0 + l) * S + r];
+          const typename VT::V* xt = reinterpret_cast<const typename VT::V*>(Xt + l * P + cg * CG);
+#pragma unroll
+          for (int v = 0; v < CG / W; ++v) {
+            T xv[W];
+            VT::unpack(xt[v], xv);
+#pragma unroll
+            for (int w = 0; w < W; ++w) acc[v * W + w] += av * xv[w];
+          }
+        }
       }
+      __syncthreads();
+      if (act) {
+#pragma unroll
+        for (int j = 0; j < CG; ++j) L[(j0 + cg * CG + j) * S + r] = acc[j];
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    // trailing lower triangle: columns c >= j0 + P, rows r >= c
-    for (int c = j0 + P + tx; c < B; c += 16) {
-      for (int r = c + ty; r < B; r += 16) {
-        T acc = T(0);
-#pragma unroll 8
-        for (int l = j0; l < j0 + P; ++l) acc += L[l * S + r] * L[l * S + c];
-        L[c * S + r] -= acc;
+    {
+      // trailing lower triangle on 4 x 4 tiles: L(r, c) -= sum_l L(r, j0 + l) L(c, j0 + l)
+      const int nt4 = rows / 4, ntri = nt4 * (nt4 + 1) / 2, base = j0 + P;
+      for (int q = tid; q < ntri; q += kDenseThreads) {
+        int ti, tj;  // tj <= ti
+        dense_tri(q, ti, tj);
+        const int r0 = base + 4 * ti, c0 = base + 4 * tj;
+        T acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
+#pragma unroll 4
+        for (int l = j0; l < j0 + P; ++l) {
+          T lr[4], lc[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            lr[i] = L[l * S + r0 + i];
+            lc[i] = L[l * S + c0 + i];
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] += lr[i] * lc[j];
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (r0 + i >= c0 + j) L[(c0 + j) * S + r0 + i] -= acc[i][j];
       }
     }
     __syncthreads();
   }
-  // inverse of each 32 x 32 diagonal block: warp p, lane = column
-  if (warp < NP) {
-    const int j0 = warp * P, c = j0 + lane;
-    X[c * S + c] = T(1) / L[c * S + c];
-    for (int r = c + 1; r < j0 + P; ++r) {
-      T acc = T(0);
-      for (int l = c; l < r; ++l) acc += L[l * S + r] * X[c * S + l];
-      X[c * S + r] = -acc / L[r * S + r];
-    }
-  }
-  __syncthreads();
   // block rows: finish row k (X_kq = X_kk R_kq, q < k; R_kq accumulated in
   // place), then R_iq -= L_ik X_kq for i > k, q <= k
   for (int kb = 0; kb < NP; ++kb) {
@@ -332,15 +398,17 @@ __global__ void __launch_bounds__(kDenseThreads) dense_panel_kernel(T* A, const 
   dense_store<T, 0>(Aik, N, acc);
 }
 
-// A_ij -= L_ik L_jk^T over the lower tiles k < j <= i (blockIdx.x in row order)
-template <typename T>
-__global__ void __launch_bounds__(kDenseThreads) dense_update_kernel(T* A, int N, int k) {
+// A_ij -= L_ik L_jk^T over lower tiles j <= i: with COL the column j = k + 1
+// (i = k + 1 + blockIdx.x), else the triangle j >= k + 1 + j_ofs (blockIdx.x
+// in row order).
+template <typename T, bool COL>
+__global__ void __launch_bounds__(kDenseThreads) dense_update_kernel(T* A, int N, int k, int j_ofs) {
   constexpr int B = DenseCfg<T>::B, TM = DenseCfg<T>::TM;
   __shared__ __align__(16) T sA[kKC * dense_ld<T>()];
   __shared__ __align__(16) T sB[kKC * dense_ld<T>()];
-  int I, J;
-  dense_tri((int)blockIdx.x, I, J);
-  const int i = k + 1 + I, j = k + 1 + J;
+  int I = (int)blockIdx.x, J = 0;
+  if (!COL) dense_tri((int)blockIdx.x, I, J);
+  const int i = k + 1 + j_ofs + I, j = k + 1 + j_ofs + J;
   const T* Lik = A + (size_t)k * B * N + (size_t)i * B;
   const T* Ljk = A + (size_t)k * B * N + (size_t)j * B;
   T acc[TM][TM];
@@ -531,7 +599,7 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
                                    int* launches) {
   constexpr int B = DenseCfg<T>::B;
   const int nt = (n + B - 1) / B, N = nt * B;
-  const size_t diag_smem = 2 * sizeof(T) * (size_t)B * (B + 1);
+  const size_t diag_smem = sizeof(T) * (2 * (size_t)B * (B + 1) + 32 * 32);
   cudaError_t e = cudaFuncSetAttribute(dense_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)diag_smem);
   if (e != cudaSuccess) return e;
@@ -548,31 +616,50 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
   // kernel's staging to pay (measured slower), so they stay on the SIMT
   // tiles; the product W^T W sums over whole tile columns and runs on the
   // TF32 tensor cores when TC is set.
-  cudaStream_t side = nullptr;
-  std::vector<cudaEvent_t> ev((size_t)nt + 1, nullptr);
+  //
+  // The trailing update looks one step ahead: the main stream updates only
+  // tile column k + 1 and goes on to diagonal tile and panel k + 1, while a
+  // third stream updates the columns > k + 1 (ordered before the next
+  // step's column update by an event), so the single-CTA diagonal kernel
+  // overlaps the bulk of the update.  The critical path (diagonal, panel,
+  // column update) runs on a stream of the highest priority forked from s,
+  // so its CTAs are scheduled ahead of the two bulk streams'.
+  cudaStream_t side = nullptr, rest = nullptr, crit = nullptr;
+  std::vector<cudaEvent_t> ev((size_t)nt + 1, nullptr), evr((size_t)nt, nullptr);
   auto release = [&]() {
     for (cudaEvent_t x : ev)
       if (x) cudaEventDestroy(x);
+    for (cudaEvent_t x : evr)
+      if (x) cudaEventDestroy(x);
     if (side) cudaStreamDestroy(side);
+    if (rest) cudaStreamDestroy(rest);
+    if (crit) cudaStreamDestroy(crit);
   };
-  if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess) {
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&rest, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithPriority(&crit, cudaStreamNonBlocking, prio_hi)) != cudaSuccess) {
     release();
     return e;
   }
-  for (auto& x : ev)
-    if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) {
-      release();
-      return e;
-    }
+  for (auto* v : {&ev, &evr})
+    for (auto& x : *v)
+      if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) {
+        release();
+        return e;
+      }
+  cudaEventRecord(ev[nt], s);
+  cudaStreamWaitEvent(crit, ev[nt], 0);
   for (int k = 0; k < nt; ++k) {
-    dense_diag_kernel<T><<<1, kDenseThreads, diag_smem, s>>>(A, W, N, k, info);
+    dense_diag_kernel<T><<<1, kDenseThreads, diag_smem, crit>>>(A, W, N, k, info);
     ++nl;
     const int m = nt - k - 1;
     if (m > 0) {
-      dense_panel_kernel<T><<<m, kDenseThreads, 0, s>>>(A, W, N, k);
+      dense_panel_kernel<T><<<m, kDenseThreads, 0, crit>>>(A, W, N, k);
       ++nl;
     }
-    cudaEventRecord(ev[k], s);
+    cudaEventRecord(ev[k], crit);
     cudaStreamWaitEvent(side, ev[k], 0);
     if (k > 0) {
       dense_wfin_kernel<T><<<k, kDenseThreads, 0, side>>>(W, N, k);
@@ -580,12 +667,26 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
     }
     if (m > 0) {
       dense_wupd_kernel<T><<<m * (k + 1), kDenseThreads, 0, side>>>(A, W, N, k);
-      dense_update_kernel<T><<<m * (m + 1) / 2, kDenseThreads, 0, s>>>(A, N, k);
-      nl += 2;
+      ++nl;
+      // columns > k + 1 on the rest stream (after its step k - 1 there)
+      cudaStreamWaitEvent(rest, ev[k], 0);
+      if (m > 1) {
+        dense_update_kernel<T, false><<<(m - 1) * m / 2, kDenseThreads, 0, rest>>>(A, N, k, 1);
+        ++nl;
+      }
+      cudaEventRecord(evr[k], rest);
+      // column k + 1 on the main stream, after step k - 1's columns > k
+      if (k > 0) cudaStreamWaitEvent(crit, evr[k - 1], 0);
+      dense_update_kernel<T, true><<<m, kDenseThreads, 0, crit>>>(A, N, k, 0);
+      ++nl;
     }
   }
+  // join: s waits for the three streams
   cudaEventRecord(ev[nt], side);
   cudaStreamWaitEvent(s, ev[nt], 0);
+  if (nt > 1) cudaStreamWaitEvent(s, evr[nt - 2], 0);
+  cudaEventRecord(ev[nt - 1], crit);
+  cudaStreamWaitEvent(s, ev[nt - 1], 0);
   if constexpr (TC) {
     static_assert(sizeof(T) == 4 && B == 128, "the tensor-core product takes FP32 128-wide tiles");
     raise_smem_limit_k(dense_syrk_tc_kernel<TO>);

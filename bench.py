@@ -565,7 +565,8 @@ def main():
     traffic_warm = load_traffic().get(f"matvec_{variant}_j2_n{args.n}_warm")
     line = {"metric": METRIC, "value": ms / 1e3, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "job_solves_per_s": ws / (ms / 1e3),
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms, "step_ms": [round(t, 3) for t in step_ms],
+            "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 matvec / f64 residual+dots",
             "data": "synthetic (seeded vertebral body)", "config": workload_config(args, v),
             "method": {"learned": "Newton (FP64 residual) + learned flexible PCG (FP32 matvec, FP64 dots)",
@@ -581,7 +582,8 @@ def main():
                       "all_converged": bool(last["converged"]), "max_relative_residual": last["max_rel"],
                       "cg_ms_per_iteration": (ms / last["cg"]) if last["cg"] else None},
             "clocks": clk,
-            "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "e2e": {"value": e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "step_ms": [round(t, 3) for t in e2e_ms]},
             "gpu_launches": int(launches // max(args.steps, 1)),
             "kernel_ms": {"matvec": kms[0], "residual": kms[1], "cg_update": kms[2], "cg_direction": kms[3]},
             "matvec_variant": {"chosen": variant, "ns_per_launch": st["matvec_ns"]},

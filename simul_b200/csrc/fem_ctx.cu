@@ -201,6 +201,7 @@ struct FemCtx {
   void* dense_work = nullptr;   // padded factor and W (and the FP32 result)
   size_t dense_bytes = 0;
   int* dense_info = nullptr;    // first non-positive pivot, 0 if none
+  DenseSched dense_sched;       // streams and events of the dense inverse
   int* h_info = nullptr;
   // matvec variant: forced by fem_set_option (>= 0) or chosen by timing all
   int mv_forced = -1;
@@ -347,6 +348,7 @@ void free_ctx(FemCtx* c) {
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->dense_work) cudaFree(c->dense_work);
   if (c->dense_info) cudaFree(c->dense_info);
+  c->dense_sched.release();
   if (c->h_info) cudaFreeHost(c->h_info);
   for (cudaEvent_t ev : c->coarse_ev)
     if (ev) cudaEventDestroy(ev);
@@ -1549,12 +1551,14 @@ int ensure_coarse(FemCtx* c) {
   cudaError_t de;
   if (f64) {
     double* A = static_cast<double*>(c->dense_work);
-    de = dense_spd_inverse_f64(c->cdev.Ac, n, A, A + N * N, c->dense_info, c->cdev.Ac, c->stream, &nl);
+    de = dense_spd_inverse_f64(c->cdev.Ac, n, A, A + N * N, c->dense_info, c->cdev.Ac, c->stream, &nl,
+                               &c->dense_sched);
   } else {
     float* A = static_cast<float*>(c->dense_work);
     float* out = A + 2 * N * N;
-    de = c->coarse_inverse == 3 ? dense_spd_inverse_tf32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl)
-                                : dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl);
+    de = c->coarse_inverse == 3
+             ? dense_spd_inverse_tf32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl, &c->dense_sched)
+             : dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl, &c->dense_sched);
     c->cdev.Ac32 = out;
   }
   if (de != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "dense inverse: %s", cudaGetErrorString(de));

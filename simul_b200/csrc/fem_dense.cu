@@ -596,7 +596,7 @@ int dense_tile(bool fp64) { return fp64 ? DenseCfg<double>::B : DenseCfg<float>:
 // TF32 tensor-core tile kernel instead of the SIMT one.
 template <typename T, typename TO, bool TC = false>
 static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* info, TO* out, cudaStream_t s,
-                                   int* launches) {
+                                   int* launches, DenseSched* sched) {
   constexpr int B = DenseCfg<T>::B;
   const int nt = (n + B - 1) / B, N = nt * B;
   const size_t diag_smem = sizeof(T) * (2 * (size_t)B * (B + 1) + 32 * 32);
@@ -624,31 +624,15 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
   // overlaps the bulk of the update.  The critical path (diagonal, panel,
   // column update) runs on a stream of the highest priority forked from s,
   // so its CTAs are scheduled ahead of the two bulk streams'.
-  cudaStream_t side = nullptr, rest = nullptr, crit = nullptr;
-  std::vector<cudaEvent_t> ev((size_t)nt + 1, nullptr), evr((size_t)nt, nullptr);
-  auto release = [&]() {
-    for (cudaEvent_t x : ev)
-      if (x) cudaEventDestroy(x);
-    for (cudaEvent_t x : evr)
-      if (x) cudaEventDestroy(x);
-    if (side) cudaStreamDestroy(side);
-    if (rest) cudaStreamDestroy(rest);
-    if (crit) cudaStreamDestroy(crit);
-  };
-  int prio_lo = 0, prio_hi = 0;
-  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
-  if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaStreamCreateWithFlags(&rest, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaStreamCreateWithPriority(&crit, cudaStreamNonBlocking, prio_hi)) != cudaSuccess) {
-    release();
+  DenseSched local;
+  DenseSched* sc = sched ? sched : &local;
+  if ((e = sc->ensure(nt)) != cudaSuccess) {
+    local.release();
     return e;
   }
-  for (auto* v : {&ev, &evr})
-    for (auto& x : *v)
-      if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) {
-        release();
-        return e;
-      }
+  cudaStream_t side = sc->side, rest = sc->rest, crit = sc->crit;
+  cudaEvent_t* ev = sc->ev.data();
+  cudaEvent_t* evr = sc->evr.data();
   cudaEventRecord(ev[nt], s);
   cudaStreamWaitEvent(crit, ev[nt], 0);
   for (int k = 0; k < nt; ++k) {
@@ -696,24 +680,57 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
     dense_syrk_kernel<T, TO><<<nt * (nt + 1) / 2, kDenseThreads, 0, s>>>(W, N, nt, out, n);
     ++nl;
   }
-  release();
+  local.release();
   if (launches) *launches += nl;
   return cudaGetLastError();
 }
 
+cudaError_t DenseSched::ensure(int nt) {
+  cudaError_t e;
+  if (!crit) {
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if ((e = cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&rest, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&crit, cudaStreamNonBlocking, prio_hi)) != cudaSuccess)
+      return e;
+  }
+  for (auto* v : {&ev, &evr}) {
+    const size_t want = (size_t)nt + (v == &ev ? 1 : 0);
+    while (v->size() < want) {
+      cudaEvent_t x = nullptr;
+      if ((e = cudaEventCreateWithFlags(&x, cudaEventDisableTiming)) != cudaSuccess) return e;
+      v->push_back(x);
+    }
+  }
+  return cudaSuccess;
+}
+
+void DenseSched::release() {
+  for (auto* v : {&ev, &evr}) {
+    for (cudaEvent_t x : *v)
+      if (x) cudaEventDestroy(x);
+    v->clear();
+  }
+  for (cudaStream_t* x : {&side, &rest, &crit}) {
+    if (*x) cudaStreamDestroy(*x);
+    *x = nullptr;
+  }
+}
+
 cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                  cudaStream_t s, int* launches) {
-  return dense_inverse_t<float, float>(Ac, n, A, W, info, out, s, launches);
+                                  cudaStream_t s, int* launches, DenseSched* sched) {
+  return dense_inverse_t<float, float>(Ac, n, A, W, info, out, s, launches, sched);
 }
 
 cudaError_t dense_spd_inverse_tf32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                   cudaStream_t s, int* launches) {
-  return dense_inverse_t<float, float, true>(Ac, n, A, W, info, out, s, launches);
+                                   cudaStream_t s, int* launches, DenseSched* sched) {
+  return dense_inverse_t<float, float, true>(Ac, n, A, W, info, out, s, launches, sched);
 }
 
 cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
-                                  cudaStream_t s, int* launches) {
-  return dense_inverse_t<double, double>(Ac, n, A, W, info, out, s, launches);
+                                  cudaStream_t s, int* launches, DenseSched* sched) {
+  return dense_inverse_t<double, double>(Ac, n, A, W, info, out, s, launches, sched);
 }
 
 }  // namespace femb200
@@ -739,12 +756,12 @@ extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precisi
     return set_global_error(FEM_ERR_CUDA, "cudaMalloc of the dense work space (%zu bytes) failed", 2 * N * N * elem);
   }
   cudaError_t e = f64 ? dense_inverse_t<double, double>(A, n, static_cast<double*>(wa), static_cast<double*>(ww),
-                                                          info, out, s, nullptr)
+                                                          info, out, s, nullptr, nullptr)
                   : precision == 19
                       ? dense_inverse_t<float, double, true>(A, n, static_cast<float*>(wa), static_cast<float*>(ww),
-                                                             info, out, s, nullptr)
+                                                             info, out, s, nullptr, nullptr)
                       : dense_inverse_t<float, double>(A, n, static_cast<float*>(wa), static_cast<float*>(ww), info,
-                                                         out, s, nullptr);
+                                                         out, s, nullptr, nullptr);
   int h_info = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -5,6 +5,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fem_device.cuh"
 
 namespace femb200 {
@@ -352,15 +354,23 @@ inline void raise_smem_limit_k(K kernel) {
 // FP64 column-major, lower triangle read) into out (n x n column-major).  A
 // and W are work matrices of N x N, N = n rounded up to dense_tile(fp64);
 // *info receives the first non-positive pivot (1-based), 0 if none.
+// sched holds the streams and events of its multi-stream schedule; a caller
+// that inverts repeatedly keeps one (null: created and released per call).
+struct DenseSched {
+  cudaStream_t side = nullptr, rest = nullptr, crit = nullptr;
+  std::vector<cudaEvent_t> ev, evr;  // nt + 1 and nt events
+  cudaError_t ensure(int nt);
+  void release();
+};
 int dense_tile(bool fp64);
 cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                  cudaStream_t s, int* launches);
+                                  cudaStream_t s, int* launches, DenseSched* sched);
 // FP32 Cholesky, then W = L^-1 and W^T W on TF32 tensor-core tiles (tcgen05);
 // *info = -1 if a tensor-core completion wait timed out
 cudaError_t dense_spd_inverse_tf32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                   cudaStream_t s, int* launches);
+                                   cudaStream_t s, int* launches, DenseSched* sched);
 cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
-                                  cudaStream_t s, int* launches);
+                                  cudaStream_t s, int* launches, DenseSched* sched);
 
 // Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
 // returns `code`.

@@ -296,13 +296,22 @@ int fem_selftest_umma(const void* A, const void* B, float* D, int32_t N, int32_t
  * device array (FP64, lower
  * triangle read); out: n x n column-major device array receiving the lower
  * triangle of A^-1; precision 64, 32 (FP32 arithmetic) or 19 (FP32
- * Cholesky, then W and W^T W on TF32 tensor-core tiles: tcgen05.mma
+ * Cholesky and W, then W^T W on TF32 tensor-core tiles: tcgen05.mma
  * kind::tf32, operands rounded to a 10-bit mantissa, FP32 sums).  Blocked
  * Cholesky A = L L^T, W = L^-1, A^-1 = W^T W on the project's tile kernels.
  * FEM_ERR_NAN if a pivot is not positive, FEM_ERR_BUDGET if a tensor-core
  * completion wait timed out.  Allocates its work space.
  * Errors: fem_last_error(NULL). */
 int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream);
+/* The same for a matrix with an envelope: row_first (host, n entries,
+ * 0 <= row_first[r] <= r) is the lowest column of row r that may be
+ * nonzero in A's lower triangle.  The Cholesky factor's fill stays inside
+ * that envelope, so the factorisation and W's update skip the tiles outside
+ * it; the result is bitwise that of fem_dense_spd_inverse (the skipped
+ * products would add exact zeros).  The solver's coarse inverse uses it
+ * with the lattice envelope of the coarse operator. */
+int fem_dense_spd_inverse_banded(const double* A, int32_t n, int32_t precision, const int32_t* row_first,
+                                 double* out, void* stream);
 
 /* ---- node-to-node contact between two bodies (backend/fea/framework/contact.py) ----
  * Device arrays in the caller's node order, FP64 current coordinates

@@ -113,6 +113,7 @@ SIGNATURES = {
     "fem_step_info": (C.c_int, [_VP, C.POINTER(C.c_int64)]),
     "fem_selftest_umma": (C.c_int, [_VP, _VP, _VP, C.c_int32, C.c_int32, _VP]),
     "fem_dense_spd_inverse": (C.c_int, [_VP, C.c_int32, C.c_int32, _VP, _VP]),
+    "fem_dense_spd_inverse_banded": (C.c_int, [_VP, C.c_int32, C.c_int32, C.POINTER(C.c_int32), _VP, _VP]),
     "fem_contact_nearest": (C.c_int, [_VP, _VP, C.c_int32, _VP, _VP, C.c_int32, _VP, _VP, _VP]),
     "fem_contact_penalty": (C.c_int, [_VP, _VP, C.c_int32, _VP, _VP, C.c_int32, C.c_double, C.c_double, _VP, _VP,
                                       C.POINTER(C.c_int32), C.POINTER(C.c_double), _VP]),

@@ -202,6 +202,7 @@ struct FemCtx {
   size_t dense_bytes = 0;
   int* dense_info = nullptr;    // first non-positive pivot, 0 if none
   DenseSched dense_sched;       // streams and events of the dense inverse
+  std::vector<int> coarse_row_first;  // Ac's row envelope (lowest coupled DOF per row)
   int* h_info = nullptr;
   // matvec variant: forced by fem_set_option (>= 0) or chosen by timing all
   int mv_forced = -1;
@@ -1193,6 +1194,7 @@ int drop_coarse(FemCtx* c) {
   if (c->dense_work) cudaFree(c->dense_work);
   c->dense_work = nullptr;
   c->dense_bytes = 0;
+  c->coarse_row_first.clear();
   c->coarse_built = false;
   c->coarse_valid = false;
   for (int k : {GRAPH_TWO_LEVEL, GRAPH_LEARNED}) {
@@ -1416,6 +1418,21 @@ int build_coarse(FemCtx* c) {
       const int cnode = cell_corner[8 * cl + q];
       cn_cells[8 * cnode + cn_fill[cnode]++] = cl * 8 + q;
     }
+  // Envelope of Ac (DOF 3 a + d of coarse node a): two coarse nodes couple
+  // only through a shared cell, so row 3 a + d is zero left of column
+  // 3 min{b : b shares a cell with a}; the dense inverse skips the tiles
+  // outside it (the lattice order makes Ac banded).
+  {
+    std::vector<int> cn_first(n_cn);
+    for (int a = 0; a < n_cn; ++a) cn_first[a] = a;
+    for (int cl = 0; cl < n_cells; ++cl) {
+      int mn = cell_corner[8 * cl];
+      for (int q = 1; q < 8; ++q) mn = std::min(mn, cell_corner[8 * cl + q]);
+      for (int q = 0; q < 8; ++q) cn_first[cell_corner[8 * cl + q]] = std::min(cn_first[cell_corner[8 * cl + q]], mn);
+    }
+    c->coarse_row_first.resize(3 * (size_t)n_cn);
+    for (int r = 0; r < 3 * n_cn; ++r) c->coarse_row_first[r] = 3 * cn_first[r / 3];
+  }
   std::vector<int> node_cell(Nn, -1);
   std::vector<int> cell_elem_ptr(n_cells + 1, 0), cell_elems(Ne);
   for (int e = 0; e < Ne; ++e) cell_elem_ptr[cell_of_lin[ecell[e]] + 1]++;
@@ -1530,6 +1547,7 @@ int ensure_coarse(FemCtx* c) {
   CKL();
   CK(cudaEventRecord(em, c->stream));
   const int n = c->cdev.n_dof;
+  const int* row_first = (int)c->coarse_row_first.size() == n ? c->coarse_row_first.data() : nullptr;
   c->cdev.Ac32 = nullptr;
   // Cholesky, W = L^-1, Ac^-1 = W^T W on the project's dense tile kernels:
   // FP32 arithmetic for the FP32 / TF32-class options (the inverse is
@@ -1552,13 +1570,15 @@ int ensure_coarse(FemCtx* c) {
   if (f64) {
     double* A = static_cast<double*>(c->dense_work);
     de = dense_spd_inverse_f64(c->cdev.Ac, n, A, A + N * N, c->dense_info, c->cdev.Ac, c->stream, &nl,
-                               &c->dense_sched);
+                               &c->dense_sched, row_first);
   } else {
     float* A = static_cast<float*>(c->dense_work);
     float* out = A + 2 * N * N;
     de = c->coarse_inverse == 3
-             ? dense_spd_inverse_tf32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl, &c->dense_sched)
-             : dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl, &c->dense_sched);
+             ? dense_spd_inverse_tf32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl,
+                                      &c->dense_sched, row_first)
+             : dense_spd_inverse_f32(c->cdev.Ac, n, A, A + N * N, c->dense_info, out, c->stream, &nl,
+                                     &c->dense_sched, row_first);
     c->cdev.Ac32 = out;
   }
   if (de != cudaSuccess) return set_err(c, FEM_ERR_CUDA, "dense inverse: %s", cudaGetErrorString(de));

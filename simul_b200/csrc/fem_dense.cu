@@ -596,9 +596,30 @@ int dense_tile(bool fp64) { return fp64 ? DenseCfg<double>::B : DenseCfg<float>:
 // TF32 tensor-core tile kernel instead of the SIMT one.
 template <typename T, typename TO, bool TC = false>
 static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* info, TO* out, cudaStream_t s,
-                                   int* launches, DenseSched* sched) {
+                                   int* launches, DenseSched* sched, const int* row_first) {
   constexpr int B = DenseCfg<T>::B;
   const int nt = (n + B - 1) / B, N = nt * B;
+  // Envelope: row r of Ac's lower triangle is zero left of row_first[r], and
+  // the Cholesky factor's fill stays inside that envelope, so tile (i, k)
+  // of L is zero unless first tile column of tile row i <= k.  With the
+  // suffix minimum over tile rows (a superset, non-decreasing in i), column
+  // k's nonzero tiles are rows k + 1 .. last[k], and every product outside
+  // them would add exact zeros: skipping them leaves the result bitwise
+  // unchanged.  No row_first: dense (last[k] = nt - 1).
+  std::vector<int> last((size_t)nt, nt - 1);
+  if (row_first) {
+    std::vector<int> fm((size_t)nt);
+    for (int i = 0; i < nt; ++i) {
+      int f = i;  // the diagonal tile (padding rows: the identity)
+      for (int r = i * B; r < std::min(n, (i + 1) * B); ++r) f = std::min(f, std::max(0, row_first[r]) / B);
+      fm[i] = f;
+    }
+    for (int i = nt - 2; i >= 0; --i) fm[i] = std::min(fm[i], fm[i + 1]);
+    for (int k = 0, i = 0; k < nt; ++k) {
+      while (i + 1 < nt && fm[i + 1] <= k) ++i;
+      last[k] = std::max(i, k);
+    }
+  }
   const size_t diag_smem = sizeof(T) * (2 * (size_t)B * (B + 1) + 32 * 32);
   cudaError_t e = cudaFuncSetAttribute(dense_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)diag_smem);
@@ -638,7 +659,7 @@ static cudaError_t dense_inverse_t(const double* Ac, int n, T* A, T* W, int* inf
   for (int k = 0; k < nt; ++k) {
     dense_diag_kernel<T><<<1, kDenseThreads, diag_smem, crit>>>(A, W, N, k, info);
     ++nl;
-    const int m = nt - k - 1;
+    const int m = last[k] - k;  // nonzero tiles below the diagonal in column k
     if (m > 0) {
       dense_panel_kernel<T><<<m, kDenseThreads, 0, crit>>>(A, W, N, k);
       ++nl;
@@ -719,29 +740,34 @@ void DenseSched::release() {
 }
 
 cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                  cudaStream_t s, int* launches, DenseSched* sched) {
-  return dense_inverse_t<float, float>(Ac, n, A, W, info, out, s, launches, sched);
+                                  cudaStream_t s, int* launches, DenseSched* sched, const int* row_first) {
+  return dense_inverse_t<float, float>(Ac, n, A, W, info, out, s, launches, sched, row_first);
 }
 
 cudaError_t dense_spd_inverse_tf32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                   cudaStream_t s, int* launches, DenseSched* sched) {
-  return dense_inverse_t<float, float, true>(Ac, n, A, W, info, out, s, launches, sched);
+                                   cudaStream_t s, int* launches, DenseSched* sched, const int* row_first) {
+  return dense_inverse_t<float, float, true>(Ac, n, A, W, info, out, s, launches, sched, row_first);
 }
 
 cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
-                                  cudaStream_t s, int* launches, DenseSched* sched) {
-  return dense_inverse_t<double, double>(Ac, n, A, W, info, out, s, launches, sched);
+                                  cudaStream_t s, int* launches, DenseSched* sched, const int* row_first) {
+  return dense_inverse_t<double, double>(Ac, n, A, W, info, out, s, launches, sched, row_first);
 }
 
 }  // namespace femb200
 
 using namespace femb200;
 
-extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream) {
+static int dense_spd_inverse_c(const double* A, int32_t n, int32_t precision, const int32_t* row_first,
+                               double* out, void* stream) {
   if (!A || !out) return set_global_error(FEM_ERR_INVALID, "null matrix");
   if (n < 1 || n > 32768) return set_global_error(FEM_ERR_INVALID, "n = %d not in [1, 32768]", n);
   if (precision != 32 && precision != 64 && precision != 19)
     return set_global_error(FEM_ERR_INVALID, "precision %d: 64, 32 or 19 (TF32 tensor cores)", precision);
+  if (row_first)
+    for (int r = 0; r < n; ++r)
+      if (row_first[r] < 0 || row_first[r] > r)
+        return set_global_error(FEM_ERR_INVALID, "row_first[%d] = %d not in [0, %d]", r, row_first[r], r);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const bool f64 = precision == 64;
   const int B = dense_tile(f64);
@@ -756,12 +782,12 @@ extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precisi
     return set_global_error(FEM_ERR_CUDA, "cudaMalloc of the dense work space (%zu bytes) failed", 2 * N * N * elem);
   }
   cudaError_t e = f64 ? dense_inverse_t<double, double>(A, n, static_cast<double*>(wa), static_cast<double*>(ww),
-                                                          info, out, s, nullptr, nullptr)
+                                                          info, out, s, nullptr, nullptr, row_first)
                   : precision == 19
                       ? dense_inverse_t<float, double, true>(A, n, static_cast<float*>(wa), static_cast<float*>(ww),
-                                                             info, out, s, nullptr, nullptr)
+                                                             info, out, s, nullptr, nullptr, row_first)
                       : dense_inverse_t<float, double>(A, n, static_cast<float*>(wa), static_cast<float*>(ww), info,
-                                                         out, s, nullptr, nullptr);
+                                                         out, s, nullptr, nullptr, row_first);
   int h_info = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -773,4 +799,14 @@ extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precisi
   if (h_info != 0)
     return set_global_error(FEM_ERR_NAN, "matrix is not positive definite (pivot %d is not positive)", h_info);
   return FEM_OK;
+}
+
+extern "C" int fem_dense_spd_inverse(const double* A, int32_t n, int32_t precision, double* out, void* stream) {
+  return dense_spd_inverse_c(A, n, precision, nullptr, out, stream);
+}
+
+extern "C" int fem_dense_spd_inverse_banded(const double* A, int32_t n, int32_t precision, const int32_t* row_first,
+                                            double* out, void* stream) {
+  if (!row_first) return set_global_error(FEM_ERR_INVALID, "null row_first");
+  return dense_spd_inverse_c(A, n, precision, row_first, out, stream);
 }

@@ -356,6 +356,9 @@ inline void raise_smem_limit_k(K kernel) {
 // *info receives the first non-positive pivot (1-based), 0 if none.
 // sched holds the streams and events of its multi-stream schedule; a caller
 // that inverts repeatedly keeps one (null: created and released per call).
+// row_first (host, n entries, or null for dense): the lowest column of each
+// row of Ac's lower triangle that may be nonzero; tiles outside that
+// envelope are skipped (bitwise the same result).
 struct DenseSched {
   cudaStream_t side = nullptr, rest = nullptr, crit = nullptr;
   std::vector<cudaEvent_t> ev, evr;  // nt + 1 and nt events
@@ -364,13 +367,16 @@ struct DenseSched {
 };
 int dense_tile(bool fp64);
 cudaError_t dense_spd_inverse_f32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                  cudaStream_t s, int* launches, DenseSched* sched);
+                                  cudaStream_t s, int* launches, DenseSched* sched,
+                                  const int* row_first);
 // FP32 Cholesky, then W = L^-1 and W^T W on TF32 tensor-core tiles (tcgen05);
 // *info = -1 if a tensor-core completion wait timed out
 cudaError_t dense_spd_inverse_tf32(const double* Ac, int n, float* A, float* W, int* info, float* out,
-                                   cudaStream_t s, int* launches, DenseSched* sched);
+                                   cudaStream_t s, int* launches, DenseSched* sched,
+                                  const int* row_first);
 cudaError_t dense_spd_inverse_f64(const double* Ac, int n, double* A, double* W, int* info, double* out,
-                                  cudaStream_t s, int* launches, DenseSched* sched);
+                                  cudaStream_t s, int* launches, DenseSched* sched,
+                                  const int* row_first);
 
 // Records a failure for fem_last_error(NULL) (thread-local, fem_ctx.cu) and
 // returns `code`.

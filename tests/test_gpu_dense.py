@@ -79,3 +79,58 @@ def test_dense_spd_inverse_validates_arguments(cuda):
     assert _lib.load().fem_dense_spd_inverse(C.c_void_p(A.data_ptr()), 4, 16, C.c_void_p(out.data_ptr()),
                                              None) == _lib.FEM_ERR_INVALID
     assert "precision" in _lib.last_error()
+
+
+def _enveloped_spd(n, width, seed):
+    """Symmetric, diagonally dominant (so SPD) matrix whose lower-triangle
+    row r is nonzero only from column first[r] (a ragged, non-monotone
+    envelope, as the coarse operator of a lattice has)."""
+    rng = np.random.default_rng(seed)
+    first = np.maximum(0, np.arange(n) - rng.integers(0, width + 1, n))
+    A = np.zeros((n, n))
+    for r in range(n):
+        A[r, first[r]:r] = rng.standard_normal(r - first[r])
+    A = A + A.T
+    A[np.arange(n), np.arange(n)] = np.abs(A).sum(1) + 1.0
+    return A, first.astype(np.int32)
+
+
+def _run_banded(A, first, precision, cuda):
+    n = A.shape[0]
+    dA = torch.as_tensor(np.asfortranarray(A).ravel(order="F"), dtype=torch.float64, device=cuda)
+    out = torch.full((n * n,), float("nan"), dtype=torch.float64, device=cuda)
+    rf = np.ascontiguousarray(first, dtype=np.int32)
+    rc = _lib.load().fem_dense_spd_inverse_banded(C.c_void_p(dA.data_ptr()), n, precision,
+                                                  rf.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                  C.c_void_p(out.data_ptr()), None)
+    return rc, out.cpu().numpy().reshape(n, n, order="F")
+
+
+@pytest.mark.parametrize("n,width", [(700, 150), (1000, 300), (513, 40)])
+@pytest.mark.parametrize("precision", [64, 32, 19])
+def test_banded_inverse_skips_only_zero_tiles(cuda, n, width, precision):
+    """The envelope form skips the tiles of L (and of W's update) outside
+    the rows' envelope: the products it leaves out would add exact zeros,
+    so its result equals the dense entry point's, entry for entry."""
+    A, first = _enveloped_spd(n, width, seed=n + width)
+    rc, Xb = _run_banded(A, first, precision, cuda)
+    assert rc == 0, _lib.last_error()
+    rc, Xd = _run(A, precision, cuda)
+    assert rc == 0, _lib.last_error()
+    lo = np.tril(np.ones((n, n), dtype=bool))
+    assert np.array_equal(Xb[lo], Xd[lo])
+    ref = np.linalg.inv(A)
+    tol = {64: 1e-11, 32: 2e-4, 19: 5e-2}[precision]
+    assert np.abs(Xb[lo] - ref[lo]).max() / np.abs(ref).max() < tol
+
+
+def test_banded_inverse_validates_envelope(cuda):
+    A = torch.eye(4, dtype=torch.float64, device=cuda)
+    out = torch.empty_like(A)
+    lib = _lib.load()
+    bad = np.array([0, 0, 3, 1], dtype=np.int32)  # row 2 cannot start right of its diagonal
+    assert lib.fem_dense_spd_inverse_banded(C.c_void_p(A.data_ptr()), 4, 64, bad.ctypes.data_as(C.POINTER(C.c_int32)),
+                                            C.c_void_p(out.data_ptr()), None) == _lib.FEM_ERR_INVALID
+    assert "row_first" in _lib.last_error()
+    assert lib.fem_dense_spd_inverse_banded(C.c_void_p(A.data_ptr()), 4, 64, None, C.c_void_p(out.data_ptr()),
+                                            None) == _lib.FEM_ERR_INVALID

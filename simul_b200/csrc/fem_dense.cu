@@ -202,6 +202,11 @@ __global__ void __launch_bounds__(256) dense_pad_kernel(const double* __restrict
   W[q] = T(0);
 }
 
+// Correctly rounded 1 / sqrt(x) (FP32) or CUDA's rsqrt (FP64): one per pivot,
+// multiplied through the column instead of a division per entry.
+__device__ __forceinline__ float dense_rsqrt(float x) { return __frsqrt_rn(x); }
+__device__ __forceinline__ double dense_rsqrt(double x) { return rsqrt(x); }
+
 // Diagonal tile k: L_kk = chol(A_kk) and X = L_kk^-1 in shared memory
 // (L[c * S + r] = L(r, c)), both blocked in 32-wide panels so the sequential
 // parts run inside one warp, in registers, and the CTA synchronises a few
@@ -223,6 +228,7 @@ __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, i
   T* L = reinterpret_cast<T*>(s_raw);  // L[c * S + r]
   T* X = L + B * S;                     // X[c * S + r] = (L^-1)(r, c)
   T* Xt = X + B * S;                    // Xt[l * P + j] = (L_pp^-1)(j, l), current panel
+  __shared__ T s_rinv[32];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const size_t off = (size_t)k * B * N + (size_t)k * B;
 #pragma unroll 8
@@ -237,6 +243,7 @@ __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, i
     const int j0 = p * P;
     if (warp == 0) {
       T a[P];  // row j0 + lane of the diagonal block
+      T rinv = T(0);  // lane r: 1 / L(j0 + r, j0 + r)
 #pragma unroll
       for (int c = 0; c < P; ++c) a[c] = c <= lane ? L[(j0 + c) * S + j0 + lane] : T(0);
 #pragma unroll
@@ -246,9 +253,12 @@ __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, i
           if (lane == 0) atomicCAS(info, 0, k * B + j0 + j + 1);
           d = T(1);
         }
-        d = sqrt(d);
-        if (lane == j) a[j] = d;
-        if (lane > j) a[j] = a[j] / d;
+        const T rs = dense_rsqrt(d);  // 1 / L(j, j)
+        if (lane == j) {
+          a[j] = d * rs;
+          rinv = rs;
+        }
+        if (lane > j) a[j] *= rs;
 #pragma unroll
         for (int c = 1; c < P; ++c) {  // c > j: constant trip counts unroll fully
           if (c > j) {
@@ -260,6 +270,7 @@ __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, i
 #pragma unroll
       for (int c = 0; c < P; ++c)
         if (c <= lane) L[(j0 + c) * S + j0 + lane] = a[c];
+      s_rinv[lane] = rinv;
       __syncwarp();
       // column lane of L_pp^-1: x[r] = (delta(r, lane) - sum_{l < r} L(r, l) x[l]) / L(r, r)
       T x[P];
@@ -269,7 +280,7 @@ __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, i
 #pragma unroll
         for (int l = 0; l < P - 1; ++l)
           if (l < r) acc -= L[(j0 + l) * S + j0 + r] * x[l];
-        x[r] = acc / L[(j0 + r) * S + j0 + r];
+        x[r] = acc * s_rinv[r];
       }
 #pragma unroll
       for (int r = 0; r < P; ++r) {
@@ -345,34 +356,53 @@ __global__ void __launch_bounds__(kDenseThreads) dense_diag_kernel(T* A, T* W, i
     }
     __syncthreads();
   }
-  // block rows: finish row k (X_kq = X_kk R_kq, q < k; R_kq accumulated in
-  // place), then R_iq -= L_ik X_kq for i > k, q <= k
+  // block rows of X: finish row block kb (X_kq = X_kk R_kq, q < kb; R
+  // accumulated in place), then R_iq -= L_ik X_kq for the row blocks below,
+  // for kb = 0, 1, ...: register-tiled, lane = row, the other operand
+  // broadcast from shared memory
+  constexpr int NW = kDenseThreads / 32;
   for (int kb = 0; kb < NP; ++kb) {
     const int k0 = kb * P;
     if (kb > 0) {
-      // kb * P * P entries, at most 3 * 1024 / 256 = 12 per thread
-      T v[(NP - 1) * P * P / kDenseThreads + 1];
-      int nv = 0;
-      for (int q = tid; q < kb * P * P; q += kDenseThreads, ++nv) {
-        const int c = q / P, r = k0 + q % P;  // column c < k0, row r in block kb
-        T acc = T(0);
-        for (int l = 0; l < P; ++l) acc += X[(k0 + l) * S + r] * X[c * S + k0 + l];
-        v[nv] = acc;
+      // X(k0 + lane, c) for the columns c = warp + NW t < k0
+      constexpr int NV = (NP - 1) * P / NW;
+      const int nc = k0 / NW;
+      T v[NV];
+#pragma unroll
+      for (int t = 0; t < NV; ++t) v[t] = T(0);
+      for (int l = 0; l < P; ++l) {
+        const T xl = X[(k0 + l) * S + k0 + lane];
+#pragma unroll
+        for (int t = 0; t < NV; ++t)
+          if (t < nc) v[t] += xl * X[(warp + NW * t) * S + k0 + l];
       }
       __syncthreads();
-      nv = 0;
-      for (int q = tid; q < kb * P * P; q += kDenseThreads, ++nv) X[(q / P) * S + k0 + q % P] = v[nv];
+#pragma unroll
+      for (int t = 0; t < NV; ++t)
+        if (t < nc) X[(warp + NW * t) * S + k0 + lane] = v[t];
       __syncthreads();
     }
-    // rows below block kb, columns up to the end of block kb
+    // rows below block kb, columns up to the end of block kb: items of 32
+    // rows x CW columns, one per warp in turn
     const int rows = B - k0 - P, cols = k0 + P;
-    for (int q = tid; q < rows * cols; q += kDenseThreads) {
-      const int c = q / rows, r = k0 + P + q % rows;
-      T acc = T(0);
-      for (int l = (c > k0 ? c : k0); l < k0 + P; ++l) acc += L[l * S + r] * X[c * S + l];
-      X[c * S + r] -= acc;
+    if (rows > 0) {
+      constexpr int CW = 8;
+      const int rw32 = rows / 32, items = rw32 * (cols / CW);
+      for (int it = warp; it < items; it += NW) {
+        const int r = k0 + P + (it % rw32) * 32 + lane, c0 = (it / rw32) * CW;
+        T acc[CW];
+#pragma unroll
+        for (int w = 0; w < CW; ++w) acc[w] = T(0);
+        for (int l = 0; l < P; ++l) {
+          const T lv = L[(k0 + l) * S + r];
+#pragma unroll
+          for (int w = 0; w < CW; ++w) acc[w] += lv * X[(c0 + w) * S + k0 + l];
+        }
+#pragma unroll
+        for (int w = 0; w < CW; ++w) X[(c0 + w) * S + r] -= acc[w];
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   for (int q = tid; q < B * B; q += kDenseThreads) {
     const int c = q / B, r = q % B;
